@@ -1,0 +1,273 @@
+/*
+ * castro_b200.h -- C-ABI of the B200 CTU hydro advance (libcastro_b200.so).
+ *
+ * Two layers:
+ *
+ * 1. The reference's Fortran entry points, Source/Castro_F.H:11-161, with the
+ *    same names, argument order and meaning.  Each takes a whole box [lo,hi]
+ *    and launches one kernel over it on the library stream; arrays are device
+ *    (or managed) pointers in BL_FORT_FAB_ARG_3D form (pointer, lo[3], hi[3]),
+ *    Fortran order, component slowest; lo/hi/dx pointers are host pointers.
+ *    The reference calls these per zone from inside an AMReX device lambda
+ *    (Source/Castro.H:23-27); a host replacing the Fortran objects calls them
+ *    once per box instead.  Like the reference they
+ *    return void; errors are reported through castro_last_error().
+ *
+ * 2. Coarse entry points with no reference counterpart at the ABI level but
+ *    replacing whole host routines: castro_construct_hydro_source_box
+ *    (Castro::construct_hydro_source's MFIter body, Source/Castro_hydro.cpp:31-397)
+ *    and the castro_sim_* family (Castro::advance / estTimeStep /
+ *    computeNewDt / post_timestep and the Amr coarse step loop,
+ *    Source/Castro_advance.cpp:12-100, Source/Castro.cpp:162-426,
+ *    Source/main.cpp:127-168), in a plain per-box form and a batched form
+ *    that advances every box of every instance with one fused kernel
+ *    sequence per step.
+ *
+ * Species: the reference fixes nspec = 13 at compile time
+ * (Source/network.F90:7); this library takes the network at run time through
+ * castro_network_init and supports nspec = 2 and nspec = 13.
+ */
+#ifndef CASTRO_B200_H
+#define CASTRO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CASTRO_MAX_SPEC 13
+
+/* ------------------------------------------------------------------------- */
+/* Library state and errors (no reference counterpart: the Fortran returns    */
+/* void and aborts through amrex_error)                                       */
+/* ------------------------------------------------------------------------- */
+enum {
+    CASTRO_OK = 0,
+    CASTRO_ERR_CUDA = 1,        /* a CUDA call failed; see castro_error_string */
+    CASTRO_ERR_NO_TABLE = 2,    /* eos_init has not succeeded */
+    CASTRO_ERR_TABLE_IO = 3,    /* helm_table.dat missing or malformed */
+    CASTRO_ERR_NSPEC = 4,       /* network size other than 2 or 13 */
+    CASTRO_ERR_ARG = 5,         /* invalid argument */
+    CASTRO_ERR_EOS = 6          /* EOS Newton iteration did not converge */
+};
+int         castro_last_error(void);          /* sticky: first error since castro_clear_error */
+void        castro_clear_error(void);
+const char* castro_error_string(void);
+int         castro_version(void);
+/* stream used by every launch (a cudaStream_t); default is the legacy stream 0 */
+void        castro_set_stream(void* stream);
+void*       castro_get_stream(void);
+/* 1 when the library was built with CASTRO_EXACT (no FMA contraction, the
+ * reference's operation order everywhere) */
+int         castro_exact_build(void);
+
+/* ------------------------------------------------------------------------- */
+/* Source/Castro_F.H:11-17                                                    */
+/* ------------------------------------------------------------------------- */
+void network_init(void);                      /* Castro_F.H:11: the 13-species network of Source/network.F90 */
+void network_finalize(void);                  /* Castro_F.H:13 */
+/* run-time network (replaces the compile-time parameters of Source/network.F90:7-19) */
+int  castro_network_init(int nspec, const double* aion, const double* zion);
+int  castro_nspec(void);
+void eos_init(void);                          /* Castro_F.H:15: reads ./helm_table.dat (or $CASTRO_HELM_TABLE), eos.F90:580-734 */
+void eos_finalize(void);                      /* Castro_F.H:17 */
+int  castro_eos_init_path(const char* path);  /* eos_init with an explicit table path; returns an error code */
+
+/* ------------------------------------------------------------------------- */
+/* Per-routine entry points, Source/Castro_F.H:19-161                         */
+/* ------------------------------------------------------------------------- */
+/* Castro_F.H:19-23 -> Castro_hydro_nd.F90:73 */
+void ctoprim(const int* lo, const int* hi,
+             const double* u, const int* u_lo, const int* u_hi,
+             const double* q, const int* q_lo, const int* q_hi,
+             const double* qaux, const int* qa_lo, const int* qa_hi);
+/* Castro_F.H:25-27 -> Castro_nd.F90:69 */
+void enforce_minimum_density(const int* lo, const int* hi, double* state, const int* s_lo, const int* s_hi);
+/* Castro_F.H:29-31 -> Castro_nd.F90:129 */
+void normalize_species(const int* lo, const int* hi, double* state, const int* s_lo, const int* s_hi);
+/* Castro_F.H:33-35 -> Castro_nd.F90:164 */
+void reset_internal_e(const int* lo, const int* hi, double* state, const int* s_lo, const int* s_hi);
+/* Castro_F.H:37-39 -> Castro_nd.F90:253 */
+void compute_temp(const int* lo, const int* hi, double* state, const int* s_lo, const int* s_hi);
+/* Castro_F.H:41-45 -> timestep.F90:12; dt is a device/managed double lowered atomically */
+void estdt(const int* lo, const int* hi, const double* state, const int* s_lo, const int* s_hi,
+           const double* dx, double* dt);
+/* Castro_F.H:47-53 -> Castro_hydro_nd.F90:301 */
+void store_flux(const int* lo, const int* hi,
+                double* flux_out, const int* fo_lo, const int* fo_hi,
+                double* flux_in, const int* fi_lo, const int* fi_hi,
+                double* area, const int* a_lo, const int* a_hi, const double dt);
+/* Castro_F.H:55-71 -> Castro_hydro_nd.F90:344 (consup) */
+void fill_hydro_source(const int* lo, const int* hi,
+                       const double* state, const int* s_lo, const int* s_hi,
+                       const double* q, const int* q_lo, const int* q_hi,
+                       double* source, const int* sr_lo, const int* sr_hi,
+                       const double* flux0, const int* f0_lo, const int* f0_hi,
+                       const double* flux1, const int* f1_lo, const int* f1_hi,
+                       const double* flux2, const int* f2_lo, const int* f2_hi,
+                       const double* qe0, const int* qe0_lo, const int* qe0_hi,
+                       const double* qe1, const int* qe1_lo, const int* qe1_hi,
+                       const double* qe2, const int* qe2_lo, const int* qe2_hi,
+                       const double* area0, const int* a0_lo, const int* a0_hi,
+                       const double* area1, const int* a1_lo, const int* a1_hi,
+                       const double* area2, const int* a2_lo, const int* a2_hi,
+                       const double* volume, const int* v_lo, const int* v_hi,
+                       const double* dx, const double dt);
+/* Castro_F.H:73-76 -> Castro_hydro_nd.F90:248 */
+void normalize_species_fluxes(const int* lo, const int* hi, double* flux, const int* f_lo, const int* f_hi);
+/* Castro_F.H:78-84 -> Castro_hydro_nd.F90:174; idir is 1-based */
+void apply_av(const int* lo, const int* hi, const int idir, const double* dx,
+              double* div, const int* d_lo, const int* d_hi,
+              double* Sborder, const int* s_lo, const int* s_hi,
+              double* flux, const int* f_lo, const int* f_hi);
+/* Castro_F.H:86-96 -> trans.F90:14 */
+void trans1(const int* lo, const int* hi, const int idir1, const int idir2,
+            const double* q2m, const int* q2m_lo, const int* q2m_hi,
+            double* q2mo, const int* q2mo_lo, const int* q2mo_hi,
+            const double* q2p, const int* q2p_lo, const int* q2p_hi,
+            double* q2po, const int* q2po_lo, const int* q2po_hi,
+            const double* qaux, const int* qa_lo, const int* qa_hi,
+            const double* f1, const int* f1_lo, const int* f1_hi,
+            const double* q1, const int* q1_lo, const int* q1_hi,
+            const double cdtdx);
+/* Castro_F.H:98-110 -> trans.F90:250 */
+void trans2(const int* lo, const int* hi, const int idir1, const int idir2, const int idir3,
+            const double* qm, const int* qm_lo, const int* qm_hi,
+            double* qmo, const int* qmo_lo, const int* qmo_hi,
+            const double* qp, const int* qp_lo, const int* qp_hi,
+            double* qpo, const int* qpo_lo, const int* qpo_hi,
+            const double* qaux, const int* qa_lo, const int* qa_hi,
+            const double* fyz, const int* fyz_lo, const int* fyz_hi,
+            const double* fzy, const int* fzy_lo, const int* fzy_hi,
+            const double* qy, const int* qy_lo, const int* qy_hi,
+            const double* qz, const int* qz_lo, const int* qz_hi,
+            const double hdtdx, const double cdtdy, const double cdtdz);
+/* Castro_F.H:112-121 -> riemann.F90:10 (riemanncg) */
+void compute_flux(const int* lo, const int* hi,
+                  const double* ql, const int* ql_lo, const int* ql_hi,
+                  const double* qr, const int* qr_lo, const int* qr_hi,
+                  double* flux, const int* fx_lo, const int* fx_hi,
+                  double* q_int, const int* qi_lo, const int* qi_hi,
+                  double* qe, const int* qe_lo, const int* qe_hi,
+                  const double* qaux, const int* qa_lo, const int* qa_hi,
+                  const int idir);
+/* Castro_F.H:123-128 -> Castro_hydro_nd.F90:11 */
+void divu(const int* lo, const int* hi, double* q, const int* q_lo, const int* q_hi,
+          const double* dx, double* div, const int* d_lo, const int* d_hi);
+/* Castro_F.H:130-140 -> ppm.F90:309 */
+void trace_ppm(const int* lo, const int* hi, const int* vlo, const int* vhi, const int idir,
+               const double* q, const int* q_lo, const int* q_hi,
+               const double* qaux, const int* qa_lo, const int* qa_hi,
+               double* qm, const int* qm_lo, const int* qm_hi,
+               double* qp, const int* qp_lo, const int* qp_hi,
+               const int* domlo, const int* domhi, const double* dx, const double dt);
+/* Castro_F.H:142-146 -> Prob.F90:19; problem constants from castro_set_problem */
+void initdata(const int* lo, const int* hi, double* state, const int* s_lo, const int* s_hi,
+              const double* dx, const double* problo, const double* probhi);
+/* Castro_F.H:148-153 -> Castro_nd.F90:301 */
+void denerror(const int* lo, const int* hi, int8_t* tag, const int* tag_lo, const int* tag_hi,
+              const double* den, const int* den_lo, const int* den_hi,
+              const int8_t tagval, const int8_t clearval);
+/* Castro_F.H:155-161 -> Castro_nd.F90:349; blast_mass/blast_radius are device doubles */
+void calculate_blast_radius(const int* lo, const int* hi, double* state, const int* s_lo, const int* s_hi,
+                            const double* dx, const double* problo, const double* probhi,
+                            double* blast_mass, double* blast_radius, const double max_density);
+
+/* ------------------------------------------------------------------------- */
+/* Problem constants (Source/Prob.F90:11-15 plus the knobs of the benchmark   */
+/* configurations)                                                            */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    int    ambient_from_T;   /* 0: ambient e from EOS(rho,p) as Prob.F90:51-59; 1: from EOS(rho,T) */
+    double dens_ambient;     /* g/cc */
+    double p_ambient;        /* erg/cc (ambient_from_T == 0) */
+    double T_ambient;        /* K (ambient_from_T == 1) */
+    double exp_energy;       /* erg */
+    double r_init;           /* cm */
+    int    nsub;             /* subzones per dimension (Prob.F90:15: 10) */
+    double X[CASTRO_MAX_SPEC];   /* initial mass fractions */
+    double T_init;           /* UTEMP at init (Prob.F90:115: 1e9) */
+    const double* pert;      /* optional device array over pert_lo..pert_hi: rho = dens_ambient*(1+pert_amp*pert) */
+    int    pert_lo[3], pert_hi[3];
+    double pert_amp;
+} castro_problem;
+
+/* Source/Prob.F90 defaults: rho=1e4, p=1e21, E=1e52, r=1.25e8, nsub=10, X1=1 */
+void castro_problem_defaults(castro_problem* p);
+int  castro_set_problem(const castro_problem* p);
+
+/* ------------------------------------------------------------------------- */
+/* Coarse entry point: construct_hydro_source for one box                     */
+/* ------------------------------------------------------------------------- */
+/* Castro::construct_hydro_source's body for one box (Source/Castro_hydro.cpp:31-397),
+ * fused: Sborder (grow(box,4), NVAR comps, already cleaned) -> source on the box
+ * (accumulated into 'source', which the caller zeroes like hydro_source.setVal(0)).
+ * fluxes_out[d] (optional, may be NULL): dt*F*A on the faces of the box
+ * (store_flux).  Uses library-managed scratch. */
+int castro_construct_hydro_source_box(const int* lo, const int* hi,
+                                      const double* sborder, const int* sb_lo, const int* sb_hi,
+                                      double* source, const int* sr_lo, const int* sr_hi,
+                                      double* const* fluxes_out, const int* fo_lo3x3, const int* fo_hi3x3,
+                                      const int* domlo, const int* domhi, const double* dx, double dt);
+
+/* ------------------------------------------------------------------------- */
+/* Simulation driver: one level per instance, many instances per sim          */
+/* ------------------------------------------------------------------------- */
+typedef struct castro_sim castro_sim;
+
+enum { CASTRO_BC_PERIODIC = 0, CASTRO_BC_OUTFLOW = 1 };
+enum { CASTRO_MODE_PLAIN = 0,     /* per-box launches of the per-routine kernels, reference call sequence */
+       CASTRO_MODE_BATCHED = 1 }; /* fused kernels over every box of every instance, CUDA-graph replay */
+
+typedef struct {
+    int dom_lo[3], dom_hi[3];
+    double problo[3], probhi[3];
+    int bc;                       /* CASTRO_BC_* */
+    int nbox;
+    const int* box_lo;            /* 3*nbox, global indices */
+    const int* box_hi;            /* 3*nbox */
+    castro_problem prob;
+    double stop_time;             /* < 0: none (Source/main.cpp:66 default is 0.01) */
+} castro_instance_desc;
+
+castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int mode);
+void   castro_sim_destroy(castro_sim* sim);
+int    castro_sim_nbox(const castro_sim* sim, int inst);
+/* number of doubles of box b's state FAB (valid box x NVAR) */
+size_t castro_sim_box_size(const castro_sim* sim, int inst, int b);
+/* device pointer of box b's state FAB (Fortran order, NVAR comps) */
+double* castro_sim_box_state(castro_sim* sim, int inst, int b);
+int    castro_sim_init_data(castro_sim* sim);
+/* copy all boxes' state of every instance from/to one host buffer (instances
+ * in order, boxes in order, each FAB contiguous); async on the library stream */
+int    castro_sim_upload(castro_sim* sim, const double* host);
+int    castro_sim_download(castro_sim* sim, double* host);
+size_t castro_sim_total_size(const castro_sim* sim);
+/* one Amr coarse step for every instance (dt choice, advance, post_timestep) */
+int    castro_sim_step(castro_sim* sim);
+int    castro_sim_run(castro_sim* sim, int nsteps);
+/* host <-> device whole-run call: upload 'host_in', nsteps coarse steps,
+ * download into 'host_out' (may alias host_in) */
+int    castro_sim_run_host(castro_sim* sim, const double* host_in, int nsteps, double* host_out);
+int    castro_sim_sync(castro_sim* sim);
+double castro_sim_time(castro_sim* sim, int inst);
+double castro_sim_dt(castro_sim* sim, int inst);
+int    castro_sim_steps(castro_sim* sim, int inst);
+/* estTimeStep on the current state of instance inst (cfl included) */
+double castro_sim_est_time_step(castro_sim* sim, int inst);
+/* blast radius diagnostic of Source/Castro.cpp:371-424, cm */
+double castro_sim_blast_radius(castro_sim* sim, int inst, double* blast_mass);
+/* kernel launches issued by the last castro_sim_step (graph nodes for the batched mode) */
+int    castro_sim_launches_per_step(const castro_sim* sim);
+/* per-step EOS Newton failures seen so far (non-converged zones) */
+long long castro_sim_eos_failures(castro_sim* sim);
+
+/* the mini-app driver with the reference's command-line keys (Source/main.cpp) */
+int castro_main(int argc, char** argv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,306 @@
+// castro_host.cu -- library state: error reporting, stream, network, the
+// Helmholtz table (eos_init, Source/eos.F90:580-734) and the problem
+// constants of initdata (Source/Prob.F90:11-15).
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "castro_common.cuh"
+#include "../../include/castro_b200.h"
+
+namespace castro {
+
+// constant upload hooks of the other translation units
+void upload_constants_abi(const EosTableDev& e, const NetworkDev& n);
+void upload_constants_sim(const EosTableDev& e, const NetworkDev& n);
+
+namespace {
+std::mutex g_mu;
+int g_err = 0;
+std::string g_errmsg;
+cudaStream_t g_stream = 0;
+
+NetworkDev g_net;
+bool g_net_set = false;
+
+bool g_table = false;
+double* d_node = nullptr;
+double* d_trow = nullptr;
+double* d_drow = nullptr;
+unsigned long long* d_fail = nullptr;
+EosTableDev g_eos;
+
+castro_problem g_prob;
+bool g_prob_set = false;
+
+void default_network()
+{
+    static const double a13[13] = {4., 12., 16., 20., 24., 28., 32., 36., 40., 44., 48., 52., 56.};
+    static const double z13[13] = {2., 6., 8., 10., 12., 14., 16., 18., 20., 22., 24., 26., 28.};
+    memset(&g_net, 0, sizeof g_net);
+    g_net.nspec = 13;
+    for (int n = 0; n < 13; ++n) {
+        g_net.aion[n] = a13[n];
+        g_net.zion[n] = z13[n];
+        g_net.aion_inv[n] = 1.0 / a13[n];
+    }
+    g_net_set = true;
+}
+
+void upload_all()
+{
+    if (!g_net_set) default_network();
+    upload_constants_abi(g_eos, g_net);
+    upload_constants_sim(g_eos, g_net);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) set_error(CASTRO_ERR_CUDA, cudaGetErrorString(e));
+}
+
+// one list-directed READ of n values (starts a new record, may span records)
+bool read_record(FILE* fp, double* v, int n)
+{
+    char line[4096];
+    int got = 0;
+    while (got < n) {
+        if (!fgets(line, sizeof line, fp)) return false;
+        for (char* c = line; *c; ++c)
+            if (*c == 'D' || *c == 'd') *c = 'E';
+        char* s = line;
+        while (got < n) {
+            char* e;
+            double x = strtod(s, &e);
+            if (e == s) break;
+            v[got++] = x;
+            s = e;
+            while (*s == ',' || *s == ' ' || *s == '\t') ++s;
+        }
+    }
+    return true;
+}
+}  // namespace
+
+void set_error(int code, const char* what)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_err == 0) {
+        g_err = code;
+        g_errmsg = what ? what : "";
+    }
+}
+cudaStream_t stream() { return g_stream; }
+bool table_ready() { return g_table; }
+int nspec() { return g_net_set ? g_net.nspec : 13; }
+const castro_problem& problem()
+{
+    if (!g_prob_set) {
+        castro_problem_defaults(&g_prob);
+        g_prob_set = true;
+    }
+    return g_prob;
+}
+const NetworkDev& network_host()
+{
+    if (!g_net_set) default_network();
+    return g_net;
+}
+unsigned long long* eos_fail_counter() { return d_fail; }
+
+}  // namespace castro
+
+using namespace castro;
+
+extern "C" {
+
+int castro_last_error(void) { std::lock_guard<std::mutex> lk(g_mu); return g_err; }
+void castro_clear_error(void) { std::lock_guard<std::mutex> lk(g_mu); g_err = 0; g_errmsg.clear(); }
+const char* castro_error_string(void) { std::lock_guard<std::mutex> lk(g_mu); return g_errmsg.c_str(); }
+int castro_version(void) { return 100; }
+void castro_set_stream(void* s) { g_stream = (cudaStream_t)s; }
+void* castro_get_stream(void) { return (void*)g_stream; }
+int castro_exact_build(void)
+{
+#ifdef CASTRO_EXACT
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+void network_init(void)
+{
+    default_network();
+    if (g_table) upload_all();
+}
+
+void network_finalize(void) {}
+
+int castro_network_init(int ns, const double* aion, const double* zion)
+{
+    if (ns != 2 && ns != 13) {
+        set_error(CASTRO_ERR_NSPEC, "castro_network_init: nspec must be 2 or 13");
+        return CASTRO_ERR_NSPEC;
+    }
+    memset(&g_net, 0, sizeof g_net);
+    g_net.nspec = ns;
+    for (int n = 0; n < ns; ++n) {
+        g_net.aion[n] = aion[n];
+        g_net.zion[n] = zion[n];
+        g_net.aion_inv[n] = 1.0 / aion[n];
+    }
+    g_net_set = true;
+    if (g_table) upload_all();
+    return CASTRO_OK;
+}
+
+int castro_nspec(void) { return nspec(); }
+
+int castro_eos_init_path(const char* path)
+{
+    const int IM = IMAX, JM = JMAX;
+    // grid and deltas, Source/eos.F90:62-71,626-632,700-712
+    const double tlo = 3.0, thi = 13.0, dlo = -12.0, dhi = 15.0;
+    const double tstp = (thi - tlo) / (double)(float)(JM - 1);
+    const double dstp = (dhi - dlo) / (double)(float)(IM - 1);
+    std::vector<double> t(JM), d(IM);
+    for (int j = 0; j < JM; ++j) t[j] = pow(10.0, tlo + j * tstp);
+    for (int i = 0; i < IM; ++i) d[i] = pow(10.0, dlo + i * dstp);
+
+    FILE* fp = fopen(path, "r");
+    if (!fp) {
+        std::string m = std::string("eos_init: cannot open ") + path;
+        set_error(CASTRO_ERR_TABLE_IO, m.c_str());
+        return CASTRO_ERR_TABLE_IO;
+    }
+    // the 13 tables the hydro path reads, packed per node
+    std::vector<double> node((size_t)JM * IM * NODE_STRIDE, 0.0);
+    double v[9];
+    bool ok = true;
+    for (int j = 0; j < JM && ok; ++j)
+        for (int i = 0; i < IM && ok; ++i) {
+            if (!read_record(fp, v, 9)) { ok = false; break; }
+            double* r = &node[((size_t)j * IM + i) * NODE_STRIDE];
+            // file order f, fd, ft, fdd, ftt, fdt, fddt, fdtt, fddtt (eos.F90:646-647)
+            r[N_F] = v[0]; r[N_FD] = v[1]; r[N_FT] = v[2]; r[N_FDD] = v[3]; r[N_FTT] = v[4];
+            r[N_FDT] = v[5]; r[N_FDDT] = v[6]; r[N_FDTT] = v[7]; r[N_FDDTT] = v[8];
+        }
+    for (int j = 0; j < JM && ok; ++j)
+        for (int i = 0; i < IM && ok; ++i) {
+            if (!read_record(fp, v, 4)) { ok = false; break; }
+            double* r = &node[((size_t)j * IM + i) * NODE_STRIDE];
+            // dpdf, dpdfd, dpdft, dpdfdt (eos.F90:654)
+            r[N_DPDF] = v[0]; r[N_DPDFD] = v[1]; r[N_DPDFT] = v[2]; r[N_DPDFDT] = v[3];
+        }
+    // the chemical-potential and number-density blocks (eos.F90:659-670) are
+    // read for format validation only; no hydro quantity depends on them
+    for (int b = 0; b < 2 && ok; ++b)
+        for (int j = 0; j < JM && ok; ++j)
+            for (int i = 0; i < IM && ok; ++i)
+                if (!read_record(fp, v, 4)) ok = false;
+    fclose(fp);
+    if (!ok) {
+        set_error(CASTRO_ERR_TABLE_IO, "eos_init: helm_table.dat is truncated or malformed");
+        return CASTRO_ERR_TABLE_IO;
+    }
+    std::vector<double> trow((size_t)JM * ROW_STRIDE, 0.0), drow((size_t)IM * ROW_STRIDE, 0.0);
+    for (int j = 0; j < JM; ++j) {
+        double dt = (j < JM - 1) ? t[j + 1] - t[j] : 0.0;
+        double dt2 = dt * dt;
+        trow[(size_t)j * ROW_STRIDE + 0] = t[j];
+        trow[(size_t)j * ROW_STRIDE + 1] = dt;
+        trow[(size_t)j * ROW_STRIDE + 2] = dt2;
+        trow[(size_t)j * ROW_STRIDE + 3] = (j < JM - 1) ? 1.0 / dt : 0.0;
+        trow[(size_t)j * ROW_STRIDE + 4] = (j < JM - 1) ? 1.0 / dt2 : 0.0;
+    }
+    for (int i = 0; i < IM; ++i) {
+        double dd = (i < IM - 1) ? d[i + 1] - d[i] : 0.0;
+        double dd2 = dd * dd;
+        drow[(size_t)i * ROW_STRIDE + 0] = d[i];
+        drow[(size_t)i * ROW_STRIDE + 1] = dd;
+        drow[(size_t)i * ROW_STRIDE + 2] = dd2;
+        drow[(size_t)i * ROW_STRIDE + 3] = (i < IM - 1) ? 1.0 / dd : 0.0;
+        drow[(size_t)i * ROW_STRIDE + 4] = (i < IM - 1) ? 1.0 / dd2 : 0.0;
+    }
+
+    eos_finalize();
+    cudaError_t e = cudaMalloc(&d_node, node.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_trow, trow.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_drow, drow.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_fail, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemcpy(d_node, node.data(), node.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_trow, trow.data(), trow.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_drow, drow.data(), drow.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(d_fail, 0, sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        set_error(CASTRO_ERR_CUDA, cudaGetErrorString(e));
+        return CASTRO_ERR_CUDA;
+    }
+    // physical constants, Source/eos.F90:129-137
+    const double h = 6.6260689633e-27, avo_eos = 6.0221417930e23, clight = 2.99792458e10;
+    const double kerg = 1.380650424e-16, amu = 1.66053878283e-24;
+    const double asol = 4.0 * 5.67051e-5 / clight;
+    g_eos.node = d_node;
+    g_eos.trow = d_trow;
+    g_eos.drow = d_drow;
+    g_eos.tlo = tlo;
+    g_eos.dlo = dlo;
+    g_eos.tstpi = 1.0 / tstp;
+    g_eos.dstpi = 1.0 / dstp;
+    g_eos.mintemp = pow(10.0, tlo);
+    g_eos.asoli3 = asol / 3.0;
+    g_eos.kergavo = kerg * avo_eos;
+    g_eos.avo_eos = avo_eos;
+    g_eos.sioncon = (2.0 * M_PI * amu * kerg) / (h * h);
+    g_eos.fail_count = d_fail;
+    g_table = true;
+    upload_all();
+    return castro_last_error() == 0 ? CASTRO_OK : castro_last_error();
+}
+
+void eos_init(void)
+{
+    const char* p = getenv("CASTRO_HELM_TABLE");
+    castro_eos_init_path(p && *p ? p : "helm_table.dat");
+}
+
+void eos_finalize(void)
+{
+    if (d_node) cudaFree(d_node);
+    if (d_trow) cudaFree(d_trow);
+    if (d_drow) cudaFree(d_drow);
+    if (d_fail) cudaFree(d_fail);
+    d_node = d_trow = d_drow = nullptr;
+    d_fail = nullptr;
+    g_table = false;
+}
+
+void castro_problem_defaults(castro_problem* p)
+{
+    memset(p, 0, sizeof *p);
+    p->ambient_from_T = 0;
+    p->dens_ambient = 1.e4;
+    p->p_ambient = 1.e21;
+    p->T_ambient = 1.e6;
+    p->exp_energy = 1.e52;
+    p->r_init = 1.25e8;
+    p->nsub = 10;
+    p->X[0] = 1.0;
+    p->T_init = 1.e9;
+}
+
+int castro_set_problem(const castro_problem* p)
+{
+    if (!p || p->nsub < 1 || !(p->dens_ambient > 0.0)) {
+        set_error(CASTRO_ERR_ARG, "castro_set_problem: invalid problem");
+        return CASTRO_ERR_ARG;
+    }
+    g_prob = *p;
+    g_prob_set = true;
+    return CASTRO_OK;
+}
+
+}  // extern "C"

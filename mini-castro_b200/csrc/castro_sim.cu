@@ -1,0 +1,1328 @@
+// castro_sim.cu -- single-level Sedov simulations on one GPU.
+//
+// CASTRO_MODE_PLAIN replays the reference's host sequence box by box through
+// the per-routine entry points (Castro::advance, Source/Castro_advance.cpp:12-100,
+// with construct_hydro_source's 36 launches per box, Source/Castro_hydro.cpp:31-397).
+//
+// CASTRO_MODE_BATCHED advances every box of every instance with eight fused
+// kernels per step, each walking a static work list of (box, region, chunk)
+// items built once per BoxArray, and replays the step as one CUDA graph:
+//
+//   front   : clean_state(S_old) -> clean_state(Sborder) -> ctoprim   (per valid zone)
+//   ghost   : Q / Sborder ghost zones gathered from the owning boxes (periodic or outflow)
+//   trace   : uflatten once, trace_ppm in x, y, z, divu                (per zone of grow(bx,1))
+//   riemann1: compute_flux on tbx[d][d]                                 (normal fluxes)
+//   riemann2: trans1 + compute_flux on tbx[a][b], a != b                (cross fluxes)
+//   riemann3: trans2 + compute_flux + apply_av + normalize_species_fluxes on ebx[d]
+//   update  : fill_hydro_source + Saxpy + clean_state x2 + estdt        (per valid zone)
+//   dt      : computeNewDt (change_max 1.1, stop_time clamp) on the device
+//
+// Because clean_state, ctoprim and estdt are pointwise, a ghost zone's value
+// equals its source zone's value bit for bit, so primitive variables are formed
+// once per zone and gathered instead of recomputed in every box's halo.
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "castro_common.cuh"
+#include "../../include/castro_b200.h"
+
+namespace castro {
+
+void upload_constants_sim(const EosTableDev& e, const NetworkDev& n)
+{
+    cudaMemcpyToSymbol(c_eos, &e, sizeof e);
+    cudaMemcpyToSymbol(c_net, &n, sizeof n);
+}
+
+const castro_problem& problem();
+unsigned long long* eos_fail_counter();
+
+namespace {
+
+constexpr int NG = 4;   // ghost zones of Sborder, Source/Castro_advance.cpp:37
+constexpr int BLOCK = 128;
+
+// ordered pair (a,b), a != b -> 0..5
+__host__ __device__ __forceinline__ int pair_index(int a, int b) { return a * 2 + (b > a ? b - 1 : b); }
+
+struct BoxDev {
+    int lo[3], hi[3];
+    int inst;
+    long long offU, offUb, offQ, offDiv;
+    long long offTr[3], offF1[3], offF2[6], offFx[3];
+};
+
+struct InstDev {
+    int dom_lo[3], dom_hi[3];
+    int bc;
+    int g;            // owner map granularity
+    int on[3];        // owner map dims
+    long long owner_off;
+    double dx[3];
+};
+
+struct InstState {
+    double dt, time, dt_est, stop_time;
+    int steps, pad;
+};
+
+struct Work { int box, sub, start, count; };
+
+enum Region { R_VALID = 0, R_G1, R_G4, R_TBX, R_EBX };
+
+struct Reg {
+    int lx, ly, lz, nx, ny, nz;
+    long long np;
+};
+
+__host__ __device__ __forceinline__ Reg make_reg(const int* lo, const int* hi, int kind, int sub)
+{
+    int l[3] = {lo[0], lo[1], lo[2]}, h[3] = {hi[0], hi[1], hi[2]};
+    if (kind == R_G1) { for (int d = 0; d < 3; ++d) { l[d] -= 1; h[d] += 1; } }
+    else if (kind == R_G4) { for (int d = 0; d < 3; ++d) { l[d] -= NG; h[d] += NG; } }
+    else if (kind == R_EBX) { h[sub] += 1; }
+    else if (kind == R_TBX) {
+        // sub = 3*a + b: faces normal to a; grown by 1 in the directions other
+        // than a and b (Source/Castro_hydro.cpp:93-101)
+        int a = sub / 3, b = sub % 3;
+        h[a] += 1;
+        for (int d = 0; d < 3; ++d)
+            if (d != a && d != b) { l[d] -= 1; h[d] += 1; }
+    }
+    Reg r;
+    r.lx = l[0]; r.ly = l[1]; r.lz = l[2];
+    r.nx = h[0] - l[0] + 1; r.ny = h[1] - l[1] + 1; r.nz = h[2] - l[2] + 1;
+    r.np = (long long)r.nx * r.ny * r.nz;
+    return r;
+}
+
+__device__ __forceinline__ long long ridx(const Reg& r, int i, int j, int k)
+{
+    return (long long)(i - r.lx) + (long long)r.nx * ((long long)(j - r.ly) + (long long)r.ny * (k - r.lz));
+}
+
+struct SimDev {
+    const BoxDev* boxes;
+    const InstDev* inst;
+    InstState* st;
+    double* U;
+    double* Ub;
+    double* Q;
+    double* Div;
+    double* Tr;
+    double* F1;
+    double* F2;
+    double* Fx;
+    const int* owner;
+};
+
+// item of a work list -> (box, zone index); returns false for idle threads
+__device__ __forceinline__ bool work_point(const Work* wl, const SimDev& S, int kind, int subkind_tbx,
+                                          int& b, int& sub, Reg& R, int& i, int& j, int& k)
+{
+    const Work w = wl[blockIdx.x];
+    if ((int)threadIdx.x >= w.count) return false;
+    b = w.box;
+    sub = w.sub;
+    const BoxDev& B = S.boxes[b];
+    int rs = sub;
+    if (kind == R_TBX && subkind_tbx == 0) rs = 4 * sub;   // tbx[d][d]
+    if (kind == R_TBX && subkind_tbx == 1) {               // pair index -> (a,b)
+        int a = sub / 2, r2 = sub % 2;
+        int bb = (r2 < a) ? r2 : r2 + 1;
+        rs = 3 * a + bb;
+    }
+    R = make_reg(B.lo, B.hi, kind, rs);
+    long long t = (long long)w.start + threadIdx.x;
+    i = R.lx + (int)(t % R.nx);
+    long long t2 = t / R.nx;
+    j = R.ly + (int)(t2 % R.ny);
+    k = R.lz + (int)(t2 / R.ny);
+    return true;
+}
+
+// Q record: rho, u, v, w, p, rhoe, X[NS], gamc, c
+template <int NS>
+struct QF {
+    static constexpr int RHO = 0, U = 1, P = 4, RE = 5, X = 6, GAMC = 6 + NS, C = 7 + NS, N = 8 + NS;
+};
+
+template <int NS>
+struct QLoader {
+    const double* base;
+    Reg R;
+    __device__ __forceinline__ double at(int i, int j, int k, int c) const { return base[ridx(R, i, j, k) + R.np * c]; }
+    __device__ __forceinline__ double q(int i, int j, int k, int n) const
+    {
+        int c = (n == QRHO) ? QF<NS>::RHO : (n <= QW) ? n : (n == QPRES) ? QF<NS>::P : (n == QREINT) ? QF<NS>::RE : QF<NS>::X + (n - QFS);
+        return at(i, j, k, c);
+    }
+    __device__ __forceinline__ double gamc(int i, int j, int k) const { return at(i, j, k, QF<NS>::GAMC); }
+    __device__ __forceinline__ double c(int i, int j, int k) const { return at(i, j, k, QF<NS>::C); }
+};
+
+__device__ __forceinline__ void atomic_min_pos(double* addr, double v)
+{
+    unsigned long long* a = reinterpret_cast<unsigned long long*>(addr);
+    unsigned long long old = *a, assumed;
+    while (true) {
+        double cur = __longlong_as_double((long long)old);
+        if (!(v < cur)) break;
+        assumed = old;
+        old = atomicCAS(a, assumed, (unsigned long long)__double_as_longlong(v));
+        if (old == assumed) break;
+    }
+}
+
+__device__ __forceinline__ double block_min(double m)
+{
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = DMIN(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 1.79769313486231570e+308;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = DMIN(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    return m;
+}
+
+// ---------------------------------------------------------------------------
+// fused kernels
+// ---------------------------------------------------------------------------
+
+// front: clean_state(S_old) -> S_new base; clean_state(Sborder); ctoprim
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_front(SimDev S, const Work* wl)
+{
+    int b, sub, i, j, k;
+    Reg R;
+    if (!work_point(wl, S, R_VALID, -1, b, sub, R, i, j, k)) return;
+    const BoxDev& B = S.boxes[b];
+    constexpr int NVAR = Dims<NS>::NVAR, QVAR = Dims<NS>::QVAR;
+    double u[NVAR];
+    double* U = S.U + B.offU;
+    long long id = ridx(R, i, j, k);
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) u[n] = U[id + R.np * n];
+    clean_state_pt<NS>(u);                          // Castro_advance.cpp:51
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) U[id + R.np * n] = u[n];
+    clean_state_pt<NS>(u);                          // Castro_advance.cpp:66 (valid part of Sborder)
+    Reg R1 = make_reg(B.lo, B.hi, R_G1, 0);
+    double* Ub = S.Ub + B.offUb;
+    long long id1 = ridx(R1, i, j, k);
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) Ub[id1 + R1.np * n] = u[n];
+    double q[QVAR], qa[NQAUX];
+    ctoprim_pt<NS>(u, q, qa);                       // Castro_hydro.cpp:64-70
+    Reg R4 = make_reg(B.lo, B.hi, R_G4, 0);
+    double* Q = S.Q + B.offQ;
+    long long id4 = ridx(R4, i, j, k);
+    using F = QF<NS>;
+    Q[id4 + R4.np * F::RHO] = q[QRHO];
+    Q[id4 + R4.np * (F::U + 0)] = q[QU];
+    Q[id4 + R4.np * (F::U + 1)] = q[QV];
+    Q[id4 + R4.np * (F::U + 2)] = q[QW];
+    Q[id4 + R4.np * F::P] = q[QPRES];
+    Q[id4 + R4.np * F::RE] = q[QREINT];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) Q[id4 + R4.np * (F::X + n)] = q[QFS + n];
+    Q[id4 + R4.np * F::GAMC] = qa[QGAMC];
+    Q[id4 + R4.np * F::C] = qa[QC];
+}
+
+__device__ __forceinline__ int map_bc(int i, int lo, int hi, int bc)
+{
+    if (bc == CASTRO_BC_PERIODIC) {
+        int n = hi - lo + 1;
+        int r = (i - lo) % n;
+        if (r < 0) r += n;
+        return lo + r;
+    }
+    return i < lo ? lo : (i > hi ? hi : i);
+}
+
+// ghost: Q on grow(bx,4) and Sborder on grow(bx,1) outside the valid box
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_ghost(SimDev S, const Work* wl)
+{
+    int b, sub, i, j, k;
+    Reg R;
+    if (!work_point(wl, S, R_G4, -1, b, sub, R, i, j, k)) return;
+    const BoxDev& B = S.boxes[b];
+    if (i >= B.lo[0] && i <= B.hi[0] && j >= B.lo[1] && j <= B.hi[1] && k >= B.lo[2] && k <= B.hi[2]) return;
+    const InstDev& I = S.inst[B.inst];
+    int ii = map_bc(i, I.dom_lo[0], I.dom_hi[0], I.bc);
+    int jj = map_bc(j, I.dom_lo[1], I.dom_hi[1], I.bc);
+    int kk = map_bc(k, I.dom_lo[2], I.dom_hi[2], I.bc);
+    int ob = S.owner[I.owner_off + (long long)((ii - I.dom_lo[0]) / I.g) +
+                     (long long)I.on[0] * ((long long)((jj - I.dom_lo[1]) / I.g) + (long long)I.on[1] * ((kk - I.dom_lo[2]) / I.g))];
+    const BoxDev& O = S.boxes[ob];
+    Reg RO4 = make_reg(O.lo, O.hi, R_G4, 0);
+    const double* Qs = S.Q + O.offQ;
+    double* Qd = S.Q + B.offQ;
+    long long is = ridx(RO4, ii, jj, kk), id = ridx(R, i, j, k);
+#pragma unroll
+    for (int c = 0; c < QF<NS>::N; ++c) Qd[id + R.np * c] = Qs[is + RO4.np * c];
+    if (i >= B.lo[0] - 1 && i <= B.hi[0] + 1 && j >= B.lo[1] - 1 && j <= B.hi[1] + 1 && k >= B.lo[2] - 1 && k <= B.hi[2] + 1) {
+        Reg R1 = make_reg(B.lo, B.hi, R_G1, 0), RO1 = make_reg(O.lo, O.hi, R_G1, 0);
+        const double* Us = S.Ub + O.offUb;
+        double* Ud = S.Ub + B.offUb;
+        long long is1 = ridx(RO1, ii, jj, kk), id1 = ridx(R1, i, j, k);
+#pragma unroll
+        for (int n = 0; n < Dims<NS>::NVAR; ++n) Ud[id1 + R1.np * n] = Us[is1 + RO1.np * n];
+    }
+}
+
+// trace: flattening once per zone, the three directional traces, divu
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_trace(SimDev S, const Work* wl)
+{
+    int b, sub, i, j, k;
+    Reg R;
+    if (!work_point(wl, S, R_G1, -1, b, sub, R, i, j, k)) return;
+    const BoxDev& B = S.boxes[b];
+    const InstDev& I = S.inst[B.inst];
+    const double dt = S.st[B.inst].dt;
+    QLoader<NS> ld;
+    ld.base = S.Q + B.offQ;
+    ld.R = make_reg(B.lo, B.hi, R_G4, 0);
+    constexpr int NQS = Dims<NS>::NQS;
+
+    // divu at node (i,j,k), Castro_hydro_nd.F90:45-63
+    {
+        double dxinv = 1.0 / I.dx[0], dyinv = 1.0 / I.dx[1], dzinv = 1.0 / I.dx[2];
+        auto Qv = [&](int a, int bq, int c, int n) { return ld.at(a, bq, c, QF<NS>::U + n); };
+        double ux = 0.25 * (+Qv(i, j, k, 0) - Qv(i - 1, j, k, 0)
+                            + Qv(i, j, k - 1, 0) - Qv(i - 1, j, k - 1, 0)
+                            + Qv(i, j - 1, k, 0) - Qv(i - 1, j - 1, k, 0)
+                            + Qv(i, j - 1, k - 1, 0) - Qv(i - 1, j - 1, k - 1, 0)) * dxinv;
+        double vy = 0.25 * (+Qv(i, j, k, 1) - Qv(i, j - 1, k, 1)
+                            + Qv(i, j, k - 1, 1) - Qv(i, j - 1, k - 1, 1)
+                            + Qv(i - 1, j, k, 1) - Qv(i - 1, j - 1, k, 1)
+                            + Qv(i - 1, j, k - 1, 1) - Qv(i - 1, j - 1, k - 1, 1)) * dyinv;
+        double wz = 0.25 * (+Qv(i, j, k, 2) - Qv(i, j, k - 1, 2)
+                            + Qv(i, j - 1, k, 2) - Qv(i, j - 1, k - 1, 2)
+                            + Qv(i - 1, j, k, 2) - Qv(i - 1, j, k - 1, 2)
+                            + Qv(i - 1, j - 1, k, 2) - Qv(i - 1, j - 1, k - 1, 2)) * dzinv;
+        S.Div[B.offDiv + ridx(R, i, j, k)] = ux + vy + wz;
+    }
+
+    double flatn = uflatten(ld, i, j, k);
+#pragma unroll 1
+    for (int d = 0; d < 3; ++d) {
+        double qplus[NQS], qminus[NQS];
+        trace_zone<NS>(ld, i, j, k, d, dt / I.dx[d], flatn, qplus, qminus);
+        Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * d);
+        double* T = S.Tr + B.offTr[d];
+        int idx = d == 0 ? i : d == 1 ? j : k;
+        if (idx >= B.lo[d]) {
+            long long f = ridx(RT, i, j, k);
+#pragma unroll
+            for (int c = 0; c < NQS; ++c) T[f + RT.np * (NQS + c)] = qplus[c];
+        }
+        if (idx <= B.hi[d]) {
+            long long f = ridx(RT, i + (d == 0), j + (d == 1), k + (d == 2));
+#pragma unroll
+            for (int c = 0; c < NQS; ++c) T[f + RT.np * c] = qminus[c];
+        }
+    }
+}
+
+template <int NS>
+__device__ __forceinline__ void store_tf(double* base, const Reg& R, long long f, const double* flx, const double* qg, int normal)
+{
+    using T = TF<NS>;
+    base[f + R.np * T::RHO] = flx[URHO];
+    base[f + R.np * T::MX] = flx[UMX];
+    base[f + R.np * T::MY] = flx[UMY];
+    base[f + R.np * T::MZ] = flx[UMZ];
+    base[f + R.np * T::ED] = flx[UEDEN];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) base[f + R.np * (T::X + n)] = flx[UFS + n];
+    base[f + R.np * T::PG] = qg[GDPRES];
+    base[f + R.np * T::UG] = qg[GDU + normal];
+}
+
+template <int NS>
+__device__ __forceinline__ void load_tf(const double* base, const Reg& R, long long f, double* r)
+{
+#pragma unroll
+    for (int c = 0; c < TF<NS>::N; ++c) r[c] = base[f + R.np * c];
+}
+
+// riemann1: compute_flux on tbx[d][d] (Castro_hydro.cpp:214-224)
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_riemann1(SimDev S, const Work* wl)
+{
+    int b, d, i, j, k;
+    Reg R;
+    if (!work_point(wl, S, R_TBX, 0, b, d, R, i, j, k)) return;
+    const BoxDev& B = S.boxes[b];
+    constexpr int NQS = Dims<NS>::NQS, NVAR = Dims<NS>::NVAR;
+    const double* T = S.Tr + B.offTr[d];
+    long long f = ridx(R, i, j, k);
+    double ql[NQS], qr[NQS];
+#pragma unroll
+    for (int c = 0; c < NQS; ++c) { ql[c] = T[f + R.np * c]; qr[c] = T[f + R.np * (NQS + c)]; }
+    QLoader<NS> ld;
+    ld.base = S.Q + B.offQ;
+    ld.R = make_reg(B.lo, B.hi, R_G4, 0);
+    const int ex = d == 0, ey = d == 1, ez = d == 2;
+    double flx[NVAR], qg[NGDNV];
+    riemann_cgf<NS>(ql, qr, ld.gamc(i - ex, j - ey, k - ez), ld.gamc(i, j, k), ld.c(i - ex, j - ey, k - ez),
+                    ld.c(i, j, k), d, flx, qg, nullptr);
+    store_tf<NS>(S.F1 + B.offF1[d], R, f, flx, qg, d);
+}
+
+// riemann2: trans1 of the a-normal states with the b fluxes, then
+// compute_flux -> F^{a|b} on tbx[a][b] (Castro_hydro.cpp:228-255, 280-304)
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_riemann2(SimDev S, const Work* wl)
+{
+    int bx, p, i, j, k;
+    Reg R;
+    if (!work_point(wl, S, R_TBX, 1, bx, p, R, i, j, k)) return;
+    const BoxDev& B = S.boxes[bx];
+    const InstDev& I = S.inst[B.inst];
+    const double dt = S.st[B.inst].dt;
+    const int a = p / 2, r2 = p % 2;
+    const int bdir = (r2 < a) ? r2 : r2 + 1;
+    constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF, NVAR = Dims<NS>::NVAR;
+    const double cdtdx = dt / I.dx[bdir] / 3.0;
+    QLoader<NS> ld;
+    ld.base = S.Q + B.offQ;
+    ld.R = make_reg(B.lo, B.hi, R_G4, 0);
+    Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * a);
+    Reg RF = make_reg(B.lo, B.hi, R_TBX, 4 * bdir);
+    const double* T = S.Tr + B.offTr[a];
+    const double* F = S.F1 + B.offF1[bdir];
+    const int eax = a == 0, eay = a == 1, eaz = a == 2;
+    const int ebx_ = bdir == 0, eby = bdir == 1, ebz = bdir == 2;
+    long long ft = ridx(RT, i, j, k);
+    double st2[2][NQS];
+#pragma unroll
+    for (int D = -1; D <= 0; ++D) {
+        double lq[NQS], fr[NTF], fl[NTF];
+        const int off = (D == -1) ? 0 : NQS;
+#pragma unroll
+        for (int c = 0; c < NQS; ++c) lq[c] = T[ft + RT.np * (off + c)];
+        int il = i + D * eax, jl = j + D * eay, kl = k + D * eaz;
+        load_tf<NS>(F, RF, ridx(RF, il + ebx_, jl + eby, kl + ebz), fr);
+        load_tf<NS>(F, RF, ridx(RF, il, jl, kl), fl);
+        trans1_state<NS>(lq, fr, fl, ld.gamc(il, jl, kl), cdtdx, st2[D + 1]);
+    }
+    double flx[NVAR], qg[NGDNV];
+    riemann_cgf<NS>(st2[0], st2[1], ld.gamc(i - eax, j - eay, k - eaz), ld.gamc(i, j, k),
+                    ld.c(i - eax, j - eay, k - eaz), ld.c(i, j, k), a, flx, qg, nullptr);
+    store_tf<NS>(S.F2 + B.offF2[p], R, ridx(R, i, j, k), flx, qg, a);
+}
+
+// riemann3: trans2 + compute_flux + apply_av + normalize_species_fluxes on ebx[d]
+// (Castro_hydro.cpp:307-359)
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_riemann3(SimDev S, const Work* wl)
+{
+    int bx, d, i, j, k;
+    Reg R;
+    if (!work_point(wl, S, R_EBX, -1, bx, d, R, i, j, k)) return;
+    const BoxDev& B = S.boxes[bx];
+    const InstDev& I = S.inst[B.inst];
+    const double dt = S.st[B.inst].dt;
+    const int t1 = (d == 0) ? 1 : 0;
+    const int t2 = (d == 2) ? 1 : 2;
+    constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF, NVAR = Dims<NS>::NVAR;
+    const double hdt1 = 0.5 * dt / I.dx[t1], hdt2 = 0.5 * dt / I.dx[t2];
+    QLoader<NS> ld;
+    ld.base = S.Q + B.offQ;
+    ld.R = make_reg(B.lo, B.hi, R_G4, 0);
+    Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * d);
+    const int p12 = pair_index(t1, t2), p21 = pair_index(t2, t1);
+    Reg R12 = make_reg(B.lo, B.hi, R_TBX, 3 * t1 + t2);
+    Reg R21 = make_reg(B.lo, B.hi, R_TBX, 3 * t2 + t1);
+    const double* T = S.Tr + B.offTr[d];
+    const double* F12 = S.F2 + B.offF2[p12];
+    const double* F21 = S.F2 + B.offF2[p21];
+    const int ex = d == 0, ey = d == 1, ez = d == 2;
+    const int e1x = t1 == 0, e1y = t1 == 1, e1z = t1 == 2;
+    const int e2x = t2 == 0, e2y = t2 == 1, e2z = t2 == 2;
+    long long ft = ridx(RT, i, j, k);
+    double st2[2][NQS];
+#pragma unroll
+    for (int D = -1; D <= 0; ++D) {
+        double lq[NQS], f2r[NTF], f2l[NTF], f3r[NTF], f3l[NTF];
+        const int off = (D == -1) ? 0 : NQS;
+#pragma unroll
+        for (int c = 0; c < NQS; ++c) lq[c] = T[ft + RT.np * (off + c)];
+        int il = i + D * ex, jl = j + D * ey, kl = k + D * ez;
+        load_tf<NS>(F12, R12, ridx(R12, il + e1x, jl + e1y, kl + e1z), f2r);
+        load_tf<NS>(F12, R12, ridx(R12, il, jl, kl), f2l);
+        load_tf<NS>(F21, R21, ridx(R21, il + e2x, jl + e2y, kl + e2z), f3r);
+        load_tf<NS>(F21, R21, ridx(R21, il, jl, kl), f3l);
+        trans2_state<NS>(lq, f2r, f2l, f3r, f3l, ld.gamc(il, jl, kl), hdt1, hdt2, st2[D + 1]);
+    }
+    double flx[NVAR], qg[NGDNV];
+    riemann_cgf<NS>(st2[0], st2[1], ld.gamc(i - ex, j - ey, k - ez), ld.gamc(i, j, k),
+                    ld.c(i - ex, j - ey, k - ez), ld.c(i, j, k), d, flx, qg, nullptr);
+
+    // apply_av, Castro_hydro_nd.F90:207-237 (the x and y four-node sums as written there)
+    {
+        Reg R1 = make_reg(B.lo, B.hi, R_G1, 0);
+        const double* Dv = S.Div + B.offDiv;
+        auto dv = [&](int a, int bq, int c) { return Dv[ridx(R1, a, bq, c)]; };
+        double ds;
+        if (d == 0) ds = dv(i, j, k) + dv(i, j + 1, k) + dv(i, j, k + 1) + dv(i, j + 1, k);
+        else if (d == 1) ds = dv(i, j, k) + dv(i + 1, j, k) + dv(i, j, k + 1) + dv(i + 1, j, k);
+        else ds = dv(i, j, k) + dv(i + 1, j, k) + dv(i, j + 1, k) + dv(i + 1, j + 1, k);
+        const double* Ub = S.Ub + B.offUb;
+        long long c0 = ridx(R1, i, j, k), cm = ridx(R1, i - ex, j - ey, k - ez);
+        const double dxd = I.dx[d];
+#pragma unroll
+        for (int n = 0; n < NVAR; ++n) {
+            if (n == UTEMP) continue;
+            double div1 = av_term(ds, Ub[c0 + R1.np * n] - Ub[cm + R1.np * n]);
+            flx[n] = flx[n] + dxd * div1;
+        }
+    }
+    // normalize_species_fluxes, Castro_hydro_nd.F90:277-291
+    {
+        double sum = 0.0;
+#pragma unroll
+        for (int n = 0; n < NS; ++n) sum = sum + flx[UFS + n];
+        double fac = (sum != 0.0) ? flx[URHO] / sum : 1.0;
+#pragma unroll
+        for (int n = 0; n < NS; ++n) flx[UFS + n] = flx[UFS + n] * fac;
+    }
+    // final record: every flux component but UTEMP (always zero), GDPRES, GDU_d
+    double* X = S.Fx + B.offFx[d];
+    long long f = ridx(R, i, j, k);
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) {
+        if (n == UTEMP) continue;
+        X[f + R.np * (n < UTEMP ? n : n - 1)] = flx[n];
+    }
+    X[f + R.np * (NVAR - 1)] = qg[GDPRES];
+    X[f + R.np * NVAR] = qg[GDU + d];
+}
+
+// update: fill_hydro_source, Saxpy, clean_state (advance), clean_state
+// (post_timestep), estdt of the new state
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_update(SimDev S, const Work* wl)
+{
+    int b, sub, i, j, k;
+    Reg R;
+    bool active = work_point(wl, S, R_VALID, -1, b, sub, R, i, j, k);
+    const Work w = wl[blockIdx.x];
+    const BoxDev& B = S.boxes[w.box];
+    const InstDev& I = S.inst[B.inst];
+    double m = 1.79769313486231570e+308;
+    if (active) {
+        constexpr int NVAR = Dims<NS>::NVAR;
+        const double dt = S.st[B.inst].dt;
+        const double a0 = I.dx[1] * I.dx[2], a1 = I.dx[0] * I.dx[2], a2 = I.dx[0] * I.dx[1];
+        const double volinv = 1.0 / (I.dx[0] * I.dx[1] * I.dx[2]);
+        Reg RX[3];
+        const double* X[3];
+        long long f0[3], f1[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            RX[d] = make_reg(B.lo, B.hi, R_EBX, d);
+            X[d] = S.Fx + B.offFx[d];
+            f0[d] = ridx(RX[d], i, j, k);
+            f1[d] = ridx(RX[d], i + (d == 0), j + (d == 1), k + (d == 2));
+        }
+        double* U = S.U + B.offU;
+        long long id = ridx(R, i, j, k);
+        double u[NVAR];
+#pragma unroll
+        for (int n = 0; n < NVAR; ++n) {
+            double un = U[id + R.np * n];
+            if (n == UTEMP) { u[n] = un + dt * 0.0; continue; }
+            const int c = n < UTEMP ? n : n - 1;
+            double src = 0.0 + (X[0][f0[0] + RX[0].np * c] * a0 - X[0][f1[0] + RX[0].np * c] * a0
+                              + X[1][f0[1] + RX[1].np * c] * a1 - X[1][f1[1] + RX[1].np * c] * a1
+                              + X[2][f0[2] + RX[2].np * c] * a2 - X[2][f1[2] + RX[2].np * c] * a2) * volinv;
+            if (n == UEINT) {
+                const int P = NVAR - 1, V = NVAR;
+                double pdivu = 0.5 * (X[0][f1[0] + RX[0].np * P] + X[0][f0[0] + RX[0].np * P]) *
+                                   (X[0][f1[0] + RX[0].np * V] - X[0][f0[0] + RX[0].np * V]) / I.dx[0] +
+                               0.5 * (X[1][f1[1] + RX[1].np * P] + X[1][f0[1] + RX[1].np * P]) *
+                                   (X[1][f1[1] + RX[1].np * V] - X[1][f0[1] + RX[1].np * V]) / I.dx[1] +
+                               0.5 * (X[2][f1[2] + RX[2].np * P] + X[2][f0[2] + RX[2].np * P]) *
+                                   (X[2][f1[2] + RX[2].np * V] - X[2][f0[2] + RX[2].np * V]) / I.dx[2];
+                src = src - pdivu;
+            }
+            u[n] = un + dt * src;                        // MultiFab::Saxpy, Castro_advance.cpp:74
+        }
+        clean_state_pt<NS>(u);                           // Castro_advance.cpp:78
+        clean_state_pt<NS>(u);                           // Castro.cpp:369
+#pragma unroll
+        for (int n = 0; n < NVAR; ++n) U[id + R.np * n] = u[n];
+        m = estdt_pt<NS>(u, I.dx[0], I.dx[1], I.dx[2]);  // Castro.cpp:191-203 of the next coarse step
+    }
+    // one box per block: the block reduction has a single instance target
+    m = block_min(m);
+    if (threadIdx.x == 0) atomic_min_pos(&S.st[B.inst].dt_est, m);
+}
+
+// estdt on the current state (computeInitialDt / castro_sim_est_time_step)
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_estdt_state(SimDev S, const Work* wl)
+{
+    int b, sub, i, j, k;
+    Reg R;
+    bool active = work_point(wl, S, R_VALID, -1, b, sub, R, i, j, k);
+    const Work w = wl[blockIdx.x];
+    const BoxDev& B = S.boxes[w.box];
+    const InstDev& I = S.inst[B.inst];
+    double m = 1.79769313486231570e+308;
+    if (active) {
+        constexpr int NVAR = Dims<NS>::NVAR;
+        const double* U = S.U + B.offU;
+        long long id = ridx(R, i, j, k);
+        double u[NVAR];
+#pragma unroll
+        for (int n = 0; n < NVAR; ++n) u[n] = U[id + R.np * n];
+        m = estdt_pt<NS>(u, I.dx[0], I.dx[1], I.dx[2]);
+    }
+    m = block_min(m);
+    if (threadIdx.x == 0) atomic_min_pos(&S.st[B.inst].dt_est, m);
+}
+
+// computeInitialDt (first) or, after a step, time/step bookkeeping and
+// computeNewDt (Source/Castro.cpp:162-341)
+__global__ void k_dt(SimDev S, int ninst, int first)
+{
+    int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ninst) return;
+    InstState& st = S.st[n];
+    double est = st.dt_est * cfl;                       // estTimeStep, Castro.cpp:212-213
+    double dt_0;
+    if (first) {
+        dt_0 = DMIN(1.0e+100, 0.01 * est);               // initialTimeStep, Castro.cpp:168-170
+    } else {
+        st.time = st.time + st.dt;
+        st.steps = st.steps + 1;
+        double dt_min = DMIN(est, 1.1e0 * st.dt);        // Castro.cpp:264-267
+        dt_0 = DMIN(1.0e+100, dt_min);
+    }
+    double eps = 0.001 * dt_0;
+    if (st.stop_time >= 0.0) {
+        if ((st.time + dt_0) > (st.stop_time - eps)) dt_0 = st.stop_time - st.time;
+    }
+    st.dt = dt_0;
+    st.dt_est = 1.79769313486231570e+308;
+}
+
+// FillPatch of Sborder for the plain path: every zone of grow(bx,4) from the
+// owning box's state under the instance boundary condition
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_fill_sborder(SimDev S, int b, double* sb)
+{
+    const BoxDev& B = S.boxes[b];
+    Reg R = make_reg(B.lo, B.hi, R_G4, 0);
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= R.np) return;
+    int i = R.lx + (int)(t % R.nx);
+    long long t2 = t / R.nx;
+    int j = R.ly + (int)(t2 % R.ny);
+    int k = R.lz + (int)(t2 / R.ny);
+    const InstDev& I = S.inst[B.inst];
+    int ii = map_bc(i, I.dom_lo[0], I.dom_hi[0], I.bc);
+    int jj = map_bc(j, I.dom_lo[1], I.dom_hi[1], I.bc);
+    int kk = map_bc(k, I.dom_lo[2], I.dom_hi[2], I.bc);
+    int ob = S.owner[I.owner_off + (long long)((ii - I.dom_lo[0]) / I.g) +
+                     (long long)I.on[0] * ((long long)((jj - I.dom_lo[1]) / I.g) + (long long)I.on[1] * ((kk - I.dom_lo[2]) / I.g))];
+    const BoxDev& O = S.boxes[ob];
+    Reg RO = make_reg(O.lo, O.hi, R_VALID, 0);
+    const double* Us = S.U + O.offU;
+    long long is = ridx(RO, ii, jj, kk);
+#pragma unroll
+    for (int n = 0; n < Dims<NS>::NVAR; ++n) sb[t + R.np * n] = Us[is + RO.np * n];
+}
+
+__global__ void k_saxpy(double* u, const double* s, long long n, const double* dtp)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) u[t] += *dtp * s[t];
+}
+
+__global__ void k_fill(double* p, long long n, double v)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) p[t] = v;
+}
+
+}  // namespace
+}  // namespace castro
+
+using namespace castro;
+
+// ===========================================================================
+// the simulation object
+// ===========================================================================
+struct castro_sim {
+    int mode = CASTRO_MODE_BATCHED;
+    int ns = 2;
+    int nvar = 9;
+    int ninst = 0;
+    cudaStream_t st = nullptr;
+    std::vector<castro_instance_desc> desc;
+    std::vector<castro_problem> probs;
+    std::vector<std::vector<int>> inst_boxes;   // global box ids per instance
+    std::vector<BoxDev> hboxes;
+    std::vector<InstDev> hinst;
+    std::vector<double> hdx;                    // 3 per instance
+    BoxDev* dboxes = nullptr;
+    InstDev* dinst = nullptr;
+    InstState* dstate = nullptr;
+    int* downer = nullptr;
+    double *U = nullptr, *Ub = nullptr, *Q = nullptr, *Div = nullptr;
+    double *Tr = nullptr, *F1 = nullptr, *F2 = nullptr, *Fx = nullptr;
+    long long nU = 0;
+    // work lists
+    Work *w_valid = nullptr, *w_g4 = nullptr, *w_g1 = nullptr, *w_tbx = nullptr, *w_pair = nullptr, *w_ebx = nullptr;
+    int n_valid = 0, n_g4 = 0, n_g1 = 0, n_tbx = 0, n_pair = 0, n_ebx = 0;
+    bool dt_ready = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int launches = 0;
+    // plain-path scratch (largest box)
+    double* sb = nullptr;      // Sborder per box (grow 4) for all boxes
+    double* src = nullptr;     // hydro_source per box for all boxes
+    std::vector<long long> offSb, offSrc;
+    double* scratch = nullptr;
+    long long scratch_n = 0;
+    double* d_dtloc = nullptr; // managed-style reduction target of estdt
+    double* d_dtbox = nullptr; // dt per instance for the plain saxpy
+    SimDev dev() const
+    {
+        SimDev S;
+        S.boxes = dboxes; S.inst = dinst; S.st = dstate;
+        S.U = U; S.Ub = Ub; S.Q = Q; S.Div = Div; S.Tr = Tr; S.F1 = F1; S.F2 = F2; S.Fx = Fx;
+        S.owner = downer;
+        return S;
+    }
+};
+
+namespace {
+
+long long npts_reg(const int* lo, const int* hi, int kind, int sub)
+{
+    Reg r = make_reg(lo, hi, kind, sub);
+    return r.np;
+}
+
+bool cuda_ok(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess) {
+        char buf[256];
+        snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+        set_error(CASTRO_ERR_CUDA, buf);
+        return false;
+    }
+    return true;
+}
+
+template <class T>
+bool dalloc(T** p, size_t n, const char* what)
+{
+    if (n == 0) n = 1;
+    return cuda_ok(cudaMalloc((void**)p, n * sizeof(T)), what);
+}
+
+void build_work(castro_sim* s, int kind, int nsub, int tbx_mode, Work** out, int* count)
+{
+    std::vector<Work> w;
+    for (size_t b = 0; b < s->hboxes.size(); ++b) {
+        const BoxDev& B = s->hboxes[b];
+        for (int sub = 0; sub < nsub; ++sub) {
+            int rs = sub;
+            if (kind == R_TBX && tbx_mode == 0) rs = 4 * sub;
+            if (kind == R_TBX && tbx_mode == 1) {
+                int a = sub / 2, r2 = sub % 2;
+                rs = 3 * a + ((r2 < a) ? r2 : r2 + 1);
+            }
+            long long np = npts_reg(B.lo, B.hi, kind, rs);
+            for (long long st = 0; st < np; st += BLOCK) {
+                Work it;
+                it.box = (int)b;
+                it.sub = sub;
+                it.start = (int)st;
+                it.count = (int)std::min<long long>(BLOCK, np - st);
+                w.push_back(it);
+            }
+        }
+    }
+    *count = (int)w.size();
+    if (dalloc(out, w.size(), "work list"))
+        cuda_ok(cudaMemcpy(*out, w.data(), w.size() * sizeof(Work), cudaMemcpyHostToDevice), "work list copy");
+}
+
+template <int NS>
+void batched_step_kernels(castro_sim* s)
+{
+    SimDev S = s->dev();
+    cudaStream_t st = s->st;
+    k_front<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid);
+    k_ghost<NS><<<s->n_g4, BLOCK, 0, st>>>(S, s->w_g4);
+    k_trace<NS><<<s->n_g1, BLOCK, 0, st>>>(S, s->w_g1);
+    k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(S, s->w_tbx);
+    k_riemann2<NS><<<s->n_pair, BLOCK, 0, st>>>(S, s->w_pair);
+    k_riemann3<NS><<<s->n_ebx, BLOCK, 0, st>>>(S, s->w_ebx);
+    k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid);
+    k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0);
+}
+
+template <int NS>
+void initial_dt_kernels(castro_sim* s)
+{
+    SimDev S = s->dev();
+    k_estdt_state<NS><<<s->n_valid, BLOCK, 0, s->st>>>(S, s->w_valid);
+    k_dt<<<(s->ninst + 63) / 64, 64, 0, s->st>>>(S, s->ninst, 1);
+}
+
+// ---- plain path: the reference host sequence through the per-routine ABI ----
+
+struct PlainScratch {
+    // FABs of Castro_hydro.cpp:54-170 for one box
+    double *q, *qaux, *flux[3], *qe[3], *qm[3][3], *qp[3][3], *div, *q_int, *ftmp1, *ftmp2, *qg1, *qg2, *ql, *qr;
+    double *area[3], *vol;
+};
+
+struct IBox { int lo[3], hi[3]; };
+IBox grow(IBox b, int gx, int gy, int gz)
+{
+    b.lo[0] -= gx; b.lo[1] -= gy; b.lo[2] -= gz;
+    b.hi[0] += gx; b.hi[1] += gy; b.hi[2] += gz;
+    return b;
+}
+long long npts(const IBox& b) { return (long long)(b.hi[0] - b.lo[0] + 1) * (b.hi[1] - b.lo[1] + 1) * (b.hi[2] - b.lo[2] + 1); }
+
+void plain_clean(const int* lo, const int* hi, double* u, const int* ulo, const int* uhi)
+{
+    // Castro::clean_state, Source/Castro.cpp:563-591
+    enforce_minimum_density(lo, hi, u, ulo, uhi);
+    normalize_species(lo, hi, u, ulo, uhi);
+    reset_internal_e(lo, hi, u, ulo, uhi);
+    compute_temp(lo, hi, u, ulo, uhi);
+}
+
+// Castro::construct_hydro_source for one box through the per-routine entry
+// points, Source/Castro_hydro.cpp:31-397
+void plain_hydro_box(castro_sim* s, const IBox& bx, double* sbp, double* srcp, const int* domlo, const int* domhi,
+                     const double* dx, double dt)
+{
+    const int NV = s->nvar, QV = s->nvar + 1;
+    IBox obx = grow(bx, 1, 1, 1), qbx = grow(bx, NG, NG, NG);
+    IBox sbx = qbx;
+    IBox ebx[3], gebx[3], tbx[3][3];
+    double* cur = s->scratch;
+    auto take = [&](const IBox& b, int nc) { double* p = cur; cur += npts(b) * nc; return p; };
+    PlainScratch P;
+    P.q = take(qbx, QV);
+    P.qaux = take(qbx, NQAUX);
+    ctoprim(qbx.lo, qbx.hi, sbp, sbx.lo, sbx.hi, P.q, qbx.lo, qbx.hi, P.qaux, qbx.lo, qbx.hi);
+    for (int d = 0; d < 3; ++d) {
+        ebx[d] = bx; ebx[d].hi[d] += 1;
+        gebx[d] = grow(ebx[d], 1, 1, 1);
+        P.flux[d] = take(gebx[d], NV);
+        P.qe[d] = take(gebx[d], NGDNV);
+        P.area[d] = take(gebx[d], 1);
+    }
+    tbx[0][0] = grow(ebx[0], 0, 1, 1); tbx[0][1] = grow(ebx[0], 0, 0, 1); tbx[0][2] = grow(ebx[0], 0, 1, 0);
+    tbx[1][0] = grow(ebx[1], 0, 0, 1); tbx[1][1] = grow(ebx[1], 1, 0, 1); tbx[1][2] = grow(ebx[1], 1, 0, 0);
+    tbx[2][0] = grow(ebx[2], 0, 1, 0); tbx[2][1] = grow(ebx[2], 1, 0, 0); tbx[2][2] = grow(ebx[2], 1, 1, 0);
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) { P.qm[a][b] = take(tbx[a][b], QV); P.qp[a][b] = take(tbx[a][b], QV); }
+    P.div = take(obx, 1);
+    divu(obx.lo, obx.hi, P.q, qbx.lo, qbx.hi, dx, P.div, obx.lo, obx.hi);
+    P.q_int = take(obx, QV);
+    P.ftmp1 = take(obx, NV);
+    P.ftmp2 = take(obx, NV);
+    P.qg1 = take(obx, NGDNV);
+    P.qg2 = take(obx, NGDNV);
+    P.ql = take(obx, QV);
+    P.qr = take(obx, QV);
+    P.vol = take(bx, 1);
+    if (cur - s->scratch > s->scratch_n) { set_error(CASTRO_ERR_ARG, "plain path scratch overflow"); return; }
+
+    double hdtdx[3], cdtdx[3];
+    for (int d = 0; d < 3; ++d) { hdtdx[d] = 0.5 * dt / dx[d]; cdtdx[d] = dt / dx[d] / 3.0; }
+    for (int d = 0; d < 3; ++d)
+        trace_ppm(obx.lo, obx.hi, bx.lo, bx.hi, d + 1, P.q, qbx.lo, qbx.hi, P.qaux, qbx.lo, qbx.hi,
+                  P.qm[d][d], tbx[d][d].lo, tbx[d][d].hi, P.qp[d][d], tbx[d][d].lo, tbx[d][d].hi, domlo, domhi, dx, dt);
+    for (int d = 0; d < 3; ++d) {
+        int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+        const IBox& b = tbx[d][d];
+        compute_flux(b.lo, b.hi, P.qm[d][d], b.lo, b.hi, P.qp[d][d], b.lo, b.hi, P.ftmp1, obx.lo, obx.hi,
+                     P.q_int, obx.lo, obx.hi, P.qg1, obx.lo, obx.hi, P.qaux, qbx.lo, qbx.hi, d + 1);
+        trans1(tbx[t1][d].lo, tbx[t1][d].hi, d + 1, t1 + 1, P.qm[t1][t1], tbx[t1][t1].lo, tbx[t1][t1].hi,
+               P.qm[t1][d], tbx[t1][d].lo, tbx[t1][d].hi, P.qp[t1][t1], tbx[t1][t1].lo, tbx[t1][t1].hi,
+               P.qp[t1][d], tbx[t1][d].lo, tbx[t1][d].hi, P.qaux, qbx.lo, qbx.hi, P.ftmp1, obx.lo, obx.hi,
+               P.qg1, obx.lo, obx.hi, cdtdx[d]);
+        trans1(tbx[t2][d].lo, tbx[t2][d].hi, d + 1, t2 + 1, P.qm[t2][t2], tbx[t2][t2].lo, tbx[t2][t2].hi,
+               P.qm[t2][d], tbx[t2][d].lo, tbx[t2][d].hi, P.qp[t2][t2], tbx[t2][t2].lo, tbx[t2][t2].hi,
+               P.qp[t2][d], tbx[t2][d].lo, tbx[t2][d].hi, P.qaux, qbx.lo, qbx.hi, P.ftmp1, obx.lo, obx.hi,
+               P.qg1, obx.lo, obx.hi, cdtdx[d]);
+    }
+    for (int d = 0; d < 3; ++d) {
+        int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+        compute_flux(tbx[t1][t2].lo, tbx[t1][t2].hi, P.qm[t1][t2], tbx[t1][t2].lo, tbx[t1][t2].hi,
+                     P.qp[t1][t2], tbx[t1][t2].lo, tbx[t1][t2].hi, P.ftmp1, obx.lo, obx.hi, P.q_int, obx.lo, obx.hi,
+                     P.qg1, obx.lo, obx.hi, P.qaux, qbx.lo, qbx.hi, t1 + 1);
+        compute_flux(tbx[t2][t1].lo, tbx[t2][t1].hi, P.qm[t2][t1], tbx[t2][t1].lo, tbx[t2][t1].hi,
+                     P.qp[t2][t1], tbx[t2][t1].lo, tbx[t2][t1].hi, P.ftmp2, obx.lo, obx.hi, P.q_int, obx.lo, obx.hi,
+                     P.qg2, obx.lo, obx.hi, P.qaux, qbx.lo, qbx.hi, t2 + 1);
+        trans2(ebx[d].lo, ebx[d].hi, d + 1, t1 + 1, t2 + 1, P.qm[d][d], tbx[d][d].lo, tbx[d][d].hi,
+               P.ql, obx.lo, obx.hi, P.qp[d][d], tbx[d][d].lo, tbx[d][d].hi, P.qr, obx.lo, obx.hi,
+               P.qaux, qbx.lo, qbx.hi, P.ftmp1, obx.lo, obx.hi, P.ftmp2, obx.lo, obx.hi,
+               P.qg1, obx.lo, obx.hi, P.qg2, obx.lo, obx.hi, hdtdx[d], hdtdx[t1], hdtdx[t2]);
+        compute_flux(ebx[d].lo, ebx[d].hi, P.ql, obx.lo, obx.hi, P.qr, obx.lo, obx.hi, P.flux[d], gebx[d].lo,
+                     gebx[d].hi, P.q_int, obx.lo, obx.hi, P.qe[d], gebx[d].lo, gebx[d].hi, P.qaux, qbx.lo, qbx.hi,
+                     d + 1);
+    }
+    for (int d = 0; d < 3; ++d) {
+        apply_av(ebx[d].lo, ebx[d].hi, d + 1, dx, P.div, obx.lo, obx.hi, sbp, sbx.lo, sbx.hi, P.flux[d], gebx[d].lo,
+                 gebx[d].hi);
+        normalize_species_fluxes(ebx[d].lo, ebx[d].hi, P.flux[d], gebx[d].lo, gebx[d].hi);
+    }
+    // geometry (Cartesian GetFaceArea / GetVolume)
+    double area[3] = {dx[1] * dx[2], dx[0] * dx[2], dx[0] * dx[1]};
+    for (int d = 0; d < 3; ++d) {
+        long long n = npts(gebx[d]);
+        k_fill<<<(unsigned)((n + 255) / 256), 256, 0, s->st>>>(P.area[d], n, area[d]);
+    }
+    {
+        long long n = npts(bx);
+        k_fill<<<(unsigned)((n + 255) / 256), 256, 0, s->st>>>(P.vol, n, dx[0] * dx[1] * dx[2]);
+    }
+    fill_hydro_source(bx.lo, bx.hi, sbp, sbx.lo, sbx.hi, P.q, qbx.lo, qbx.hi, srcp, bx.lo, bx.hi,
+                      P.flux[0], gebx[0].lo, gebx[0].hi, P.flux[1], gebx[1].lo, gebx[1].hi,
+                      P.flux[2], gebx[2].lo, gebx[2].hi, P.qe[0], gebx[0].lo, gebx[0].hi,
+                      P.qe[1], gebx[1].lo, gebx[1].hi, P.qe[2], gebx[2].lo, gebx[2].hi,
+                      P.area[0], gebx[0].lo, gebx[0].hi, P.area[1], gebx[1].lo, gebx[1].hi,
+                      P.area[2], gebx[2].lo, gebx[2].hi, P.vol, bx.lo, bx.hi, dx, dt);
+}
+
+long long plain_scratch_size(const IBox& bx, int nvar)
+{
+    const int NV = nvar, QV = nvar + 1;
+    IBox obx = grow(bx, 1, 1, 1), qbx = grow(bx, NG, NG, NG);
+    long long n = npts(qbx) * (QV + NQAUX);
+    for (int d = 0; d < 3; ++d) {
+        IBox e = bx; e.hi[d] += 1;
+        IBox g = grow(e, 1, 1, 1);
+        n += npts(g) * (NV + NGDNV + 1);
+    }
+    n += 18 * npts(obx) * QV;   // qm/qp: tbx boxes are contained in obx-sized boxes plus one face
+    n += npts(obx) * (1 + QV + 2 * NV + 2 * NGDNV + 2 * QV);
+    n += npts(bx);
+    return n + 1024;
+}
+
+template <int NS>
+void plain_step(castro_sim* s)
+{
+    SimDev S = s->dev();
+    cudaStream_t saved = castro::stream();
+    castro_set_stream(s->st);
+    for (int in = 0; in < s->ninst; ++in) {
+        InstState hs;
+        cudaMemcpyAsync(&hs, s->dstate + in, sizeof hs, cudaMemcpyDeviceToHost, s->st);
+        cudaStreamSynchronize(s->st);
+        const castro_instance_desc& D = s->desc[in];
+        const double* dx = &s->hdx[3 * in];
+        // computeInitialDt / computeNewDt, Source/Castro.cpp:175-341
+        {
+            double big = 1.79769313486231570e+308;
+            cudaMemcpyAsync(s->d_dtloc, &big, sizeof big, cudaMemcpyHostToDevice, s->st);
+            for (int b : s->inst_boxes[in]) {
+                const BoxDev& B = s->hboxes[b];
+                estdt(B.lo, B.hi, s->U + B.offU, B.lo, B.hi, dx, s->d_dtloc);
+            }
+            double dtl;
+            cudaMemcpyAsync(&dtl, s->d_dtloc, sizeof dtl, cudaMemcpyDeviceToHost, s->st);
+            cudaStreamSynchronize(s->st);
+            dtl *= cfl;
+            double dt_0;
+            if (hs.steps == 0) dt_0 = std::min(1.0e+100, 0.01 * dtl);
+            else dt_0 = std::min(1.0e+100, std::min(dtl, 1.1e0 * hs.dt));
+            double eps = 0.001 * dt_0;
+            if (hs.stop_time >= 0.0 && (hs.time + dt_0) > (hs.stop_time - eps)) dt_0 = hs.stop_time - hs.time;
+            hs.dt = dt_0;
+        }
+        const double dt = hs.dt;
+        // Castro::advance, Source/Castro_advance.cpp:32-97
+        for (int b : s->inst_boxes[in]) {
+            const BoxDev& B = s->hboxes[b];
+            plain_clean(B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
+        }
+        for (int b : s->inst_boxes[in]) {
+            const BoxDev& B = s->hboxes[b];
+            long long n = npts_reg(B.lo, B.hi, R_G4, 0);
+            k_fill_sborder<NS><<<(unsigned)((n + BLOCK - 1) / BLOCK), BLOCK, 0, s->st>>>(S, b, s->sb + s->offSb[b]);
+        }
+        for (int b : s->inst_boxes[in]) {
+            const BoxDev& B = s->hboxes[b];
+            IBox bx{{B.lo[0], B.lo[1], B.lo[2]}, {B.hi[0], B.hi[1], B.hi[2]}};
+            IBox g = grow(bx, NG, NG, NG);
+            plain_clean(g.lo, g.hi, s->sb + s->offSb[b], g.lo, g.hi);
+        }
+        for (int b : s->inst_boxes[in]) {
+            const BoxDev& B = s->hboxes[b];
+            IBox bx{{B.lo[0], B.lo[1], B.lo[2]}, {B.hi[0], B.hi[1], B.hi[2]}};
+            long long n = npts(bx) * s->nvar;
+            cudaMemsetAsync(s->src + s->offSrc[b], 0, n * sizeof(double), s->st);   // hydro_source.setVal(0)
+            plain_hydro_box(s, bx, s->sb + s->offSb[b], s->src + s->offSrc[b], D.dom_lo, D.dom_hi, dx, dt);
+        }
+        cudaMemcpyAsync(s->d_dtbox, &hs.dt, sizeof(double), cudaMemcpyHostToDevice, s->st);
+        for (int b : s->inst_boxes[in]) {
+            const BoxDev& B = s->hboxes[b];
+            long long n = npts_reg(B.lo, B.hi, R_VALID, 0) * s->nvar;
+            k_saxpy<<<(unsigned)((n + 255) / 256), 256, 0, s->st>>>(s->U + B.offU, s->src + s->offSrc[b], n, s->d_dtbox);
+        }
+        for (int b : s->inst_boxes[in]) {
+            const BoxDev& B = s->hboxes[b];
+            plain_clean(B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
+        }
+        // post_timestep: clean_state(S_new), Source/Castro.cpp:369
+        for (int b : s->inst_boxes[in]) {
+            const BoxDev& B = s->hboxes[b];
+            plain_clean(B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
+        }
+        hs.time = hs.time + hs.dt;
+        hs.steps += 1;
+        cudaMemcpyAsync(s->dstate + in, &hs, sizeof hs, cudaMemcpyHostToDevice, s->st);
+        cudaStreamSynchronize(s->st);
+    }
+    castro_set_stream(saved);
+}
+
+template <int NS>
+int step_impl(castro_sim* s)
+{
+    if (s->mode == CASTRO_MODE_PLAIN) {
+        plain_step<NS>(s);
+        s->launches = 0;
+        for (int in = 0; in < s->ninst; ++in) s->launches += 55 * (int)s->inst_boxes[in].size();
+        return castro_last_error();
+    }
+    if (!s->dt_ready) {
+        initial_dt_kernels<NS>(s);
+        s->dt_ready = true;
+    }
+    if (!s->gexec) {
+        if (!cuda_ok(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal), "begin capture")) return castro_last_error();
+        batched_step_kernels<NS>(s);
+        if (!cuda_ok(cudaStreamEndCapture(s->st, &s->graph), "end capture")) return castro_last_error();
+        if (!cuda_ok(cudaGraphInstantiate(&s->gexec, s->graph, 0), "graph instantiate")) return castro_last_error();
+    }
+    cuda_ok(cudaGraphLaunch(s->gexec, s->st), "graph launch");
+    s->launches = 8;
+    return castro_last_error();
+}
+
+}  // namespace
+
+// ===========================================================================
+// extern "C"
+// ===========================================================================
+extern "C" {
+
+castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int mode)
+{
+    if (!table_ready()) { set_error(CASTRO_ERR_NO_TABLE, "castro_sim_create: eos_init has not run"); return nullptr; }
+    if (ninst < 1 || !desc) { set_error(CASTRO_ERR_ARG, "castro_sim_create: no instances"); return nullptr; }
+    int ns = nspec();
+    if (ns != 2 && ns != 13) { set_error(CASTRO_ERR_NSPEC, "castro_sim_create: nspec"); return nullptr; }
+    castro_sim* s = new castro_sim();
+    s->mode = mode;
+    s->ns = ns;
+    s->nvar = 7 + ns;
+    s->ninst = ninst;
+    s->desc.assign(desc, desc + ninst);
+    cuda_ok(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking), "stream create");
+    const int NQS = 6 + ns, NTF = 7 + ns, NQF = 8 + ns, NV = 7 + ns;
+
+    long long oU = 0, oUb = 0, oQ = 0, oDiv = 0, oTr = 0, oF1 = 0, oF2 = 0, oFx = 0;
+    std::vector<int> owner_all;
+    for (int in = 0; in < ninst; ++in) {
+        const castro_instance_desc& D = desc[in];
+        InstDev I;
+        memset(&I, 0, sizeof I);
+        for (int d = 0; d < 3; ++d) {
+            I.dom_lo[d] = D.dom_lo[d];
+            I.dom_hi[d] = D.dom_hi[d];
+            I.dx[d] = (D.probhi[d] - D.problo[d]) / (double)(D.dom_hi[d] - D.dom_lo[d] + 1);
+            s->hdx.push_back(I.dx[d]);
+        }
+        I.bc = D.bc;
+        // owner map granularity: gcd of every box edge offset
+        int g = 0;
+        for (int d = 0; d < 3; ++d) g = std::gcd(g, D.dom_hi[d] - D.dom_lo[d] + 1);
+        std::vector<int> ids;
+        for (int b = 0; b < D.nbox; ++b)
+            for (int d = 0; d < 3; ++d) {
+                g = std::gcd(g, D.box_lo[3 * b + d] - D.dom_lo[d]);
+                g = std::gcd(g, D.box_hi[3 * b + d] + 1 - D.dom_lo[d]);
+            }
+        if (g <= 0) g = 1;
+        I.g = g;
+        for (int d = 0; d < 3; ++d) I.on[d] = (D.dom_hi[d] - D.dom_lo[d] + 1) / g;
+        I.owner_off = (long long)owner_all.size();
+        size_t nown = (size_t)I.on[0] * I.on[1] * I.on[2];
+        owner_all.resize(owner_all.size() + nown, -1);
+        for (int b = 0; b < D.nbox; ++b) {
+            BoxDev B;
+            memset(&B, 0, sizeof B);
+            for (int d = 0; d < 3; ++d) { B.lo[d] = D.box_lo[3 * b + d]; B.hi[d] = D.box_hi[3 * b + d]; }
+            B.inst = in;
+            B.offU = oU; oU += npts_reg(B.lo, B.hi, R_VALID, 0) * NV;
+            B.offUb = oUb; oUb += npts_reg(B.lo, B.hi, R_G1, 0) * NV;
+            B.offQ = oQ; oQ += npts_reg(B.lo, B.hi, R_G4, 0) * NQF;
+            B.offDiv = oDiv; oDiv += npts_reg(B.lo, B.hi, R_G1, 0);
+            for (int d = 0; d < 3; ++d) {
+                B.offTr[d] = oTr; oTr += npts_reg(B.lo, B.hi, R_TBX, 4 * d) * 2 * NQS;
+                B.offF1[d] = oF1; oF1 += npts_reg(B.lo, B.hi, R_TBX, 4 * d) * NTF;
+                B.offFx[d] = oFx; oFx += npts_reg(B.lo, B.hi, R_EBX, d) * (NV + 1);
+            }
+            for (int a = 0; a < 3; ++a)
+                for (int bb = 0; bb < 3; ++bb) {
+                    if (a == bb) continue;
+                    int p = pair_index(a, bb);
+                    B.offF2[p] = oF2; oF2 += npts_reg(B.lo, B.hi, R_TBX, 3 * a + bb) * NTF;
+                }
+            int gid = (int)s->hboxes.size();
+            ids.push_back(gid);
+            s->hboxes.push_back(B);
+            for (int k = B.lo[2]; k <= B.hi[2]; k += g)
+                for (int j = B.lo[1]; j <= B.hi[1]; j += g)
+                    for (int i = B.lo[0]; i <= B.hi[0]; i += g)
+                        owner_all[I.owner_off + (i - D.dom_lo[0]) / g +
+                                  (long long)I.on[0] * ((j - D.dom_lo[1]) / g + (long long)I.on[1] * ((k - D.dom_lo[2]) / g))] = gid;
+        }
+        for (size_t m = I.owner_off; m < owner_all.size(); ++m)
+            if (owner_all[m] < 0) { set_error(CASTRO_ERR_ARG, "castro_sim_create: boxes do not cover the domain"); delete s; return nullptr; }
+        s->inst_boxes.push_back(ids);
+        s->hinst.push_back(I);
+    }
+    s->nU = oU;
+    bool ok = dalloc(&s->dboxes, s->hboxes.size(), "boxes") && dalloc(&s->dinst, s->hinst.size(), "instances") &&
+              dalloc(&s->dstate, ninst, "state") && dalloc(&s->downer, owner_all.size(), "owner") &&
+              dalloc(&s->U, oU, "U") && dalloc(&s->d_dtloc, 1, "dtloc") && dalloc(&s->d_dtbox, 1, "dtbox");
+    if (ok) {
+        cuda_ok(cudaMemcpy(s->dboxes, s->hboxes.data(), s->hboxes.size() * sizeof(BoxDev), cudaMemcpyHostToDevice), "boxes");
+        cuda_ok(cudaMemcpy(s->dinst, s->hinst.data(), s->hinst.size() * sizeof(InstDev), cudaMemcpyHostToDevice), "inst");
+        cuda_ok(cudaMemcpy(s->downer, owner_all.data(), owner_all.size() * sizeof(int), cudaMemcpyHostToDevice), "owner");
+        std::vector<InstState> hs(ninst);
+        for (int in = 0; in < ninst; ++in) {
+            memset(&hs[in], 0, sizeof(InstState));
+            hs[in].dt_est = 1.79769313486231570e+308;
+            hs[in].stop_time = desc[in].stop_time;
+        }
+        cuda_ok(cudaMemcpy(s->dstate, hs.data(), ninst * sizeof(InstState), cudaMemcpyHostToDevice), "state");
+    }
+    if (ok && mode == CASTRO_MODE_BATCHED) {
+        ok = dalloc(&s->Ub, oUb, "Ub") && dalloc(&s->Q, oQ, "Q") && dalloc(&s->Div, oDiv, "Div") &&
+             dalloc(&s->Tr, oTr, "Tr") && dalloc(&s->F1, oF1, "F1") && dalloc(&s->F2, oF2, "F2") && dalloc(&s->Fx, oFx, "Fx");
+        build_work(s, R_VALID, 1, -1, &s->w_valid, &s->n_valid);
+        build_work(s, R_G4, 1, -1, &s->w_g4, &s->n_g4);
+        build_work(s, R_G1, 1, -1, &s->w_g1, &s->n_g1);
+        build_work(s, R_TBX, 3, 0, &s->w_tbx, &s->n_tbx);
+        build_work(s, R_TBX, 6, 1, &s->w_pair, &s->n_pair);
+        build_work(s, R_EBX, 3, -1, &s->w_ebx, &s->n_ebx);
+    }
+    if (ok && mode == CASTRO_MODE_PLAIN) {
+        long long nsb = 0, nsrc = 0, mx = 0;
+        for (const BoxDev& B : s->hboxes) {
+            s->offSb.push_back(nsb);
+            nsb += npts_reg(B.lo, B.hi, R_G4, 0) * NV;
+            s->offSrc.push_back(nsrc);
+            nsrc += npts_reg(B.lo, B.hi, R_VALID, 0) * NV;
+            IBox bx{{B.lo[0], B.lo[1], B.lo[2]}, {B.hi[0], B.hi[1], B.hi[2]}};
+            mx = std::max(mx, plain_scratch_size(bx, NV));
+        }
+        s->scratch_n = mx;
+        ok = dalloc(&s->sb, nsb, "Sborder") && dalloc(&s->src, nsrc, "hydro_source") && dalloc(&s->scratch, mx, "scratch");
+        // the work list of the valid region is still used by estdt of the sim API
+        build_work(s, R_VALID, 1, -1, &s->w_valid, &s->n_valid);
+    }
+    s->probs.resize(ninst);
+    for (int in = 0; in < ninst; ++in) s->probs[in] = desc[in].prob;
+    if (!ok || castro_last_error()) { castro_sim_destroy(s); return nullptr; }
+    return s;
+}
+
+void castro_sim_destroy(castro_sim* s)
+{
+    if (!s) return;
+    if (s->gexec) cudaGraphExecDestroy(s->gexec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    void* ptrs[] = {s->dboxes, s->dinst, s->dstate, s->downer, s->U, s->Ub, s->Q, s->Div, s->Tr, s->F1, s->F2, s->Fx,
+                    s->w_valid, s->w_g4, s->w_g1, s->w_tbx, s->w_pair, s->w_ebx, s->sb, s->src, s->scratch,
+                    s->d_dtloc, s->d_dtbox};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (s->st) cudaStreamDestroy(s->st);
+    delete s;
+}
+
+int castro_sim_nbox(const castro_sim* s, int inst) { return (int)s->inst_boxes[inst].size(); }
+
+size_t castro_sim_box_size(const castro_sim* s, int inst, int b)
+{
+    const BoxDev& B = s->hboxes[s->inst_boxes[inst][b]];
+    return (size_t)npts_reg(B.lo, B.hi, R_VALID, 0) * s->nvar;
+}
+
+double* castro_sim_box_state(castro_sim* s, int inst, int b)
+{
+    return s->U + s->hboxes[s->inst_boxes[inst][b]].offU;
+}
+
+size_t castro_sim_total_size(const castro_sim* s) { return (size_t)s->nU; }
+
+int castro_sim_init_data(castro_sim* s)
+{
+    cudaStream_t saved = castro::stream();
+    castro_set_stream(s->st);
+    for (int in = 0; in < s->ninst; ++in) {
+        castro_set_problem(&s->probs[in]);
+        const castro_instance_desc& D = s->desc[in];
+        for (int b : s->inst_boxes[in]) {
+            const BoxDev& B = s->hboxes[b];
+            initdata(B.lo, B.hi, s->U + B.offU, B.lo, B.hi, &s->hdx[3 * in], D.problo, D.probhi);
+        }
+    }
+    castro_set_stream(saved);
+    cuda_ok(cudaStreamSynchronize(s->st), "init_data");
+    return castro_last_error();
+}
+
+int castro_sim_upload(castro_sim* s, const double* host)
+{
+    cuda_ok(cudaMemcpyAsync(s->U, host, (size_t)s->nU * sizeof(double), cudaMemcpyHostToDevice, s->st), "upload");
+    return castro_last_error();
+}
+
+int castro_sim_download(castro_sim* s, double* host)
+{
+    cuda_ok(cudaMemcpyAsync(host, s->U, (size_t)s->nU * sizeof(double), cudaMemcpyDeviceToHost, s->st), "download");
+    return castro_last_error();
+}
+
+int castro_sim_step(castro_sim* s)
+{
+    if (s->ns == 2) return step_impl<2>(s);
+    return step_impl<13>(s);
+}
+
+int castro_sim_run(castro_sim* s, int nsteps)
+{
+    for (int n = 0; n < nsteps; ++n) {
+        int e = castro_sim_step(s);
+        if (e) return e;
+    }
+    return castro_last_error();
+}
+
+int castro_sim_run_host(castro_sim* s, const double* host_in, int nsteps, double* host_out)
+{
+    castro_sim_upload(s, host_in);
+    castro_sim_run(s, nsteps);
+    castro_sim_download(s, host_out);
+    cuda_ok(cudaStreamSynchronize(s->st), "run_host");
+    return castro_last_error();
+}
+
+int castro_sim_sync(castro_sim* s)
+{
+    cuda_ok(cudaStreamSynchronize(s->st), "sync");
+    return castro_last_error();
+}
+
+static InstState read_state(castro_sim* s, int inst)
+{
+    InstState h;
+    memset(&h, 0, sizeof h);
+    cudaStreamSynchronize(s->st);
+    cuda_ok(cudaMemcpy(&h, s->dstate + inst, sizeof h, cudaMemcpyDeviceToHost), "read state");
+    return h;
+}
+
+double castro_sim_time(castro_sim* s, int inst) { return read_state(s, inst).time; }
+double castro_sim_dt(castro_sim* s, int inst) { return read_state(s, inst).dt; }
+int castro_sim_steps(castro_sim* s, int inst) { return read_state(s, inst).steps; }
+
+double castro_sim_est_time_step(castro_sim* s, int inst)
+{
+    double big = 1.79769313486231570e+308;
+    cuda_ok(cudaMemcpyAsync(s->d_dtloc, &big, sizeof big, cudaMemcpyHostToDevice, s->st), "est");
+    cudaStream_t saved = castro::stream();
+    castro_set_stream(s->st);
+    for (int b : s->inst_boxes[inst]) {
+        const BoxDev& B = s->hboxes[b];
+        estdt(B.lo, B.hi, s->U + B.offU, B.lo, B.hi, &s->hdx[3 * inst], s->d_dtloc);
+    }
+    castro_set_stream(saved);
+    double dt;
+    cuda_ok(cudaMemcpyAsync(&dt, s->d_dtloc, sizeof dt, cudaMemcpyDeviceToHost, s->st), "est read");
+    cudaStreamSynchronize(s->st);
+    return dt * cfl;
+}
+
+double castro_sim_blast_radius(castro_sim* s, int inst, double* blast_mass)
+{
+    // max density on the host (diagnostic only), then the device reduction
+    double maxd = -1.79769313486231570e+308;
+    std::vector<double> h;
+    for (int b : s->inst_boxes[inst]) {
+        const BoxDev& B = s->hboxes[b];
+        long long n = npts_reg(B.lo, B.hi, R_VALID, 0);
+        h.resize(n);
+        cudaStreamSynchronize(s->st);
+        cuda_ok(cudaMemcpy(h.data(), s->U + B.offU, n * sizeof(double), cudaMemcpyDeviceToHost), "blast read");
+        for (double v : h) maxd = std::max(maxd, v);
+    }
+    double* d2;
+    if (!dalloc(&d2, 2, "blast")) return 0.0;
+    cudaMemset(d2, 0, 2 * sizeof(double));
+    cudaStream_t saved = castro::stream();
+    castro_set_stream(s->st);
+    const castro_instance_desc& D = s->desc[inst];
+    for (int b : s->inst_boxes[inst]) {
+        const BoxDev& B = s->hboxes[b];
+        calculate_blast_radius(B.lo, B.hi, s->U + B.offU, B.lo, B.hi, &s->hdx[3 * inst], D.problo, D.probhi, d2, d2 + 1, maxd);
+    }
+    castro_set_stream(saved);
+    double hr[2];
+    cudaStreamSynchronize(s->st);
+    cuda_ok(cudaMemcpy(hr, d2, sizeof hr, cudaMemcpyDeviceToHost), "blast result");
+    cudaFree(d2);
+    if (blast_mass) *blast_mass = hr[0];
+    return hr[1] / hr[0];
+}
+
+int castro_sim_launches_per_step(const castro_sim* s) { return s->launches; }
+
+long long castro_sim_eos_failures(castro_sim* s)
+{
+    unsigned long long* p = eos_fail_counter();
+    if (!p) return 0;
+    unsigned long long v = 0;
+    cudaStreamSynchronize(s->st);
+    cuda_ok(cudaMemcpy(&v, p, sizeof v, cudaMemcpyDeviceToHost), "eos failures");
+    return (long long)v;
+}
+
+}  // extern "C"
