@@ -259,10 +259,21 @@ int    castro_sim_steps(castro_sim* sim, int inst);
 double castro_sim_est_time_step(castro_sim* sim, int inst);
 /* blast radius diagnostic of Source/Castro.cpp:371-424, cm */
 double castro_sim_blast_radius(castro_sim* sim, int inst, double* blast_mass);
+/* the CUDA stream (cudaStream_t) every launch of this sim is issued on */
+void*  castro_sim_stream(castro_sim* sim);
+/* batched mode: one step with a CUDA event around each of the fused kernels
+ * (no graph); ms[k] receives the duration of kernel k and names[k] its name;
+ * returns the number of kernels (at most 16) */
+int    castro_sim_profile_step(castro_sim* sim, double* ms, const char** names);
 /* kernel launches issued by the last castro_sim_step (graph nodes for the batched mode) */
 int    castro_sim_launches_per_step(const castro_sim* sim);
 /* per-step EOS Newton failures seen so far (non-converged zones) */
 long long castro_sim_eos_failures(castro_sim* sim);
+
+/* FP64 fused-multiply-add throughput of the current device in TFLOP/s,
+ * measured with a dependent-chain DFMA kernel over every SM (roofline
+ * denominator of the FP64 kernels; no reference counterpart) */
+double castro_measure_fp64_tflops(void);
 
 /* the mini-app driver with the reference's command-line keys (Source/main.cpp) */
 int castro_main(int argc, char** argv);

@@ -22,7 +22,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 OBJDIR = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-SOURCES = ["castro_host.cu", "castro_abi.cu", "castro_sim.cu"]
+SOURCES = ["castro_host.cu", "castro_abi.cu", "castro_sim.cu", "castro_main.cu", "castro_peak.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-fPIC",
           "-Xcompiler", "-Wno-subobject-linkage"]
@@ -77,6 +77,16 @@ def build(force: bool = False, verbose: bool = False, variants=None) -> list[str
             r = subprocess.run(cmd, capture_output=True, text=True)
             if r.returncode != 0:
                 raise RuntimeError(f"link failed for {out}:\n{r.stdout}\n{r.stderr}")
+    exe = os.path.join(LIBDIR, "castro_b200.ex")
+    if "libcastro_b200.so" in names and (force or _stale(exe)):
+        main = os.path.join(OBJDIR, "exe_main.cu")
+        with open(main, "w") as fp:
+            fp.write('extern "C" int castro_main(int, char**);\nint main(int c, char** v) { return castro_main(c, v); }\n')
+        cmd = [NVCC, *ARCH, "-o", exe, main, "-L" + LIBDIR, "-lcastro_b200", "-Xlinker", "-rpath=$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed for {exe}:\n{r.stdout}\n{r.stderr}")
+        outs.append(exe)
     return outs
 
 

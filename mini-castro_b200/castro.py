@@ -73,6 +73,7 @@ ABI_SYMBOLS = [
     "castro_sim_download", "castro_sim_total_size", "castro_sim_step", "castro_sim_run", "castro_sim_run_host",
     "castro_sim_sync", "castro_sim_time", "castro_sim_dt", "castro_sim_steps", "castro_sim_est_time_step",
     "castro_sim_blast_radius", "castro_sim_launches_per_step", "castro_sim_eos_failures", "castro_main",
+    "castro_sim_stream", "castro_sim_profile_step", "castro_measure_fp64_tflops",
 ]
 
 
@@ -120,6 +121,10 @@ def load(exact: bool = False) -> C.CDLL:
     L.castro_sim_blast_radius.restype = C.c_double
     L.castro_sim_blast_radius.argtypes = [C.c_void_p, C.c_int, _dp]
     L.castro_sim_launches_per_step.argtypes = [C.c_void_p]
+    L.castro_sim_stream.restype = C.c_void_p
+    L.castro_sim_stream.argtypes = [C.c_void_p]
+    L.castro_sim_profile_step.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_char_p)]
+    L.castro_measure_fp64_tflops.restype = C.c_double
     L.castro_sim_eos_failures.restype = C.c_longlong
     L.castro_sim_eos_failures.argtypes = [C.c_void_p]
     _libs[exact] = L
@@ -307,6 +312,17 @@ class Sim:
         r = self.L.castro_sim_blast_radius(self.h, inst, C.byref(m))
         check(self.L, "blast_radius")
         return r, m.value
+
+    def stream(self) -> int:
+        return int(self.L.castro_sim_stream(self.h))
+
+    def profile_step(self) -> dict:
+        """One batched step with an event around each fused kernel: {name: ms}."""
+        ms = (C.c_double * 16)()
+        names = (C.c_char_p * 16)()
+        n = self.L.castro_sim_profile_step(self.h, ms, names)
+        check(self.L, "castro_sim_profile_step")
+        return {names[k].decode(): ms[k] for k in range(n)}
 
     def launches_per_step(self) -> int:
         return self.L.castro_sim_launches_per_step(self.h)

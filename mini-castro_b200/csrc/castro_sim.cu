@@ -67,7 +67,9 @@ struct InstDev {
 };
 
 struct InstState {
-    double dt, time, dt_est, stop_time;
+    double dt;        // dt of the next step
+    double time, dt_est, stop_time;
+    double dt_last;   // dt of the last completed step (AMReX dtLevel after the step)
     int steps, pad;
 };
 
@@ -612,6 +614,7 @@ __global__ void k_dt(SimDev S, int ninst, int first)
     } else {
         st.time = st.time + st.dt;
         st.steps = st.steps + 1;
+        st.dt_last = st.dt;
         double dt_min = DMIN(est, 1.1e0 * st.dt);        // Castro.cpp:264-267
         dt_0 = DMIN(1.0e+100, dt_min);
     }
@@ -648,6 +651,106 @@ __global__ void __launch_bounds__(BLOCK) k_fill_sborder(SimDev S, int b, double*
     long long is = ridx(RO, ii, jj, kk);
 #pragma unroll
     for (int n = 0; n < Dims<NS>::NVAR; ++n) sb[t + R.np * n] = Us[is + RO.np * n];
+}
+
+// primitive variables straight from a caller's Sborder over grow(bx,4)
+// (construct_hydro_source's ctoprim, Source/Castro_hydro.cpp:64-70)
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_box_prim(SimDev S, const Work* wl, Fab SB)
+{
+    int b, sub, i, j, k;
+    Reg R;
+    if (!work_point(wl, S, R_G4, -1, b, sub, R, i, j, k)) return;
+    const BoxDev& B = S.boxes[b];
+    constexpr int NVAR = Dims<NS>::NVAR, QVAR = Dims<NS>::QVAR;
+    double u[NVAR], q[QVAR], qa[NQAUX];
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) u[n] = SB(i, j, k, n);
+    ctoprim_pt<NS>(u, q, qa);
+    double* Q = S.Q + B.offQ;
+    long long id = ridx(R, i, j, k);
+    using F = QF<NS>;
+    Q[id + R.np * F::RHO] = q[QRHO];
+    Q[id + R.np * (F::U + 0)] = q[QU];
+    Q[id + R.np * (F::U + 1)] = q[QV];
+    Q[id + R.np * (F::U + 2)] = q[QW];
+    Q[id + R.np * F::P] = q[QPRES];
+    Q[id + R.np * F::RE] = q[QREINT];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) Q[id + R.np * (F::X + n)] = q[QFS + n];
+    Q[id + R.np * F::GAMC] = qa[QGAMC];
+    Q[id + R.np * F::C] = qa[QC];
+    if (i >= B.lo[0] - 1 && i <= B.hi[0] + 1 && j >= B.lo[1] - 1 && j <= B.hi[1] + 1 && k >= B.lo[2] - 1 && k <= B.hi[2] + 1) {
+        Reg R1 = make_reg(B.lo, B.hi, R_G1, 0);
+        double* Ub = S.Ub + B.offUb;
+        long long i1 = ridx(R1, i, j, k);
+#pragma unroll
+        for (int n = 0; n < NVAR; ++n) Ub[i1 + R1.np * n] = u[n];
+    }
+}
+
+// fill_hydro_source into the caller's source FAB (Castro_hydro_nd.F90:411-439)
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_box_source(SimDev S, const Work* wl, Fab SRC)
+{
+    int b, sub, i, j, k;
+    Reg R;
+    if (!work_point(wl, S, R_VALID, -1, b, sub, R, i, j, k)) return;
+    const BoxDev& B = S.boxes[b];
+    const InstDev& I = S.inst[B.inst];
+    constexpr int NVAR = Dims<NS>::NVAR;
+    const double a0 = I.dx[1] * I.dx[2], a1 = I.dx[0] * I.dx[2], a2 = I.dx[0] * I.dx[1];
+    const double volinv = 1.0 / (I.dx[0] * I.dx[1] * I.dx[2]);
+    Reg RX[3];
+    const double* X[3];
+    long long f0[3], f1[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        RX[d] = make_reg(B.lo, B.hi, R_EBX, d);
+        X[d] = S.Fx + B.offFx[d];
+        f0[d] = ridx(RX[d], i, j, k);
+        f1[d] = ridx(RX[d], i + (d == 0), j + (d == 1), k + (d == 2));
+    }
+#pragma unroll
+    for (int n = 0; n < NVAR; ++n) {
+        if (n == UTEMP) { SRC(i, j, k, n) = SRC(i, j, k, n) + 0.0 * volinv; continue; }
+        const int c = n < UTEMP ? n : n - 1;
+        double s = SRC(i, j, k, n) + (X[0][f0[0] + RX[0].np * c] * a0 - X[0][f1[0] + RX[0].np * c] * a0
+                                    + X[1][f0[1] + RX[1].np * c] * a1 - X[1][f1[1] + RX[1].np * c] * a1
+                                    + X[2][f0[2] + RX[2].np * c] * a2 - X[2][f1[2] + RX[2].np * c] * a2) * volinv;
+        if (n == UEINT) {
+            const int P = NVAR - 1, V = NVAR;
+            double pdivu = 0.5 * (X[0][f1[0] + RX[0].np * P] + X[0][f0[0] + RX[0].np * P]) *
+                               (X[0][f1[0] + RX[0].np * V] - X[0][f0[0] + RX[0].np * V]) / I.dx[0] +
+                           0.5 * (X[1][f1[1] + RX[1].np * P] + X[1][f0[1] + RX[1].np * P]) *
+                               (X[1][f1[1] + RX[1].np * V] - X[1][f0[1] + RX[1].np * V]) / I.dx[1] +
+                           0.5 * (X[2][f1[2] + RX[2].np * P] + X[2][f0[2] + RX[2].np * P]) *
+                               (X[2][f1[2] + RX[2].np * V] - X[2][f0[2] + RX[2].np * V]) / I.dx[2];
+            s = s - pdivu;
+        }
+        SRC(i, j, k, n) = s;
+    }
+}
+
+// store_flux (Castro_hydro_nd.F90:330-338): dt * F * A on the faces of ebx[d]
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_box_store_flux(SimDev S, const Work* wl, Fab FO0, Fab FO1, Fab FO2, double dt)
+{
+    int b, d, i, j, k;
+    Reg R;
+    if (!work_point(wl, S, R_EBX, -1, b, d, R, i, j, k)) return;
+    const BoxDev& B = S.boxes[b];
+    const InstDev& I = S.inst[B.inst];
+    const Fab& FO = d == 0 ? FO0 : d == 1 ? FO1 : FO2;
+    if (!FO.p) return;
+    const double area = d == 0 ? I.dx[1] * I.dx[2] : d == 1 ? I.dx[0] * I.dx[2] : I.dx[0] * I.dx[1];
+    const double* X = S.Fx + B.offFx[d];
+    long long f = ridx(R, i, j, k);
+#pragma unroll
+    for (int n = 0; n < Dims<NS>::NVAR; ++n) {
+        double F = (n == UTEMP) ? 0.0 : X[f + R.np * (n < UTEMP ? n : n - 1)];
+        FO(i, j, k, n) = dt * F * area;
+    }
 }
 
 __global__ void k_saxpy(double* u, const double* s, long long n, const double* dtp)
@@ -781,6 +884,22 @@ void batched_step_kernels(castro_sim* s)
     k_riemann3<NS><<<s->n_ebx, BLOCK, 0, st>>>(S, s->w_ebx);
     k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid);
     k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0);
+}
+
+template <int NS>
+void profile_kernel(castro_sim* s, const SimDev& S, int k)
+{
+    cudaStream_t st = s->st;
+    switch (k) {
+    case 0: k_front<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid); break;
+    case 1: k_ghost<NS><<<s->n_g4, BLOCK, 0, st>>>(S, s->w_g4); break;
+    case 2: k_trace<NS><<<s->n_g1, BLOCK, 0, st>>>(S, s->w_g1); break;
+    case 3: k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(S, s->w_tbx); break;
+    case 4: k_riemann2<NS><<<s->n_pair, BLOCK, 0, st>>>(S, s->w_pair); break;
+    case 5: k_riemann3<NS><<<s->n_ebx, BLOCK, 0, st>>>(S, s->w_ebx); break;
+    case 6: k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid); break;
+    default: k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0); break;
+    }
 }
 
 template <int NS>
@@ -1002,6 +1121,7 @@ void plain_step(castro_sim* s)
         }
         hs.time = hs.time + hs.dt;
         hs.steps += 1;
+        hs.dt_last = hs.dt;
         cudaMemcpyAsync(s->dstate + in, &hs, sizeof hs, cudaMemcpyHostToDevice, s->st);
         cudaStreamSynchronize(s->st);
     }
@@ -1261,7 +1381,11 @@ static InstState read_state(castro_sim* s, int inst)
 }
 
 double castro_sim_time(castro_sim* s, int inst) { return read_state(s, inst).time; }
-double castro_sim_dt(castro_sim* s, int inst) { return read_state(s, inst).dt; }
+double castro_sim_dt(castro_sim* s, int inst)
+{
+    InstState h = read_state(s, inst);
+    return h.steps > 0 ? h.dt_last : h.dt;
+}
 int castro_sim_steps(castro_sim* s, int inst) { return read_state(s, inst).steps; }
 
 double castro_sim_est_time_step(castro_sim* s, int inst)
@@ -1313,7 +1437,126 @@ double castro_sim_blast_radius(castro_sim* s, int inst, double* blast_mass)
     return hr[1] / hr[0];
 }
 
+}  // extern "C"
+
+// Library-managed scratch of castro_construct_hydro_source_box, reused while
+// the box shape does not change.
+struct BoxScratch {
+    int lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
+    int ns = 0;
+    castro_sim* s = nullptr;
+};
+static BoxScratch g_box;
+
+template <int NS>
+static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const int* sb_lo, const int* sb_hi,
+                          double* source, const int* sr_lo, const int* sr_hi, double* const* fo, const int* fo_lo,
+                          const int* fo_hi, const double* dx, double dt)
+{
+    for (int d = 0; d < 3; ++d)
+        if (sb_lo[d] > lo[d] - NG || sb_hi[d] < hi[d] + NG) {
+            set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box: Sborder needs 4 ghost zones");
+            return CASTRO_ERR_ARG;
+        }
+    bool same = g_box.s && g_box.ns == NS;
+    for (int d = 0; d < 3 && same; ++d) same = g_box.lo[d] == lo[d] && g_box.hi[d] == hi[d];
+    if (!same) {
+        if (g_box.s) castro_sim_destroy(g_box.s);
+        g_box.s = nullptr;
+        castro_instance_desc D;
+        memset(&D, 0, sizeof D);
+        for (int d = 0; d < 3; ++d) {
+            D.dom_lo[d] = lo[d]; D.dom_hi[d] = hi[d];
+            D.problo[d] = 0.0; D.probhi[d] = 1.0;
+        }
+        D.bc = CASTRO_BC_OUTFLOW;
+        D.nbox = 1;
+        D.box_lo = lo;
+        D.box_hi = hi;
+        castro_problem_defaults(&D.prob);
+        D.stop_time = -1.0;
+        g_box.s = castro_sim_create(1, &D, CASTRO_MODE_BATCHED);
+        if (!g_box.s) return castro_last_error();
+        for (int d = 0; d < 3; ++d) { g_box.lo[d] = lo[d]; g_box.hi[d] = hi[d]; }
+        g_box.ns = NS;
+    }
+    castro_sim* s = g_box.s;
+    // geometry and dt of this call
+    InstDev I = s->hinst[0];
+    for (int d = 0; d < 3; ++d) I.dx[d] = dx[d];
+    InstState st;
+    memset(&st, 0, sizeof st);
+    st.dt = dt;
+    st.stop_time = -1.0;
+    cudaStream_t cs = castro::stream();
+    cuda_ok(cudaMemcpyAsync(s->dinst, &I, sizeof I, cudaMemcpyHostToDevice, cs), "box geometry");
+    cuda_ok(cudaMemcpyAsync(s->dstate, &st, sizeof st, cudaMemcpyHostToDevice, cs), "box dt");
+    SimDev S = s->dev();
+    k_box_prim<NS><<<s->n_g4, BLOCK, 0, cs>>>(S, s->w_g4, make_fab(sb, sb_lo, sb_hi));
+    k_trace<NS><<<s->n_g1, BLOCK, 0, cs>>>(S, s->w_g1);
+    k_riemann1<NS><<<s->n_tbx, BLOCK, 0, cs>>>(S, s->w_tbx);
+    k_riemann2<NS><<<s->n_pair, BLOCK, 0, cs>>>(S, s->w_pair);
+    k_riemann3<NS><<<s->n_ebx, BLOCK, 0, cs>>>(S, s->w_ebx);
+    k_box_source<NS><<<s->n_valid, BLOCK, 0, cs>>>(S, s->w_valid, make_fab(source, sr_lo, sr_hi));
+    if (fo) {
+        Fab F[3];
+        for (int d = 0; d < 3; ++d) {
+            F[d] = fo[d] ? make_fab(fo[d], fo_lo + 3 * d, fo_hi + 3 * d) : Fab{};
+            if (!fo[d]) F[d].p = nullptr;
+        }
+        k_box_store_flux<NS><<<s->n_ebx, BLOCK, 0, cs>>>(S, s->w_ebx, F[0], F[1], F[2], dt);
+    }
+    check_launch("castro_construct_hydro_source_box");
+    return castro_last_error();
+}
+
+extern "C" {
+
+int castro_construct_hydro_source_box(const int* lo, const int* hi, const double* sborder, const int* sb_lo,
+                                      const int* sb_hi, double* source, const int* sr_lo, const int* sr_hi,
+                                      double* const* fluxes_out, const int* fo_lo3x3, const int* fo_hi3x3,
+                                      const int* domlo, const int* domhi, const double* dx, double dt)
+{
+    (void)domlo; (void)domhi;
+    if (!table_ready()) { set_error(CASTRO_ERR_NO_TABLE, "castro_construct_hydro_source_box: eos_init has not run"); return CASTRO_ERR_NO_TABLE; }
+    if (nspec() == 2) return box_hydro_impl<2>(lo, hi, sborder, sb_lo, sb_hi, source, sr_lo, sr_hi, fluxes_out, fo_lo3x3, fo_hi3x3, dx, dt);
+    if (nspec() == 13) return box_hydro_impl<13>(lo, hi, sborder, sb_lo, sb_hi, source, sr_lo, sr_hi, fluxes_out, fo_lo3x3, fo_hi3x3, dx, dt);
+    set_error(CASTRO_ERR_NSPEC, "castro_construct_hydro_source_box: nspec");
+    return CASTRO_ERR_NSPEC;
+}
+
 int castro_sim_launches_per_step(const castro_sim* s) { return s->launches; }
+
+void* castro_sim_stream(castro_sim* s) { return (void*)s->st; }
+
+int castro_sim_profile_step(castro_sim* s, double* ms, const char** names)
+{
+    if (s->mode != CASTRO_MODE_BATCHED) { set_error(CASTRO_ERR_ARG, "castro_sim_profile_step: batched mode only"); return 0; }
+    static const char* kn[8] = {"front", "ghost", "trace", "riemann1", "riemann2", "riemann3", "update", "dt"};
+    cudaEvent_t ev[9];
+    for (int k = 0; k < 9; ++k) cudaEventCreate(&ev[k]);
+    if (!s->dt_ready) {
+        if (s->ns == 2) initial_dt_kernels<2>(s); else initial_dt_kernels<13>(s);
+        s->dt_ready = true;
+    }
+    SimDev S = s->dev();
+    cudaStream_t st = s->st;
+    cudaEventRecord(ev[0], st);
+    for (int k = 0; k < 8; ++k) {
+        if (s->ns == 2) profile_kernel<2>(s, S, k); else profile_kernel<13>(s, S, k);
+        cudaEventRecord(ev[k + 1], st);
+    }
+    cudaEventSynchronize(ev[8]);
+    for (int k = 0; k < 8; ++k) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+        ms[k] = t;
+        names[k] = kn[k];
+    }
+    for (int k = 0; k < 9; ++k) cudaEventDestroy(ev[k]);
+    check_launch("castro_sim_profile_step");
+    return 8;
+}
 
 long long castro_sim_eos_failures(castro_sim* s)
 {

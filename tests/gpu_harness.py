@@ -1,0 +1,88 @@
+"""Helpers of the GPU parity tests: oracle <-> device array transfer and the
+comparison criteria.
+
+Tolerances (FP64):
+* exact build (-DCASTRO_EXACT --fmad=false): bit-for-bit equality with the oracle;
+* production build: per component, max |gpu - oracle| / max(|oracle|, FLOOR * scale_c)
+  <= RTOL_STEP after one step, where scale_c is the component's largest
+  magnitude in the array (this keeps zones whose value is round-off noise around
+  zero -- e.g. momentum far from the blast -- from dominating), and relative L1
+  per component <= RTOL_L1 after a full run.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+RTOL_KERNEL = 1e-12   # one routine on identical inputs
+RTOL_STEP = 1e-12     # state after one coarse step
+RTOL_L1 = 1e-9        # relative L1 after a full run
+FLOOR = 1e-3
+
+
+def to_dev(a: np.ndarray) -> torch.Tensor:
+    """Fortran-order (nx,ny,nz,nc) numpy array -> device buffer with the same memory layout."""
+    if a.ndim == 3:
+        a = a[..., None]
+    return torch.from_numpy(np.ascontiguousarray(a.transpose(3, 2, 1, 0))).cuda()
+
+
+def from_dev(t: torch.Tensor) -> np.ndarray:
+    return t.cpu().numpy().transpose(3, 2, 1, 0)
+
+
+def nan_dev(lo, hi, nc) -> torch.Tensor:
+    shape = (nc,) + tuple(h - l + 1 for l, h in reversed(list(zip(lo, hi))))
+    return torch.full(shape, float("nan"), dtype=torch.float64, device="cuda")
+
+
+def scaled_err(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Per component: max over zones of |a-b| / max(|b|, FLOOR * max|b|); NaNs must coincide."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if a.ndim == 3:
+        a, b = a[..., None], b[..., None]
+    na, nb = np.isnan(a), np.isnan(b)
+    assert np.array_equal(na, nb), "NaN pattern differs (a value the reference never writes was produced or read)"
+    nc = a.shape[-1]
+    out = np.zeros(nc)
+    for c in range(nc):
+        ac, bc = a[..., c], b[..., c]
+        m = ~np.isnan(bc)
+        if not m.any():
+            continue
+        scale = np.abs(bc[m]).max()
+        if scale == 0:
+            out[c] = np.abs(ac[m]).max()
+            continue
+        den = np.maximum(np.abs(bc[m]), FLOOR * scale)
+        out[c] = (np.abs(ac[m] - bc[m]) / den).max()
+    return out
+
+
+def assert_match(gpu: np.ndarray, ref: np.ndarray, exact: bool, rtol: float = RTOL_KERNEL, what: str = ""):
+    if exact:
+        np.testing.assert_array_equal(gpu, ref, err_msg=f"{what}: exact build must match the oracle bit for bit")
+    else:
+        e = scaled_err(gpu, ref)
+        assert (e <= rtol).all(), f"{what}: scaled error {e.max():.3e} > {rtol:g} (per component {e})"
+
+
+def rel_l1(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    nc = a.shape[-1]
+    A, B = a.reshape(-1, nc), b.reshape(-1, nc)
+    num = np.abs(A - B).sum(0)
+    den = np.abs(B).sum(0)
+    return np.where(den > 0, num / np.where(den > 0, den, 1), num)
+
+
+def sborder_from_domain(G: np.ndarray, dom_lo, lo, hi, bc: int, ng: int = 4) -> np.ndarray:
+    """FillPatch of one box's Sborder (grow(box, ng)) from a domain array:
+    periodic wrap (bc 0) or zero-gradient copy of the nearest zone (bc 1)."""
+    idx = []
+    for d in range(3):
+        n = G.shape[d]
+        r = np.arange(lo[d] - ng, hi[d] + ng + 1) - dom_lo[d]
+        r = np.mod(r, n) if bc == 0 else np.clip(r, 0, n - 1)
+        idx.append(r)
+    return np.asfortranarray(G[np.ix_(idx[0], idx[1], idx[2])])
