@@ -145,7 +145,7 @@ def run_b200(args, pkg, rank, world):
     import numpy as np
     import torch
 
-    cfg = pkg.configs.WORKLOADS[args.workload]()
+    cfg = pkg.configs.WORKLOADS[args.workload](scale=args.scale)
     A, Z = cfg["network"]
     nspec = len(A)
     table = pkg.helm_table.ensure_table()
@@ -250,7 +250,8 @@ def run_b200(args, pkg, rank, world):
         "dtype": "f64",
         "data": "synthetic: Sedov blast, seeded Gaussian density perturbation (numpy PCG64), generated Helmholtz table",
         "config": {"workload": f"{args.workload}: 128^3 zones in 64 boxes of 32^3, 2 species, outflow, "
-                               "rho=1*(1+1e-3 g), T=1e6 K, E=1e50 erg in r=4 zones, CFL 0.5, 50 coarse steps",
+                               "rho=1*(1+1e-3 g), T=1e6 K, E=1e50 erg in r=4 zones, CFL 0.5, 50 coarse steps"
+                               + (f" (zone counts divided by {args.scale})" if args.scale > 1 else ""),
                    "zones": zones, "boxes": sum(len(i["boxes"]) for i in cfg["instances"]),
                    "path": "batched fused kernels, one CUDA graph per step",
                    "l2": "no flush: state 151 MB plus ~3.6 GB of per-step intermediates exceed the 126 MB L2",
@@ -342,6 +343,7 @@ def main():
     ap.add_argument("--workload", default="sedov128_pert")
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scale", type=int, default=1, help="divide the workload's zone counts (profiling runs only)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -145,33 +145,40 @@ void estdt_impl(const int* lo, const int* hi, Fab U, const double* dx, double* d
     check_launch("estdt");
 }
 
-template <int NS>
-void trace_impl(const int* lo, const int* hi, const int* vlo, const int* vhi, int idir,
-                Fab Q, Fab QA, Fab QM, Fab QP, double dtdx)
+template <int NS, int D>
+void trace_dir(const int* lo, const int* hi, int vl, int vh, FabLoader ld, Fab QM, Fab QP, double dtdx)
 {
-    const int vl = vlo[idir], vh = vhi[idir];
-    FabLoader ld{Q, QA};
     launch_box("trace_ppm", lo, hi, [=] __device__(int i, int j, int k) {
         double flatn = uflatten(ld, i, j, k);
         double qplus[Dims<NS>::NQS], qminus[Dims<NS>::NQS];
-        trace_zone<NS>(ld, i, j, k, idir, dtdx, flatn, qplus, qminus);
-        int idx = idir == 0 ? i : idir == 1 ? j : k;
+        trace_zone<NS, D>(ld, i, j, k, dtdx, flatn, qplus, qminus);
+        int idx = D == 0 ? i : D == 1 ? j : k;
         if (idx >= vl) store_state<NS>(QP, i, j, k, qplus);
-        if (idx <= vh) store_state<NS>(QM, i + (idir == 0), j + (idir == 1), k + (idir == 2), qminus);
+        if (idx <= vh) store_state<NS>(QM, i + (D == 0), j + (D == 1), k + (D == 2), qminus);
     });
 }
 
 template <int NS>
-void compute_flux_impl(const int* lo, const int* hi, Fab QL, Fab QR, Fab FX, Fab QI, Fab QG, Fab QA, int idir)
+void trace_impl(const int* lo, const int* hi, const int* vlo, const int* vhi, int idir,
+                Fab Q, Fab QA, Fab QM, Fab QP, double dtdx)
+{
+    FabLoader ld{Q, QA};
+    if (idir == 0) trace_dir<NS, 0>(lo, hi, vlo[0], vhi[0], ld, QM, QP, dtdx);
+    else if (idir == 1) trace_dir<NS, 1>(lo, hi, vlo[1], vhi[1], ld, QM, QP, dtdx);
+    else trace_dir<NS, 2>(lo, hi, vlo[2], vhi[2], ld, QM, QP, dtdx);
+}
+
+template <int NS, int D>
+void compute_flux_dir(const int* lo, const int* hi, Fab QL, Fab QR, Fab FX, Fab QI, Fab QG, Fab QA)
 {
     launch_box("compute_flux", lo, hi, [=] __device__(int i, int j, int k) {
         constexpr int NQS = Dims<NS>::NQS, NVAR = Dims<NS>::NVAR, QVAR = Dims<NS>::QVAR;
         double ql[NQS], qr[NQS], flx[NVAR], qg[NGDNV], qint[QVAR];
         load_state<NS>(QL, i, j, k, ql);
         load_state<NS>(QR, i, j, k, qr);
-        const int ex = idir == 0, ey = idir == 1, ez = idir == 2;
-        riemann_cgf<NS>(ql, qr, QA(i - ex, j - ey, k - ez, QGAMC), QA(i, j, k, QGAMC),
-                        QA(i - ex, j - ey, k - ez, QC), QA(i, j, k, QC), idir, flx, qg, qint);
+        constexpr int ex = D == 0, ey = D == 1, ez = D == 2;
+        riemann_cgf<NS, D>(ql, qr, QA(i - ex, j - ey, k - ez, QGAMC), QA(i, j, k, QGAMC),
+                           QA(i - ex, j - ey, k - ez, QC), QA(i, j, k, QC), flx, qg, qint);
 #pragma unroll
         for (int n = 0; n < NVAR; ++n) FX(i, j, k, n) = flx[n];
 #pragma unroll
@@ -180,6 +187,14 @@ void compute_flux_impl(const int* lo, const int* hi, Fab QL, Fab QR, Fab FX, Fab
         for (int n = 0; n < QVAR; ++n)
             if (n != QTEMP) QI(i, j, k, n) = qint[n];
     });
+}
+
+template <int NS>
+void compute_flux_impl(const int* lo, const int* hi, Fab QL, Fab QR, Fab FX, Fab QI, Fab QG, Fab QA, int idir)
+{
+    if (idir == 0) compute_flux_dir<NS, 0>(lo, hi, QL, QR, FX, QI, QG, QA);
+    else if (idir == 1) compute_flux_dir<NS, 1>(lo, hi, QL, QR, FX, QI, QG, QA);
+    else compute_flux_dir<NS, 2>(lo, hi, QL, QR, FX, QI, QG, QA);
 }
 
 template <int NS>

@@ -702,23 +702,22 @@ __device__ __forceinline__ void trace_project(const double I[3][4], double gam_g
     p_o = DMAX(small_pres, p_ref + (alphap + alpham) * csq_ref);
 }
 
-// trace_ppm for one zone and one direction (Source/ppm.F90:437-737): the plus
-// state on face i (left face of the zone) and the minus state on face i+1,
-// in compact face-state layout.
-template <int NS, class L>
-__device__ __forceinline__ void trace_zone(const L& ld, int i, int j, int k, int idir, double dtdx, double flatn,
+// trace_ppm for one zone and one direction D (Source/ppm.F90:437-737): the
+// plus state on face i (left face of the zone) and the minus state on face
+// i+1, in compact face-state layout.  flatn is uflatten of the zone.
+template <int NS, int D, class L>
+__device__ __forceinline__ void trace_zone(const L& ld, int i, int j, int k, double dtdx, double flatn,
                                            double* qplus, double* qminus)
 {
-    const int ex = idir == 0, ey = idir == 1, ez = idir == 2;
-    const int qun = QU + idir;
-    const int qut = QU + (idir == 0 ? 1 : idir == 1 ? 2 : 0);
-    const int qutt = QU + (idir == 0 ? 2 : idir == 1 ? 0 : 1);
+    constexpr int ex = D == 0, ey = D == 1, ez = D == 2;
+    constexpr int qun = QU + D;
+    constexpr int qut = QU + (D == 0 ? 1 : D == 1 ? 2 : 0);
+    constexpr int qutt = QU + (D == 0 ? 2 : D == 1 ? 0 : 1);
     double cc = ld.c(i, j, k);
     double un = ld.q(i, j, k, qun);
-    // reconstructed thermodynamic and velocity variables: rho, un, p, rhoe
-    // feed the projection; the transverse velocities only need wave 2.
+    // rho, un, p, rhoe feed the characteristic projection
     double Ip[3][4], Im[3][4];
-    const int vars[4] = {QRHO, qun, QPRES, QREINT};
+    constexpr int vars[4] = {QRHO, qun, QPRES, QREINT};
     double s[5], sm, sp;
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
@@ -730,6 +729,7 @@ __device__ __forceinline__ void trace_zone(const L& ld, int i, int j, int k, int
         ppm_int_wave(sm, sp, s6, un, dtdx, Ip[1][v], Im[1][v]);
         ppm_int_wave(sm, sp, s6, un + cc, dtdx, Ip[2][v], Im[2][v]);
     }
+    // transverse velocities: only the u wave
     double Ipt, Imt, Iptt, Imtt;
     {
 #pragma unroll
@@ -743,7 +743,8 @@ __device__ __forceinline__ void trace_zone(const L& ld, int i, int j, int k, int
         s6 = 6.0 * s[2] - 3.0 * (sm + sp);
         ppm_int_wave(sm, sp, s6, un, dtdx, Iptt, Imtt);
     }
-    double gp0, gm0, gp2, gm2;   // gamc integrals of waves u-c (0) and u+c (2)
+    // gamma_c: waves u-c (plus state) and u+c (minus state)
+    double gp0, gm0, gp2, gm2;
     {
 #pragma unroll
         for (int m = -2; m <= 2; ++m) s[m + 2] = ld.gamc(i + m * ex, j + m * ey, k + m * ez);
@@ -763,23 +764,21 @@ __device__ __forceinline__ void trace_zone(const L& ld, int i, int j, int k, int
         qplus[SX + n] = imx;
         qminus[SX + n] = ipx;
     }
-    // plus state on face i: projection of the Im integrals
     {
         double r, u, re, p;
         trace_project(Im, gm0, un, cc, true, r, u, re, p);
         qplus[SRHO] = r;
-        qplus[SU + idir] = u;
+        qplus[SU + D] = u;
         qplus[SREI] = re;
         qplus[SPRES] = p;
         qplus[qut - QU + SU] = Imt;
         qplus[qutt - QU + SU] = Imtt;
     }
-    // minus state on face i+1: projection of the Ip integrals
     {
         double r, u, re, p;
         trace_project(Ip, gp2, un, cc, false, r, u, re, p);
         qminus[SRHO] = r;
-        qminus[SU + idir] = u;
+        qminus[SU + D] = u;
         qminus[SREI] = re;
         qminus[SPRES] = p;
         qminus[qut - QU + SU] = Ipt;
@@ -790,20 +789,20 @@ __device__ __forceinline__ void trace_zone(const L& ld, int i, int j, int k, int
 // ---------------------------------------------------------------------------
 // CGF Riemann solver on one face, Source/riemann.F90:114-325
 // ---------------------------------------------------------------------------
-// ql/qr: compact face states; gamcl/cl of the left zone, gamcr/cr of the
-// right zone.  Outputs: flx (NVAR, conserved order), qg (NGDNV) and, when
+// D is the direction normal to the face.  ql/qr: compact face states;
+// gamcl/cl of the left zone, gamcr/cr of the right zone.  Outputs: flx (NVAR, conserved order), qg (NGDNV) and, when
 // qint is non-null, the interface state in full QVAR numbering (QRHO, velocities,
 // QPRES, QGAME, QREINT, species).
-template <int NS>
+template <int NS, int D>
 __device__ __forceinline__ void riemann_cgf(const double* ql, const double* qr, double gamcl, double gamcr,
-                                            double cl, double cr, int idir, double* flx, double* qg, double* qint)
+                                            double cl, double cr, double* flx, double* qg, double* qint)
 {
-    const int iu = SU + idir;
-    const int iv1 = SU + (idir == 0 ? 1 : 0);
-    const int iv2 = SU + (idir == 2 ? 1 : 2);
-    const int im1 = UMX + idir;
-    const int im2 = UMX + (idir == 0 ? 1 : 0);
-    const int im3 = UMX + (idir == 2 ? 1 : 2);
+    constexpr int iu = SU + D;
+    constexpr int iv1 = SU + (D == 0 ? 1 : 0);
+    constexpr int iv2 = SU + (D == 2 ? 1 : 2);
+    constexpr int im1 = UMX + D;
+    constexpr int im2 = UMX + (D == 0 ? 1 : 0);
+    constexpr int im3 = UMX + (D == 2 ? 1 : 2);
 
     double rl = DMAX(ql[SRHO], small_dens);
     double ul = ql[iu], v1l = ql[iv1], v2l = ql[iv2];
@@ -872,7 +871,7 @@ __device__ __forceinline__ void riemann_cgf(const double* ql, const double* qr, 
     qp = DMAX(qp, small_pres);
 
     double vel[3];
-    vel[idir] = qu;
+    vel[D] = qu;
     vel[iv1 - SU] = qv1;
     vel[iv2 - SU] = qv2;
     qg[GDRHO] = qrho;

@@ -284,63 +284,95 @@ __global__ void __launch_bounds__(BLOCK) k_ghost(SimDev S, const Work* wl)
     }
 }
 
-// trace: flattening once per zone, the three directional traces, divu
+// prep: divu at the nodes of grow(bx,1) (Castro_hydro_nd.F90:45-63) and the
+// flattening coefficient of every zone of grow(bx,1) (ppm.F90:11-128), which
+// trace_ppm recomputes per direction in the reference and is formed once here
 template <int NS>
-__global__ void __launch_bounds__(BLOCK) k_trace(SimDev S, const Work* wl)
+__global__ void __launch_bounds__(BLOCK) k_prep(SimDev S, const Work* wl)
 {
     int b, sub, i, j, k;
     Reg R;
     if (!work_point(wl, S, R_G1, -1, b, sub, R, i, j, k)) return;
     const BoxDev& B = S.boxes[b];
     const InstDev& I = S.inst[B.inst];
+    QLoader<NS> ld;
+    ld.base = S.Q + B.offQ;
+    ld.R = make_reg(B.lo, B.hi, R_G4, 0);
+    double dxinv = 1.0 / I.dx[0], dyinv = 1.0 / I.dx[1], dzinv = 1.0 / I.dx[2];
+    auto Qv = [&](int a, int bq, int c, int n) { return ld.at(a, bq, c, QF<NS>::U + n); };
+    double ux = 0.25 * (+Qv(i, j, k, 0) - Qv(i - 1, j, k, 0)
+                        + Qv(i, j, k - 1, 0) - Qv(i - 1, j, k - 1, 0)
+                        + Qv(i, j - 1, k, 0) - Qv(i - 1, j - 1, k, 0)
+                        + Qv(i, j - 1, k - 1, 0) - Qv(i - 1, j - 1, k - 1, 0)) * dxinv;
+    double vy = 0.25 * (+Qv(i, j, k, 1) - Qv(i, j - 1, k, 1)
+                        + Qv(i, j, k - 1, 1) - Qv(i, j - 1, k - 1, 1)
+                        + Qv(i - 1, j, k, 1) - Qv(i - 1, j - 1, k, 1)
+                        + Qv(i - 1, j, k - 1, 1) - Qv(i - 1, j - 1, k - 1, 1)) * dyinv;
+    double wz = 0.25 * (+Qv(i, j, k, 2) - Qv(i, j, k - 1, 2)
+                        + Qv(i, j - 1, k, 2) - Qv(i, j - 1, k - 1, 2)
+                        + Qv(i - 1, j, k, 2) - Qv(i - 1, j, k - 1, 2)
+                        + Qv(i - 1, j - 1, k, 2) - Qv(i - 1, j - 1, k - 1, 2)) * dzinv;
+    long long id = ridx(R, i, j, k);
+    S.Div[B.offDiv + id] = ux + vy + wz;
+    S.Div[B.offDiv + id + R.np] = uflatten(ld, i, j, k);
+}
+
+template <int NS, int D>
+__device__ __forceinline__ void trace_dir(const SimDev& S, const BoxDev& B, const QLoader<NS>& ld, const Reg& R1,
+                                          int i, int j, int k, double dtdx)
+{
+    constexpr int NQS = Dims<NS>::NQS;
+    double flatn = S.Div[B.offDiv + ridx(R1, i, j, k) + R1.np];
+    double qplus[NQS], qminus[NQS];
+    trace_zone<NS, D>(ld, i, j, k, dtdx, flatn, qplus, qminus);
+    Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * D);
+    double* T = S.Tr + B.offTr[D];
+    int idx = D == 0 ? i : D == 1 ? j : k;
+    if (idx >= B.lo[D]) {
+        long long f = ridx(RT, i, j, k);
+#pragma unroll
+        for (int c = 0; c < NQS; ++c) T[f + RT.np * (NQS + c)] = qplus[c];
+    }
+    if (idx <= B.hi[D]) {
+        long long f = ridx(RT, i + (D == 0), j + (D == 1), k + (D == 2));
+#pragma unroll
+        for (int c = 0; c < NQS; ++c) T[f + RT.np * c] = qminus[c];
+    }
+}
+
+// trace: trace_ppm of one zone of grow(bx,1) in one direction (work sub = direction)
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_trace(SimDev S, const Work* wl)
+{
+    int b, d, i, j, k;
+    Reg R;
+    if (!work_point(wl, S, R_G1, -1, b, d, R, i, j, k)) return;
+    const BoxDev& B = S.boxes[b];
+    const InstDev& I = S.inst[B.inst];
     const double dt = S.st[B.inst].dt;
     QLoader<NS> ld;
     ld.base = S.Q + B.offQ;
     ld.R = make_reg(B.lo, B.hi, R_G4, 0);
-    constexpr int NQS = Dims<NS>::NQS;
+    if (d == 0) trace_dir<NS, 0>(S, B, ld, R, i, j, k, dt / I.dx[0]);
+    else if (d == 1) trace_dir<NS, 1>(S, B, ld, R, i, j, k, dt / I.dx[1]);
+    else trace_dir<NS, 2>(S, B, ld, R, i, j, k, dt / I.dx[2]);
+}
 
-    // divu at node (i,j,k), Castro_hydro_nd.F90:45-63
-    {
-        double dxinv = 1.0 / I.dx[0], dyinv = 1.0 / I.dx[1], dzinv = 1.0 / I.dx[2];
-        auto Qv = [&](int a, int bq, int c, int n) { return ld.at(a, bq, c, QF<NS>::U + n); };
-        double ux = 0.25 * (+Qv(i, j, k, 0) - Qv(i - 1, j, k, 0)
-                            + Qv(i, j, k - 1, 0) - Qv(i - 1, j, k - 1, 0)
-                            + Qv(i, j - 1, k, 0) - Qv(i - 1, j - 1, k, 0)
-                            + Qv(i, j - 1, k - 1, 0) - Qv(i - 1, j - 1, k - 1, 0)) * dxinv;
-        double vy = 0.25 * (+Qv(i, j, k, 1) - Qv(i, j - 1, k, 1)
-                            + Qv(i, j, k - 1, 1) - Qv(i, j - 1, k - 1, 1)
-                            + Qv(i - 1, j, k, 1) - Qv(i - 1, j - 1, k, 1)
-                            + Qv(i - 1, j, k - 1, 1) - Qv(i - 1, j - 1, k - 1, 1)) * dyinv;
-        double wz = 0.25 * (+Qv(i, j, k, 2) - Qv(i, j, k - 1, 2)
-                            + Qv(i, j - 1, k, 2) - Qv(i, j - 1, k - 1, 2)
-                            + Qv(i - 1, j, k, 2) - Qv(i - 1, j, k - 1, 2)
-                            + Qv(i - 1, j - 1, k, 2) - Qv(i - 1, j - 1, k - 1, 2)) * dzinv;
-        S.Div[B.offDiv + ridx(R, i, j, k)] = ux + vy + wz;
-    }
-
-    double flatn = uflatten(ld, i, j, k);
-#pragma unroll 1
-    for (int d = 0; d < 3; ++d) {
-        double qplus[NQS], qminus[NQS];
-        trace_zone<NS>(ld, i, j, k, d, dt / I.dx[d], flatn, qplus, qminus);
-        Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * d);
-        double* T = S.Tr + B.offTr[d];
-        int idx = d == 0 ? i : d == 1 ? j : k;
-        if (idx >= B.lo[d]) {
-            long long f = ridx(RT, i, j, k);
-#pragma unroll
-            for (int c = 0; c < NQS; ++c) T[f + RT.np * (NQS + c)] = qplus[c];
-        }
-        if (idx <= B.hi[d]) {
-            long long f = ridx(RT, i + (d == 0), j + (d == 1), k + (d == 2));
-#pragma unroll
-            for (int c = 0; c < NQS; ++c) T[f + RT.np * c] = qminus[c];
-        }
-    }
+// compute_flux on the face (i,j,k) normal to D: left zone i-e_D, right zone i
+// returns (GDPRES, Godunov velocity normal to the face)
+template <int NS, int D>
+__device__ __forceinline__ double2 riemann_at(const QLoader<NS>& ld, int i, int j, int k, const double* ql,
+                                              const double* qr, double* flx)
+{
+    constexpr int ex = D == 0, ey = D == 1, ez = D == 2;
+    double qg[NGDNV];
+    riemann_cgf<NS, D>(ql, qr, ld.gamc(i - ex, j - ey, k - ez), ld.gamc(i, j, k), ld.c(i - ex, j - ey, k - ez),
+                       ld.c(i, j, k), flx, qg, nullptr);
+    return make_double2(qg[GDPRES], qg[GDU + D]);
 }
 
 template <int NS>
-__device__ __forceinline__ void store_tf(double* base, const Reg& R, long long f, const double* flx, const double* qg, int normal)
+__device__ __forceinline__ void store_tf(double* base, const Reg& R, long long f, const double* flx, double pg, double ug)
 {
     using T = TF<NS>;
     base[f + R.np * T::RHO] = flx[URHO];
@@ -350,8 +382,8 @@ __device__ __forceinline__ void store_tf(double* base, const Reg& R, long long f
     base[f + R.np * T::ED] = flx[UEDEN];
 #pragma unroll
     for (int n = 0; n < NS; ++n) base[f + R.np * (T::X + n)] = flx[UFS + n];
-    base[f + R.np * T::PG] = qg[GDPRES];
-    base[f + R.np * T::UG] = qg[GDU + normal];
+    base[f + R.np * T::PG] = pg;
+    base[f + R.np * T::UG] = ug;
 }
 
 template <int NS>
@@ -378,11 +410,12 @@ __global__ void __launch_bounds__(BLOCK) k_riemann1(SimDev S, const Work* wl)
     QLoader<NS> ld;
     ld.base = S.Q + B.offQ;
     ld.R = make_reg(B.lo, B.hi, R_G4, 0);
-    const int ex = d == 0, ey = d == 1, ez = d == 2;
-    double flx[NVAR], qg[NGDNV];
-    riemann_cgf<NS>(ql, qr, ld.gamc(i - ex, j - ey, k - ez), ld.gamc(i, j, k), ld.c(i - ex, j - ey, k - ez),
-                    ld.c(i, j, k), d, flx, qg, nullptr);
-    store_tf<NS>(S.F1 + B.offF1[d], R, f, flx, qg, d);
+    double flx[NVAR];
+    double2 g;
+    if (d == 0) g = riemann_at<NS, 0>(ld, i, j, k, ql, qr, flx);
+    else if (d == 1) g = riemann_at<NS, 1>(ld, i, j, k, ql, qr, flx);
+    else g = riemann_at<NS, 2>(ld, i, j, k, ql, qr, flx);
+    store_tf<NS>(S.F1 + B.offF1[d], R, f, flx, g.x, g.y);
 }
 
 // riemann2: trans1 of the a-normal states with the b fluxes, then
@@ -422,10 +455,12 @@ __global__ void __launch_bounds__(BLOCK) k_riemann2(SimDev S, const Work* wl)
         load_tf<NS>(F, RF, ridx(RF, il, jl, kl), fl);
         trans1_state<NS>(lq, fr, fl, ld.gamc(il, jl, kl), cdtdx, st2[D + 1]);
     }
-    double flx[NVAR], qg[NGDNV];
-    riemann_cgf<NS>(st2[0], st2[1], ld.gamc(i - eax, j - eay, k - eaz), ld.gamc(i, j, k),
-                    ld.c(i - eax, j - eay, k - eaz), ld.c(i, j, k), a, flx, qg, nullptr);
-    store_tf<NS>(S.F2 + B.offF2[p], R, ridx(R, i, j, k), flx, qg, a);
+    double flx[NVAR];
+    double2 g;
+    if (a == 0) g = riemann_at<NS, 0>(ld, i, j, k, st2[0], st2[1], flx);
+    else if (a == 1) g = riemann_at<NS, 1>(ld, i, j, k, st2[0], st2[1], flx);
+    else g = riemann_at<NS, 2>(ld, i, j, k, st2[0], st2[1], flx);
+    store_tf<NS>(S.F2 + B.offF2[p], R, ridx(R, i, j, k), flx, g.x, g.y);
 }
 
 // riemann3: trans2 + compute_flux + apply_av + normalize_species_fluxes on ebx[d]
@@ -471,9 +506,11 @@ __global__ void __launch_bounds__(BLOCK) k_riemann3(SimDev S, const Work* wl)
         load_tf<NS>(F21, R21, ridx(R21, il, jl, kl), f3l);
         trans2_state<NS>(lq, f2r, f2l, f3r, f3l, ld.gamc(il, jl, kl), hdt1, hdt2, st2[D + 1]);
     }
-    double flx[NVAR], qg[NGDNV];
-    riemann_cgf<NS>(st2[0], st2[1], ld.gamc(i - ex, j - ey, k - ez), ld.gamc(i, j, k),
-                    ld.c(i - ex, j - ey, k - ez), ld.c(i, j, k), d, flx, qg, nullptr);
+    double flx[NVAR];
+    double2 g;
+    if (d == 0) g = riemann_at<NS, 0>(ld, i, j, k, st2[0], st2[1], flx);
+    else if (d == 1) g = riemann_at<NS, 1>(ld, i, j, k, st2[0], st2[1], flx);
+    else g = riemann_at<NS, 2>(ld, i, j, k, st2[0], st2[1], flx);
 
     // apply_av, Castro_hydro_nd.F90:207-237 (the x and y four-node sums as written there)
     {
@@ -511,8 +548,8 @@ __global__ void __launch_bounds__(BLOCK) k_riemann3(SimDev S, const Work* wl)
         if (n == UTEMP) continue;
         X[f + R.np * (n < UTEMP ? n : n - 1)] = flx[n];
     }
-    X[f + R.np * (NVAR - 1)] = qg[GDPRES];
-    X[f + R.np * NVAR] = qg[GDU + d];
+    X[f + R.np * (NVAR - 1)] = g.x;
+    X[f + R.np * NVAR] = g.y;
 }
 
 // update: fill_hydro_source, Saxpy, clean_state (advance), clean_state
@@ -793,8 +830,9 @@ struct castro_sim {
     double *Tr = nullptr, *F1 = nullptr, *F2 = nullptr, *Fx = nullptr;
     long long nU = 0;
     // work lists
-    Work *w_valid = nullptr, *w_g4 = nullptr, *w_g1 = nullptr, *w_tbx = nullptr, *w_pair = nullptr, *w_ebx = nullptr;
-    int n_valid = 0, n_g4 = 0, n_g1 = 0, n_tbx = 0, n_pair = 0, n_ebx = 0;
+    Work *w_valid = nullptr, *w_g4 = nullptr, *w_g1 = nullptr, *w_g1x3 = nullptr, *w_tbx = nullptr, *w_pair = nullptr,
+         *w_ebx = nullptr;
+    int n_valid = 0, n_g4 = 0, n_g1 = 0, n_g1x3 = 0, n_tbx = 0, n_pair = 0, n_ebx = 0;
     bool dt_ready = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -878,7 +916,8 @@ void batched_step_kernels(castro_sim* s)
     cudaStream_t st = s->st;
     k_front<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid);
     k_ghost<NS><<<s->n_g4, BLOCK, 0, st>>>(S, s->w_g4);
-    k_trace<NS><<<s->n_g1, BLOCK, 0, st>>>(S, s->w_g1);
+    k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(S, s->w_g1);
+    k_trace<NS><<<s->n_g1x3, BLOCK, 0, st>>>(S, s->w_g1x3);
     k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(S, s->w_tbx);
     k_riemann2<NS><<<s->n_pair, BLOCK, 0, st>>>(S, s->w_pair);
     k_riemann3<NS><<<s->n_ebx, BLOCK, 0, st>>>(S, s->w_ebx);
@@ -893,11 +932,12 @@ void profile_kernel(castro_sim* s, const SimDev& S, int k)
     switch (k) {
     case 0: k_front<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid); break;
     case 1: k_ghost<NS><<<s->n_g4, BLOCK, 0, st>>>(S, s->w_g4); break;
-    case 2: k_trace<NS><<<s->n_g1, BLOCK, 0, st>>>(S, s->w_g1); break;
-    case 3: k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(S, s->w_tbx); break;
-    case 4: k_riemann2<NS><<<s->n_pair, BLOCK, 0, st>>>(S, s->w_pair); break;
-    case 5: k_riemann3<NS><<<s->n_ebx, BLOCK, 0, st>>>(S, s->w_ebx); break;
-    case 6: k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid); break;
+    case 2: k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(S, s->w_g1); break;
+    case 3: k_trace<NS><<<s->n_g1x3, BLOCK, 0, st>>>(S, s->w_g1x3); break;
+    case 4: k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(S, s->w_tbx); break;
+    case 5: k_riemann2<NS><<<s->n_pair, BLOCK, 0, st>>>(S, s->w_pair); break;
+    case 6: k_riemann3<NS><<<s->n_ebx, BLOCK, 0, st>>>(S, s->w_ebx); break;
+    case 7: k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid); break;
     default: k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0); break;
     }
 }
@@ -1148,7 +1188,7 @@ int step_impl(castro_sim* s)
         if (!cuda_ok(cudaGraphInstantiate(&s->gexec, s->graph, 0), "graph instantiate")) return castro_last_error();
     }
     cuda_ok(cudaGraphLaunch(s->gexec, s->st), "graph launch");
-    s->launches = 8;
+    s->launches = 9;
     return castro_last_error();
 }
 
@@ -1210,7 +1250,7 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
             B.offU = oU; oU += npts_reg(B.lo, B.hi, R_VALID, 0) * NV;
             B.offUb = oUb; oUb += npts_reg(B.lo, B.hi, R_G1, 0) * NV;
             B.offQ = oQ; oQ += npts_reg(B.lo, B.hi, R_G4, 0) * NQF;
-            B.offDiv = oDiv; oDiv += npts_reg(B.lo, B.hi, R_G1, 0);
+            B.offDiv = oDiv; oDiv += npts_reg(B.lo, B.hi, R_G1, 0) * 2;   // divu, flatn
             for (int d = 0; d < 3; ++d) {
                 B.offTr[d] = oTr; oTr += npts_reg(B.lo, B.hi, R_TBX, 4 * d) * 2 * NQS;
                 B.offF1[d] = oF1; oF1 += npts_reg(B.lo, B.hi, R_TBX, 4 * d) * NTF;
@@ -1258,6 +1298,7 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
         build_work(s, R_VALID, 1, -1, &s->w_valid, &s->n_valid);
         build_work(s, R_G4, 1, -1, &s->w_g4, &s->n_g4);
         build_work(s, R_G1, 1, -1, &s->w_g1, &s->n_g1);
+        build_work(s, R_G1, 3, -1, &s->w_g1x3, &s->n_g1x3);
         build_work(s, R_TBX, 3, 0, &s->w_tbx, &s->n_tbx);
         build_work(s, R_TBX, 6, 1, &s->w_pair, &s->n_pair);
         build_work(s, R_EBX, 3, -1, &s->w_ebx, &s->n_ebx);
@@ -1289,7 +1330,7 @@ void castro_sim_destroy(castro_sim* s)
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     if (s->graph) cudaGraphDestroy(s->graph);
     void* ptrs[] = {s->dboxes, s->dinst, s->dstate, s->downer, s->U, s->Ub, s->Q, s->Div, s->Tr, s->F1, s->F2, s->Fx,
-                    s->w_valid, s->w_g4, s->w_g1, s->w_tbx, s->w_pair, s->w_ebx, s->sb, s->src, s->scratch,
+                    s->w_valid, s->w_g4, s->w_g1, s->w_g1x3, s->w_tbx, s->w_pair, s->w_ebx, s->sb, s->src, s->scratch,
                     s->d_dtloc, s->d_dtbox};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1493,7 +1534,8 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
     cuda_ok(cudaMemcpyAsync(s->dstate, &st, sizeof st, cudaMemcpyHostToDevice, cs), "box dt");
     SimDev S = s->dev();
     k_box_prim<NS><<<s->n_g4, BLOCK, 0, cs>>>(S, s->w_g4, make_fab(sb, sb_lo, sb_hi));
-    k_trace<NS><<<s->n_g1, BLOCK, 0, cs>>>(S, s->w_g1);
+    k_prep<NS><<<s->n_g1, BLOCK, 0, cs>>>(S, s->w_g1);
+    k_trace<NS><<<s->n_g1x3, BLOCK, 0, cs>>>(S, s->w_g1x3);
     k_riemann1<NS><<<s->n_tbx, BLOCK, 0, cs>>>(S, s->w_tbx);
     k_riemann2<NS><<<s->n_pair, BLOCK, 0, cs>>>(S, s->w_pair);
     k_riemann3<NS><<<s->n_ebx, BLOCK, 0, cs>>>(S, s->w_ebx);
@@ -1532,9 +1574,9 @@ void* castro_sim_stream(castro_sim* s) { return (void*)s->st; }
 int castro_sim_profile_step(castro_sim* s, double* ms, const char** names)
 {
     if (s->mode != CASTRO_MODE_BATCHED) { set_error(CASTRO_ERR_ARG, "castro_sim_profile_step: batched mode only"); return 0; }
-    static const char* kn[8] = {"front", "ghost", "trace", "riemann1", "riemann2", "riemann3", "update", "dt"};
-    cudaEvent_t ev[9];
-    for (int k = 0; k < 9; ++k) cudaEventCreate(&ev[k]);
+    static const char* kn[9] = {"front", "ghost", "prep", "trace", "riemann1", "riemann2", "riemann3", "update", "dt"};
+    cudaEvent_t ev[10];
+    for (int k = 0; k < 10; ++k) cudaEventCreate(&ev[k]);
     if (!s->dt_ready) {
         if (s->ns == 2) initial_dt_kernels<2>(s); else initial_dt_kernels<13>(s);
         s->dt_ready = true;
@@ -1542,20 +1584,20 @@ int castro_sim_profile_step(castro_sim* s, double* ms, const char** names)
     SimDev S = s->dev();
     cudaStream_t st = s->st;
     cudaEventRecord(ev[0], st);
-    for (int k = 0; k < 8; ++k) {
+    for (int k = 0; k < 9; ++k) {
         if (s->ns == 2) profile_kernel<2>(s, S, k); else profile_kernel<13>(s, S, k);
         cudaEventRecord(ev[k + 1], st);
     }
-    cudaEventSynchronize(ev[8]);
-    for (int k = 0; k < 8; ++k) {
+    cudaEventSynchronize(ev[9]);
+    for (int k = 0; k < 9; ++k) {
         float t = 0.f;
         cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
         ms[k] = t;
         names[k] = kn[k];
     }
-    for (int k = 0; k < 9; ++k) cudaEventDestroy(ev[k]);
+    for (int k = 0; k < 10; ++k) cudaEventDestroy(ev[k]);
     check_launch("castro_sim_profile_step");
-    return 8;
+    return 9;
 }
 
 long long castro_sim_eos_failures(castro_sim* s)
