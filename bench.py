@@ -145,7 +145,11 @@ def run_b200(args, pkg, rank, world):
     import numpy as np
     import torch
 
-    cfg = pkg.configs.WORKLOADS[args.workload](scale=args.scale)
+    if args.workload == "sedov128_pert" and args.scale > 1:
+        # fewer boxes of the same 32^3 shape, so per-zone traffic stays comparable
+        cfg = pkg.configs.sedov128_pert(scale=args.scale, max_box=32 * args.scale)
+    else:
+        cfg = pkg.configs.WORKLOADS[args.workload](scale=args.scale)
     A, Z = cfg["network"]
     nspec = len(A)
     table = pkg.helm_table.ensure_table()

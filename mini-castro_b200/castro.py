@@ -78,6 +78,10 @@ ABI_SYMBOLS = [
 
 
 def lib_path(exact: bool = False) -> str:
+    """Path of the library; CASTRO_B200_LIB / CASTRO_B200_EXACT_LIB override it."""
+    env = os.environ.get("CASTRO_B200_EXACT_LIB" if exact else "CASTRO_B200_LIB")
+    if env:
+        return env
     return os.path.join(LIBDIR, "libcastro_b200_exact.so" if exact else "libcastro_b200.so")
 
 

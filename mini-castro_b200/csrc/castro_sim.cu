@@ -46,6 +46,23 @@ namespace {
 
 constexpr int NG = 4;   // ghost zones of Sborder, Source/Castro_advance.cpp:37
 constexpr int BLOCK = 128;
+// Optional minimum resident blocks per SM for the register allocator
+// (-DCASTRO_MINB_EOS=n etc.); without them the compiler picks the register count.
+#ifdef CASTRO_MINB_EOS
+#define LB_EOS __launch_bounds__(BLOCK, CASTRO_MINB_EOS)
+#else
+#define LB_EOS __launch_bounds__(BLOCK)
+#endif
+#ifdef CASTRO_MINB_TRACE
+#define LB_TRACE __launch_bounds__(BLOCK, CASTRO_MINB_TRACE)
+#else
+#define LB_TRACE __launch_bounds__(BLOCK)
+#endif
+#ifdef CASTRO_MINB_RIEMANN
+#define LB_RIEMANN __launch_bounds__(BLOCK, CASTRO_MINB_RIEMANN)
+#else
+#define LB_RIEMANN __launch_bounds__(BLOCK)
+#endif
 
 // ordered pair (a,b), a != b -> 0..5
 __host__ __device__ __forceinline__ int pair_index(int a, int b) { return a * 2 + (b > a ? b - 1 : b); }
@@ -202,7 +219,7 @@ __device__ __forceinline__ double block_min(double m)
 
 // front: clean_state(S_old) -> S_new base; clean_state(Sborder); ctoprim
 template <int NS>
-__global__ void __launch_bounds__(BLOCK) k_front(SimDev S, const Work* wl)
+__global__ void LB_EOS k_front(SimDev S, const Work* wl)
 {
     int b, sub, i, j, k;
     Reg R;
@@ -342,7 +359,7 @@ __device__ __forceinline__ void trace_dir(const SimDev& S, const BoxDev& B, cons
 
 // trace: trace_ppm of one zone of grow(bx,1) in one direction (work sub = direction)
 template <int NS>
-__global__ void __launch_bounds__(BLOCK) k_trace(SimDev S, const Work* wl)
+__global__ void LB_TRACE k_trace(SimDev S, const Work* wl)
 {
     int b, d, i, j, k;
     Reg R;
@@ -395,7 +412,7 @@ __device__ __forceinline__ void load_tf(const double* base, const Reg& R, long l
 
 // riemann1: compute_flux on tbx[d][d] (Castro_hydro.cpp:214-224)
 template <int NS>
-__global__ void __launch_bounds__(BLOCK) k_riemann1(SimDev S, const Work* wl)
+__global__ void LB_RIEMANN k_riemann1(SimDev S, const Work* wl)
 {
     int b, d, i, j, k;
     Reg R;
@@ -421,7 +438,7 @@ __global__ void __launch_bounds__(BLOCK) k_riemann1(SimDev S, const Work* wl)
 // riemann2: trans1 of the a-normal states with the b fluxes, then
 // compute_flux -> F^{a|b} on tbx[a][b] (Castro_hydro.cpp:228-255, 280-304)
 template <int NS>
-__global__ void __launch_bounds__(BLOCK) k_riemann2(SimDev S, const Work* wl)
+__global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
 {
     int bx, p, i, j, k;
     Reg R;
@@ -466,7 +483,7 @@ __global__ void __launch_bounds__(BLOCK) k_riemann2(SimDev S, const Work* wl)
 // riemann3: trans2 + compute_flux + apply_av + normalize_species_fluxes on ebx[d]
 // (Castro_hydro.cpp:307-359)
 template <int NS>
-__global__ void __launch_bounds__(BLOCK) k_riemann3(SimDev S, const Work* wl)
+__global__ void LB_RIEMANN k_riemann3(SimDev S, const Work* wl)
 {
     int bx, d, i, j, k;
     Reg R;
@@ -555,7 +572,7 @@ __global__ void __launch_bounds__(BLOCK) k_riemann3(SimDev S, const Work* wl)
 // update: fill_hydro_source, Saxpy, clean_state (advance), clean_state
 // (post_timestep), estdt of the new state
 template <int NS>
-__global__ void __launch_bounds__(BLOCK) k_update(SimDev S, const Work* wl)
+__global__ void LB_EOS k_update(SimDev S, const Work* wl)
 {
     int b, sub, i, j, k;
     Reg R;
@@ -883,10 +900,12 @@ bool dalloc(T** p, size_t n, const char* what)
 
 void build_work(castro_sim* s, int kind, int nsub, int tbx_mode, Work** out, int* count)
 {
+    // sub-major order: every box's items of one direction (or pair) before the
+    // next, so the blocks resident on an SM run the same code path
     std::vector<Work> w;
-    for (size_t b = 0; b < s->hboxes.size(); ++b) {
-        const BoxDev& B = s->hboxes[b];
-        for (int sub = 0; sub < nsub; ++sub) {
+    for (int sub = 0; sub < nsub; ++sub) {
+        for (size_t b = 0; b < s->hboxes.size(); ++b) {
+            const BoxDev& B = s->hboxes[b];
             int rs = sub;
             if (kind == R_TBX && tbx_mode == 0) rs = 4 * sub;
             if (kind == R_TBX && tbx_mode == 1) {

@@ -184,9 +184,12 @@ IDS = [f"{c}-{'exact' if e else 'fast'}" for c, e in PARAMS]
 
 
 @pytest.fixture(params=PARAMS, ids=IDS)
-def env(request, cases, pkg, table):
+def env(request, cases, pkg, table, oracle):
     name, exact = request.param
     C = cases[name]
+    # the oracle's network is process-global: select this case's species set
+    # before any oracle call of the test (array sizes depend on it)
+    oracle.network_init(*C.network)
     L = gpu_lib(pkg, table, C.network, exact)
     return C, L, exact, pkg.castro
 
