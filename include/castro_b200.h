@@ -212,6 +212,28 @@ int castro_construct_hydro_source_box(const int* lo, const int* hi,
                                       double* const* fluxes_out, const int* fo_lo3x3, const int* fo_hi3x3,
                                       const int* domlo, const int* domhi, const double* dx, double dt);
 
+/* castro_construct_hydro_source_box without any device allocation.  No
+ * counterpart in the reference.  For callers that cannot allocate device
+ * memory while they advance a box: hosts that give out all device memory from
+ * their own pool reserved at start-up, and hosts that must not call cudaMalloc
+ * inside the time step because it synchronizes the device.  Same arguments,
+ * meaning and result as castro_construct_hydro_source_box; its scratch lives in
+ * one static device array of 18 MiB inside the library (held by every GPU that
+ * loads the library until the process exits), which fits a box of at most
+ * 16^3 zones with 13 species or 21^3 zones with 2 species; larger boxes are
+ * rejected with CASTRO_ERR_ARG before anything is launched.  The first call
+ * on each device looks up the array's device address (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  Every call shares the
+ * array and overwrites it: calls that overlap on the GPU (two streams, two
+ * host threads) race and must be serialized by the caller.  Kernels launch on
+ * the library stream (castro_set_stream); allocates neither device nor host
+ * memory on its success path. */
+int castro_construct_hydro_source_box_noalloc(const int* lo, const int* hi,
+                                              const double* sborder, const int* sb_lo, const int* sb_hi,
+                                              double* source, const int* sr_lo, const int* sr_hi,
+                                              double* const* fluxes_out, const int* fo_lo3x3, const int* fo_hi3x3,
+                                              const int* domlo, const int* domhi, const double* dx, double dt);
+
 /* ------------------------------------------------------------------------- */
 /* Simulation driver: one level per instance, many instances per sim          */
 /* ------------------------------------------------------------------------- */

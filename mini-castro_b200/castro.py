@@ -74,6 +74,7 @@ ABI_SYMBOLS = [
     "castro_sim_sync", "castro_sim_time", "castro_sim_dt", "castro_sim_steps", "castro_sim_est_time_step",
     "castro_sim_blast_radius", "castro_sim_launches_per_step", "castro_sim_eos_failures", "castro_main",
     "castro_sim_stream", "castro_sim_profile_step", "castro_measure_fp64_tflops",
+    "castro_construct_hydro_source_box_noalloc",
 ]
 
 

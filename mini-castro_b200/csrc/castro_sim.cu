@@ -1571,6 +1571,192 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
     return castro_last_error();
 }
 
+// ---------------------------------------------------------------------------
+// castro_construct_hydro_source_box_noalloc: the same fused per-box hydro
+// source, with every scratch array carved out of one file-scope device array
+// instead of device memory the library allocates.  For callers that cannot
+// allocate device memory while they advance a box: hosts that hand out all
+// device memory from their own preallocated pool (an AMReX-style arena sized
+// at start-up), and hosts that must not call cudaMalloc from inside the time
+// step because it synchronizes the device.
+// ---------------------------------------------------------------------------
+namespace castro {
+namespace {
+
+// 18 MiB: a box of up to 16^3 zones with 13 species, or up to 21^3 zones with
+// 2 species, including the box / work-list records at its head.
+constexpr long long NOALLOC_DOUBLES = 2359296;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+constexpr long long NOALLOC_META_BYTES = 65536;   // BoxDev, InstDev, InstState, work lists
+
+// Every GPU that loads the library holds this array until the process exits.
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
+
+// device address of g_noalloc_scratch per device, from cudaGetSymbolAddress
+double* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+
+enum { NL_VALID = 0, NL_G4, NL_G1, NL_G1X3, NL_TBX, NL_PAIR, NL_EBX, NL_COUNT };
+
+struct NoallocLists {
+    int nsub[NL_COUNT];
+    long long np[NL_COUNT][6];    // points of each sub-region
+    int first[NL_COUNT];          // first work item of each list
+    int total;
+};
+
+__global__ void k_noalloc_setup(BoxDev B, InstDev I, InstState st, NoallocLists NLs, BoxDev* dB, InstDev* dI,
+                                InstState* dS, Work* work)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) {
+        *dB = B;
+        *dI = I;
+        *dS = st;
+    }
+    if (t >= NLs.total) return;
+    int l = NL_COUNT - 1;
+    while (l > 0 && t < NLs.first[l]) --l;
+    int item = t - NLs.first[l];
+    for (int sub = 0; sub < NLs.nsub[l]; ++sub) {
+        long long np = NLs.np[l][sub];
+        int nb = (int)((np + BLOCK - 1) / BLOCK);
+        if (item < nb) {
+            Work w;
+            w.box = 0;
+            w.sub = sub;
+            w.start = item * BLOCK;
+            w.count = (int)(np - (long long)item * BLOCK < BLOCK ? np - (long long)item * BLOCK : BLOCK);
+            work[t] = w;
+            return;
+        }
+        item -= nb;
+    }
+}
+
+template <int NS>
+int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const int* sb_lo, const int* sb_hi,
+                           double* source, const int* sr_lo, const int* sr_hi, double* const* fo, const int* fo_lo,
+                           const int* fo_hi, const double* dx, double dt)
+{
+    for (int d = 0; d < 3; ++d)
+        if (sb_lo[d] > lo[d] - NG || sb_hi[d] < hi[d] + NG) {
+            set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box_noalloc: Sborder needs 4 ghost zones");
+            return CASTRO_ERR_ARG;
+        }
+    int dev = 0;
+    if (!cuda_ok(cudaGetDevice(&dev), "castro_construct_hydro_source_box_noalloc: cudaGetDevice")) return CASTRO_ERR_CUDA;
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+        set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box_noalloc: device index beyond 63");
+        return CASTRO_ERR_ARG;
+    }
+    if (!g_noalloc_addr[dev]) {
+        // once per device: the host-side name of a __device__ array is only a
+        // stand-in; kernels need its device address
+        void* p = nullptr;
+        if (!cuda_ok(cudaGetSymbolAddress(&p, g_noalloc_scratch), "castro_construct_hydro_source_box_noalloc: cudaGetSymbolAddress"))
+            return CASTRO_ERR_CUDA;
+        g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    double* base = g_noalloc_addr[dev];
+
+    // layout: records and work lists in the first NOALLOC_META_BYTES, then the pools
+    const int NV = Dims<NS>::NVAR, NQF = QF<NS>::N, NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF;
+    BoxDev B;
+    memset(&B, 0, sizeof B);
+    for (int d = 0; d < 3; ++d) { B.lo[d] = lo[d]; B.hi[d] = hi[d]; }
+    B.inst = 0;
+    long long o = 0;
+    auto take = [&](long long n) { long long r = o; o += (n + 31) / 32 * 32; return r; };   // 256-byte aligned
+    B.offU = 0;
+    B.offUb = take(npts_reg(B.lo, B.hi, R_G1, 0) * NV);
+    B.offQ = take(npts_reg(B.lo, B.hi, R_G4, 0) * NQF);
+    B.offDiv = take(npts_reg(B.lo, B.hi, R_G1, 0) * 2);
+    for (int d = 0; d < 3; ++d) {
+        B.offTr[d] = take(npts_reg(B.lo, B.hi, R_TBX, 4 * d) * 2 * NQS);
+        B.offF1[d] = take(npts_reg(B.lo, B.hi, R_TBX, 4 * d) * NTF);
+        B.offFx[d] = take(npts_reg(B.lo, B.hi, R_EBX, d) * (NV + 1));
+    }
+    for (int a = 0; a < 3; ++a)
+        for (int bb = 0; bb < 3; ++bb)
+            if (a != bb) B.offF2[pair_index(a, bb)] = take(npts_reg(B.lo, B.hi, R_TBX, 3 * a + bb) * NTF);
+
+    NoallocLists NLs;
+    memset(&NLs, 0, sizeof NLs);
+    const int kinds[NL_COUNT] = {R_VALID, R_G4, R_G1, R_G1, R_TBX, R_TBX, R_EBX};
+    const int nsubs[NL_COUNT] = {1, 1, 1, 3, 3, 6, 3};
+    int total = 0;
+    int nblocks[NL_COUNT];
+    for (int l = 0; l < NL_COUNT; ++l) {
+        NLs.nsub[l] = nsubs[l];
+        NLs.first[l] = total;
+        int nb = 0;
+        for (int sub = 0; sub < nsubs[l]; ++sub) {
+            int rs = sub;
+            if (l == NL_TBX) rs = 4 * sub;
+            if (l == NL_PAIR) { int a = sub / 2, r2 = sub % 2; rs = 3 * a + ((r2 < a) ? r2 : r2 + 1); }
+            NLs.np[l][sub] = npts_reg(B.lo, B.hi, kinds[l], rs);
+            nb += (int)((NLs.np[l][sub] + BLOCK - 1) / BLOCK);
+        }
+        nblocks[l] = nb;
+        total += nb;
+    }
+    NLs.total = total;
+    const long long meta = 1024 + (long long)total * (long long)sizeof(Work);
+    const long long meta_doubles = NOALLOC_META_BYTES / 8;
+    if (meta > NOALLOC_META_BYTES || meta_doubles + o > NOALLOC_DOUBLES) {
+        char msg[200];
+        snprintf(msg, sizeof msg,
+                 "castro_construct_hydro_source_box_noalloc: box needs %lld doubles of scratch, the static array holds %lld "
+                 "(at most 16^3 zones with 13 species, 21^3 with 2)", meta_doubles + o, NOALLOC_DOUBLES);
+        set_error(CASTRO_ERR_ARG, msg);
+        return CASTRO_ERR_ARG;
+    }
+    char* mb = reinterpret_cast<char*>(base);
+    BoxDev* dB = reinterpret_cast<BoxDev*>(mb);
+    InstDev* dI = reinterpret_cast<InstDev*>(mb + 256);
+    InstState* dS = reinterpret_cast<InstState*>(mb + 512);
+    Work* work = reinterpret_cast<Work*>(mb + 1024);
+    double* pools = base + meta_doubles;
+
+    InstDev I;
+    memset(&I, 0, sizeof I);
+    for (int d = 0; d < 3; ++d) { I.dom_lo[d] = lo[d]; I.dom_hi[d] = hi[d]; I.dx[d] = dx[d]; }
+    I.bc = CASTRO_BC_OUTFLOW;
+    I.g = 1;
+    InstState st;
+    memset(&st, 0, sizeof st);
+    st.dt = dt;
+    st.stop_time = -1.0;
+
+    cudaStream_t cs = castro::stream();
+    k_noalloc_setup<<<(total + 127) / 128, 128, 0, cs>>>(B, I, st, NLs, dB, dI, dS, work);
+    SimDev S;
+    memset(&S, 0, sizeof S);
+    S.boxes = dB; S.inst = dI; S.st = dS;
+    S.Ub = pools; S.Q = pools; S.Div = pools; S.Tr = pools; S.F1 = pools; S.F2 = pools; S.Fx = pools;
+    const Work* W = work;
+    k_box_prim<NS><<<nblocks[NL_G4], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G4], make_fab(sb, sb_lo, sb_hi));
+    k_prep<NS><<<nblocks[NL_G1], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G1]);
+    k_trace<NS><<<nblocks[NL_G1X3], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G1X3]);
+    k_riemann1<NS><<<nblocks[NL_TBX], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TBX]);
+    k_riemann2<NS><<<nblocks[NL_PAIR], BLOCK, 0, cs>>>(S, W + NLs.first[NL_PAIR]);
+    k_riemann3<NS><<<nblocks[NL_EBX], BLOCK, 0, cs>>>(S, W + NLs.first[NL_EBX]);
+    k_box_source<NS><<<nblocks[NL_VALID], BLOCK, 0, cs>>>(S, W + NLs.first[NL_VALID], make_fab(source, sr_lo, sr_hi));
+    if (fo) {
+        Fab F[3];
+        for (int d = 0; d < 3; ++d) {
+            F[d] = fo[d] ? make_fab(fo[d], fo_lo + 3 * d, fo_hi + 3 * d) : Fab{};
+            if (!fo[d]) F[d].p = nullptr;
+        }
+        k_box_store_flux<NS><<<nblocks[NL_EBX], BLOCK, 0, cs>>>(S, W + NLs.first[NL_EBX], F[0], F[1], F[2], dt);
+    }
+    check_launch("castro_construct_hydro_source_box_noalloc");
+    return castro_last_error();
+}
+
+}  // namespace
+}  // namespace castro
+
 extern "C" {
 
 int castro_construct_hydro_source_box(const int* lo, const int* hi, const double* sborder, const int* sb_lo,
@@ -1583,6 +1769,26 @@ int castro_construct_hydro_source_box(const int* lo, const int* hi, const double
     if (nspec() == 2) return box_hydro_impl<2>(lo, hi, sborder, sb_lo, sb_hi, source, sr_lo, sr_hi, fluxes_out, fo_lo3x3, fo_hi3x3, dx, dt);
     if (nspec() == 13) return box_hydro_impl<13>(lo, hi, sborder, sb_lo, sb_hi, source, sr_lo, sr_hi, fluxes_out, fo_lo3x3, fo_hi3x3, dx, dt);
     set_error(CASTRO_ERR_NSPEC, "castro_construct_hydro_source_box: nspec");
+    return CASTRO_ERR_NSPEC;
+}
+
+int castro_construct_hydro_source_box_noalloc(const int* lo, const int* hi, const double* sborder, const int* sb_lo,
+                                              const int* sb_hi, double* source, const int* sr_lo, const int* sr_hi,
+                                              double* const* fluxes_out, const int* fo_lo3x3, const int* fo_hi3x3,
+                                              const int* domlo, const int* domhi, const double* dx, double dt)
+{
+    (void)domlo; (void)domhi;
+    if (!table_ready()) {
+        set_error(CASTRO_ERR_NO_TABLE, "castro_construct_hydro_source_box_noalloc: eos_init has not run");
+        return CASTRO_ERR_NO_TABLE;
+    }
+    if (nspec() == 2)
+        return box_hydro_noalloc_impl<2>(lo, hi, sborder, sb_lo, sb_hi, source, sr_lo, sr_hi, fluxes_out, fo_lo3x3,
+                                         fo_hi3x3, dx, dt);
+    if (nspec() == 13)
+        return box_hydro_noalloc_impl<13>(lo, hi, sborder, sb_lo, sb_hi, source, sr_lo, sr_hi, fluxes_out, fo_lo3x3,
+                                          fo_hi3x3, dx, dt);
+    set_error(CASTRO_ERR_NSPEC, "castro_construct_hydro_source_box_noalloc: nspec");
     return CASTRO_ERR_NSPEC;
 }
 
