@@ -46,13 +46,18 @@ namespace {
 
 constexpr int NG = 4;   // ghost zones of Sborder, Source/Castro_advance.cpp:37
 constexpr int BLOCK = 128;
-// Optional minimum resident blocks per SM for the register allocator
-// (-DCASTRO_MINB_EOS=n etc.); without them the compiler picks the register count.
-#ifdef CASTRO_MINB_EOS
-#define LB_EOS __launch_bounds__(BLOCK, CASTRO_MINB_EOS)
-#else
-#define LB_EOS __launch_bounds__(BLOCK)
+// Minimum resident blocks per SM for the register allocator, chosen by a
+// timing sweep on B200: 4 blocks (128 registers) for the EOS kernels and the
+// final Riemann kernel, whose spills stay in L1; trace and the other Riemann
+// kernels keep the compiler's choice.  Override with -DCASTRO_MINB_*.
+#ifndef CASTRO_MINB_EOS
+#define CASTRO_MINB_EOS 4
 #endif
+#ifndef CASTRO_MINB_R3
+#define CASTRO_MINB_R3 4
+#endif
+#define LB_EOS __launch_bounds__(BLOCK, CASTRO_MINB_EOS)
+#define LB_R3 __launch_bounds__(BLOCK, CASTRO_MINB_R3)
 #ifdef CASTRO_MINB_TRACE
 #define LB_TRACE __launch_bounds__(BLOCK, CASTRO_MINB_TRACE)
 #else
@@ -483,7 +488,7 @@ __global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
 // riemann3: trans2 + compute_flux + apply_av + normalize_species_fluxes on ebx[d]
 // (Castro_hydro.cpp:307-359)
 template <int NS>
-__global__ void LB_RIEMANN k_riemann3(SimDev S, const Work* wl)
+__global__ void LB_R3 k_riemann3(SimDev S, const Work* wl)
 {
     int bx, d, i, j, k;
     Reg R;
