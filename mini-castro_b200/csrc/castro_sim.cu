@@ -97,7 +97,7 @@ struct InstState {
 
 struct Work { int box, sub, start, count; };
 
-enum Region { R_VALID = 0, R_G1, R_G4, R_TBX, R_EBX };
+enum Region { R_VALID = 0, R_G1, R_G4, R_TBX, R_EBX, R_GHOST };
 
 struct Reg {
     int lx, ly, lz, nx, ny, nz;
@@ -110,6 +110,14 @@ __host__ __device__ __forceinline__ Reg make_reg(const int* lo, const int* hi, i
     if (kind == R_G1) { for (int d = 0; d < 3; ++d) { l[d] -= 1; h[d] += 1; } }
     else if (kind == R_G4) { for (int d = 0; d < 3; ++d) { l[d] -= NG; h[d] += NG; } }
     else if (kind == R_EBX) { h[sub] += 1; }
+    else if (kind == R_GHOST) {
+        // slab sub of grow(bx,4) minus bx: 0/1 low/high z (all of x, y), 2/3 low/high y
+        // (all of x, valid z), 4/5 low/high x (valid y, z)
+        const int a = 2 - sub / 2;
+        for (int d = 0; d < a; ++d) { l[d] -= NG; h[d] += NG; }
+        if (sub % 2 == 0) { h[a] = l[a] - 1; l[a] -= NG; }
+        else { l[a] = h[a] + 1; h[a] += NG; }
+    }
     else if (kind == R_TBX) {
         // sub = 3*a + b: faces normal to a; grown by 1 in the directions other
         // than a and b (Source/Castro_hydro.cpp:93-101)
@@ -274,15 +282,16 @@ __device__ __forceinline__ int map_bc(int i, int lo, int hi, int bc)
     return i < lo ? lo : (i > hi ? hi : i);
 }
 
-// ghost: Q on grow(bx,4) and Sborder on grow(bx,1) outside the valid box
+// ghost: Q on grow(bx,4) and Sborder on grow(bx,1) outside the valid box,
+// one thread per ghost zone (the work list walks the six slabs)
 template <int NS>
 __global__ void __launch_bounds__(BLOCK) k_ghost(SimDev S, const Work* wl)
 {
     int b, sub, i, j, k;
-    Reg R;
-    if (!work_point(wl, S, R_G4, -1, b, sub, R, i, j, k)) return;
+    Reg RS;
+    if (!work_point(wl, S, R_GHOST, -1, b, sub, RS, i, j, k)) return;
     const BoxDev& B = S.boxes[b];
-    if (i >= B.lo[0] && i <= B.hi[0] && j >= B.lo[1] && j <= B.hi[1] && k >= B.lo[2] && k <= B.hi[2]) return;
+    const Reg R = make_reg(B.lo, B.hi, R_G4, 0);
     const InstDev& I = S.inst[B.inst];
     int ii = map_bc(i, I.dom_lo[0], I.dom_hi[0], I.bc);
     int jj = map_bc(j, I.dom_lo[1], I.dom_hi[1], I.bc);
@@ -440,30 +449,20 @@ __global__ void LB_RIEMANN k_riemann1(SimDev S, const Work* wl)
     store_tf<NS>(S.F1 + B.offF1[d], R, f, flx, g.x, g.y);
 }
 
-// riemann2: trans1 of the a-normal states with the b fluxes, then
-// compute_flux -> F^{a|b} on tbx[a][b] (Castro_hydro.cpp:228-255, 280-304)
-template <int NS>
-__global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
+// F^{A|Bd} on the A-normal face (i,j,k) of tbx[A][Bd]: trans1 of the face's
+// two A-normal trace states with the Bd normal fluxes, then compute_flux
+// (Castro_hydro.cpp:228-255, 280-304).  rec receives the transverse-flux record.
+template <int NS, int A, int Bd>
+__device__ __forceinline__ void cross_flux(const SimDev& S, const BoxDev& B, const QLoader<NS>& ld, int i, int j,
+                                           int k, double cdtdx, double* rec)
 {
-    int bx, p, i, j, k;
-    Reg R;
-    if (!work_point(wl, S, R_TBX, 1, bx, p, R, i, j, k)) return;
-    const BoxDev& B = S.boxes[bx];
-    const InstDev& I = S.inst[B.inst];
-    const double dt = S.st[B.inst].dt;
-    const int a = p / 2, r2 = p % 2;
-    const int bdir = (r2 < a) ? r2 : r2 + 1;
     constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF, NVAR = Dims<NS>::NVAR;
-    const double cdtdx = dt / I.dx[bdir] / 3.0;
-    QLoader<NS> ld;
-    ld.base = S.Q + B.offQ;
-    ld.R = make_reg(B.lo, B.hi, R_G4, 0);
-    Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * a);
-    Reg RF = make_reg(B.lo, B.hi, R_TBX, 4 * bdir);
-    const double* T = S.Tr + B.offTr[a];
-    const double* F = S.F1 + B.offF1[bdir];
-    const int eax = a == 0, eay = a == 1, eaz = a == 2;
-    const int ebx_ = bdir == 0, eby = bdir == 1, ebz = bdir == 2;
+    constexpr int eax = A == 0, eay = A == 1, eaz = A == 2;
+    constexpr int ebx_ = Bd == 0, eby = Bd == 1, ebz = Bd == 2;
+    Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * A);
+    Reg RF = make_reg(B.lo, B.hi, R_TBX, 4 * Bd);
+    const double* T = S.Tr + B.offTr[A];
+    const double* F = S.F1 + B.offF1[Bd];
     long long ft = ridx(RT, i, j, k);
     double st2[2][NQS];
 #pragma unroll
@@ -478,61 +477,83 @@ __global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
         trans1_state<NS>(lq, fr, fl, ld.gamc(il, jl, kl), cdtdx, st2[D + 1]);
     }
     double flx[NVAR];
-    double2 g;
-    if (a == 0) g = riemann_at<NS, 0>(ld, i, j, k, st2[0], st2[1], flx);
-    else if (a == 1) g = riemann_at<NS, 1>(ld, i, j, k, st2[0], st2[1], flx);
-    else g = riemann_at<NS, 2>(ld, i, j, k, st2[0], st2[1], flx);
-    store_tf<NS>(S.F2 + B.offF2[p], R, ridx(R, i, j, k), flx, g.x, g.y);
+    double2 g = riemann_at<NS, A>(ld, i, j, k, st2[0], st2[1], flx);
+    using T_ = TF<NS>;
+    rec[T_::RHO] = flx[URHO];
+    rec[T_::MX] = flx[UMX];
+    rec[T_::MY] = flx[UMY];
+    rec[T_::MZ] = flx[UMZ];
+    rec[T_::ED] = flx[UEDEN];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) rec[T_::X + n] = flx[UFS + n];
+    rec[T_::PG] = g.x;
+    rec[T_::UG] = g.y;
 }
 
-// riemann3: trans2 + compute_flux + apply_av + normalize_species_fluxes on ebx[d]
-// (Castro_hydro.cpp:307-359)
+// riemann2: F^{a|b} on tbx[a][b] for the six ordered pairs
 template <int NS>
-__global__ void LB_R3 k_riemann3(SimDev S, const Work* wl)
+__global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
 {
-    int bx, d, i, j, k;
+    int bx, p, i, j, k;
     Reg R;
-    if (!work_point(wl, S, R_EBX, -1, bx, d, R, i, j, k)) return;
+    if (!work_point(wl, S, R_TBX, 1, bx, p, R, i, j, k)) return;
     const BoxDev& B = S.boxes[bx];
     const InstDev& I = S.inst[B.inst];
     const double dt = S.st[B.inst].dt;
-    const int t1 = (d == 0) ? 1 : 0;
-    const int t2 = (d == 2) ? 1 : 2;
-    constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF, NVAR = Dims<NS>::NVAR;
-    const double hdt1 = 0.5 * dt / I.dx[t1], hdt2 = 0.5 * dt / I.dx[t2];
+    constexpr int NTF = Dims<NS>::NTF;
     QLoader<NS> ld;
     ld.base = S.Q + B.offQ;
     ld.R = make_reg(B.lo, B.hi, R_G4, 0);
-    Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * d);
-    const int p12 = pair_index(t1, t2), p21 = pair_index(t2, t1);
-    Reg R12 = make_reg(B.lo, B.hi, R_TBX, 3 * t1 + t2);
-    Reg R21 = make_reg(B.lo, B.hi, R_TBX, 3 * t2 + t1);
-    const double* T = S.Tr + B.offTr[d];
-    const double* F12 = S.F2 + B.offF2[p12];
-    const double* F21 = S.F2 + B.offF2[p21];
-    const int ex = d == 0, ey = d == 1, ez = d == 2;
-    const int e1x = t1 == 0, e1y = t1 == 1, e1z = t1 == 2;
-    const int e2x = t2 == 0, e2y = t2 == 1, e2z = t2 == 2;
+    double rec[NTF];
+    switch (p) {   // pair_index order: (0,1) (0,2) (1,0) (1,2) (2,0) (2,1)
+    case 0: cross_flux<NS, 0, 1>(S, B, ld, i, j, k, dt / I.dx[1] / 3.0, rec); break;
+    case 1: cross_flux<NS, 0, 2>(S, B, ld, i, j, k, dt / I.dx[2] / 3.0, rec); break;
+    case 2: cross_flux<NS, 1, 0>(S, B, ld, i, j, k, dt / I.dx[0] / 3.0, rec); break;
+    case 3: cross_flux<NS, 1, 2>(S, B, ld, i, j, k, dt / I.dx[2] / 3.0, rec); break;
+    case 4: cross_flux<NS, 2, 0>(S, B, ld, i, j, k, dt / I.dx[0] / 3.0, rec); break;
+    default: cross_flux<NS, 2, 1>(S, B, ld, i, j, k, dt / I.dx[1] / 3.0, rec); break;
+    }
+    double* out = S.F2 + B.offF2[p];
+    long long f = ridx(R, i, j, k);
+#pragma unroll
+    for (int c = 0; c < NTF; ++c) out[f + R.np * c] = rec[c];
+}
+
+// The final flux on the D-normal face (i,j,k) of ebx[D]: trans2 of the face's
+// two D-normal trace states with the cross fluxes F^{t1|t2} (f12) and
+// F^{t2|t1} (f21), compute_flux, apply_av, normalize_species_fluxes
+// (Castro_hydro.cpp:307-359), written to the final-flux record of ebx[D].
+// f12(i,j,k,rec) / f21(i,j,k,rec) load the cross-flux record at a face.
+template <int NS, int D, class L12, class L21>
+__device__ __forceinline__ void final_flux(const SimDev& S, const BoxDev& B, const InstDev& I, const QLoader<NS>& ld,
+                                           int i, int j, int k, double dt, const L12& f12, const L21& f21)
+{
+    constexpr int T1 = (D == 0) ? 1 : 0;
+    constexpr int T2 = (D == 2) ? 1 : 2;
+    constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF, NVAR = Dims<NS>::NVAR;
+    constexpr int ex = D == 0, ey = D == 1, ez = D == 2;
+    constexpr int e1x = T1 == 0, e1y = T1 == 1, e1z = T1 == 2;
+    constexpr int e2x = T2 == 0, e2y = T2 == 1, e2z = T2 == 2;
+    const double hdt1 = 0.5 * dt / I.dx[T1], hdt2 = 0.5 * dt / I.dx[T2];
+    Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * D);
+    const double* T = S.Tr + B.offTr[D];
     long long ft = ridx(RT, i, j, k);
     double st2[2][NQS];
 #pragma unroll
-    for (int D = -1; D <= 0; ++D) {
+    for (int Dm = -1; Dm <= 0; ++Dm) {
         double lq[NQS], f2r[NTF], f2l[NTF], f3r[NTF], f3l[NTF];
-        const int off = (D == -1) ? 0 : NQS;
+        const int off = (Dm == -1) ? 0 : NQS;
 #pragma unroll
         for (int c = 0; c < NQS; ++c) lq[c] = T[ft + RT.np * (off + c)];
-        int il = i + D * ex, jl = j + D * ey, kl = k + D * ez;
-        load_tf<NS>(F12, R12, ridx(R12, il + e1x, jl + e1y, kl + e1z), f2r);
-        load_tf<NS>(F12, R12, ridx(R12, il, jl, kl), f2l);
-        load_tf<NS>(F21, R21, ridx(R21, il + e2x, jl + e2y, kl + e2z), f3r);
-        load_tf<NS>(F21, R21, ridx(R21, il, jl, kl), f3l);
-        trans2_state<NS>(lq, f2r, f2l, f3r, f3l, ld.gamc(il, jl, kl), hdt1, hdt2, st2[D + 1]);
+        int il = i + Dm * ex, jl = j + Dm * ey, kl = k + Dm * ez;
+        f12(il + e1x, jl + e1y, kl + e1z, f2r);
+        f12(il, jl, kl, f2l);
+        f21(il + e2x, jl + e2y, kl + e2z, f3r);
+        f21(il, jl, kl, f3l);
+        trans2_state<NS>(lq, f2r, f2l, f3r, f3l, ld.gamc(il, jl, kl), hdt1, hdt2, st2[Dm + 1]);
     }
     double flx[NVAR];
-    double2 g;
-    if (d == 0) g = riemann_at<NS, 0>(ld, i, j, k, st2[0], st2[1], flx);
-    else if (d == 1) g = riemann_at<NS, 1>(ld, i, j, k, st2[0], st2[1], flx);
-    else g = riemann_at<NS, 2>(ld, i, j, k, st2[0], st2[1], flx);
+    double2 g = riemann_at<NS, D>(ld, i, j, k, st2[0], st2[1], flx);
 
     // apply_av, Castro_hydro_nd.F90:207-237 (the x and y four-node sums as written there)
     {
@@ -540,12 +561,12 @@ __global__ void LB_R3 k_riemann3(SimDev S, const Work* wl)
         const double* Dv = S.Div + B.offDiv;
         auto dv = [&](int a, int bq, int c) { return Dv[ridx(R1, a, bq, c)]; };
         double ds;
-        if (d == 0) ds = dv(i, j, k) + dv(i, j + 1, k) + dv(i, j, k + 1) + dv(i, j + 1, k);
-        else if (d == 1) ds = dv(i, j, k) + dv(i + 1, j, k) + dv(i, j, k + 1) + dv(i + 1, j, k);
+        if (D == 0) ds = dv(i, j, k) + dv(i, j + 1, k) + dv(i, j, k + 1) + dv(i, j + 1, k);
+        else if (D == 1) ds = dv(i, j, k) + dv(i + 1, j, k) + dv(i, j, k + 1) + dv(i + 1, j, k);
         else ds = dv(i, j, k) + dv(i + 1, j, k) + dv(i, j + 1, k) + dv(i + 1, j + 1, k);
         const double* Ub = S.Ub + B.offUb;
         long long c0 = ridx(R1, i, j, k), cm = ridx(R1, i - ex, j - ey, k - ez);
-        const double dxd = I.dx[d];
+        const double dxd = I.dx[D];
 #pragma unroll
         for (int n = 0; n < NVAR; ++n) {
             if (n == UTEMP) continue;
@@ -562,8 +583,9 @@ __global__ void LB_R3 k_riemann3(SimDev S, const Work* wl)
 #pragma unroll
         for (int n = 0; n < NS; ++n) flx[UFS + n] = flx[UFS + n] * fac;
     }
-    // final record: every flux component but UTEMP (always zero), GDPRES, GDU_d
-    double* X = S.Fx + B.offFx[d];
+    // final record: every flux component but UTEMP (always zero), GDPRES, GDU_D
+    Reg R = make_reg(B.lo, B.hi, R_EBX, D);
+    double* X = S.Fx + B.offFx[D];
     long long f = ridx(R, i, j, k);
 #pragma unroll
     for (int n = 0; n < NVAR; ++n) {
@@ -572,6 +594,42 @@ __global__ void LB_R3 k_riemann3(SimDev S, const Work* wl)
     }
     X[f + R.np * (NVAR - 1)] = g.x;
     X[f + R.np * NVAR] = g.y;
+}
+
+template <int NS>
+struct GlobalTF {   // cross-flux records in the F2 pool
+    const double* base;
+    Reg R;
+    __device__ __forceinline__ void operator()(int i, int j, int k, double* r) const { load_tf<NS>(base, R, ridx(R, i, j, k), r); }
+};
+
+template <int NS, int D>
+__device__ __forceinline__ void riemann3_dir(const SimDev& S, const BoxDev& B, const InstDev& I, const QLoader<NS>& ld,
+                                             int i, int j, int k, double dt)
+{
+    constexpr int T1 = (D == 0) ? 1 : 0;
+    constexpr int T2 = (D == 2) ? 1 : 2;
+    GlobalTF<NS> f12{S.F2 + B.offF2[pair_index(T1, T2)], make_reg(B.lo, B.hi, R_TBX, 3 * T1 + T2)};
+    GlobalTF<NS> f21{S.F2 + B.offF2[pair_index(T2, T1)], make_reg(B.lo, B.hi, R_TBX, 3 * T2 + T1)};
+    final_flux<NS, D>(S, B, I, ld, i, j, k, dt, f12, f21);
+}
+
+// riemann3: the final fluxes on ebx[d] from the F2 pool
+template <int NS>
+__global__ void LB_R3 k_riemann3(SimDev S, const Work* wl)
+{
+    int bx, d, i, j, k;
+    Reg R;
+    if (!work_point(wl, S, R_EBX, -1, bx, d, R, i, j, k)) return;
+    const BoxDev& B = S.boxes[bx];
+    const InstDev& I = S.inst[B.inst];
+    const double dt = S.st[B.inst].dt;
+    QLoader<NS> ld;
+    ld.base = S.Q + B.offQ;
+    ld.R = make_reg(B.lo, B.hi, R_G4, 0);
+    if (d == 0) riemann3_dir<NS, 0>(S, B, I, ld, i, j, k, dt);
+    else if (d == 1) riemann3_dir<NS, 1>(S, B, I, ld, i, j, k, dt);
+    else riemann3_dir<NS, 2>(S, B, I, ld, i, j, k, dt);
 }
 
 // update: fill_hydro_source, Saxpy, clean_state (advance), clean_state
@@ -853,8 +911,8 @@ struct castro_sim {
     long long nU = 0;
     // work lists
     Work *w_valid = nullptr, *w_g4 = nullptr, *w_g1 = nullptr, *w_g1x3 = nullptr, *w_tbx = nullptr, *w_pair = nullptr,
-         *w_ebx = nullptr;
-    int n_valid = 0, n_g4 = 0, n_g1 = 0, n_g1x3 = 0, n_tbx = 0, n_pair = 0, n_ebx = 0;
+         *w_ebx = nullptr, *w_ghost = nullptr;
+    int n_valid = 0, n_g4 = 0, n_g1 = 0, n_g1x3 = 0, n_tbx = 0, n_pair = 0, n_ebx = 0, n_ghost = 0;
     bool dt_ready = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -939,7 +997,7 @@ void batched_step_kernels(castro_sim* s)
     SimDev S = s->dev();
     cudaStream_t st = s->st;
     k_front<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid);
-    k_ghost<NS><<<s->n_g4, BLOCK, 0, st>>>(S, s->w_g4);
+    k_ghost<NS><<<s->n_ghost, BLOCK, 0, st>>>(S, s->w_ghost);
     k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(S, s->w_g1);
     k_trace<NS><<<s->n_g1x3, BLOCK, 0, st>>>(S, s->w_g1x3);
     k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(S, s->w_tbx);
@@ -955,7 +1013,7 @@ void profile_kernel(castro_sim* s, const SimDev& S, int k)
     cudaStream_t st = s->st;
     switch (k) {
     case 0: k_front<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid); break;
-    case 1: k_ghost<NS><<<s->n_g4, BLOCK, 0, st>>>(S, s->w_g4); break;
+    case 1: k_ghost<NS><<<s->n_ghost, BLOCK, 0, st>>>(S, s->w_ghost); break;
     case 2: k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(S, s->w_g1); break;
     case 3: k_trace<NS><<<s->n_g1x3, BLOCK, 0, st>>>(S, s->w_g1x3); break;
     case 4: k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(S, s->w_tbx); break;
@@ -1326,6 +1384,7 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
         build_work(s, R_TBX, 3, 0, &s->w_tbx, &s->n_tbx);
         build_work(s, R_TBX, 6, 1, &s->w_pair, &s->n_pair);
         build_work(s, R_EBX, 3, -1, &s->w_ebx, &s->n_ebx);
+        build_work(s, R_GHOST, 6, -1, &s->w_ghost, &s->n_ghost);
     }
     if (ok && mode == CASTRO_MODE_PLAIN) {
         long long nsb = 0, nsrc = 0, mx = 0;
@@ -1354,7 +1413,7 @@ void castro_sim_destroy(castro_sim* s)
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     if (s->graph) cudaGraphDestroy(s->graph);
     void* ptrs[] = {s->dboxes, s->dinst, s->dstate, s->downer, s->U, s->Ub, s->Q, s->Div, s->Tr, s->F1, s->F2, s->Fx,
-                    s->w_valid, s->w_g4, s->w_g1, s->w_g1x3, s->w_tbx, s->w_pair, s->w_ebx, s->sb, s->src, s->scratch,
+                    s->w_valid, s->w_g4, s->w_g1, s->w_g1x3, s->w_tbx, s->w_pair, s->w_ebx, s->w_ghost, s->sb, s->src, s->scratch,
                     s->d_dtloc, s->d_dtbox};
     for (void* p : ptrs)
         if (p) cudaFree(p);
