@@ -174,11 +174,7 @@ def run_b200(args, pkg, rank, world):
         e1.record(stream)
         e1.synchronize()
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = pkg.replicas.max_over_ranks(e0.elapsed_time(e1), device="cuda")
     launches = sim.launches_per_step() * args.steps
     failures = sim.eos_failures()
 
@@ -196,10 +192,7 @@ def run_b200(args, pkg, rank, world):
     t_e2e = time.perf_counter() - t0
     pkg.castro.check(L, f"castro_sim_run_host rc={rc}")
     sim2.close()
-    if world > 1:
-        t = torch.tensor([t_e2e], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = pkg.replicas.max_over_ranks(t_e2e, device="cuda")
 
     # plain per-box path (the reference's launch structure), a few steps
     plain = None
@@ -219,7 +212,11 @@ def run_b200(args, pkg, rank, world):
                  "steps": args.plain_steps, "launches_per_step": sim3.launches_per_step()}
         sim3.close()
 
-    value = world * zones * args.steps / (ms * 1e-3)
+    batched_cfg = None
+    if rank == 0 and args.batched_steps > 0:
+        batched_cfg = run_batched_config(pkg, L, args)
+
+    value = pkg.replicas.whole_job_rate(zones, args.steps, ms, world)
     hbm, peak_kind = peaks()
     kb = kernel_bytes(cfg, nspec)
     dom = max((k for k in prof if k in kb), key=lambda k: prof[k])
@@ -260,7 +257,7 @@ def run_b200(args, pkg, rank, world):
                    "path": "batched fused kernels, one CUDA graph per step",
                    "l2": "no flush: state 151 MB plus ~3.6 GB of per-step intermediates exceed the 126 MB L2",
                    "parallelism": f"replicas x{world}"},
-        "e2e": {"value": world * zones * args.steps / t_e2e, "unit": "zone-updates/s",
+        "e2e": {"value": pkg.replicas.whole_job_rate(zones, args.steps, t_e2e * 1e3, world), "unit": "zone-updates/s",
                 "h2d_bytes_per_step": host_in.numel() * 8 / args.steps,
                 "d2h_bytes_per_step": host_out.numel() * 8 / args.steps,
                 "call": "castro_sim_run_host (upload state, K steps, download state)"},
@@ -271,11 +268,43 @@ def run_b200(args, pkg, rank, world):
                      "algorithmic_bytes_per_launch": kb[dom]},
         "fp64": fp64,
         "plain_per_box": plain,
+        "batched_config": batched_cfg,
         "adjoint_forward_ratio": None,
         "eos_newton_failures": failures,
         "clocks": clk.summary(),
     }
     return line
+
+
+def run_batched_config(pkg, L, args):
+    """a 256^3 Sedov domain on an uneven BoxArray (per-axis box sizes
+    drawn from {16,24,32,48,64}) plus 32 independent instances of 32^3..96^3
+    zones, advanced together; batched fused path vs the per-box path."""
+    import torch
+
+    cfg = pkg.configs.batched()
+    zones = pkg.configs.zones(cfg)
+    out = {"workload": "batched: 256^3 uneven BoxArray + 32 instances 32^3..96^3, E 1e49-1e51, rho 0.1-10, 2 species",
+           "zones": zones, "instances": len(cfg["instances"]),
+           "boxes": sum(len(i["boxes"]) for i in cfg["instances"])}
+    for mode, key, steps in ((pkg.castro.MODE_BATCHED, "batched", args.batched_steps),
+                             (pkg.castro.MODE_PLAIN, "plain_per_box", 2)):
+        sim = pkg.make_sim(L, cfg, mode)
+        sim.init_data()
+        sim.step(2)
+        sim.sync()
+        st = torch.cuda.ExternalStream(sim.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        sim.step(steps)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[key] = {"value": zones * steps / (ms * 1e-3), "ms_per_step": ms / steps, "steps": steps,
+                    "launches_per_step": sim.launches_per_step()}
+        sim.close()
+    out["speedup_batched_over_plain"] = out["batched"]["value"] / out["plain_per_box"]["value"]
+    return out
 
 
 def cpu_baseline(pkg, args, steps=2):
@@ -346,6 +375,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="sedov128_pert")
     ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--batched-steps", type=int, default=18, help="timed steps of the batched configuration (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scale", type=int, default=1, help="divide the workload's zone counts (profiling runs only)")
     args = ap.parse_args()

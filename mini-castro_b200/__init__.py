@@ -6,11 +6,12 @@ The product is the CUDA library ``lib/libcastro_b200.so`` (C-ABI in
 * ``castro``     -- ctypes binding of the C-ABI (simulation objects, per-routine calls)
 * ``configs``    -- the Sedov workloads (BoxArrays, networks, problem constants)
 * ``helm_table`` -- writer of the Helmholtz table file read by ``eos_init``
+* ``replicas``   -- the multi-GPU (one replica per rank) reductions
 * ``build``      -- nvcc recipe for the sm_100a libraries
 """
-from . import castro, configs, helm_table  # noqa: F401
+from . import castro, configs, helm_table, replicas  # noqa: F401
 
-__all__ = ["castro", "configs", "helm_table", "make_sim"]
+__all__ = ["castro", "configs", "helm_table", "replicas", "make_sim"]
 
 
 def make_sim(L, cfg, mode=castro.MODE_BATCHED):

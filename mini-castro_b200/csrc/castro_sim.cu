@@ -47,14 +47,14 @@ namespace {
 constexpr int NG = 4;   // ghost zones of Sborder, Source/Castro_advance.cpp:37
 constexpr int BLOCK = 128;
 // Minimum resident blocks per SM for the register allocator, chosen by a
-// timing sweep on B200: 4 blocks (128 registers) for the EOS kernels and the
-// final Riemann kernel, whose spills stay in L1; trace and the other Riemann
-// kernels keep the compiler's choice.  Override with -DCASTRO_MINB_*.
+// timing sweep on B200: 4 blocks (128 registers) for the EOS kernels, whose
+// spills stay in L1, and 3 blocks for the final Riemann kernel; trace and the
+// other Riemann kernels keep the compiler's choice.  Override with -DCASTRO_MINB_*.
 #ifndef CASTRO_MINB_EOS
 #define CASTRO_MINB_EOS 4
 #endif
 #ifndef CASTRO_MINB_R3
-#define CASTRO_MINB_R3 4
+#define CASTRO_MINB_R3 3
 #endif
 #define LB_EOS __launch_bounds__(BLOCK, CASTRO_MINB_EOS)
 #define LB_R3 __launch_bounds__(BLOCK, CASTRO_MINB_R3)
