@@ -55,52 +55,84 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """SM clock and clock-event (throttle) reasons of this process's GPU, read
+    through NVML every 10 ms on a background thread while the timed region
+    runs (the GPU is found by its PCI bus id, so CUDA_VISIBLE_DEVICES does not
+    matter).  Readings only: no setting of the GPU is touched.  The samples go
+    to gpurun_out/clocks_rank<r>.csv as well."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_S = 0.01
 
-    def __init__(self, gpu_index: int):
-        self.idx = gpu_index
-        self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+    def __init__(self, cuda_index: int):
+        self.cuda_index = cuda_index
+        self.rows = []
+        self.err = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{cuda_index}.csv")
+
+    def _handle(self):
+        import pynvml as nv
+        import torch
+
+        nv.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.cuda_index)
+        try:
+            return nv.nvmlDeviceGetHandleByPciBusId(f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0")
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.cuda_index)
+
+    def _loop(self):
+        import pynvml as nv
+
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+                self.rows.append((time.time(), sm, pw, [n for n, b in bits.items() if r & b]))
+            except Exception as e:          # keep the first error for the summary
+                self.err = self.err or repr(e)
+            self.stop.wait(self.PERIOD_S)
 
     def __enter__(self):
+        import threading
+
+        import pynvml as nv
+
+        self.stop = threading.Event()
+        self.t = None
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.fp = open(self.path, "w")
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.fp, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.p = None
+            self.h = self._handle()
+            self.sm_max = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            self.t = threading.Thread(target=self._loop, daemon=True)
+            self.t.start()
+        except Exception as e:
+            self.err = repr(e)
         return self
 
     def __exit__(self, *a):
-        if self.p:
-            self.p.terminate()
-            try:
-                self.p.wait(timeout=5)
-            except Exception:
-                self.p.kill()
-            self.fp.close()
+        if self.t:
+            self.stop.set()
+            self.t.join(timeout=5)
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            with open(self.path, "w") as fp:
+                fp.write("unix_time,sm_mhz,sm_max_mhz,power_w,reasons\n")
+                for t, sm, pw, rs in self.rows:
+                    fp.write(f"{t:.3f},{sm},{getattr(self, 'sm_max', '')},{pw:.1f},{'|'.join(rs)}\n")
+        except OSError:
+            pass
 
     def summary(self):
-        try:
-            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
-        except Exception:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = sorted(float(r[1]) for r in rows)
-        reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            for n, v in zip(names, r[5:9]):
-                if v.strip().lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(rows[0][2]), "reasons": sorted(reasons),
-                "samples": len(rows)}
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "error": self.err}
+        sm = sorted(r[1] for r in self.rows)
+        reasons = sorted({n for r in self.rows for n in r[3]})
+        return {"sm_mhz": float(sm[len(sm) // 2]), "sm_max_mhz": float(self.sm_max), "reasons": reasons,
+                "samples": len(self.rows), "sm_mhz_min": float(sm[0]), "source": "NVML, 10 ms"}
 
 
 def kernel_bytes(cfg, nspec):
