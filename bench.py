@@ -247,6 +247,9 @@ def run_b200(args, pkg, rank, world):
     batched_cfg = None
     if rank == 0 and args.batched_steps > 0:
         batched_cfg = run_batched_config(pkg, L, args)
+    adjoint_cfg = None
+    if rank == 0 and args.adjoint_reps > 0:
+        adjoint_cfg = run_adjoint_config(pkg, args)
 
     value = pkg.replicas.whole_job_rate(zones, args.steps, ms, world)
     hbm, peak_kind = peaks()
@@ -301,7 +304,8 @@ def run_b200(args, pkg, rank, world):
         "fp64": fp64,
         "plain_per_box": plain,
         "batched_config": batched_cfg,
-        "adjoint_forward_ratio": None,
+        "adjoint_config": adjoint_cfg,
+        "adjoint_forward_ratio": adjoint_cfg["adjoint_forward_ratio"] if adjoint_cfg else None,
         "eos_newton_failures": failures,
         "clocks": clk.summary(),
     }
@@ -336,6 +340,72 @@ def run_batched_config(pkg, L, args):
                     "launches_per_step": sim.launches_per_step()}
         sim.close()
     out["speedup_batched_over_plain"] = out["batched"]["value"] / out["plain_per_box"]["value"]
+    return out
+
+
+def run_adjoint_config(pkg, args):
+    """gradient of the shell kinetic energy (0.3 <= r/L <= 0.4) of a
+    64^3 perturbed Sedov run over 20 steps with respect to the blast energy,
+    the ambient density and the per-zone density perturbation, checkpoint every
+    5 steps.  Reports forward and reverse device times (the forward is the
+    reference launch sequence the reverse sweep recomputes; the fused batched
+    forward of the same run is timed beside it) and central finite differences
+    (relative step 1e-6) along 16 seeded directions."""
+    import numpy as np
+    import torch
+
+    cfg = pkg.configs.adjoint64()
+    inst = cfg["instances"][0]
+    table = pkg.helm_table.ensure_table()
+    L = pkg.castro.init(*cfg["network"], table)
+    run = pkg.adjoint.SedovAdjoint(L, inst, cfg["steps"], cfg["checkpoint"], cfg["shell"])
+    p = inst["problem"]
+    E0, R0 = p["exp_energy"], p["dens_ambient"]
+    pert0 = run.pert.clone()
+    run.forward(E0, R0, pert0)                     # warm-up (allocations, first launches)
+    run.backward()
+    fwd_ms, bwd_ms = [], []
+    for _ in range(max(1, args.adjoint_reps)):
+        J0 = run.forward(E0, R0, pert0)
+        dE, dR, dP = run.backward()
+        f, b = run.time_ms()
+        fwd_ms.append(f)
+        bwd_ms.append(b)
+    f_ms, b_ms = float(np.median(fwd_ms)), float(np.median(bwd_ms))
+    # the same run through the fused batched forward (one CUDA graph per step)
+    sim = pkg.make_sim(L, cfg, pkg.castro.MODE_BATCHED)
+    sim.init_data()
+    sim.sync()
+    st = torch.cuda.ExternalStream(sim.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    sim.step(cfg["steps"])
+    e1.record(st)
+    e1.synchronize()
+    batched_ms = e0.elapsed_time(e1)
+    sim.close()
+    fd = None
+    if args.adjoint_fd > 0:
+        rng = np.random.default_rng(2019)
+        n = run.n[0]
+        h = 1e-6
+        errs = []
+        for _ in range(args.adjoint_fd):
+            a, b, c = rng.standard_normal(), rng.standard_normal(), rng.standard_normal((n, n, n))
+            ct = torch.from_numpy(np.ascontiguousarray(c.transpose(2, 1, 0))).cuda()
+            ad = dE * E0 * a + dR * R0 * b + float((dP * ct).sum())
+            Jp = run.forward(E0 * (1 + h * a), R0 * (1 + h * b), pert0 + h * ct)
+            Jm = run.forward(E0 * (1 - h * a), R0 * (1 - h * b), pert0 - h * ct)
+            fdv = (Jp - Jm) / (2 * h)
+            errs.append(abs(ad - fdv) / max(abs(ad), abs(fdv)))
+        fd = {"directions": len(errs), "relative_step": h, "max_rel_err": max(errs),
+              "median_rel_err": float(np.median(errs)), "rel_errs": [float("%.3e" % e) for e in errs]}
+    out = {"workload": "adjoint64: 64^3 Sedov, perturbed density, 20 steps, checkpoint 5, shell 0.3-0.4",
+           "J": J0, "dJ_dE": dE, "dJ_drho_ambient": dR, "dJ_dpert_norm": float(dP.norm()),
+           "forward_ms": f_ms, "backward_ms": b_ms, "adjoint_forward_ratio": b_ms / f_ms,
+           "batched_forward_ms": batched_ms, "backward_over_batched_forward": b_ms / batched_ms,
+           "device_bytes": run.device_bytes(), "reps": len(fwd_ms), "fd_check": fd}
+    run.close()
     return out
 
 
@@ -408,6 +478,8 @@ def main():
     ap.add_argument("--workload", default="sedov128_pert")
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--batched-steps", type=int, default=18, help="timed steps of the batched configuration (0: skip)")
+    ap.add_argument("--adjoint-reps", type=int, default=3, help="timed forward+reverse runs of the adjoint configuration (0: skip)")
+    ap.add_argument("--adjoint-fd", type=int, default=16, help="finite-difference directions of the gradient check (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scale", type=int, default=1, help="divide the workload's zone counts (profiling runs only)")
     args = ap.parse_args()

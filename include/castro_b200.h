@@ -300,6 +300,118 @@ double castro_measure_fp64_tflops(void);
 /* the mini-app driver with the reference's command-line keys (Source/main.cpp) */
 int castro_main(int argc, char** argv);
 
+/* ------------------------------------------------------------------------- */
+/* Reverse mode (adjoint).  No counterpart in the reference: each entry point  */
+/* is the adjoint of the Castro_F.H routine it is named after, over the same   */
+/* [lo,hi] and FAB conventions.  Given the routine's primal inputs and the     */
+/* adjoint of its outputs (suffix b), it ACCUMULATES J^T * (output adjoint)     */
+/* into the adjoint of its inputs.  Branch decisions (limiters, floors, the    */
+/* Riemann sampling) follow the forward at the given inputs.  Components with  */
+/* no consumer on the hydro path carry no adjoint: QGAME and QTEMP of face      */
+/* states, the Riemann interface state q_int, and UTEMP (a Newton initial      */
+/* guess only).  Scatters into shared arrays use FP64 atomics.                 */
+/* ------------------------------------------------------------------------- */
+/* Castro_F.H:19-23 */
+void ctoprim_adj(const int* lo, const int* hi, const double* u, const int* u_lo, const int* u_hi,
+                 const double* qb, const int* qb_lo, const int* qb_hi, const double* qab, const int* qab_lo,
+                 const int* qab_hi, double* ub, const int* ub_lo, const int* ub_hi);
+/* Castro::clean_state (enforce_minimum_density, normalize_species,
+ * reset_internal_e, compute_temp; Castro_F.H:25-39) on one FAB: u is the state
+ * BEFORE cleaning; ub holds the adjoint of the cleaned state on entry and of u
+ * on exit */
+void clean_state_adj(const int* lo, const int* hi, const double* u, const int* u_lo, const int* u_hi, double* ub,
+                     const int* ub_lo, const int* ub_hi);
+/* Castro_F.H:123-128 */
+void divu_adj(const int* lo, const int* hi, const double* dx, const double* divb, const int* d_lo, const int* d_hi,
+              double* qb, const int* q_lo, const int* q_hi);
+/* Castro_F.H:130-140 (uflatten included); dtb (device, may be NULL) += d/d(dt) */
+void trace_ppm_adj(const int* lo, const int* hi, const int* vlo, const int* vhi, const int idir,
+                   const double* q, const int* q_lo, const int* q_hi, const double* qaux, const int* qa_lo,
+                   const int* qa_hi, const double* qmb, const int* qm_lo, const int* qm_hi, const double* qpb,
+                   const int* qp_lo, const int* qp_hi, double* qb, const int* qb_lo, const int* qb_hi, double* qab,
+                   const int* qab_lo, const int* qab_hi, const double* dx, const double dt, double* dtb);
+/* Castro_F.H:112-121: fluxb / qeb are the adjoints of flux and qgdnv */
+void compute_flux_adj(const int* lo, const int* hi, const double* ql, const int* ql_lo, const int* ql_hi,
+                      const double* qr, const int* qr_lo, const int* qr_hi, const double* qaux, const int* qa_lo,
+                      const int* qa_hi, const double* fluxb, const int* fx_lo, const int* fx_hi, const double* qeb,
+                      const int* qe_lo, const int* qe_hi, double* qlb, const int* qlb_lo, const int* qlb_hi,
+                      double* qrb, const int* qrb_lo, const int* qrb_hi, double* qab, const int* qab_lo,
+                      const int* qab_hi, const int idir);
+/* Castro_F.H:86-96; cdtdxb (device, may be NULL) += d/d(cdtdx) */
+void trans1_adj(const int* lo, const int* hi, const int idir1, const int idir2,
+                const double* q2m, const int* q2m_lo, const int* q2m_hi, const double* q2p, const int* q2p_lo,
+                const int* q2p_hi, const double* qaux, const int* qa_lo, const int* qa_hi, const double* f1,
+                const int* f1_lo, const int* f1_hi, const double* q1, const int* q1_lo, const int* q1_hi,
+                const double cdtdx, const double* q2mob, const int* q2mob_lo, const int* q2mob_hi,
+                const double* q2pob, const int* q2pob_lo, const int* q2pob_hi, double* q2mb, const int* q2mb_lo,
+                const int* q2mb_hi, double* q2pb, const int* q2pb_lo, const int* q2pb_hi, double* qab,
+                const int* qab_lo, const int* qab_hi, double* f1b, const int* f1b_lo, const int* f1b_hi, double* q1b,
+                const int* q1b_lo, const int* q1b_hi, double* cdtdxb);
+/* Castro_F.H:98-110 (hdtdx unused, as in the forward); cdtdyb/cdtdzb (device, may be NULL) */
+void trans2_adj(const int* lo, const int* hi, const int idir1, const int idir2, const int idir3,
+                const double* qm, const int* qm_lo, const int* qm_hi, const double* qp, const int* qp_lo,
+                const int* qp_hi, const double* qaux, const int* qa_lo, const int* qa_hi, const double* fyz,
+                const int* fyz_lo, const int* fyz_hi, const double* fzy, const int* fzy_lo, const int* fzy_hi,
+                const double* qy, const int* qy_lo, const int* qy_hi, const double* qz, const int* qz_lo,
+                const int* qz_hi, const double cdtdy, const double cdtdz, const double* qmob, const int* qmob_lo,
+                const int* qmob_hi, const double* qpob, const int* qpob_lo, const int* qpob_hi, double* qmb,
+                const int* qmb_lo, const int* qmb_hi, double* qpb, const int* qpb_lo, const int* qpb_hi, double* qab,
+                const int* qab_lo, const int* qab_hi, double* fyzb, const int* fyzb_lo, const int* fyzb_hi,
+                double* fzyb, const int* fzyb_lo, const int* fzyb_hi, double* qyb, const int* qyb_lo,
+                const int* qyb_hi, double* qzb, const int* qzb_lo, const int* qzb_hi, double* cdtdyb, double* cdtdzb);
+/* Castro_F.H:78-84: the flux adjoint passes through unchanged (flux += av) */
+void apply_av_adj(const int* lo, const int* hi, const int idir, const double* dx, const double* div, const int* d_lo,
+                  const int* d_hi, const double* sb, const int* s_lo, const int* s_hi, const double* fluxb,
+                  const int* f_lo, const int* f_hi, double* divb, const int* db_lo, const int* db_hi, double* sbb,
+                  const int* sbb_lo, const int* sbb_hi);
+/* Castro_F.H:73-76: flux is the flux BEFORE normalization; fluxb in/out */
+void normalize_species_fluxes_adj(const int* lo, const int* hi, const double* flux, const int* f_lo, const int* f_hi,
+                                  double* fluxb, const int* fb_lo, const int* fb_hi);
+/* Castro_F.H:55-71 */
+void fill_hydro_source_adj(const int* lo, const int* hi, const double* sourceb, const int* sr_lo, const int* sr_hi,
+                           const double* qe0, const int* qe0_lo, const int* qe0_hi,
+                           const double* qe1, const int* qe1_lo, const int* qe1_hi,
+                           const double* qe2, const int* qe2_lo, const int* qe2_hi,
+                           const double* area0, const int* a0_lo, const int* a0_hi,
+                           const double* area1, const int* a1_lo, const int* a1_hi,
+                           const double* area2, const int* a2_lo, const int* a2_hi,
+                           const double* volume, const int* v_lo, const int* v_hi, const double* dx,
+                           double* flux0b, const int* f0_lo, const int* f0_hi,
+                           double* flux1b, const int* f1_lo, const int* f1_hi,
+                           double* flux2b, const int* f2_lo, const int* f2_hi,
+                           double* qe0b, const int* qe0b_lo, const int* qe0b_hi,
+                           double* qe1b, const int* qe1b_lo, const int* qe1b_hi,
+                           double* qe2b, const int* qe2b_lo, const int* qe2b_hi);
+
+/* Gradient of a Sedov run (one instance, one GPU).  The forward is initdata
+ * plus nsteps coarse steps (computeNewDt, Castro::advance, post_timestep) over
+ * the instance's domain as one box (the result does not depend on the
+ * BoxArray); the objective is the kinetic energy in the spherical shell
+ * r0 <= r / (probhi - problo) <= r1 about the domain centre (default 0.3-0.4).
+ * The reverse sweep keeps a checkpoint every checkpoint_interval steps and
+ * recomputes each segment; the time step's dependence on the state (CFL
+ * reduction, 1.1x growth limit, stop-time clamp) is included.
+ * desc->prob.pert (optional) must stay valid until the object is destroyed. */
+typedef struct castro_adj castro_adj;
+castro_adj* castro_adj_create(const castro_instance_desc* desc, int nsteps, int checkpoint_interval);
+void   castro_adj_destroy(castro_adj* adj);
+/* new problem constants (energy, ambient density, perturbation ...) for the next forward */
+int    castro_adj_set_problem(castro_adj* adj, const castro_problem* prob);
+int    castro_adj_set_shell(castro_adj* adj, double r0, double r1);
+/* forward run; *J receives the objective */
+int    castro_adj_forward(castro_adj* adj, double* J);
+/* reverse sweep after castro_adj_forward: dJ/d(exp_energy), dJ/d(dens_ambient)
+ * and, if dJ_dpert is non-NULL (device array shaped like prob.pert), dJ/dpert
+ * accumulated into it */
+int    castro_adj_backward(castro_adj* adj, double* dJ_dE, double* dJ_drho, double* dJ_dpert);
+double castro_adj_dt(const castro_adj* adj, int step);
+/* device copies (domain box, NVAR comps): final state / adjoint of the initial state */
+int    castro_adj_final_state(const castro_adj* adj, double* dst);
+int    castro_adj_initial_adjoint(const castro_adj* adj, double* dst);
+/* device time of the last forward (which=0) or backward (which=1) call, ms */
+double castro_adj_time_ms(const castro_adj* adj, int which);
+size_t castro_adj_device_bytes(const castro_adj* adj);
+
 #ifdef __cplusplus
 }
 #endif

@@ -22,7 +22,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 OBJDIR = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
-SOURCES = ["castro_host.cu", "castro_abi.cu", "castro_sim.cu", "castro_main.cu", "castro_peak.cu"]
+SOURCES = ["castro_host.cu", "castro_abi.cu", "castro_sim.cu", "castro_adjoint.cu", "castro_main.cu", "castro_peak.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-fPIC",
           "-Xcompiler", "-Wno-subobject-linkage"]
@@ -87,6 +87,15 @@ def build(force: bool = False, verbose: bool = False, variants=None) -> list[str
         if r.returncode != 0:
             raise RuntimeError(f"link failed for {exe}:\n{r.stdout}\n{r.stderr}")
         outs.append(exe)
+    # host-only check of the reverse-mode stages against finite differences
+    st = os.path.join(LIBDIR, "castro_adjoint_selftest")
+    if "libcastro_b200.so" in names and (force or _stale(st)):
+        cmd = [NVCC, *ARCH, "-O2", "-std=c++17", "-Xcompiler", "-Wno-subobject-linkage", "-o", st,
+               os.path.join(CSRC, "adjoint_selftest.cu")]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"build failed for {st}:\n{r.stdout}\n{r.stderr}")
+        outs.append(st)
     return outs
 
 

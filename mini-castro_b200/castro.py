@@ -75,6 +75,11 @@ ABI_SYMBOLS = [
     "castro_sim_blast_radius", "castro_sim_launches_per_step", "castro_sim_eos_failures", "castro_main",
     "castro_sim_stream", "castro_sim_profile_step", "castro_measure_fp64_tflops",
     "castro_construct_hydro_source_box_noalloc",
+    "ctoprim_adj", "clean_state_adj", "divu_adj", "trace_ppm_adj", "compute_flux_adj", "trans1_adj", "trans2_adj",
+    "apply_av_adj", "normalize_species_fluxes_adj", "fill_hydro_source_adj", "castro_adj_create",
+    "castro_adj_destroy", "castro_adj_set_problem", "castro_adj_set_shell", "castro_adj_forward",
+    "castro_adj_backward", "castro_adj_dt", "castro_adj_final_state", "castro_adj_initial_adjoint",
+    "castro_adj_time_ms", "castro_adj_device_bytes",
 ]
 
 
@@ -132,6 +137,21 @@ def load(exact: bool = False) -> C.CDLL:
     L.castro_measure_fp64_tflops.restype = C.c_double
     L.castro_sim_eos_failures.restype = C.c_longlong
     L.castro_sim_eos_failures.argtypes = [C.c_void_p]
+    L.castro_adj_create.restype = C.c_void_p
+    L.castro_adj_create.argtypes = [C.POINTER(InstanceDesc), C.c_int, C.c_int]
+    L.castro_adj_destroy.argtypes = [C.c_void_p]
+    L.castro_adj_set_problem.argtypes = [C.c_void_p, C.POINTER(Problem)]
+    L.castro_adj_set_shell.argtypes = [C.c_void_p, C.c_double, C.c_double]
+    L.castro_adj_forward.argtypes = [C.c_void_p, _dp]
+    L.castro_adj_backward.argtypes = [C.c_void_p, _dp, _dp, C.c_void_p]
+    L.castro_adj_dt.restype = C.c_double
+    L.castro_adj_dt.argtypes = [C.c_void_p, C.c_int]
+    L.castro_adj_final_state.argtypes = [C.c_void_p, C.c_void_p]
+    L.castro_adj_initial_adjoint.argtypes = [C.c_void_p, C.c_void_p]
+    L.castro_adj_time_ms.restype = C.c_double
+    L.castro_adj_time_ms.argtypes = [C.c_void_p, C.c_int]
+    L.castro_adj_device_bytes.restype = C.c_size_t
+    L.castro_adj_device_bytes.argtypes = [C.c_void_p]
     _libs[exact] = L
     return L
 

@@ -13,6 +13,9 @@ Workloads (sizes as named by the benchmark configurations):
 * ``batched``       -- 256^3 cut into an uneven BoxArray (per-axis sizes drawn from
                        {16,24,32,48,64}) plus 32 independent instances of 32^3..96^3
                        zones with log-uniform energies and ambient densities, 20 steps.
+* ``adjoint64``     -- one 64^3 box with the seeded perturbation, 20 steps: the
+                       gradient case (objective: kinetic energy in the shell
+                       0.3 <= r/L <= 0.4; checkpoint every 5 steps).
 * ``large``         -- 384^3 in boxes of 32^3..64^3 with the perturbation, 100 steps.
 * ``reference``     -- the Source/Prob.F90 problem (13 species, periodic, 1e9 cm
                        domain), the physically in-table case.
@@ -138,6 +141,14 @@ def batched(scale: int = 1, steps: int = 20, seed: int = 7, ninst: int = 32):
     return dict(name="batched", network=NET2, steps=steps, instances=insts)
 
 
+def adjoint64(scale: int = 1, steps: int = 20, seed: int = 64):
+    n = 64 // scale
+    pert = gaussian_field((n, n, n), 4.0, seed)
+    prob = problem(pert=pert, pert_amp=1e-3)
+    return dict(name="adjoint64", network=NET2, steps=steps, checkpoint=5, shell=(0.3, 0.4),
+                instances=[instance(n, uniform_boxes(n, n), bc=1, prob=prob)])
+
+
 def large(scale: int = 1, steps: int = 100, seed: int = 384):
     rng = np.random.default_rng(seed)
     n = 384 // scale
@@ -157,7 +168,8 @@ def reference(scale: int = 1, steps: int = 10, max_box: int = 64):
                 instances=[instance(n, uniform_boxes(n, max(4, max_box // scale)), bc=0, length=1e9, prob=prob)])
 
 
-WORKLOADS = dict(sedov64=sedov64, sedov128_pert=sedov128_pert, batched=batched, large=large, reference=reference)
+WORKLOADS = dict(sedov64=sedov64, sedov128_pert=sedov128_pert, batched=batched, adjoint64=adjoint64, large=large,
+                 reference=reference)
 
 
 def zones(cfg) -> int:

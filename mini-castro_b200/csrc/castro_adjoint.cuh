@@ -1,0 +1,1534 @@
+// castro_adjoint.cuh -- reverse-mode (adjoint) stages of the CTU hydro
+// advance.  Each *_adj function takes the primal inputs of its forward stage
+// in castro_device.cuh, recomputes the forward values it needs (including every
+// branch decision: PPM limiters, Riemann sampling, floors), and maps the
+// adjoint of the stage outputs to the adjoint of its inputs along the branch
+// the forward took.  Adjoints of inputs are ACCUMULATED (x_b += J^T y_b).
+//
+// EOS: the temperature of eos(re) is the root of e(rho,T,abar,zbar) = e_want;
+// its adjoint uses the implicit-function derivative at the converged root,
+// dT = (de_want - e_rho drho - e_abar dabar - e_zbar dzbar) / e_T, with the
+// partials of the tabulated Helmholtz evaluation (eos.F90:195-518) taken in
+// forward mode (the D4 scalar below: value + 4 partials) -- including the
+// second and third derivatives of the free energy that p, gamma_1 and c_s
+// carry.
+//
+// All functions are host+device so that they can be checked against finite
+// differences on a CPU.
+#pragma once
+
+#include "castro_device.cuh"
+
+namespace castro {
+
+// ---------------------------------------------------------------------------
+// D4: forward-mode scalar, value + partials along (rho, T, 1/abar, zbar/abar)
+// ---------------------------------------------------------------------------
+struct D4 {
+    double v, d[4];
+    CASTRO_HD D4() {}
+    CASTRO_HD D4(double x) : v(x) { d[0] = d[1] = d[2] = d[3] = 0.0; }
+};
+CASTRO_HD D4 d4seed(double x, int k) { D4 r(x); r.d[k] = 1.0; return r; }
+CASTRO_HD double val(double x) { return x; }
+CASTRO_HD double val(const D4& x) { return x.v; }
+
+CASTRO_HD D4 operator+(const D4& a, const D4& b) { D4 r; r.v = a.v + b.v; for (int k = 0; k < 4; ++k) r.d[k] = a.d[k] + b.d[k]; return r; }
+CASTRO_HD D4 operator-(const D4& a, const D4& b) { D4 r; r.v = a.v - b.v; for (int k = 0; k < 4; ++k) r.d[k] = a.d[k] - b.d[k]; return r; }
+CASTRO_HD D4 operator-(const D4& a) { D4 r; r.v = -a.v; for (int k = 0; k < 4; ++k) r.d[k] = -a.d[k]; return r; }
+CASTRO_HD D4 operator*(const D4& a, const D4& b) { D4 r; r.v = a.v * b.v; for (int k = 0; k < 4; ++k) r.d[k] = a.v * b.d[k] + a.d[k] * b.v; return r; }
+CASTRO_HD D4 operator/(const D4& a, const D4& b)
+{
+    D4 r;
+    double bi = 1.0 / b.v;
+    r.v = a.v * bi;
+    for (int k = 0; k < 4; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) * bi;
+    return r;
+}
+CASTRO_HD D4 operator+(const D4& a, double b) { D4 r = a; r.v += b; return r; }
+CASTRO_HD D4 operator+(double a, const D4& b) { D4 r = b; r.v += a; return r; }
+CASTRO_HD D4 operator-(const D4& a, double b) { D4 r = a; r.v -= b; return r; }
+CASTRO_HD D4 operator-(double a, const D4& b) { D4 r; r.v = a - b.v; for (int k = 0; k < 4; ++k) r.d[k] = -b.d[k]; return r; }
+CASTRO_HD D4 operator*(const D4& a, double b) { D4 r; r.v = a.v * b; for (int k = 0; k < 4; ++k) r.d[k] = a.d[k] * b; return r; }
+CASTRO_HD D4 operator*(double a, const D4& b) { return b * a; }
+CASTRO_HD D4 operator/(const D4& a, double b) { return a * (1.0 / b); }
+CASTRO_HD D4 operator/(double a, const D4& b)
+{
+    D4 r;
+    double bi = 1.0 / b.v;
+    r.v = a * bi;
+    for (int k = 0; k < 4; ++k) r.d[k] = -r.v * b.d[k] * bi;
+    return r;
+}
+
+template <class S> CASTRO_HD S smax0(const S& a) { return val(a) > 0.0 ? a : S(0.0); }   // DMAX(a, 0)
+
+// table loads: read-only cache on the device, plain loads on the host
+CASTRO_HD double tld(const double* p)
+{
+#ifdef __CUDA_ARCH__
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+
+// quintic / cubic Hermite basis (eos.F90:740-1031), any scalar type
+template <class S> CASTRO_HD S psi0t(const S& z) { return z * z * z * (z * (-6.0 * z + 15.0) - 10.0) + 1.0; }
+template <class S> CASTRO_HD S dpsi0t(const S& z) { return z * z * (z * (-30.0 * z + 60.0) - 30.0); }
+template <class S> CASTRO_HD S ddpsi0t(const S& z) { return z * (z * (-120.0 * z + 180.0) - 60.0); }
+template <class S> CASTRO_HD S psi1t(const S& z) { return z * (z * z * (z * (-3.0 * z + 8.0) - 6.0) + 1.0); }
+template <class S> CASTRO_HD S dpsi1t(const S& z) { return z * z * (z * (-15.0 * z + 32.0) - 18.0) + 1.0; }
+template <class S> CASTRO_HD S ddpsi1t(const S& z) { return z * (z * (-60.0 * z + 96.0) - 36.0); }
+template <class S> CASTRO_HD S psi2t(const S& z) { return 0.5 * (z * z * (z * (z * (-z + 3.0) - 3.0) + 1.0)); }
+template <class S> CASTRO_HD S dpsi2t(const S& z) { return 0.5 * (z * (z * (z * (-5.0 * z + 12.0) - 9.0) + 2.0)); }
+template <class S> CASTRO_HD S ddpsi2t(const S& z) { return 0.5 * (z * (z * (-20.0 * z + 36.0) - 18.0) + 2.0); }
+template <class S> CASTRO_HD S xpsi0t(const S& z) { return z * z * (2.0 * z - 3.0) + 1.0; }
+template <class S> CASTRO_HD S xpsi1t(const S& z) { return z * (z * (z - 2.0) + 1.0); }
+
+template <class S>
+struct EosOutT {
+    S p, e, dpdT, dpdr, dedT, dedr, gam1;
+};
+
+// The Helmholtz evaluation of eos.F90:195-518 at (den, temp) for composition
+// (ytot1 = 1/abar, ye = zbar/abar), in any scalar type: with S = D4 it
+// carries the partials along its seeds.  Same formulas as eos_eval (factored
+// biquintic), table read through 'tb'.
+template <class S>
+CASTRO_HD void eos_eval_t(const EosTableDev& tb, const S& temp, const S& den, const S& ytot1, const S& ye,
+                          EosOutT<S>& r)
+{
+    S deni = 1.0 / den;
+    S din = ye * den;
+    S tempi = 1.0 / temp;
+    S prad = tb.asoli3 * temp * temp * temp * temp;
+    S dpraddt = 4.0 * prad * tempi;
+    S erad = 3.0 * prad * deni;
+    S deraddd = -erad * deni;
+    S deraddt = 3.0 * dpraddt * deni;
+    S pion = tb.kergavo * ytot1 * den * temp;
+    S dpiondd = tb.kergavo * ytot1 * temp;
+    S dpiondt = tb.kergavo * ytot1 * den;
+    S eion = 1.5 * pion * deni;
+    S deiondd = (1.5 * dpiondd - eion) * deni;
+    S deiondt = 1.5 * dpiondt * deni;
+
+    int jat = table_trunc((log10(val(temp)) - tb.tlo) * tb.tstpi);
+    jat = jat > JMAX - 2 ? JMAX - 2 : jat;
+    jat = jat < 0 ? 0 : jat;
+    int iat = table_trunc((log10(val(din)) - tb.dlo) * tb.dstpi);
+    iat = iat > IMAX - 2 ? IMAX - 2 : iat;
+    iat = iat < 0 ? 0 : iat;
+    const double* tr = tb.trow + (size_t)jat * ROW_STRIDE;
+    const double t0 = tld(tr + 0), dt = tld(tr + 1), dt2 = tld(tr + 2), dti = tld(tr + 3), dt2i = tld(tr + 4);
+    const double* dr = tb.drow + (size_t)iat * ROW_STRIDE;
+    const double d0 = tld(dr + 0), dd = tld(dr + 1), dd2 = tld(dr + 2), ddi = tld(dr + 3);
+    S xt = smax0((temp - t0) * dti);
+    S mxt = 1.0 - xt;
+    S xd = smax0((din - d0) * ddi);
+    S mxd = 1.0 - xd;
+
+    S st[3][2], dst[3][2], ddst[3][2], si[3][2], dsi[3][2];
+    st[0][0] = psi0t(xt); st[1][0] = psi1t(xt) * dt; st[2][0] = psi2t(xt) * dt2;
+    st[0][1] = psi0t(mxt); st[1][1] = -psi1t(mxt) * dt; st[2][1] = psi2t(mxt) * dt2;
+    dst[0][0] = dpsi0t(xt) * dti; dst[1][0] = dpsi1t(xt); dst[2][0] = dpsi2t(xt) * dt;
+    dst[0][1] = -dpsi0t(mxt) * dti; dst[1][1] = dpsi1t(mxt); dst[2][1] = -dpsi2t(mxt) * dt;
+    ddst[0][0] = ddpsi0t(xt) * dt2i; ddst[1][0] = ddpsi1t(xt) * dti; ddst[2][0] = ddpsi2t(xt);
+    ddst[0][1] = ddpsi0t(mxt) * dt2i; ddst[1][1] = -ddpsi1t(mxt) * dti; ddst[2][1] = ddpsi2t(mxt);
+    si[0][0] = psi0t(xd); si[1][0] = psi1t(xd) * dd; si[2][0] = psi2t(xd) * dd2;
+    si[0][1] = psi0t(mxd); si[1][1] = -psi1t(mxd) * dd; si[2][1] = psi2t(mxd) * dd2;
+    dsi[0][0] = dpsi0t(xd) * ddi; dsi[1][0] = dpsi1t(xd); dsi[2][0] = dpsi2t(xd) * dd;
+    dsi[0][1] = -dpsi0t(mxd) * ddi; dsi[1][1] = dpsi1t(mxd); dsi[2][1] = -dpsi2t(mxd) * dd;
+
+    const double* nb = tb.node + ((size_t)jat * IMAX + iat) * NODE_STRIDE;
+    const double* nc[4] = {nb, nb + NODE_STRIDE, nb + (size_t)IMAX * NODE_STRIDE,
+                           nb + (size_t)IMAX * NODE_STRIDE + NODE_STRIDE};
+    const int slot[3][3] = {{N_F, N_FT, N_FTT}, {N_FD, N_FDT, N_FDTT}, {N_FDD, N_FDDT, N_FDDTT}};
+    S free_e(0.0), df_d(0.0), df_t(0.0), df_tt(0.0), df_dt(0.0);
+    for (int a = 0; a < 3; ++a)
+        for (int di = 0; di < 2; ++di) {
+            S s0(0.0), s1(0.0), s2(0.0);
+            for (int b = 0; b < 3; ++b)
+                for (int dj = 0; dj < 2; ++dj) {
+                    double v = tld(nc[di + 2 * dj] + slot[a][b]);
+                    s0 = s0 + v * st[b][dj];
+                    s1 = s1 + v * dst[b][dj];
+                    s2 = s2 + v * ddst[b][dj];
+                }
+            free_e = free_e + s0 * si[a][di];
+            df_d = df_d + s0 * dsi[a][di];
+            df_t = df_t + s1 * si[a][di];
+            df_tt = df_tt + s2 * si[a][di];
+            df_dt = df_dt + s1 * dsi[a][di];
+        }
+
+    S xs0t = xpsi0t(xt), xs1t = xpsi1t(xt) * dt, xs0mt = xpsi0t(mxt), xs1mt = -xpsi1t(mxt) * dt;
+    S w0d = xpsi0t(xd), w1d = xpsi1t(xd) * dd, w0md = xpsi0t(mxd), w1md = -xpsi1t(mxd) * dd;
+    S dpepdd;
+    {
+        const int sl[4] = {N_DPDF, N_DPDFT, N_DPDFD, N_DPDFDT};
+        double f[16];
+        for (int m = 0; m < 4; ++m)
+            for (int c = 0; c < 4; ++c) f[4 * m + c] = tld(nc[c] + sl[m]);
+        dpepdd = f[0] * w0d * xs0t + f[1] * w0md * xs0t + f[2] * w0d * xs0mt + f[3] * w0md * xs0mt
+               + f[4] * w0d * xs1t + f[5] * w0md * xs1t + f[6] * w0d * xs1mt + f[7] * w0md * xs1mt
+               + f[8] * w1d * xs0t + f[9] * w1md * xs0t + f[10] * w1d * xs0mt + f[11] * w1md * xs0mt
+               + f[12] * w1d * xs1t + f[13] * w1md * xs1t + f[14] * w1d * xs1mt + f[15] * w1md * xs1mt;
+    }
+    dpepdd = smax0(ye * dpepdd);
+
+    S x = din * din;
+    S pele = x * df_d;
+    S dpepdt = x * df_dt;
+    S y2 = ye * ye;
+    S sele = -df_t * ye;
+    S dsepdt = -df_tt * ye;
+    S dsepdd = -df_dt * y2;
+    S eele = ye * free_e + temp * sele;
+    S deepdt = temp * dsepdt;
+    S deepdd = y2 * df_d + temp * dsepdd;
+
+    S pres = prad + pion + pele;
+    S ener = erad + eion + eele;
+    S dpresdd = dpiondd + dpepdd;
+    S dpresdt = dpraddt + dpiondt + dpepdt;
+    S denerdd = deraddd + deiondd + deepdd;
+    S denerdt = deraddt + deiondt + deepdt;
+    S zz = pres * deni;
+    S zzi = den / pres;
+    S chit = temp / pres * dpresdt;
+    S chid = dpresdd * zzi;
+    S cv = denerdt;
+    r.gam1 = chit * zz * chit / (temp * cv) + chid;
+    r.p = pres;
+    r.e = ener;
+    r.dpdT = dpresdt;
+    r.dpdr = dpresdd;
+    r.dedT = denerdt;
+    r.dedr = denerdd;
+}
+
+// Newton inversion of eos.F90:520-552 with the generic evaluation; returns the
+// converged temperature (the one the last evaluation used) and that
+// evaluation in r.
+template <int MODE>
+CASTRO_HD double eos_solve_t(const EosTableDev& tb, double rho, double T, double v_want, double abar, double zbar,
+                             EosOutT<double>& r)
+{
+    const double ytot1 = 1.0 / abar, ye = zbar / abar;
+    bool converged = (MODE == EOS_RT);
+    for (int iter = 1; iter <= 100; ++iter) {
+        double temp = T;
+        eos_eval_t<double>(tb, temp, rho, ytot1, ye, r);
+        if (converged) break;
+        double temp_old = temp;
+        double v = (MODE == EOS_RE) ? r.e : r.p;
+        double dvdx = (MODE == EOS_RE) ? r.dedT : r.dpdT;
+        temp = temp - (v - v_want) / dvdx;
+        temp = DMAX(0.5 * temp_old, DMIN(temp, 2.0 * temp_old));
+        temp = DMAX(tb.mintemp, temp);
+        T = temp;
+        double error = fabs((temp - temp_old) / temp_old);
+        if (error < 1.e-8) converged = true;
+    }
+    return T;
+}
+
+// Adjoints of the eos() outputs the hydro path can consume.
+struct EosBar {
+    double T, p, e, gam1, cs, dpde, dpdr_e;
+};
+
+// Adjoint of eos_solve<MODE> (MODE = EOS_RE or EOS_RT) at the converged T.
+// Inputs: rho, the mode's second input (e_want for EOS_RE, T for EOS_RT),
+// abar, zbar; outputs their adjoints (accumulated).  For EOS_RE the e output
+// equals e_want (eos.F90:566-574) and ob.e is passed straight to it.
+template <int MODE>
+CASTRO_HD void eos_vjp(const EosTableDev& tb, double rho, double T, double abar, double zbar, const EosBar& ob,
+                       double& rho_b, double& v_b, double& abar_b, double& zbar_b)
+{
+    const double ytot1 = 1.0 / abar, ye = zbar / abar;
+    EosOutT<D4> o;
+    eos_eval_t<D4>(tb, d4seed(T, 1), d4seed(rho, 0), d4seed(ytot1, 2), d4seed(ye, 3), o);
+    const double p = o.p.v, g = o.gam1.v;
+    double gb = ob.gam1, pb = ob.p, rb = 0.0;
+    if (ob.cs != 0.0) {   // cs = sqrt(gam1 * p / rho), eos.F90:556
+        double A = g * p / rho;
+        double Ab = ob.cs * 0.5 / sqrt(A);
+        gb += Ab * p / rho;
+        pb += Ab * g / rho;
+        rb -= Ab * A / rho;
+    }
+    const double dpdT = o.dpdT.v, dedT = o.dedT.v, dedr = o.dedr.v;
+    double dpdTb = 0.0, dedTb = 0.0, dpdrb = 0.0, dedrb = 0.0;
+    // dpde = dpdT / dedT; dpdr_e = dpdr - dpdT * dedr / dedT (eos.F90:502-503)
+    dpdTb += ob.dpde / dedT;
+    dedTb -= ob.dpde * dpdT / (dedT * dedT);
+    dpdrb += ob.dpdr_e;
+    dpdTb -= ob.dpdr_e * dedr / dedT;
+    dedrb -= ob.dpdr_e * dpdT / dedT;
+    dedTb += ob.dpdr_e * dpdT * dedr / (dedT * dedT);
+    const double eb = (MODE == EOS_RE) ? 0.0 : ob.e;
+    double g4[4];
+    for (int k = 0; k < 4; ++k)
+        g4[k] = pb * o.p.d[k] + gb * o.gam1.d[k] + dpdTb * o.dpdT.d[k] + dedTb * o.dedT.d[k] + dpdrb * o.dpdr.d[k] +
+                dedrb * o.dedr.d[k] + eb * o.e.d[k];
+    double y1b, yeb;
+    if (MODE == EOS_RE) {
+        const double Tb = g4[1] + ob.T;
+        const double eT = o.e.d[1];
+        v_b += Tb / eT + ob.e;
+        rho_b += g4[0] - Tb * o.e.d[0] / eT + rb;
+        y1b = g4[2] - Tb * o.e.d[2] / eT;
+        yeb = g4[3] - Tb * o.e.d[3] / eT;
+    } else {
+        v_b += g4[1] + ob.T;
+        rho_b += g4[0] + rb;
+        y1b = g4[2];
+        yeb = g4[3];
+    }
+    abar_b += -y1b * ytot1 * ytot1 - yeb * ye / abar;
+    zbar_b += yeb / abar;
+}
+
+// ---------------------------------------------------------------------------
+// State cleaning (Source/Castro_nd.F90:69-297) on one zone.  UTEMP is only
+// ever a Newton initial guess downstream (ctoprim, estdt and compute_temp
+// re-solve for T), so its adjoint is identically zero: compute_temp is the
+// identity on the differentiable components.
+// ---------------------------------------------------------------------------
+template <int NS>
+CASTRO_HD void abar_zbar_cons_n(const NetworkDev& net, const double* u, double rhoInv, double& abar, double& zbar,
+                                double& s1, double& s2)
+{
+    s1 = 0.0; s2 = 0.0;
+    for (int n = 0; n < NS; ++n) s1 = s1 + u[UFS + n] * net.aion_inv[n];
+    for (int n = 0; n < NS; ++n) s2 = s2 + u[UFS + n] * net.zion[n] * net.aion_inv[n];
+    abar = 1.0 / (s1 * rhoInv);
+    zbar = abar * (s2 * rhoInv);
+}
+
+// adjoint of abar = 1/(s1*rinv), zbar = abar*(s2*rinv) with s1 = sum u_X ainv,
+// s2 = sum u_X z ainv: accumulates into u_b[UFS..] and rinv_b
+template <int NS>
+CASTRO_HD void abar_zbar_cons_adj(const NetworkDev& net, const double* u, double rhoInv, double abar, double s1,
+                                  double s2, double abar_b, double zbar_b, double* u_b, double& rinv_b)
+{
+    // zbar = abar * (s2 * rinv)
+    abar_b += zbar_b * (s2 * rhoInv);
+    double t2b = zbar_b * abar;            // t2 = s2*rinv
+    double s2b = t2b * rhoInv;
+    rinv_b += t2b * s2;
+    // abar = 1/(s1*rinv)
+    double t1b = -abar_b * abar * abar;    // t1 = s1*rinv
+    double s1b = t1b * rhoInv;
+    rinv_b += t1b * s1;
+    for (int n = 0; n < NS; ++n) u_b[UFS + n] += s1b * net.aion_inv[n] + s2b * net.zion[n] * net.aion_inv[n];
+}
+
+// clean_state_pt with the generic EOS (host-callable twin of clean_state_pt)
+template <int NS>
+CASTRO_HD void clean_state_pt_t(const EosTableDev& tb, const NetworkDev& net, double* u)
+{
+    EosOutT<double> r;
+    if (u[URHO] < small_dens) {
+        for (int n = 0; n < NS; ++n) u[UFS + n] = u[UFS + n] * (small_dens / u[URHO]);
+        double s1 = 0.0, s2 = 0.0;
+        for (int n = 0; n < NS; ++n) s1 = s1 + u[UFS + n] * net.aion_inv[n];
+        for (int n = 0; n < NS; ++n) s2 = s2 + u[UFS + n] * net.zion[n] * net.aion_inv[n];
+        double abar = 1.0 / (s1 / small_dens);
+        double zbar = abar * (s2 / small_dens);
+        double T = eos_solve_t<EOS_RT>(tb, small_dens, small_temp, 0.0, abar, zbar, r);
+        u[URHO] = small_dens;
+        u[UTEMP] = T;
+        u[UMX] = 0.0; u[UMY] = 0.0; u[UMZ] = 0.0;
+        u[UEINT] = small_dens * r.e;
+        u[UEDEN] = u[UEINT];
+    }
+    {
+        double rho = u[URHO];
+        for (int n = 0; n < NS; ++n) u[UFS + n] = DMAX(1.0e-30 * rho, DMIN(rho, u[UFS + n]));
+        double sum = 0.0;
+        for (int n = 0; n < NS; ++n) sum = sum + u[UFS + n];
+        for (int n = 0; n < NS; ++n) u[UFS + n] = u[UFS + n] / sum;
+    }
+    {
+        double rhoInv = 1.0 / u[URHO];
+        double Up = u[UMX] * rhoInv, Vp = u[UMY] * rhoInv, Wp = u[UMZ] * rhoInv;
+        double ke = 0.5 * (Up * Up + Vp * Vp + Wp * Wp);
+        double abar, zbar, s1, s2;
+        if (u[UEDEN] < 0.0) {
+            if (u[UEINT] < 0.0) {
+                abar_zbar_cons_n<NS>(net, u, rhoInv, abar, zbar, s1, s2);
+                eos_solve_t<EOS_RT>(tb, u[URHO], small_temp, 0.0, abar, zbar, r);
+                u[UEINT] = u[URHO] * r.e;
+            }
+            u[UEDEN] = u[UEINT] + u[URHO] * ke;
+        } else {
+            double rho_eint = u[UEDEN] - u[URHO] * ke;
+            if (rho_eint > 0.0 && rho_eint / u[UEDEN] > dual_energy_eta2) {
+                u[UEINT] = rho_eint;
+            } else if (u[UEINT] <= 0.0) {
+                abar_zbar_cons_n<NS>(net, u, rhoInv, abar, zbar, s1, s2);
+                eos_solve_t<EOS_RT>(tb, u[URHO], small_temp, 0.0, abar, zbar, r);
+                u[UEINT] = u[URHO] * r.e;
+            }
+        }
+    }
+    {
+        double rhoInv = 1.0 / u[URHO];
+        double abar, zbar, s1, s2;
+        abar_zbar_cons_n<NS>(net, u, rhoInv, abar, zbar, s1, s2);
+        double T = eos_solve_t<EOS_RE>(tb, u[URHO], u[UTEMP], u[UEINT] * rhoInv, abar, zbar, r);
+        u[UTEMP] = T;
+        u[UEINT] = u[URHO] * (u[UEINT] * rhoInv);
+    }
+}
+
+// ub: on entry the adjoint of clean_state(u0)'s output, on exit the adjoint
+// of u0 (u0 = the state before cleaning).
+template <int NS>
+CASTRO_HD void clean_state_pt_adj(const EosTableDev& tb, const NetworkDev& net, const double* u0, double* ub)
+{
+    constexpr int NV = Dims<NS>::NVAR;
+    EosOutT<double> r;
+    double u1[NV], u2[NV];
+    for (int n = 0; n < NV; ++n) u1[n] = u0[n];
+    // ---- forward: enforce_minimum_density ----
+    const bool emd = u0[URHO] < small_dens;
+    double emd_abar = 0.0, emd_zbar = 0.0, emd_s1 = 0.0, emd_s2 = 0.0, emd_T = 0.0;
+    if (emd) {
+        for (int n = 0; n < NS; ++n) u1[UFS + n] = u0[UFS + n] * (small_dens / u0[URHO]);
+        for (int n = 0; n < NS; ++n) emd_s1 = emd_s1 + u1[UFS + n] * net.aion_inv[n];
+        for (int n = 0; n < NS; ++n) emd_s2 = emd_s2 + u1[UFS + n] * net.zion[n] * net.aion_inv[n];
+        emd_abar = 1.0 / (emd_s1 / small_dens);
+        emd_zbar = emd_abar * (emd_s2 / small_dens);
+        emd_T = eos_solve_t<EOS_RT>(tb, small_dens, small_temp, 0.0, emd_abar, emd_zbar, r);
+        u1[URHO] = small_dens;
+        u1[UTEMP] = emd_T;
+        u1[UMX] = 0.0; u1[UMY] = 0.0; u1[UMZ] = 0.0;
+        u1[UEINT] = small_dens * r.e;
+        u1[UEDEN] = u1[UEINT];
+    }
+    // ---- forward: normalize_species ----
+    for (int n = 0; n < NV; ++n) u2[n] = u1[n];
+    double cl[MAX_SPEC], sum = 0.0;
+    const double rho1 = u1[URHO];
+    for (int n = 0; n < NS; ++n) {
+        cl[n] = DMAX(1.0e-30 * rho1, DMIN(rho1, u1[UFS + n]));
+        sum = sum + cl[n];
+    }
+    for (int n = 0; n < NS; ++n) u2[UFS + n] = cl[n] / sum;
+    // ---- forward: reset_internal_e (branch only) ----
+    const double rinv2 = 1.0 / u2[URHO];
+    const double Up = u2[UMX] * rinv2, Vp = u2[UMY] * rinv2, Wp = u2[UMZ] * rinv2;
+    const double ke = 0.5 * (Up * Up + Vp * Vp + Wp * Wp);
+    int rie_case;   // 0 unchanged, 1 ei = E - rho ke, 2 ei from EOS(rt) (E >= 0), 3 E<0: E = ei + rho ke, 4 E<0 and ei from EOS
+    if (u2[UEDEN] < 0.0) {
+        rie_case = (u2[UEINT] < 0.0) ? 4 : 3;
+    } else {
+        double rho_eint = u2[UEDEN] - u2[URHO] * ke;
+        if (rho_eint > 0.0 && rho_eint / u2[UEDEN] > dual_energy_eta2) rie_case = 1;
+        else if (u2[UEINT] <= 0.0) rie_case = 2;
+        else rie_case = 0;
+    }
+
+    // ---- reverse: compute_temp (identity on the differentiable components) ----
+    ub[UTEMP] = 0.0;
+    // ---- reverse: reset_internal_e ----
+    double rinv_b = 0.0, ke_b = 0.0;
+    if (rie_case == 1) {
+        double eib = ub[UEINT];
+        ub[UEINT] = 0.0;
+        ub[UEDEN] += eib;
+        ub[URHO] -= eib * ke;
+        ke_b -= eib * u2[URHO];
+    } else if (rie_case == 3 || rie_case == 4) {
+        double Eb = ub[UEDEN];
+        ub[UEDEN] = 0.0;
+        ub[UEINT] += Eb;                 // E = ei + rho ke (ei after a possible reset)
+        ub[URHO] += Eb * ke;
+        ke_b += Eb * u2[URHO];
+    }
+    if (rie_case == 2 || rie_case == 4) {
+        // ei = rho * e(rho, small_temp, abar, zbar)
+        double eib = ub[UEINT];
+        ub[UEINT] = 0.0;
+        double abar, zbar, s1, s2;
+        abar_zbar_cons_n<NS>(net, u2, rinv2, abar, zbar, s1, s2);
+        eos_solve_t<EOS_RT>(tb, u2[URHO], small_temp, 0.0, abar, zbar, r);
+        ub[URHO] += eib * r.e;
+        EosBar ob{0.0, 0.0, eib * u2[URHO], 0.0, 0.0, 0.0, 0.0};
+        double rb = 0.0, Tb = 0.0, ab = 0.0, zb = 0.0;
+        eos_vjp<EOS_RT>(tb, u2[URHO], small_temp, abar, zbar, ob, rb, Tb, ab, zb);
+        ub[URHO] += rb;
+        abar_zbar_cons_adj<NS>(net, u2, rinv2, abar, s1, s2, ab, zb, ub, rinv_b);
+    }
+    if (ke_b != 0.0) {
+        double Ub = ke_b * Up, Vb = ke_b * Vp, Wb = ke_b * Wp;
+        ub[UMX] += Ub * rinv2; rinv_b += Ub * u2[UMX];
+        ub[UMY] += Vb * rinv2; rinv_b += Vb * u2[UMY];
+        ub[UMZ] += Wb * rinv2; rinv_b += Wb * u2[UMZ];
+    }
+    ub[URHO] -= rinv_b * rinv2 * rinv2;
+    // ---- reverse: normalize_species ----
+    {
+        double sumb = 0.0;
+        for (int n = 0; n < NS; ++n) sumb -= ub[UFS + n] * cl[n] / (sum * sum);
+        for (int n = 0; n < NS; ++n) {
+            double clb = ub[UFS + n] / sum + sumb;
+            ub[UFS + n] = 0.0;
+            double inner = DMIN(rho1, u1[UFS + n]);
+            if (1.0e-30 * rho1 > inner) {
+                ub[URHO] += 1.0e-30 * clb;
+            } else if (rho1 < u1[UFS + n]) {
+                ub[URHO] += clb;
+            } else {
+                ub[UFS + n] += clb;
+            }
+        }
+    }
+    // ---- reverse: enforce_minimum_density ----
+    if (emd) {
+        // outputs: rho = const, m = 0, ei = E = small_dens * e_rt(abar, zbar), X' = X * small/rho
+        double eb = (ub[UEINT] + ub[UEDEN]) * small_dens;
+        ub[UEINT] = 0.0; ub[UEDEN] = 0.0; ub[URHO] = 0.0;
+        ub[UMX] = 0.0; ub[UMY] = 0.0; ub[UMZ] = 0.0;
+        EosBar ob{0.0, 0.0, eb, 0.0, 0.0, 0.0, 0.0};
+        double rb = 0.0, Tb = 0.0, ab = 0.0, zb = 0.0;
+        eos_vjp<EOS_RT>(tb, small_dens, small_temp, emd_abar, emd_zbar, ob, rb, Tb, ab, zb);
+        // abar = 1/(s1/small), zbar = abar*(s2/small)
+        ab += zb * (emd_s2 / small_dens);
+        double s2b = zb * emd_abar / small_dens;
+        double s1b = -ab * emd_abar * emd_abar / small_dens;
+        double rho0b = 0.0;
+        for (int n = 0; n < NS; ++n) {
+            double x1b = ub[UFS + n] + s1b * net.aion_inv[n] + s2b * net.zion[n] * net.aion_inv[n];
+            ub[UFS + n] = x1b * (small_dens / u0[URHO]);
+            rho0b -= x1b * u0[UFS + n] * small_dens / (u0[URHO] * u0[URHO]);
+        }
+        ub[URHO] = rho0b;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ctoprim (Source/Castro_hydro_nd.F90:115-164) on one zone
+// ---------------------------------------------------------------------------
+template <int NS>
+CASTRO_HD void ctoprim_pt_t(const EosTableDev& tb, const NetworkDev& net, const double* u, double* q, double* qaux)
+{
+    q[QRHO] = u[URHO];
+    double rhoinv = 1.0 / q[QRHO];
+    q[QU] = u[UMX] * rhoinv;
+    q[QV] = u[UMY] * rhoinv;
+    q[QW] = u[UMZ] * rhoinv;
+    double kineng = 0.5 * q[QRHO] * (q[QU] * q[QU] + q[QV] * q[QV] + q[QW] * q[QW]);
+    if ((u[UEDEN] - kineng) / u[UEDEN] > dual_energy_eta1) q[QREINT] = (u[UEDEN] - kineng) * rhoinv;
+    else q[QREINT] = u[UEINT] * rhoinv;
+    for (int n = 0; n < NS; ++n) q[QFS + n] = u[UFS + n] * rhoinv;
+    double s1 = 0.0, s2 = 0.0;
+    for (int n = 0; n < NS; ++n) s1 = s1 + q[QFS + n] * net.aion_inv[n];
+    for (int n = 0; n < NS; ++n) s2 = s2 + q[QFS + n] * net.zion[n] * net.aion_inv[n];
+    double abar = 1.0 / s1;
+    double zbar = abar * s2;
+    EosOutT<double> r;
+    double T = eos_solve_t<EOS_RE>(tb, q[QRHO], u[UTEMP], q[QREINT], abar, zbar, r);
+    q[QTEMP] = T;
+    q[QREINT] = q[QREINT] * q[QRHO];
+    q[QPRES] = r.p;
+    q[QGAME] = q[QPRES] / q[QREINT] + 1.0;
+    qaux[QDPDR] = r.dpdr - r.dpdT * r.dedr / r.dedT;
+    qaux[QDPDE] = r.dpdT / r.dedT;
+    qaux[QGAMC] = r.gam1;
+    qaux[QC] = sqrt(r.gam1 * r.p / q[QRHO]);
+}
+
+template <int NS>
+CASTRO_HD void ctoprim_pt_adj(const EosTableDev& tb, const NetworkDev& net, const double* u, const double* qb,
+                              const double* qab, double* ub)
+{
+    const double rho = u[URHO];
+    const double rhoinv = 1.0 / rho;
+    const double vx = u[UMX] * rhoinv, vy = u[UMY] * rhoinv, vz = u[UMZ] * rhoinv;
+    const double kineng = 0.5 * rho * (vx * vx + vy * vy + vz * vz);
+    const bool brA = (u[UEDEN] - kineng) / u[UEDEN] > dual_energy_eta1;
+    const double e = brA ? (u[UEDEN] - kineng) * rhoinv : u[UEINT] * rhoinv;
+    double s1 = 0.0, s2 = 0.0;
+    for (int n = 0; n < NS; ++n) s1 = s1 + (u[UFS + n] * rhoinv) * net.aion_inv[n];
+    for (int n = 0; n < NS; ++n) s2 = s2 + (u[UFS + n] * rhoinv) * net.zion[n] * net.aion_inv[n];
+    const double abar = 1.0 / s1, zbar = abar * s2;
+    EosOutT<double> r;
+    const double T = eos_solve_t<EOS_RE>(tb, rho, u[UTEMP], e, abar, zbar, r);
+    const double rhoe_q = e * rho;
+    const double p = r.p;
+
+    double rhob = qb[QRHO];
+    const double gameb = qb[QGAME];
+    const double pb = qb[QPRES] + gameb / rhoe_q;
+    const double rhoe_qb = qb[QREINT] - gameb * p / (rhoe_q * rhoe_q);
+    double eb = rhoe_qb * rho;
+    rhob += rhoe_qb * e;
+    EosBar ob{qb[QTEMP], pb, 0.0, qab[QGAMC], qab[QC], qab[QDPDE], qab[QDPDR]};
+    double ab = 0.0, zb = 0.0;
+    eos_vjp<EOS_RE>(tb, rho, T, abar, zbar, ob, rhob, eb, ab, zb);
+    // zbar = abar * s2, abar = 1 / s1
+    ab += zb * s2;
+    const double s2b = zb * abar;
+    const double s1b = -ab * abar * abar;
+    double rinvb = 0.0;
+    for (int n = 0; n < NS; ++n) {
+        double Xb = s1b * net.aion_inv[n] + s2b * net.zion[n] * net.aion_inv[n] + qb[QFS + n];
+        ub[UFS + n] += Xb * rhoinv;
+        rinvb += Xb * u[UFS + n];
+    }
+    double keb = 0.0;
+    if (brA) {
+        ub[UEDEN] += eb * rhoinv;
+        keb = -eb * rhoinv;
+        rinvb += eb * (u[UEDEN] - kineng);
+    } else {
+        ub[UEINT] += eb * rhoinv;
+        rinvb += eb * u[UEINT];
+    }
+    rhob += 0.5 * (vx * vx + vy * vy + vz * vz) * keb;
+    const double vxb = qb[QU] + rho * vx * keb, vyb = qb[QV] + rho * vy * keb, vzb = qb[QW] + rho * vz * keb;
+    ub[UMX] += vxb * rhoinv; rinvb += vxb * u[UMX];
+    ub[UMY] += vyb * rhoinv; rinvb += vyb * u[UMY];
+    ub[UMZ] += vzb * rhoinv; rinvb += vzb * u[UMZ];
+    rhob -= rinvb * rhoinv * rhoinv;
+    ub[URHO] += rhob;
+}
+
+// ---------------------------------------------------------------------------
+// estdt on one zone (Source/timestep.F90:446-468): value and adjoint
+// ---------------------------------------------------------------------------
+template <int NS>
+CASTRO_HD double estdt_pt_t(const EosTableDev& tb, const NetworkDev& net, const double* u, const double* dx)
+{
+    const double rhoInv = 1.0 / u[URHO];
+    double abar, zbar, s1, s2;
+    abar_zbar_cons_n<NS>(net, u, rhoInv, abar, zbar, s1, s2);
+    EosOutT<double> r;
+    eos_solve_t<EOS_RE>(tb, u[URHO], u[UTEMP], u[UEINT] * rhoInv, abar, zbar, r);
+    const double c = sqrt(r.gam1 * r.p / u[URHO]);
+    double dt1 = dx[0] / (c + fabs(u[UMX] * rhoInv));
+    double dt2 = dx[1] / (c + fabs(u[UMY] * rhoInv));
+    double dt3 = dx[2] / (c + fabs(u[UMZ] * rhoInv));
+    return DMIN(DMIN(dt1, dt2), dt3);
+}
+
+template <int NS>
+CASTRO_HD void estdt_pt_adj(const EosTableDev& tb, const NetworkDev& net, const double* u, const double* dx,
+                            double dtb, double* ub)
+{
+    const double rho = u[URHO], rhoInv = 1.0 / rho;
+    double abar, zbar, s1, s2;
+    abar_zbar_cons_n<NS>(net, u, rhoInv, abar, zbar, s1, s2);
+    EosOutT<double> r;
+    const double e = u[UEINT] * rhoInv;
+    const double T = eos_solve_t<EOS_RE>(tb, rho, u[UTEMP], e, abar, zbar, r);
+    const double c = sqrt(r.gam1 * r.p / rho);
+    double v[3] = {u[UMX] * rhoInv, u[UMY] * rhoInv, u[UMZ] * rhoInv};
+    double dtd[3];
+    for (int d = 0; d < 3; ++d) dtd[d] = dx[d] / (c + fabs(v[d]));
+    const int a = (dtd[0] < dtd[1]) ? 0 : 1;
+    const int m = (dtd[a] < dtd[2]) ? a : 2;
+    const double den = c + fabs(v[m]);
+    const double denb = -dtb * dx[m] / (den * den);
+    double rinvb = 0.0;
+    const double vb = denb * (v[m] > 0.0 ? 1.0 : (v[m] < 0.0 ? -1.0 : 0.0));
+    ub[UMX + m] += vb * rhoInv;
+    rinvb += vb * u[UMX + m];
+    EosBar ob{0.0, 0.0, 0.0, 0.0, denb, 0.0, 0.0};
+    double rb = 0.0, eb = 0.0, ab = 0.0, zb = 0.0;
+    eos_vjp<EOS_RE>(tb, rho, T, abar, zbar, ob, rb, eb, ab, zb);
+    ub[UEINT] += eb * rhoInv;
+    rinvb += eb * u[UEINT];
+    abar_zbar_cons_adj<NS>(net, u, rhoInv, abar, s1, s2, ab, zb, ub, rinvb);
+    ub[URHO] += rb - rinvb * rhoInv * rhoInv;
+}
+
+// ---------------------------------------------------------------------------
+// PPM (Source/ppm.F90)
+// ---------------------------------------------------------------------------
+// adjoint of vl_slope(sm1, s0, sp1) for output adjoint rb
+CASTRO_HD void vl_slope_adj(double sm1, double s0, double sp1, double rb, double& sm1b, double& s0b, double& sp1b)
+{
+    double dsl = 2.0 * (s0 - sm1);
+    double dsr = 2.0 * (sp1 - s0);
+    if (!(dsl * dsr > 0.0)) return;
+    double dsc = 0.5 * (sp1 - sm1);
+    double adsc = fabs(dsc), adsl = fabs(dsl), adsr = fabs(dsr);
+    double m1 = (adsc < adsl) ? adsc : adsl;
+    // the selected argument has the sign of dsc (all three agree), so its
+    // adjoint is rb itself
+    if (m1 < adsr) {
+        if (adsc < adsl) { sp1b += 0.5 * rb; sm1b -= 0.5 * rb; }
+        else { s0b += 2.0 * rb; sm1b -= 2.0 * rb; }
+    } else {
+        sp1b += 2.0 * rb; s0b -= 2.0 * rb;
+    }
+}
+
+// adjoint of ppm_reconstruct(s[0..4], flatn) -> (sm, sp)
+CASTRO_HD void ppm_reconstruct_adj(const double* s, double flatn, double smb_in, double spb_in, double* sb,
+                                   double& flatnb)
+{
+    double a = vl_slope(s[0], s[1], s[2]);
+    double b = vl_slope(s[1], s[2], s[3]);
+    double c = vl_slope(s[2], s[3], s[4]);
+    double sm0 = 0.5 * (s[2] + s[1]) - SIXTH * (b - a);
+    double mn = DMIN(s[2], s[1]), mx = DMAX(s[2], s[1]);
+    double sm1 = DMAX(sm0, mn);
+    double sm2 = DMIN(sm1, mx);
+    double sp0 = 0.5 * (s[3] + s[2]) - SIXTH * (c - b);
+    double mn2 = DMIN(s[3], s[2]), mx2 = DMAX(s[3], s[2]);
+    double sp1 = DMAX(sp0, mn2);
+    double sp2 = DMIN(sp1, mx2);
+    double sm3 = flatn * sm2 + (1.0 - flatn) * s[2];
+    double sp3 = flatn * sp2 + (1.0 - flatn) * s[2];
+    double sm3b = 0.0, sp3b = 0.0;
+    if ((sp3 - s[2]) * (s[2] - sm3) <= 0.0) {
+        sb[2] += smb_in + spb_in;
+    } else if (fabs(sp3 - s[2]) >= 2.0 * fabs(sm3 - s[2])) {
+        sb[2] += 3.0 * spb_in;
+        sm3b = smb_in - 2.0 * spb_in;
+    } else if (fabs(sm3 - s[2]) >= 2.0 * fabs(sp3 - s[2])) {
+        sb[2] += 3.0 * smb_in;
+        sp3b = spb_in - 2.0 * smb_in;
+    } else {
+        sm3b = smb_in;
+        sp3b = spb_in;
+    }
+    double sm2b = flatn * sm3b, sp2b = flatn * sp3b;
+    flatnb += (sm2 - s[2]) * sm3b + (sp2 - s[2]) * sp3b;
+    sb[2] += (1.0 - flatn) * (sm3b + sp3b);
+    // sp2 = min(sp1, mx2), sp1 = max(sp0, mn2)
+    double sp1b = 0.0, sp0b = 0.0;
+    if (sp1 < mx2) sp1b = sp2b;
+    else { if (s[3] > s[2]) sb[3] += sp2b; else sb[2] += sp2b; }
+    if (sp0 > mn2) sp0b = sp1b;
+    else { if (s[3] < s[2]) sb[3] += sp1b; else sb[2] += sp1b; }
+    double sm1b = 0.0, sm0b = 0.0;
+    if (sm1 < mx) sm1b = sm2b;
+    else { if (s[2] > s[1]) sb[2] += sm2b; else sb[1] += sm2b; }
+    if (sm0 > mn) sm0b = sm1b;
+    else { if (s[2] < s[1]) sb[2] += sm1b; else sb[1] += sm1b; }
+    double ab = 0.0, bb = 0.0, cb = 0.0;
+    sb[3] += 0.5 * sp0b; sb[2] += 0.5 * sp0b; cb -= SIXTH * sp0b; bb += SIXTH * sp0b;
+    sb[2] += 0.5 * sm0b; sb[1] += 0.5 * sm0b; bb -= SIXTH * sm0b; ab += SIXTH * sm0b;
+    vl_slope_adj(s[2], s[3], s[4], cb, sb[2], sb[3], sb[4]);
+    vl_slope_adj(s[1], s[2], s[3], bb, sb[1], sb[2], sb[3]);
+    vl_slope_adj(s[0], s[1], s[2], ab, sb[0], sb[1], sb[2]);
+}
+
+// adjoint of ppm_int_wave(sm, sp, s6, speed, dtdx) -> (Ip, Im)
+CASTRO_HD void ppm_int_wave_adj(double sm, double sp, double s6, double speed, double dtdx, double Ipb, double Imb,
+                                double& smb, double& spb, double& s6b, double& speedb, double& dtdxb)
+{
+    double sigma = fabs(speed) * dtdx;
+    double sigmab = 0.0;
+    if (speed <= 0.0) {
+        spb += Ipb;
+        double w = sp - sm + (1.0 - TWO3RD * sigma) * s6;
+        smb += Imb;
+        sigmab += 0.5 * w * Imb;
+        double wb = 0.5 * sigma * Imb;
+        spb += wb; smb -= wb;
+        s6b += (1.0 - TWO3RD * sigma) * wb;
+        sigmab -= TWO3RD * s6 * wb;
+        speedb -= sigmab * dtdx;
+    } else {
+        smb += Imb;
+        double w = sp - sm - (1.0 - TWO3RD * sigma) * s6;
+        spb += Ipb;
+        sigmab -= 0.5 * w * Ipb;
+        double wb = -0.5 * sigma * Ipb;
+        spb += wb; smb -= wb;
+        s6b -= (1.0 - TWO3RD * sigma) * wb;
+        sigmab += TWO3RD * s6 * wb;
+        speedb += sigmab * dtdx;
+    }
+    dtdxb += sigmab * fabs(speed);
+}
+
+// adjoint of trace_project (un and cc only select branches)
+CASTRO_HD void trace_project_adj(const double I[3][4], double gam, double un, double cc, bool plus,
+                                 double rho_ob, double un_ob, double rhoe_ob, double p_ob, double Ib[3][4], double& gamb)
+{
+    const int wr = plus ? 0 : 2;
+    const double rho_ref0 = I[wr][0], un_ref = I[wr][1], p_ref0 = I[wr][2], rhoe_ref = I[wr][3];
+    const double rho_ref = DMAX(rho_ref0, small_dens);
+    const double rri = 1.0 / rho_ref;
+    const double p_ref = DMAX(p_ref0, small_pres);
+    const double csq = gam * p_ref * rri;
+    const double ccr = sqrt(csq);
+    const double cci = 1.0 / ccr;
+    const double h = (p_ref + rhoe_ref) * rri;
+    const double dum = un_ref - I[0][1], dptotm = p_ref - I[0][2];
+    const double drho = rho_ref - I[1][0], dptot = p_ref - I[1][2];
+    const double dup = un_ref - I[2][1], dptotp = p_ref - I[2][2];
+    const double M = dptotm * rri * cci - dum;
+    const double P = dptotp * rri * cci + dup;
+    const double am = 0.5 * M * rho_ref * cci;
+    const double ap = 0.5 * P * rho_ref * cci;
+    const double a0r = drho - dptot / csq;
+    double fm, fp, f0;   // multipliers of the projected amplitudes (0 or -1)
+    if (plus) {
+        fm = (un - cc > 0.0) ? 0.0 : -1.0;
+        fp = (un + cc > 0.0) ? 0.0 : -1.0;
+        f0 = (un > 0.0) ? 0.0 : -1.0;
+    } else {
+        fm = (un - cc > 0.0) ? -1.0 : 0.0;
+        fp = (un + cc > 0.0) ? -1.0 : 0.0;
+        f0 = (un > 0.0) ? -1.0 : 0.0;
+    }
+    const double amp = fm * am, app = fp * ap, a0rp = f0 * a0r;
+    const double X = rho_ref + app + amp + a0rp;
+    const double Y = p_ref + (app + amp) * csq;
+    const double Xb = (small_dens > X) ? 0.0 : rho_ob;
+    const double Yb = (small_pres > Y) ? 0.0 : p_ob;
+    double rho_refb = Xb, appb = Xb, ampb = Xb, a0rpb = Xb;
+    double un_refb = un_ob;
+    const double t = app - amp;
+    appb += un_ob * ccr * rri;
+    ampb -= un_ob * ccr * rri;
+    double ccrb = un_ob * t * rri;
+    double rrib = un_ob * t * ccr;
+    double rhoe_refb = rhoe_ob;
+    appb += rhoe_ob * h;
+    ampb += rhoe_ob * h;
+    double hb = rhoe_ob * (app + amp);
+    double a0epb = rhoe_ob;
+    double p_refb = Yb;
+    appb += Yb * csq;
+    ampb += Yb * csq;
+    double csqb = Yb * (app + amp);
+    const double amb = fm * ampb, apb = fp * appb, a0rb = f0 * a0rpb, a0eb = f0 * a0epb;
+    // a0e = drhoe - dptot*h/csq
+    double drhoeb = a0eb;
+    double dptotb = -a0eb * h / csq;
+    hb -= a0eb * dptot / csq;
+    csqb += a0eb * dptot * h / (csq * csq);
+    // a0r = drho - dptot/csq
+    double drhob = a0rb;
+    dptotb -= a0rb / csq;
+    csqb += a0rb * dptot / (csq * csq);
+    // ap = 0.5 * P * rho_ref * cci
+    double Pb = 0.5 * rho_ref * cci * apb;
+    rho_refb += 0.5 * P * cci * apb;
+    double ccib = 0.5 * P * rho_ref * apb;
+    double dptotpb = Pb * rri * cci;
+    rrib += Pb * dptotp * cci;
+    ccib += Pb * dptotp * rri;
+    double dupb = Pb;
+    // am = 0.5 * M * rho_ref * cci
+    double Mb = 0.5 * rho_ref * cci * amb;
+    rho_refb += 0.5 * M * cci * amb;
+    ccib += 0.5 * M * rho_ref * amb;
+    double dptotmb = Mb * rri * cci;
+    rrib += Mb * dptotm * cci;
+    ccib += Mb * dptotm * rri;
+    double dumb = -Mb;
+    // differences
+    un_refb += dumb; Ib[0][1] -= dumb;
+    p_refb += dptotmb; Ib[0][2] -= dptotmb;
+    rho_refb += drhob; Ib[1][0] -= drhob;
+    p_refb += dptotb; Ib[1][2] -= dptotb;
+    rhoe_refb += drhoeb; Ib[1][3] -= drhoeb;
+    un_refb += dupb; Ib[2][1] -= dupb;
+    p_refb += dptotpb; Ib[2][2] -= dptotpb;
+    // h = (p_ref + rhoe_ref) * rri
+    p_refb += hb * rri;
+    rhoe_refb += hb * rri;
+    rrib += hb * (p_ref + rhoe_ref);
+    // cci = 1/ccr, ccr = sqrt(csq)
+    ccrb -= ccib * cci * cci;
+    csqb += ccrb * 0.5 / ccr;
+    // csq = gam * p_ref * rri
+    gamb += csqb * p_ref * rri;
+    p_refb += csqb * gam * rri;
+    rrib += csqb * gam * p_ref;
+    rho_refb -= rrib * rri * rri;
+    if (p_ref0 > small_pres) Ib[wr][2] += p_refb;
+    if (rho_ref0 > small_dens) Ib[wr][0] += rho_refb;
+    Ib[wr][1] += un_refb;
+    Ib[wr][3] += rhoe_refb;
+}
+
+// Sink concept for the stencil adjoints: q(i,j,k,n,v) adds v to the adjoint of
+// q component n of zone (i,j,k); gamc(i,j,k,v) / c(i,j,k,v) likewise for qaux.
+
+// adjoint of trace_zone<NS,D>: qpb / qmb are the adjoints of the plus state on
+// face i and of the minus state on face i+1 (compact layout; a null pointer
+// stands for a face the forward did not write).  Returns the adjoint of flatn
+// and accumulates that of dtdx.
+template <int NS, int D, class L, class K>
+CASTRO_HD double trace_zone_adj(const L& ld, const K& sink, int i, int j, int k, double dtdx, double flatn,
+                                const double* qpb, const double* qmb, double& dtdxb)
+{
+    constexpr int ex = D == 0, ey = D == 1, ez = D == 2;
+    constexpr int qun = QU + D;
+    constexpr int qut = QU + (D == 0 ? 1 : D == 1 ? 2 : 0);
+    constexpr int qutt = QU + (D == 0 ? 2 : D == 1 ? 0 : 1);
+    const double cc = ld.c(i, j, k);
+    const double un = ld.q(i, j, k, qun);
+    const double speeds[3] = {un - cc, un, un + cc};
+    constexpr int vars[4] = {QRHO, qun, QPRES, QREINT};
+    double s[5], sm, sp;
+    double Ip[3][4], Im[3][4];
+    for (int v = 0; v < 4; ++v) {
+        for (int m = -2; m <= 2; ++m) s[m + 2] = ld.q(i + m * ex, j + m * ey, k + m * ez, vars[v]);
+        ppm_reconstruct(s, flatn, sm, sp);
+        double s6 = 6.0 * s[2] - 3.0 * (sm + sp);
+        for (int w = 0; w < 3; ++w) ppm_int_wave(sm, sp, s6, speeds[w], dtdx, Ip[w][v], Im[w][v]);
+    }
+    double gm0, gp2;
+    {
+        for (int m = -2; m <= 2; ++m) s[m + 2] = ld.gamc(i + m * ex, j + m * ey, k + m * ez);
+        ppm_reconstruct(s, flatn, sm, sp);
+        double s6 = 6.0 * s[2] - 3.0 * (sm + sp);
+        double gp0, gm2;
+        ppm_int_wave(sm, sp, s6, speeds[0], dtdx, gp0, gm0);
+        ppm_int_wave(sm, sp, s6, speeds[2], dtdx, gp2, gm2);
+    }
+    // projections
+    double Ipb[3][4] = {}, Imb[3][4] = {};
+    double gm0b = 0.0, gp2b = 0.0;
+    if (qpb) trace_project_adj(Im, gm0, un, cc, true, qpb[SRHO], qpb[SU + D], qpb[SREI], qpb[SPRES], Imb, gm0b);
+    if (qmb) trace_project_adj(Ip, gp2, un, cc, false, qmb[SRHO], qmb[SU + D], qmb[SREI], qmb[SPRES], Ipb, gp2b);
+    double unb = 0.0, ccb = 0.0, flatnb = 0.0;
+    double sbv[5];
+    auto scatter_q = [&](int n) {
+        for (int m = -2; m <= 2; ++m)
+            if (sbv[m + 2] != 0.0) sink.q(i + m * ex, j + m * ey, k + m * ez, n, sbv[m + 2]);
+    };
+    // reconstructed variables feeding the projections
+    for (int v = 0; v < 4; ++v) {
+        for (int m = -2; m <= 2; ++m) s[m + 2] = ld.q(i + m * ex, j + m * ey, k + m * ez, vars[v]);
+        ppm_reconstruct(s, flatn, sm, sp);
+        double s6 = 6.0 * s[2] - 3.0 * (sm + sp);
+        double smb = 0.0, spb = 0.0, s6b = 0.0;
+        for (int w = 0; w < 3; ++w) {
+            double speedb = 0.0;
+            ppm_int_wave_adj(sm, sp, s6, speeds[w], dtdx, Ipb[w][v], Imb[w][v], smb, spb, s6b, speedb, dtdxb);
+            unb += speedb;
+            ccb += (w == 0) ? -speedb : (w == 2 ? speedb : 0.0);
+        }
+        for (int m = 0; m < 5; ++m) sbv[m] = 0.0;
+        sbv[2] += 6.0 * s6b;
+        smb -= 3.0 * s6b;
+        spb -= 3.0 * s6b;
+        ppm_reconstruct_adj(s, flatn, smb, spb, sbv, flatnb);
+        scatter_q(vars[v]);
+    }
+    // transverse velocities: u wave only
+    for (int t = 0; t < 2; ++t) {
+        const int n = t == 0 ? qut : qutt;
+        const double Ipb1 = qmb ? qmb[n - QU + SU] : 0.0;
+        const double Imb1 = qpb ? qpb[n - QU + SU] : 0.0;
+        if (Ipb1 == 0.0 && Imb1 == 0.0) continue;
+        for (int m = -2; m <= 2; ++m) s[m + 2] = ld.q(i + m * ex, j + m * ey, k + m * ez, n);
+        ppm_reconstruct(s, flatn, sm, sp);
+        double s6 = 6.0 * s[2] - 3.0 * (sm + sp);
+        double smb = 0.0, spb = 0.0, s6b = 0.0, speedb = 0.0;
+        ppm_int_wave_adj(sm, sp, s6, speeds[1], dtdx, Ipb1, Imb1, smb, spb, s6b, speedb, dtdxb);
+        unb += speedb;
+        for (int m = 0; m < 5; ++m) sbv[m] = 0.0;
+        sbv[2] += 6.0 * s6b;
+        smb -= 3.0 * s6b;
+        spb -= 3.0 * s6b;
+        ppm_reconstruct_adj(s, flatn, smb, spb, sbv, flatnb);
+        scatter_q(n);
+    }
+    // gamma_c: u-c wave feeds the plus state, u+c the minus state
+    if (gm0b != 0.0 || gp2b != 0.0) {
+        for (int m = -2; m <= 2; ++m) s[m + 2] = ld.gamc(i + m * ex, j + m * ey, k + m * ez);
+        ppm_reconstruct(s, flatn, sm, sp);
+        double s6 = 6.0 * s[2] - 3.0 * (sm + sp);
+        double smb = 0.0, spb = 0.0, s6b = 0.0, speedb0 = 0.0, speedb2 = 0.0;
+        ppm_int_wave_adj(sm, sp, s6, speeds[0], dtdx, 0.0, gm0b, smb, spb, s6b, speedb0, dtdxb);
+        ppm_int_wave_adj(sm, sp, s6, speeds[2], dtdx, gp2b, 0.0, smb, spb, s6b, speedb2, dtdxb);
+        unb += speedb0 + speedb2;
+        ccb += speedb2 - speedb0;
+        for (int m = 0; m < 5; ++m) sbv[m] = 0.0;
+        sbv[2] += 6.0 * s6b;
+        smb -= 3.0 * s6b;
+        spb -= 3.0 * s6b;
+        ppm_reconstruct_adj(s, flatn, smb, spb, sbv, flatnb);
+        for (int m = -2; m <= 2; ++m)
+            if (sbv[m + 2] != 0.0) sink.gamc(i + m * ex, j + m * ey, k + m * ez, sbv[m + 2]);
+    }
+    // species: u wave only
+    for (int n = 0; n < NS; ++n) {
+        const double Ipb1 = qmb ? qmb[SX + n] : 0.0;
+        const double Imb1 = qpb ? qpb[SX + n] : 0.0;
+        if (Ipb1 == 0.0 && Imb1 == 0.0) continue;
+        for (int m = -2; m <= 2; ++m) s[m + 2] = ld.q(i + m * ex, j + m * ey, k + m * ez, QFS + n);
+        ppm_reconstruct(s, flatn, sm, sp);
+        double s6 = 6.0 * s[2] - 3.0 * (sm + sp);
+        double smb = 0.0, spb = 0.0, s6b = 0.0, speedb = 0.0;
+        ppm_int_wave_adj(sm, sp, s6, speeds[1], dtdx, Ipb1, Imb1, smb, spb, s6b, speedb, dtdxb);
+        unb += speedb;
+        for (int m = 0; m < 5; ++m) sbv[m] = 0.0;
+        sbv[2] += 6.0 * s6b;
+        smb -= 3.0 * s6b;
+        spb -= 3.0 * s6b;
+        ppm_reconstruct_adj(s, flatn, smb, spb, sbv, flatnb);
+        scatter_q(QFS + n);
+    }
+    if (unb != 0.0) sink.q(i, j, k, qun, unb);
+    if (ccb != 0.0) sink.c(i, j, k, ccb);
+    return flatnb;
+}
+
+// adjoint of uflatten(ld, i, j, k): scatters the pressure adjoints
+template <class L, class K>
+CASTRO_HD void uflatten_adj(const L& ld, const K& sink, int i, int j, int k, double flatnb)
+{
+    if (flatnb == 0.0) return;
+    const double shktst = 0.33, zcut1 = 0.75, zcut2 = 0.85;
+    const double dzcut = 1.0 / (zcut2 - zcut1);
+    double flatn = 1.0;
+    int sel_dir = -1, sel_term = 0, sel_s = 0;
+    for (int idir = 0; idir < 3; ++idir) {
+        const int ex = idir == 0, ey = idir == 1, ez = idir == 2;
+        const int qun = QU + idir;
+        double pr = ld.q(i + ex, j + ey, k + ez, QPRES);
+        double pl = ld.q(i - ex, j - ey, k - ez, QPRES);
+        double dp2 = ld.q(i + 2 * ex, j + 2 * ey, k + 2 * ez, QPRES) - ld.q(i - 2 * ex, j - 2 * ey, k - 2 * ez, QPRES);
+        double du = ld.q(i + ex, j + ey, k + ez, qun) - ld.q(i - ex, j - ey, k - ez, qun);
+        double dp = pr - pl;
+        int s = (dp > 0.0) ? -1 : 1;
+        double denom = DMAX(small_pres, fabs(dp2));
+        double zeta = fabs(dp) * (1.0 / denom);
+        double z = DMIN(1.0, DMAX(0.0, dzcut * (zeta - zcut1)));
+        double tst = (du <= 0.0) ? 1.0 : 0.0;
+        double chi = (fabs(dp) > shktst * DMIN(pr, pl)) ? tst : 0.0;
+        pr = ld.q(i + (1 + s) * ex, j + (1 + s) * ey, k + (1 + s) * ez, QPRES);
+        pl = ld.q(i + (s - 1) * ex, j + (s - 1) * ey, k + (s - 1) * ez, QPRES);
+        dp2 = ld.q(i + (2 + s) * ex, j + (2 + s) * ey, k + (2 + s) * ez, QPRES)
+            - ld.q(i + (s - 2) * ex, j + (s - 2) * ey, k + (s - 2) * ez, QPRES);
+        du = ld.q(i + (1 + s) * ex, j + (1 + s) * ey, k + (1 + s) * ez, qun)
+           - ld.q(i + (s - 1) * ex, j + (s - 1) * ey, k + (s - 1) * ez, qun);
+        dp = pr - pl;
+        denom = DMAX(small_pres, fabs(dp2));
+        zeta = fabs(dp) * (1.0 / denom);
+        double z2 = DMIN(1.0, DMAX(0.0, dzcut * (zeta - zcut1)));
+        tst = (du <= 0.0) ? 1.0 : 0.0;
+        double chi2 = (fabs(dp) > shktst * DMIN(pr, pl)) ? tst : 0.0;
+        double a = chi2 * z2, b = chi * z;
+        double t = 1.0 - DMAX(a, b);
+        if (!(flatn < t)) {   // DMIN(flatn, t) takes t
+            flatn = t;
+            sel_dir = idir;
+            sel_term = (a > b) ? 2 : 1;
+            sel_s = s;
+        }
+    }
+    if (sel_dir < 0) return;
+    // recompute the selected term: -d(chi*z) with chi in {0,1}
+    const int ex = sel_dir == 0, ey = sel_dir == 1, ez = sel_dir == 2;
+    const int o = (sel_term == 2) ? sel_s : 0;   // stencil shift of the selected term
+    const double pr = ld.q(i + (1 + o) * ex, j + (1 + o) * ey, k + (1 + o) * ez, QPRES);
+    const double pl = ld.q(i + (o - 1) * ex, j + (o - 1) * ey, k + (o - 1) * ez, QPRES);
+    const double p2r = ld.q(i + (2 + o) * ex, j + (2 + o) * ey, k + (2 + o) * ez, QPRES);
+    const double p2l = ld.q(i + (o - 2) * ex, j + (o - 2) * ey, k + (o - 2) * ez, QPRES);
+    const double du = ld.q(i + (1 + o) * ex, j + (1 + o) * ey, k + (1 + o) * ez, QU + sel_dir)
+                    - ld.q(i + (o - 1) * ex, j + (o - 1) * ey, k + (o - 1) * ez, QU + sel_dir);
+    const double dp = pr - pl, dp2 = p2r - p2l;
+    const double chi = (fabs(dp) > shktst * DMIN(pr, pl)) ? ((du <= 0.0) ? 1.0 : 0.0) : 0.0;
+    if (chi == 0.0) return;
+    const double denom = DMAX(small_pres, fabs(dp2));
+    const double zeta = fabs(dp) * (1.0 / denom);
+    const double inner = dzcut * (zeta - zcut1);
+    if (0.0 > inner || 1.0 < inner) return;   // z clamped
+    const double zb = -flatnb;
+    const double zetab = dzcut * zb;
+    const double dpb = zetab * (dp > 0.0 ? 1.0 : (dp < 0.0 ? -1.0 : 0.0)) / denom;
+    sink.q(i + (1 + o) * ex, j + (1 + o) * ey, k + (1 + o) * ez, QPRES, dpb);
+    sink.q(i + (o - 1) * ex, j + (o - 1) * ey, k + (o - 1) * ez, QPRES, -dpb);
+    if (!(small_pres > fabs(dp2))) {
+        const double denomb = -zetab * fabs(dp) / (denom * denom);
+        const double dp2b = denomb * (dp2 > 0.0 ? 1.0 : (dp2 < 0.0 ? -1.0 : 0.0));
+        sink.q(i + (2 + o) * ex, j + (2 + o) * ey, k + (2 + o) * ez, QPRES, dp2b);
+        sink.q(i + (o - 2) * ex, j + (o - 2) * ey, k + (o - 2) * ez, QPRES, -dp2b);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// CGF Riemann solver (Source/riemann.F90:114-325) on one face: adjoint.
+// flxb (NVAR, UTEMP ignored) and qgb (NGDNV) are the output adjoints; the
+// interface state qint has no consumer and no adjoint.
+// ---------------------------------------------------------------------------
+template <int NS, int D>
+CASTRO_HD void riemann_cgf_adj(const double* ql, const double* qr, double gamcl, double gamcr, double cl, double cr,
+                               const double* flxb, const double* qgb, double* qlb, double* qrb, double& gamclb,
+                               double& gamcrb, double& clb, double& crb)
+{
+    constexpr int iu = SU + D;
+    constexpr int iv1 = SU + (D == 0 ? 1 : 0);
+    constexpr int iv2 = SU + (D == 2 ? 1 : 2);
+    constexpr int im1 = UMX + D;
+    constexpr int im2 = UMX + (D == 0 ? 1 : 0);
+    constexpr int im3 = UMX + (D == 2 ? 1 : 2);
+    // ---- forward ----
+    const double rl = DMAX(ql[SRHO], small_dens);
+    const double ul = ql[iu], v1l = ql[iv1], v2l = ql[iv2];
+    const double pl = DMAX(ql[SPRES], small_pres);
+    const double rel = ql[SREI];
+    const double rr = DMAX(qr[SRHO], small_dens);
+    const double ur = qr[iu], v1r = qr[iv1], v2r = qr[iv2];
+    const double pr = DMAX(qr[SPRES], small_pres);
+    const double rer = qr[SREI];
+    const double cmax = DMAX(cr, cl);
+    const double csmall = DMAX(small, small * cmax);
+    const double cavg = 0.5 * (cr + cl);
+    const double wsmall = small_dens * csmall;
+    const double Al = gamcl * pl * rl, Ar = gamcr * pr * rr;
+    const double sql = sqrt(fabs(Al)), sqr = sqrt(fabs(Ar));
+    const double wl = DMAX(wsmall, sql);
+    const double wr = DMAX(wsmall, sqr);
+    const double wwinv = 1.0 / (wl + wr);
+    const double Np = (wr * pl + wl * pr) + wl * wr * (ul - ur);
+    const double Nu = (wl * ul + wr * ur) + (pl - pr);
+    const double pstar0 = Np * wwinv;
+    const double ustar0 = Nu * wwinv;
+    const double pstar = DMAX(pstar0, small_pres);
+    const bool uzero = fabs(ustar0) < smallu * 0.5 * (fabs(ul) + fabs(ur));
+    const double ustar = uzero ? 0.0 : ustar0;
+    double sgnm = copysign(1.0, ustar);
+    if (ustar == 0.0) sgnm = 0.0;
+    const double fp = 0.5 * (1.0 + sgnm), fm = 0.5 * (1.0 - sgnm);
+    const double ro0 = fp * rl + fm * rr;
+    const double uo = fp * ul + fm * ur;
+    const double po = fp * pl + fm * pr;
+    const double reo = fp * rel + fm * rer;
+    const double gamco = fp * gamcl + fm * gamcr;
+    const double ro = DMAX(small_dens, ro0);
+    const double roinv = 1.0 / ro;
+    const double A2 = gamco * po * roinv;
+    const double co0 = sqrt(fabs(A2));
+    const double co = DMAX(csmall, co0);
+    const double co2inv = 1.0 / (co * co);
+    const double qv1 = fp * v1l + fm * v1r;
+    const double qv2 = fp * v2l + fm * v2r;
+    const double drho = (pstar - po) * co2inv;
+    const double rstar0 = ro + drho;
+    const double rstar = DMAX(small_dens, rstar0);
+    const double rstarinv = 1.0 / rstar;
+    const double entho = (reo + po) * roinv * co2inv;
+    const double estar = reo + (pstar - po) * entho;
+    const double A3 = gamco * pstar * rstarinv;
+    const double cstar0 = sqrt(fabs(A3));
+    const double cstar = DMAX(cstar0, csmall);
+    const double sgnm2 = copysign(1.0, ustar);
+    const double spout0 = co - sgnm2 * uo;
+    const double spin0 = cstar - sgnm2 * ustar;
+    const double ushock = 0.5 * (spin0 + spout0);
+    const bool shock = pstar - po > 0.0;
+    const double spin = shock ? ushock : spin0;
+    const double spout = shock ? ushock : spout0;
+    const bool scr_small = (spout - spin == 0.0);
+    const double scr = scr_small ? small * cavg : spout - spin;
+    const double scrinv = 1.0 / scr;
+    const double frac0 = (1.0 + (spout + spin) * scrinv) * 0.5;
+    const double frac = DMAX(0.0, DMIN(1.0, frac0));
+    int region;   // 0 blend, 1 outer state, 2 star state
+    if (spin >= 0.0) region = 2;
+    else if (spout < 0.0) region = 1;
+    else region = 0;
+    double qrho, qu, qp_s, regdnv;
+    if (region == 2) { qrho = rstar; qu = ustar; qp_s = pstar; regdnv = estar; }
+    else if (region == 1) { qrho = ro; qu = uo; qp_s = po; regdnv = reo; }
+    else {
+        qrho = frac * rstar + (1.0 - frac) * ro;
+        qu = frac * ustar + (1.0 - frac) * uo;
+        qp_s = frac * pstar + (1.0 - frac) * po;
+        regdnv = frac * estar + (1.0 - frac) * reo;
+    }
+    const double regdnvinv = 1.0 / regdnv;
+    const double qp = DMAX(qp_s, small_pres);
+    const double F_rho = qrho * qu;
+    const double K2 = qu * qu + qv1 * qv1 + qv2 * qv2;
+    const double rhoetot = regdnv + 0.5 * qrho * K2;
+
+    // ---- reverse ----
+    double qrhob = 0.0, qub = 0.0, qv1b = 0.0, qv2b = 0.0, qpb = 0.0, regdnvb = 0.0, F_rhob = 0.0;
+    for (int n = 0; n < NS; ++n) {
+        const double x = fp * ql[SX + n] + fm * qr[SX + n];
+        const double xb = flxb[UFS + n] * F_rho;
+        F_rhob += flxb[UFS + n] * x;
+        qlb[SX + n] += fp * xb;
+        qrb[SX + n] += fm * xb;
+    }
+    qub += flxb[UEINT] * regdnv;
+    regdnvb += flxb[UEINT] * qu;
+    qub += flxb[UEDEN] * (rhoetot + qp);
+    const double rhoetotb = flxb[UEDEN] * qu;
+    qpb += flxb[UEDEN] * qu;
+    regdnvb += rhoetotb;
+    qrhob += 0.5 * K2 * rhoetotb;
+    qub += qrho * qu * rhoetotb;
+    qv1b += qrho * qv1 * rhoetotb;
+    qv2b += qrho * qv2 * rhoetotb;
+    F_rhob += flxb[im3] * qv2; qv2b += flxb[im3] * F_rho;
+    F_rhob += flxb[im2] * qv1; qv1b += flxb[im2] * F_rho;
+    F_rhob += flxb[im1] * qu; qub += flxb[im1] * F_rho;
+    F_rhob += flxb[URHO];
+    qrhob += F_rhob * qu;
+    qub += F_rhob * qrho;
+    // qg: GDRHO, velocities (absolute order), GDPRES, GDGAME
+    qrhob += qgb[GDRHO];
+    qub += qgb[GDU + D];
+    qv1b += qgb[GDU + (iv1 - SU)];
+    qv2b += qgb[GDU + (iv2 - SU)];
+    qpb += qgb[GDPRES];
+    // qgame = qp_s * regdnvinv + 1 (before the pressure floor)
+    double qp_sb = qgb[GDGAME] * regdnvinv;
+    const double regdnvinvb = qgb[GDGAME] * qp_s;
+    regdnvb -= regdnvinvb * regdnvinv * regdnvinv;
+    if (qp_s > small_pres) qp_sb += qpb;
+    double rstarb = 0.0, ustarb = 0.0, pstarb = 0.0, estarb = 0.0;
+    double rob = 0.0, uob = 0.0, pob = 0.0, reob = 0.0;
+    double spinb = 0.0, spoutb = 0.0, cavgb = 0.0;
+    if (region == 2) {
+        rstarb += qrhob; ustarb += qub; pstarb += qp_sb; estarb += regdnvb;
+    } else if (region == 1) {
+        rob += qrhob; uob += qub; pob += qp_sb; reob += regdnvb;
+    } else {
+        const double fracb = qrhob * (rstar - ro) + qub * (ustar - uo) + qp_sb * (pstar - po) + regdnvb * (estar - reo);
+        rstarb += frac * qrhob; rob += (1.0 - frac) * qrhob;
+        ustarb += frac * qub; uob += (1.0 - frac) * qub;
+        pstarb += frac * qp_sb; pob += (1.0 - frac) * qp_sb;
+        estarb += frac * regdnvb; reob += (1.0 - frac) * regdnvb;
+        if (!(1.0 < frac0) && !(0.0 > DMIN(1.0, frac0))) {
+            const double frac0b = fracb;
+            const double S = spout + spin;
+            const double Sb = 0.5 * frac0b * scrinv;
+            const double scrinvb = 0.5 * frac0b * S;
+            const double scrb = -scrinvb * scrinv * scrinv;
+            if (scr_small) cavgb += small * scrb;
+            else { spoutb += scrb; spinb -= scrb; }
+            spoutb += Sb;
+            spinb += Sb;
+        }
+    }
+    double spin0b, spout0b;
+    if (shock) {
+        const double ushockb = spinb + spoutb;
+        spin0b = 0.5 * ushockb;
+        spout0b = 0.5 * ushockb;
+    } else {
+        spin0b = spinb;
+        spout0b = spoutb;
+    }
+    double cstarb = spin0b;
+    ustarb -= sgnm2 * spin0b;
+    double cob = spout0b;
+    uob -= sgnm2 * spout0b;
+    double csmallb = 0.0;
+    double cstar0b = 0.0;
+    if (cstar0 > csmall) cstar0b = cstarb;
+    else csmallb += cstarb;
+    double gamcob = 0.0, rstarinvb = 0.0;
+    if (cstar0 > 0.0) {
+        const double A3b = cstar0b * 0.5 / cstar0 * (A3 >= 0.0 ? 1.0 : -1.0);
+        gamcob += A3b * pstar * rstarinv;
+        pstarb += A3b * gamco * rstarinv;
+        rstarinvb += A3b * gamco * pstar;
+    }
+    // estar = reo + (pstar - po) * entho
+    reob += estarb;
+    pstarb += estarb * entho;
+    pob -= estarb * entho;
+    const double enthob = estarb * (pstar - po);
+    // entho = (reo + po) * roinv * co2inv
+    reob += enthob * roinv * co2inv;
+    pob += enthob * roinv * co2inv;
+    double roinvb = enthob * (reo + po) * co2inv;
+    double co2invb = enthob * (reo + po) * roinv;
+    rstarb -= rstarinvb * rstarinv * rstarinv;
+    const double rstar0b = (small_dens > rstar0) ? 0.0 : rstarb;
+    rob += rstar0b;
+    const double drhob = rstar0b;
+    pstarb += drhob * co2inv;
+    pob -= drhob * co2inv;
+    co2invb += drhob * (pstar - po);
+    cob -= 2.0 * co2invb * co2inv / co;
+    double co0b = 0.0;
+    if (csmall > co0) csmallb += cob;
+    else co0b = cob;
+    if (co0 > 0.0) {
+        const double A2b = co0b * 0.5 / co0 * (A2 >= 0.0 ? 1.0 : -1.0);
+        gamcob += A2b * po * roinv;
+        pob += A2b * gamco * roinv;
+        roinvb += A2b * gamco * po;
+    }
+    rob -= roinvb * roinv * roinv;
+    const double ro0b = (small_dens > ro0) ? 0.0 : rob;
+    double rlb = fp * ro0b, rrb = fm * ro0b;
+    double ulb = fp * uob, urb = fm * uob;
+    double plb = fp * pob, prb = fm * pob;
+    qlb[SREI] += fp * reob;
+    qrb[SREI] += fm * reob;
+    gamclb += fp * gamcob;
+    gamcrb += fm * gamcob;
+    qlb[iv1] += fp * qv1b; qrb[iv1] += fm * qv1b;
+    qlb[iv2] += fp * qv2b; qrb[iv2] += fm * qv2b;
+    const double ustar0b = uzero ? 0.0 : ustarb;
+    const double pstar0b = (pstar0 > small_pres) ? pstarb : 0.0;
+    // ustar0 = Nu * wwinv
+    double wwinvb = ustar0b * Nu + pstar0b * Np;
+    const double Nub = ustar0b * wwinv;
+    const double Npb = pstar0b * wwinv;
+    double wlb = Nub * ul, wrb = Nub * ur;
+    ulb += Nub * wl; urb += Nub * wr;
+    plb += Nub; prb -= Nub;
+    // Np = (wr*pl + wl*pr) + wl*wr*(ul-ur)
+    wrb += Npb * (pl + wl * (ul - ur));
+    wlb += Npb * (pr + wr * (ul - ur));
+    plb += Npb * wr;
+    prb += Npb * wl;
+    ulb += Npb * wl * wr;
+    urb -= Npb * wl * wr;
+    wlb -= wwinvb * wwinv * wwinv;
+    wrb -= wwinvb * wwinv * wwinv;
+    double wsmallb = 0.0;
+    if (wsmall > sql) wsmallb += wlb;
+    else if (sql > 0.0) {
+        const double Ab = wlb * 0.5 / sql * (Al >= 0.0 ? 1.0 : -1.0);
+        gamclb += Ab * pl * rl; plb += Ab * gamcl * rl; rlb += Ab * gamcl * pl;
+    }
+    if (wsmall > sqr) wsmallb += wrb;
+    else if (sqr > 0.0) {
+        const double Ab = wrb * 0.5 / sqr * (Ar >= 0.0 ? 1.0 : -1.0);
+        gamcrb += Ab * pr * rr; prb += Ab * gamcr * rr; rrb += Ab * gamcr * pr;
+    }
+    csmallb += small_dens * wsmallb;
+    crb += 0.5 * cavgb;
+    clb += 0.5 * cavgb;
+    if (!(small > small * cmax)) {
+        const double cmaxb = small * csmallb;
+        if (cr > cl) crb += cmaxb; else clb += cmaxb;
+    }
+    qlb[iu] += ulb; qrb[iu] += urb;
+    if (ql[SRHO] > small_dens) qlb[SRHO] += rlb;
+    if (qr[SRHO] > small_dens) qrb[SRHO] += rrb;
+    if (ql[SPRES] > small_pres) qlb[SPRES] += plb;
+    if (qr[SPRES] > small_pres) qrb[SPRES] += prb;
+}
+
+// ---------------------------------------------------------------------------
+// Transverse corrections (Source/trans.F90): adjoints of trans1_state and
+// trans2_state.  Flux-record adjoints frb/flb are accumulated; cdtdxb too.
+// ---------------------------------------------------------------------------
+template <int NS>
+CASTRO_HD void trans1_state_adj(const double* lq, const double* fr, const double* fl, double gamc, double cdtdx,
+                                const double* lqob, double* lqb, double* frb, double* flb, double& gamcb,
+                                double& cdtdxb)
+{
+    using R = TF<NS>;
+    // species (always updated)
+    for (int n = 0; n < NS; ++n) {
+        const double rrnew = lq[SRHO] - cdtdx * (fr[R::RHO] - fl[R::RHO]);
+        const double compu = lq[SRHO] * lq[SX + n] - cdtdx * (fr[R::X + n] - fl[R::X + n]);
+        const double compub = lqob[SX + n] / rrnew;
+        const double rrnewb = -lqob[SX + n] * compu / (rrnew * rrnew);
+        lqb[SRHO] += compub * lq[SX + n] + rrnewb;
+        lqb[SX + n] += compub * lq[SRHO];
+        cdtdxb -= compub * (fr[R::X + n] - fl[R::X + n]) + rrnewb * (fr[R::RHO] - fl[R::RHO]);
+        frb[R::X + n] -= cdtdx * compub;
+        flb[R::X + n] += cdtdx * compub;
+        frb[R::RHO] -= cdtdx * rrnewb;
+        flb[R::RHO] += cdtdx * rrnewb;
+    }
+    const double pgp = fr[R::PG], pgm = fl[R::PG], ugp = fr[R::UG], ugm = fl[R::UG];
+    const double dup = pgp * ugp - pgm * ugm;
+    const double du = ugp - ugm;
+    const double pav = 0.5 * (pgp + pgm);
+    const double rrl2 = lq[SRHO];
+    const double vel[3] = {lq[SU], lq[SV], lq[SW]};
+    double rv[3];
+    for (int m = 0; m < 3; ++m) rv[m] = rrl2 * vel[m];
+    const double ekenl2 = 0.5 * rrl2 * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+    const double rel2 = lq[SREI] + ekenl2;
+    const int fm[3] = {R::MX, R::MY, R::MZ};
+    double rrnew = rrl2 - cdtdx * (fr[R::RHO] - fl[R::RHO]);
+    double rvnew[3];
+    for (int m = 0; m < 3; ++m) rvnew[m] = rv[m] - cdtdx * (fr[fm[m]] - fl[fm[m]]);
+    double renew = rel2 - cdtdx * (fr[R::ED] - fl[R::ED]);
+    const bool reset = rrnew < 0.0;
+    if (reset) {
+        rrnew = rrl2;
+        for (int m = 0; m < 3; ++m) rvnew[m] = rv[m];
+        renew = rel2;
+    }
+    const double rhoinv = 1.0 / rrnew;
+    const double S = rvnew[0] * rvnew[0] + rvnew[1] * rvnew[1] + rvnew[2] * rvnew[2];
+    // reverse
+    if (!reset) {
+        const double Z = dup + pav * du * (gamc - 1.0);
+        const double pnew = lq[SPRES] - cdtdx * Z;
+        if (pnew > small_pres) {
+            const double pnewb = lqob[SPRES];
+            lqb[SPRES] += pnewb;
+            cdtdxb -= pnewb * Z;
+            const double Zb = -cdtdx * pnewb;
+            const double dupb = Zb, pavb = Zb * du * (gamc - 1.0), dub = Zb * pav * (gamc - 1.0);
+            gamcb += Zb * pav * du;
+            frb[R::PG] += dupb * ugp + 0.5 * pavb;
+            frb[R::UG] += dupb * pgp + dub;
+            flb[R::PG] += -dupb * ugm + 0.5 * pavb;
+            flb[R::UG] += -dupb * pgm - dub;
+        }
+    } else {
+        lqb[SPRES] += lqob[SPRES];
+    }
+    const double renewb = lqob[SREI];
+    const double rhoekenb = -lqob[SREI];
+    double rvnewb[3], rhoinvb = rhoekenb * 0.5 * S;
+    for (int m = 0; m < 3; ++m) {
+        rvnewb[m] = rhoekenb * rvnew[m] * rhoinv + lqob[SU + m] * rhoinv;
+        rhoinvb += lqob[SU + m] * rvnew[m];
+    }
+    const double rrnewb = lqob[SRHO] - rhoinvb * rhoinv * rhoinv;
+    double rrl2b = rrnewb, rel2b = renewb, rvb[3];
+    for (int m = 0; m < 3; ++m) rvb[m] = rvnewb[m];
+    if (!reset) {
+        cdtdxb -= rrnewb * (fr[R::RHO] - fl[R::RHO]);
+        frb[R::RHO] -= cdtdx * rrnewb;
+        flb[R::RHO] += cdtdx * rrnewb;
+        for (int m = 0; m < 3; ++m) {
+            cdtdxb -= rvnewb[m] * (fr[fm[m]] - fl[fm[m]]);
+            frb[fm[m]] -= cdtdx * rvnewb[m];
+            flb[fm[m]] += cdtdx * rvnewb[m];
+        }
+        cdtdxb -= renewb * (fr[R::ED] - fl[R::ED]);
+        frb[R::ED] -= cdtdx * renewb;
+        flb[R::ED] += cdtdx * renewb;
+    }
+    lqb[SREI] += rel2b;
+    const double ekenb = rel2b;
+    rrl2b += 0.5 * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]) * ekenb;
+    for (int m = 0; m < 3; ++m) {
+        lqb[SU + m] += rrl2 * vel[m] * ekenb + rvb[m] * rrl2;
+        rrl2b += rvb[m] * vel[m];
+    }
+    lqb[SRHO] += rrl2b;
+}
+
+template <int NS>
+CASTRO_HD void trans2_state_adj(const double* lq, const double* f2r, const double* f2l, const double* f3r,
+                                const double* f3l, double gamc, double cdtdx2, double cdtdx3, const double* lqob,
+                                double* lqb, double* f2rb, double* f2lb, double* f3rb, double* f3lb, double& gamcb,
+                                double& cdtdx2b, double& cdtdx3b)
+{
+    using R = TF<NS>;
+    for (int n = 0; n < NS; ++n) {
+        const double rrr = lq[SRHO];
+        const double compr = rrr * lq[SX + n];
+        const double rrnewr = rrr - cdtdx2 * (f2r[R::RHO] - f2l[R::RHO]) - cdtdx3 * (f3r[R::RHO] - f3l[R::RHO]);
+        const double compnr = compr - cdtdx2 * (f2r[R::X + n] - f2l[R::X + n]) - cdtdx3 * (f3r[R::X + n] - f3l[R::X + n]);
+        const double compnrb = lqob[SX + n] / rrnewr;
+        const double rrnewrb = -lqob[SX + n] * compnr / (rrnewr * rrnewr);
+        lqb[SRHO] += compnrb * lq[SX + n] + rrnewrb;
+        lqb[SX + n] += compnrb * rrr;
+        cdtdx2b -= compnrb * (f2r[R::X + n] - f2l[R::X + n]) + rrnewrb * (f2r[R::RHO] - f2l[R::RHO]);
+        cdtdx3b -= compnrb * (f3r[R::X + n] - f3l[R::X + n]) + rrnewrb * (f3r[R::RHO] - f3l[R::RHO]);
+        f2rb[R::X + n] -= cdtdx2 * compnrb; f2lb[R::X + n] += cdtdx2 * compnrb;
+        f3rb[R::X + n] -= cdtdx3 * compnrb; f3lb[R::X + n] += cdtdx3 * compnrb;
+        f2rb[R::RHO] -= cdtdx2 * rrnewrb; f2lb[R::RHO] += cdtdx2 * rrnewrb;
+        f3rb[R::RHO] -= cdtdx3 * rrnewrb; f3lb[R::RHO] += cdtdx3 * rrnewrb;
+    }
+    const double pg2p = f2r[R::PG], pg2m = f2l[R::PG], ug2p = f2r[R::UG], ug2m = f2l[R::UG];
+    const double du2p = pg2p * ug2p - pg2m * ug2m, p2av = 0.5 * (pg2p + pg2m), du2 = ug2p - ug2m;
+    const double Z2 = du2p + p2av * du2 * (gamc - 1.0);
+    const double p2new = cdtdx2 * Z2;
+    const double pg3p = f3r[R::PG], pg3m = f3l[R::PG], ug3p = f3r[R::UG], ug3m = f3l[R::UG];
+    const double du3p = pg3p * ug3p - pg3m * ug3m, p3av = 0.5 * (pg3p + pg3m), du3 = ug3p - ug3m;
+    const double Z3 = du3p + p3av * du3 * (gamc - 1.0);
+    const double p3new = cdtdx3 * Z3;
+    const double rrr = lq[SRHO];
+    const double vel[3] = {lq[SU], lq[SV], lq[SW]};
+    double rv[3];
+    for (int m = 0; m < 3; ++m) rv[m] = rrr * vel[m];
+    const double ekenr = 0.5 * rrr * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+    const double rer = lq[SREI] + ekenr;
+    const int fm[3] = {R::MX, R::MY, R::MZ};
+    double rrnew = rrr - cdtdx2 * (f2r[R::RHO] - f2l[R::RHO]) - cdtdx3 * (f3r[R::RHO] - f3l[R::RHO]);
+    double rvnew[3];
+    for (int m = 0; m < 3; ++m)
+        rvnew[m] = rv[m] - cdtdx2 * (f2r[fm[m]] - f2l[fm[m]]) - cdtdx3 * (f3r[fm[m]] - f3l[fm[m]]);
+    double renew = rer - cdtdx2 * (f2r[R::ED] - f2l[R::ED]) - cdtdx3 * (f3r[R::ED] - f3l[R::ED]);
+    const bool reset = rrnew < 0.0;
+    if (reset) {
+        rrnew = rrr;
+        for (int m = 0; m < 3; ++m) rvnew[m] = rv[m];
+        renew = rer;
+    }
+    const double S = rvnew[0] * rvnew[0] + rvnew[1] * rvnew[1] + rvnew[2] * rvnew[2];
+    // reverse: pressure
+    const double pun = reset ? lq[SPRES] : lq[SPRES] - p2new - p3new;
+    const double punb = (pun > small_pres) ? lqob[SPRES] : 0.0;   // DMAX(pun, small_pres)
+    lqb[SPRES] += punb;
+    if (!reset) {
+        const double p2newb = -punb, p3newb = -punb;
+        cdtdx2b += p2newb * Z2;
+        cdtdx3b += p3newb * Z3;
+        const double Z2b = cdtdx2 * p2newb, Z3b = cdtdx3 * p3newb;
+        gamcb += Z2b * p2av * du2 + Z3b * p3av * du3;
+        {
+            const double dupb = Z2b, pavb = Z2b * du2 * (gamc - 1.0), dub = Z2b * p2av * (gamc - 1.0);
+            f2rb[R::PG] += dupb * ug2p + 0.5 * pavb;
+            f2rb[R::UG] += dupb * pg2p + dub;
+            f2lb[R::PG] += -dupb * ug2m + 0.5 * pavb;
+            f2lb[R::UG] += -dupb * pg2m - dub;
+        }
+        {
+            const double dupb = Z3b, pavb = Z3b * du3 * (gamc - 1.0), dub = Z3b * p3av * (gamc - 1.0);
+            f3rb[R::PG] += dupb * ug3p + 0.5 * pavb;
+            f3rb[R::UG] += dupb * pg3p + dub;
+            f3lb[R::PG] += -dupb * ug3m + 0.5 * pavb;
+            f3lb[R::UG] += -dupb * pg3m - dub;
+        }
+    }
+    // lqo_rei = renew - 0.5*S/rrnew ; lqo_v = rvnew/rrnew
+    const double renewb = lqob[SREI];
+    const double Sb = -0.5 * lqob[SREI] / rrnew;
+    double rrnewb = lqob[SRHO] + 0.5 * lqob[SREI] * S / (rrnew * rrnew);
+    double rvnewb[3];
+    for (int m = 0; m < 3; ++m) {
+        rvnewb[m] = 2.0 * rvnew[m] * Sb + lqob[SU + m] / rrnew;
+        rrnewb -= lqob[SU + m] * rvnew[m] / (rrnew * rrnew);
+    }
+    double rrrb = rrnewb, rerb = renewb, rvb[3];
+    for (int m = 0; m < 3; ++m) rvb[m] = rvnewb[m];
+    if (!reset) {
+        cdtdx2b -= rrnewb * (f2r[R::RHO] - f2l[R::RHO]);
+        cdtdx3b -= rrnewb * (f3r[R::RHO] - f3l[R::RHO]);
+        f2rb[R::RHO] -= cdtdx2 * rrnewb; f2lb[R::RHO] += cdtdx2 * rrnewb;
+        f3rb[R::RHO] -= cdtdx3 * rrnewb; f3lb[R::RHO] += cdtdx3 * rrnewb;
+        for (int m = 0; m < 3; ++m) {
+            cdtdx2b -= rvnewb[m] * (f2r[fm[m]] - f2l[fm[m]]);
+            cdtdx3b -= rvnewb[m] * (f3r[fm[m]] - f3l[fm[m]]);
+            f2rb[fm[m]] -= cdtdx2 * rvnewb[m]; f2lb[fm[m]] += cdtdx2 * rvnewb[m];
+            f3rb[fm[m]] -= cdtdx3 * rvnewb[m]; f3lb[fm[m]] += cdtdx3 * rvnewb[m];
+        }
+        cdtdx2b -= renewb * (f2r[R::ED] - f2l[R::ED]);
+        cdtdx3b -= renewb * (f3r[R::ED] - f3l[R::ED]);
+        f2rb[R::ED] -= cdtdx2 * renewb; f2lb[R::ED] += cdtdx2 * renewb;
+        f3rb[R::ED] -= cdtdx3 * renewb; f3lb[R::ED] += cdtdx3 * renewb;
+    }
+    lqb[SREI] += rerb;
+    const double ekenb = rerb;
+    rrrb += 0.5 * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]) * ekenb;
+    for (int m = 0; m < 3; ++m) {
+        lqb[SU + m] += rrr * vel[m] * ekenb + rvb[m] * rrr;
+        rrrb += rvb[m] * vel[m];
+    }
+    lqb[SRHO] += rrrb;
+}
+
+}  // namespace castro

@@ -15,7 +15,7 @@ struct Fab {
     double* p;
     int lx, ly, lz;
     int nx, ny, nz;
-    __device__ __forceinline__ double& operator()(int i, int j, int k, int n) const
+    __host__ __device__ __forceinline__ double& operator()(int i, int j, int k, int n) const
     {
         return p[(long long)(i - lx) + (long long)nx * ((long long)(j - ly) + (long long)ny * ((long long)(k - lz) + (long long)nz * n))];
     }

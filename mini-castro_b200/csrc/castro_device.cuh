@@ -12,6 +12,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// Stages that are plain arithmetic are callable from host code as well, so the
+// reverse-mode stages built on them can be checked on a CPU.
+#define CASTRO_HD __host__ __device__ __forceinline__
+
 namespace castro {
 
 // ---- index maps, Source/Castro_nd.F90:14-57 (0-based) ----
@@ -76,8 +80,8 @@ struct NetworkDev {
 static __constant__ EosTableDev c_eos;
 static __constant__ NetworkDev c_net;
 
-__device__ __forceinline__ double fmaxf_(double a, double b) { return (a > b) ? a : b; }
-__device__ __forceinline__ double fminf_(double a, double b) { return (a < b) ? a : b; }
+CASTRO_HD double fmaxf_(double a, double b) { return (a > b) ? a : b; }
+CASTRO_HD double fminf_(double a, double b) { return (a < b) ? a : b; }
 #define DMAX(a, b) ::castro::fmaxf_((a), (b))
 #define DMIN(a, b) ::castro::fminf_((a), (b))
 
@@ -85,22 +89,22 @@ __device__ __forceinline__ double fminf_(double a, double b) { return (a < b) ? 
 // Helmholtz EOS, Source/eos.F90:141-576
 // ---------------------------------------------------------------------------
 // quintic Hermite basis, eos.F90:740-911
-__device__ __forceinline__ double psi0(double z)   { return z * z * z * (z * (-6.0 * z + 15.0) - 10.0) + 1.0; }
-__device__ __forceinline__ double dpsi0(double z)  { return z * z * (z * (-30.0 * z + 60.0) - 30.0); }
-__device__ __forceinline__ double ddpsi0(double z) { return z * (z * (-120.0 * z + 180.0) - 60.0); }
-__device__ __forceinline__ double psi1(double z)   { return z * (z * z * (z * (-3.0 * z + 8.0) - 6.0) + 1.0); }
-__device__ __forceinline__ double dpsi1(double z)  { return z * z * (z * (-15.0 * z + 32.0) - 18.0) + 1.0; }
-__device__ __forceinline__ double ddpsi1(double z) { return z * (z * (-60.0 * z + 96.0) - 36.0); }
-__device__ __forceinline__ double psi2(double z)   { return 0.5 * z * z * (z * (z * (-z + 3.0) - 3.0) + 1.0); }
-__device__ __forceinline__ double dpsi2(double z)  { return 0.5 * z * (z * (z * (-5.0 * z + 12.0) - 9.0) + 2.0); }
-__device__ __forceinline__ double ddpsi2(double z) { return 0.5 * (z * (z * (-20.0 * z + 36.0) - 18.0) + 2.0); }
+CASTRO_HD double psi0(double z)   { return z * z * z * (z * (-6.0 * z + 15.0) - 10.0) + 1.0; }
+CASTRO_HD double dpsi0(double z)  { return z * z * (z * (-30.0 * z + 60.0) - 30.0); }
+CASTRO_HD double ddpsi0(double z) { return z * (z * (-120.0 * z + 180.0) - 60.0); }
+CASTRO_HD double psi1(double z)   { return z * (z * z * (z * (-3.0 * z + 8.0) - 6.0) + 1.0); }
+CASTRO_HD double dpsi1(double z)  { return z * z * (z * (-15.0 * z + 32.0) - 18.0) + 1.0; }
+CASTRO_HD double ddpsi1(double z) { return z * (z * (-60.0 * z + 96.0) - 36.0); }
+CASTRO_HD double psi2(double z)   { return 0.5 * z * z * (z * (z * (-z + 3.0) - 3.0) + 1.0); }
+CASTRO_HD double dpsi2(double z)  { return 0.5 * z * (z * (z * (-5.0 * z + 12.0) - 9.0) + 2.0); }
+CASTRO_HD double ddpsi2(double z) { return 0.5 * (z * (z * (-20.0 * z + 36.0) - 18.0) + 2.0); }
 // cubic Hermite basis, eos.F90:955-1031
-__device__ __forceinline__ double xpsi0(double z)  { return z * z * (2.0 * z - 3.0) + 1.0; }
-__device__ __forceinline__ double xpsi1(double z)  { return z * (z * (z - 2.0) + 1.0); }
+CASTRO_HD double xpsi0(double z)  { return z * z * (2.0 * z - 3.0) + 1.0; }
+CASTRO_HD double xpsi1(double z)  { return z * (z * (z - 2.0) + 1.0); }
 
 // Fortran INT() of a table coordinate, with the overflow/NaN guard the
 // conversion needs in C.
-__device__ __forceinline__ int table_trunc(double x)
+CASTRO_HD int table_trunc(double x)
 {
     if (!(x < 1.0e6)) x = 1.0e6;
     if (x < -1.0e6) x = -1.0e6;
@@ -560,7 +564,7 @@ __device__ __forceinline__ void ctoprim_pt(const double* u, double* q, double* q
 
 // uflatten, Source/ppm.F90:11-128
 template <class L>
-__device__ __forceinline__ double uflatten(const L& ld, int i, int j, int k)
+CASTRO_HD double uflatten(const L& ld, int i, int j, int k)
 {
     const double shktst = 0.33, zcut1 = 0.75, zcut2 = 0.85;
     const double dzcut = 1.0 / (zcut2 - zcut1);
@@ -603,7 +607,7 @@ __device__ __forceinline__ double uflatten(const L& ld, int i, int j, int k)
 }
 
 // van Leer limited slope of ppm.F90:153-169
-__device__ __forceinline__ double vl_slope(double sm1, double s0, double sp1)
+CASTRO_HD double vl_slope(double sm1, double s0, double sp1)
 {
     double dsl = 2.0 * (s0 - sm1);
     double dsr = 2.0 * (sp1 - s0);
@@ -615,7 +619,7 @@ __device__ __forceinline__ double vl_slope(double sm1, double s0, double sp1)
 }
 
 // ppm_reconstruct, Source/ppm.F90:132-236; s[0..4] = s(-2..2)
-__device__ __forceinline__ void ppm_reconstruct(const double* s, double flatn, double& smo, double& spo)
+CASTRO_HD void ppm_reconstruct(const double* s, double flatn, double& smo, double& spo)
 {
     double dsvl_l = vl_slope(s[0], s[1], s[2]);
     double dsvl_r = vl_slope(s[1], s[2], s[3]);
@@ -642,7 +646,7 @@ __device__ __forceinline__ void ppm_reconstruct(const double* s, double flatn, d
 }
 
 // ppm_int_profile for one wave speed, Source/ppm.F90:260-303
-__device__ __forceinline__ void ppm_int_wave(double sm, double sp, double s6, double speed, double dtdx,
+CASTRO_HD void ppm_int_wave(double sm, double sp, double s6, double speed, double dtdx,
                                              double& Ip, double& Im)
 {
     double sigma = fabs(speed) * dtdx;
@@ -659,7 +663,7 @@ __device__ __forceinline__ void ppm_int_wave(double sm, double sp, double s6, do
 // :637-734 for the minus state).  I[w][v] are the wave integrals of rho, un, p,
 // rhoe (v = 0..3) for waves w = u-c, u, u+c; gam is the gamc integral of the
 // reference wave.  'plus' selects the plus (right) state of face i.
-__device__ __forceinline__ void trace_project(const double I[3][4], double gam_g_ref, double un, double cc,
+CASTRO_HD void trace_project(const double I[3][4], double gam_g_ref, double un, double cc,
                                               bool plus, double& rho_o, double& un_o, double& rhoe_o, double& p_o)
 {
     const int wr = plus ? 0 : 2;   // reference wave: fastest toward the interface
@@ -706,7 +710,7 @@ __device__ __forceinline__ void trace_project(const double I[3][4], double gam_g
 // plus state on face i (left face of the zone) and the minus state on face
 // i+1, in compact face-state layout.  flatn is uflatten of the zone.
 template <int NS, int D, class L>
-__device__ __forceinline__ void trace_zone(const L& ld, int i, int j, int k, double dtdx, double flatn,
+CASTRO_HD void trace_zone(const L& ld, int i, int j, int k, double dtdx, double flatn,
                                            double* qplus, double* qminus)
 {
     constexpr int ex = D == 0, ey = D == 1, ez = D == 2;
@@ -794,7 +798,7 @@ __device__ __forceinline__ void trace_zone(const L& ld, int i, int j, int k, dou
 // qint is non-null, the interface state in full QVAR numbering (QRHO, velocities,
 // QPRES, QGAME, QREINT, species).
 template <int NS, int D>
-__device__ __forceinline__ void riemann_cgf(const double* ql, const double* qr, double gamcl, double gamcr,
+CASTRO_HD void riemann_cgf(const double* ql, const double* qr, double gamcl, double gamcr,
                                             double cl, double cr, double* flx, double* qg, double* qint)
 {
     constexpr int iu = SU + D;
@@ -923,7 +927,7 @@ struct TF {
 // direction 2, fr/fl the flux records of direction 1 on the right/left faces,
 // gamc the left zone's gamma_1.  Returns true when the density reset fired.
 template <int NS>
-__device__ __forceinline__ bool trans1_state(const double* lq, const double* fr, const double* fl, double gamc,
+CASTRO_HD bool trans1_state(const double* lq, const double* fr, const double* fl, double gamc,
                                              double cdtdx, double* lqo)
 {
     using R = TF<NS>;
@@ -975,7 +979,7 @@ __device__ __forceinline__ bool trans1_state(const double* lq, const double* fr,
 // flux records of the two transverse directions, gamc the gamma_1 of the zone
 // the state comes from.
 template <int NS>
-__device__ __forceinline__ bool trans2_state(const double* lq, const double* f2r, const double* f2l,
+CASTRO_HD bool trans2_state(const double* lq, const double* f2r, const double* f2l,
                                              const double* f3r, const double* f3l, double gamc,
                                              double cdtdx2, double cdtdx3, double* lqo)
 {
@@ -1028,7 +1032,7 @@ __device__ __forceinline__ bool trans2_state(const double* lq, const double* f2r
 
 // artificial viscosity of one face component (Castro_hydro_nd.F90:214-237):
 // divsum is the four-node sum exactly as the reference forms it.
-__device__ __forceinline__ double av_term(double divsum, double du)
+CASTRO_HD double av_term(double divsum, double du)
 {
     double div1 = 0.25 * divsum;
     div1 = 0.1 * DMIN(0.0, div1);

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "castro_common.cuh"
+#include "castro_table.h"
 #include "../../include/castro_b200.h"
 
 namespace castro {
@@ -18,6 +19,7 @@ namespace castro {
 // constant upload hooks of the other translation units
 void upload_constants_abi(const EosTableDev& e, const NetworkDev& n);
 void upload_constants_sim(const EosTableDev& e, const NetworkDev& n);
+void upload_constants_adj(const EosTableDev& e, const NetworkDev& n);
 
 namespace {
 std::mutex g_mu;
@@ -57,31 +59,11 @@ void upload_all()
     if (!g_net_set) default_network();
     upload_constants_abi(g_eos, g_net);
     upload_constants_sim(g_eos, g_net);
+    upload_constants_adj(g_eos, g_net);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) set_error(CASTRO_ERR_CUDA, cudaGetErrorString(e));
 }
 
-// one list-directed READ of n values (starts a new record, may span records)
-bool read_record(FILE* fp, double* v, int n)
-{
-    char line[4096];
-    int got = 0;
-    while (got < n) {
-        if (!fgets(line, sizeof line, fp)) return false;
-        for (char* c = line; *c; ++c)
-            if (*c == 'D' || *c == 'd') *c = 'E';
-        char* s = line;
-        while (got < n) {
-            char* e;
-            double x = strtod(s, &e);
-            if (e == s) break;
-            v[got++] = x;
-            s = e;
-            while (*s == ',' || *s == ' ' || *s == '\t') ++s;
-        }
-    }
-    return true;
-}
 }  // namespace
 
 void set_error(int code, const char* what)
@@ -161,100 +143,34 @@ int castro_nspec(void) { return nspec(); }
 
 int castro_eos_init_path(const char* path)
 {
-    const int IM = IMAX, JM = JMAX;
-    // grid and deltas, Source/eos.F90:62-71,626-632,700-712
-    const double tlo = 3.0, thi = 13.0, dlo = -12.0, dhi = 15.0;
-    const double tstp = (thi - tlo) / (double)(float)(JM - 1);
-    const double dstp = (dhi - dlo) / (double)(float)(IM - 1);
-    std::vector<double> t(JM), d(IM);
-    for (int j = 0; j < JM; ++j) t[j] = pow(10.0, tlo + j * tstp);
-    for (int i = 0; i < IM; ++i) d[i] = pow(10.0, dlo + i * dstp);
-
-    FILE* fp = fopen(path, "r");
-    if (!fp) {
+    HostTable T;
+    int rc = read_helm_table(path, T);
+    if (rc == 1) {
         std::string m = std::string("eos_init: cannot open ") + path;
         set_error(CASTRO_ERR_TABLE_IO, m.c_str());
         return CASTRO_ERR_TABLE_IO;
     }
-    // the 13 tables the hydro path reads, packed per node
-    std::vector<double> node((size_t)JM * IM * NODE_STRIDE, 0.0);
-    double v[9];
-    bool ok = true;
-    for (int j = 0; j < JM && ok; ++j)
-        for (int i = 0; i < IM && ok; ++i) {
-            if (!read_record(fp, v, 9)) { ok = false; break; }
-            double* r = &node[((size_t)j * IM + i) * NODE_STRIDE];
-            // file order f, fd, ft, fdd, ftt, fdt, fddt, fdtt, fddtt (eos.F90:646-647)
-            r[N_F] = v[0]; r[N_FD] = v[1]; r[N_FT] = v[2]; r[N_FDD] = v[3]; r[N_FTT] = v[4];
-            r[N_FDT] = v[5]; r[N_FDDT] = v[6]; r[N_FDTT] = v[7]; r[N_FDDTT] = v[8];
-        }
-    for (int j = 0; j < JM && ok; ++j)
-        for (int i = 0; i < IM && ok; ++i) {
-            if (!read_record(fp, v, 4)) { ok = false; break; }
-            double* r = &node[((size_t)j * IM + i) * NODE_STRIDE];
-            // dpdf, dpdfd, dpdft, dpdfdt (eos.F90:654)
-            r[N_DPDF] = v[0]; r[N_DPDFD] = v[1]; r[N_DPDFT] = v[2]; r[N_DPDFDT] = v[3];
-        }
-    // the chemical-potential and number-density blocks (eos.F90:659-670) are
-    // read for format validation only; no hydro quantity depends on them
-    for (int b = 0; b < 2 && ok; ++b)
-        for (int j = 0; j < JM && ok; ++j)
-            for (int i = 0; i < IM && ok; ++i)
-                if (!read_record(fp, v, 4)) ok = false;
-    fclose(fp);
-    if (!ok) {
+    if (rc != 0) {
         set_error(CASTRO_ERR_TABLE_IO, "eos_init: helm_table.dat is truncated or malformed");
         return CASTRO_ERR_TABLE_IO;
     }
-    std::vector<double> trow((size_t)JM * ROW_STRIDE, 0.0), drow((size_t)IM * ROW_STRIDE, 0.0);
-    for (int j = 0; j < JM; ++j) {
-        double dt = (j < JM - 1) ? t[j + 1] - t[j] : 0.0;
-        double dt2 = dt * dt;
-        trow[(size_t)j * ROW_STRIDE + 0] = t[j];
-        trow[(size_t)j * ROW_STRIDE + 1] = dt;
-        trow[(size_t)j * ROW_STRIDE + 2] = dt2;
-        trow[(size_t)j * ROW_STRIDE + 3] = (j < JM - 1) ? 1.0 / dt : 0.0;
-        trow[(size_t)j * ROW_STRIDE + 4] = (j < JM - 1) ? 1.0 / dt2 : 0.0;
-    }
-    for (int i = 0; i < IM; ++i) {
-        double dd = (i < IM - 1) ? d[i + 1] - d[i] : 0.0;
-        double dd2 = dd * dd;
-        drow[(size_t)i * ROW_STRIDE + 0] = d[i];
-        drow[(size_t)i * ROW_STRIDE + 1] = dd;
-        drow[(size_t)i * ROW_STRIDE + 2] = dd2;
-        drow[(size_t)i * ROW_STRIDE + 3] = (i < IM - 1) ? 1.0 / dd : 0.0;
-        drow[(size_t)i * ROW_STRIDE + 4] = (i < IM - 1) ? 1.0 / dd2 : 0.0;
-    }
-
     eos_finalize();
-    cudaError_t e = cudaMalloc(&d_node, node.size() * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&d_trow, trow.size() * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&d_drow, drow.size() * sizeof(double));
+    cudaError_t e = cudaMalloc(&d_node, T.node.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_trow, T.trow.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_drow, T.drow.size() * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&d_fail, sizeof(unsigned long long));
-    if (e == cudaSuccess) e = cudaMemcpy(d_node, node.data(), node.size() * sizeof(double), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(d_trow, trow.data(), trow.size() * sizeof(double), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(d_drow, drow.data(), drow.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_node, T.node.data(), T.node.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_trow, T.trow.data(), T.trow.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_drow, T.drow.data(), T.drow.size() * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(d_fail, 0, sizeof(unsigned long long));
     if (e != cudaSuccess) {
         set_error(CASTRO_ERR_CUDA, cudaGetErrorString(e));
         return CASTRO_ERR_CUDA;
     }
-    // physical constants, Source/eos.F90:129-137
-    const double h = 6.6260689633e-27, avo_eos = 6.0221417930e23, clight = 2.99792458e10;
-    const double kerg = 1.380650424e-16, amu = 1.66053878283e-24;
-    const double asol = 4.0 * 5.67051e-5 / clight;
+    g_eos = T.consts;
     g_eos.node = d_node;
     g_eos.trow = d_trow;
     g_eos.drow = d_drow;
-    g_eos.tlo = tlo;
-    g_eos.dlo = dlo;
-    g_eos.tstpi = 1.0 / tstp;
-    g_eos.dstpi = 1.0 / dstp;
-    g_eos.mintemp = pow(10.0, tlo);
-    g_eos.asoli3 = asol / 3.0;
-    g_eos.kergavo = kerg * avo_eos;
-    g_eos.avo_eos = avo_eos;
-    g_eos.sioncon = (2.0 * M_PI * amu * kerg) / (h * h);
     g_eos.fail_count = d_fail;
     g_table = true;
     upload_all();
