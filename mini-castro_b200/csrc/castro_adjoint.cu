@@ -18,9 +18,12 @@
 // Scatter-adds into shared adjoint arrays use FP64 atomics, so the last bits
 // of a gradient may differ from run to run.
 #include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
+#include <string>
 #include <vector>
 
 #include "castro_adjoint.cuh"
@@ -201,14 +204,14 @@ void ctoprim_adj_impl(const int* lo, const int* hi, Fab U, Fab QB, Fab QAB, Fab 
 }
 
 template <int NS>
-void clean_state_adj_impl(const int* lo, const int* hi, Fab U, Fab UB)
+void clean_state_adj_impl(const int* lo, const int* hi, Fab U, Fab UB, bool frozen = false)
 {
     launch_box("clean_state_adj", lo, hi, [=] __device__(int i, int j, int k) {
         constexpr int NV = Dims<NS>::NVAR;
         double u[NV], ub[NV];
 #pragma unroll
         for (int n = 0; n < NV; ++n) { u[n] = U(i, j, k, n); ub[n] = UB(i, j, k, n); }
-        clean_state_pt_adj<NS>(c_eos, c_net, u, ub);
+        clean_state_pt_adj<NS>(c_eos, c_net, u, ub, frozen);
 #pragma unroll
         for (int n = 0; n < NV; ++n) UB(i, j, k, n) = ub[n];
     });
@@ -428,7 +431,7 @@ void normalize_species_fluxes_adj_impl(const int* lo, const int* hi, Fab FX, Fab
         double facb = 0.0;
 #pragma unroll
         for (int n = 0; n < NS; ++n) facb += FXB(i, j, k, UFS + n) * FX(i, j, k, UFS + n);
-        const double sumb = -facb * fr / (sum * sum);
+        const double sumb = -(facb / sum) * fac;
         FXB(i, j, k, URHO) += facb / sum;
 #pragma unroll
         for (int n = 0; n < NS; ++n) FXB(i, j, k, UFS + n) = FXB(i, j, k, UFS + n) * fac + sumb;
@@ -771,10 +774,83 @@ void fill_clean_adj(castro_adj* a)
 #pragma unroll
         for (int n = 0; n < NV; ++n) { u[n] = A(ii, jj, kk, n); ub[n] = SB(i, j, k, n); any |= ub[n] != 0.0; }
         if (!any) return;
-        clean_state_pt_adj<NS>(c_eos, c_net, u, ub);
+        clean_state_pt_adj<NS>(c_eos, c_net, u, ub, true);
 #pragma unroll
         for (int n = 0; n < NV; ++n) aadd(&AB(ii, jj, kk, n), ub[n]);
     });
+}
+
+// diagnostics: with CASTRO_ADJ_CHECK set, every adjoint array is scanned after
+// each reverse stage and the first stage that leaves a non-finite value is
+// reported through castro_last_error
+__global__ void k_nonfinite(const double* p, long long n, int* flag, double* amax)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) {
+        if (!isfinite(p[t])) atomicExch(flag, 1);
+        else if (amax) {
+            double a = fabs(p[t]);
+            if (a > 0.0) atomicMax((unsigned long long*)amax, (unsigned long long)__double_as_longlong(a));
+        }
+    }
+}
+
+int adj_check_level()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char* e = getenv("CASTRO_ADJ_CHECK");
+        on = e ? atoi(e) : 0;
+        if (e && on == 0) on = 1;
+    }
+    return on;
+}
+bool adj_check_enabled() { return adj_check_level() > 0; }
+
+void adj_check(castro_adj* a, const char* stage)
+{
+    if (!adj_check_enabled()) return;
+    std::vector<std::pair<const char*, const Arr*>> arrs = {
+        {"Vb", &a->Vb}, {"Ab", &a->Ab}, {"Sbb", &a->Sbb}, {"qb", &a->qb}, {"qab", &a->qab}, {"divb", &a->divb},
+        {"srcb", &a->srcb}};
+    static const char* nm3[3] = {"x", "y", "z"};
+    for (int d = 0; d < 3; ++d) {
+        arrs.push_back({"F1b", &a->F1b[d]}); arrs.push_back({"G1b", &a->G1b[d]});
+        arrs.push_back({"qlb", &a->qlb[d]}); arrs.push_back({"qrb", &a->qrb[d]});
+        arrs.push_back({"fluxb", &a->fluxb[d]}); arrs.push_back({"qeb", &a->qeb[d]});
+        for (int e = 0; e < 3; ++e) {
+            arrs.push_back({"qmb", &a->qmb[d][e]}); arrs.push_back({"qpb", &a->qpb[d][e]});
+            arrs.push_back({"F2b", &a->F2b[d][e]}); arrs.push_back({"G2b", &a->G2b[d][e]});
+        }
+    }
+    (void)nm3;
+    const bool mags = adj_check_level() >= 2;
+    std::string line;
+    for (auto& pr : arrs) {
+        cudaMemsetAsync(a->d_idx, 0, sizeof(int), a->st);
+        cudaMemsetAsync(a->d_scal + 31, 0, sizeof(double), a->st);
+        long long n = pr.second->n();
+        k_nonfinite<<<(unsigned)((n + 255) / 256), 256, 0, a->st>>>(pr.second->p, n, a->d_idx,
+                                                                     mags ? a->d_scal + 31 : nullptr);
+        int f = 0;
+        double mx = 0.0;
+        cudaMemcpyAsync(&f, a->d_idx, sizeof f, cudaMemcpyDeviceToHost, a->st);
+        cudaMemcpyAsync(&mx, a->d_scal + 31, sizeof mx, cudaMemcpyDeviceToHost, a->st);
+        cudaStreamSynchronize(a->st);
+        if (mags && mx > 0.0) {
+            char b[64];
+            snprintf(b, sizeof b, " %s=%.1e", pr.first, mx);
+            line += b;
+        }
+        if (f) {
+            char buf[160];
+            snprintf(buf, sizeof buf, "adjoint check: non-finite %s after %s", pr.first, stage);
+            fprintf(stderr, "%s\n", buf);
+            set_error(CASTRO_ERR_EOS, buf);
+            return;
+        }
+    }
+    if (mags) fprintf(stderr, "[%s]%s\n", stage, line.c_str());
 }
 
 // B = A + dt*src (valid box); Saxpy of Source/Castro_advance.cpp:74
@@ -951,8 +1027,9 @@ double reverse_step(castro_adj* a, const Arr& Vn, double dt)
     cudaMemsetAsync(a->d_scal, 0, 32 * sizeof(double), st);
     double* sc = a->d_scal;
     // V_{n+1} = clean(C), C = clean(B)
-    clean_state_adj_impl<NS>(bx.lo, bx.hi, a->Cs.fab(), a->Vb.fab());
-    clean_state_adj_impl<NS>(bx.lo, bx.hi, a->Bs.fab(), a->Vb.fab());
+    clean_state_adj_impl<NS>(bx.lo, bx.hi, a->Cs.fab(), a->Vb.fab(), true);
+    clean_state_adj_impl<NS>(bx.lo, bx.hi, a->Bs.fab(), a->Vb.fab(), true);
+    adj_check(a, "end cleans");
     // B = A + dt*src: Ab = Bb, srcb = dt*Bb, dtb += sum(src*Bb)
     {
         Fab BB = a->Vb.fab(), AB = a->Ab.fab(), SB = a->srcb.fab(), S = a->src.fab();
@@ -968,10 +1045,12 @@ double reverse_step(castro_adj* a, const Arr& Vn, double dt)
             return s;
         }, sc + 9);
     }
+    adj_check(a, "saxpy");
     fill_hydro_source_adj_impl<NS>(bx.lo, bx.hi, a->srcb.fab(), a->qe[0].fab(), a->qe[1].fab(), a->qe[2].fab(),
                                    a->area[0].fab(), a->area[1].fab(), a->area[2].fab(), a->vol.fab(), a->dx[0],
                                    a->dx[1], a->dx[2], a->fluxb[0].fab(), a->fluxb[1].fab(), a->fluxb[2].fab(),
                                    a->qeb[0].fab(), a->qeb[1].fab(), a->qeb[2].fab());
+    adj_check(a, "fill_hydro_source");
     for (int d = 0; d < 3; ++d) {
         normalize_species_fluxes_adj_impl<NS>(a->ebx[d].lo, a->ebx[d].hi, a->Fav[d].fab(), a->fluxb[d].fab());
         apply_av_adj_impl<NS>(a->ebx[d].lo, a->ebx[d].hi, d, a->dx[d], a->div.fab(), a->Sb.fab(), a->fluxb[d].fab(),
@@ -979,6 +1058,7 @@ double reverse_step(castro_adj* a, const Arr& Vn, double dt)
         compute_flux_adj_impl<NS>(a->ebx[d].lo, a->ebx[d].hi, a->ql[d].fab(), a->qr[d].fab(), a->qaux.fab(),
                                   a->fluxb[d].fab(), a->qeb[d].fab(), a->qlb[d].fab(), a->qrb[d].fab(), a->qab.fab(), d);
     }
+    adj_check(a, "normalize/av/riemann3");
     double hdtdx[3], cdtdx[3];
     for (int d = 0; d < 3; ++d) { hdtdx[d] = 0.5 * dt / a->dx[d]; cdtdx[d] = dt / a->dx[d] / 3.0; }
     for (int d = 0; d < 3; ++d) {
@@ -989,6 +1069,7 @@ double reverse_step(castro_adj* a, const Arr& Vn, double dt)
                             a->qpb[d][d].fab(), a->qab.fab(), a->F2b[t1][t2].fab(), a->F2b[t2][t1].fab(),
                             a->G2b[t1][t2].fab(), a->G2b[t2][t1].fab(), sc + 6 + t1, sc + 6 + t2);
     }
+    adj_check(a, "trans2");
     for (int x = 0; x < 3; ++x)
         for (int y = 0; y < 3; ++y) {
             if (x == y) continue;
@@ -996,6 +1077,7 @@ double reverse_step(castro_adj* a, const Arr& Vn, double dt)
                                       a->qaux.fab(), a->F2b[x][y].fab(), a->G2b[x][y].fab(), a->qmb[x][y].fab(),
                                       a->qpb[x][y].fab(), a->qab.fab(), x);
         }
+    adj_check(a, "riemann2");
     for (int d = 0; d < 3; ++d)
         for (int tt = 0; tt < 2; ++tt) {
             int t = (tt == 0) ? (d == 0 ? 1 : 0) : (d == 2 ? 1 : 2);
@@ -1004,17 +1086,24 @@ double reverse_step(castro_adj* a, const Arr& Vn, double dt)
                                 a->qpb[t][d].fab(), a->qmb[t][t].fab(), a->qpb[t][t].fab(), a->qab.fab(),
                                 a->F1b[d].fab(), a->G1b[d].fab(), sc + 3 + d);
         }
+    adj_check(a, "trans1");
     for (int d = 0; d < 3; ++d)
         compute_flux_adj_impl<NS>(a->tbx[d][d].lo, a->tbx[d][d].hi, a->qm[d][d].fab(), a->qp[d][d].fab(),
                                   a->qaux.fab(), a->F1b[d].fab(), a->G1b[d].fab(), a->qmb[d][d].fab(),
                                   a->qpb[d][d].fab(), a->qab.fab(), d);
+    adj_check(a, "riemann1");
     for (int d = 0; d < 3; ++d)
         trace_adj_impl<NS>(obx.lo, obx.hi, bx.lo, bx.hi, d, a->q.fab(), a->qaux.fab(), a->qmb[d][d].fab(),
                            a->qpb[d][d].fab(), a->qb.fab(), a->qab.fab(), dt / a->dx[d], sc + d);
+    adj_check(a, "trace");
     divu_adj_impl<NS>(obx.lo, obx.hi, a->divb.fab(), a->qb.fab(), a->dx[0], a->dx[1], a->dx[2]);
+    adj_check(a, "divu");
     ctoprim_adj_impl<NS>(qbx.lo, qbx.hi, a->Sb.fab(), a->qb.fab(), a->qab.fab(), a->Sbb.fab());
+    adj_check(a, "ctoprim");
     fill_clean_adj<NS>(a);
-    clean_state_adj_impl<NS>(bx.lo, bx.hi, Vn.fab(), a->Ab.fab());
+    adj_check(a, "sborder fill+clean");
+    clean_state_adj_impl<NS>(bx.lo, bx.hi, Vn.fab(), a->Ab.fab(), true);
+    adj_check(a, "start clean");
     copy(a->Vb, a->Ab, st);
     double h[16];
     cudaMemcpyAsync(h, sc, 16 * sizeof(double), cudaMemcpyDeviceToHost, st);
