@@ -148,6 +148,44 @@ __device__ __forceinline__ void aadd_tflux(const Fab& f, const Fab& qg, int i, i
 }
 
 // box launch whose body returns a double; the block sums are added to *out
+// Per-block partials of the scalar reductions go to a device buffer (no
+// same-address atomics from thousands of blocks); a one-block kernel then adds
+// their sum to the output scalar(s).
+constexpr int PART_MAX = 1 << 20;
+// PART_MAX x 2 doubles, allocated on first use; shared by every reduction of
+// this library, which are issued on the library stream one after another
+double* g_part = nullptr;
+
+__global__ void k_finish_sum(const double* part, int nb, double* out0, double* out1)
+{
+    __shared__ double red[2][32];
+    double s0 = 0.0, s1 = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) { s0 += part[2 * b]; s1 += part[2 * b + 1]; }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    }
+    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = s0; red[1][threadIdx.x >> 5] = s1; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { a += red[0][w]; b += red[1][w]; }
+        if (out0) *out0 += a;
+        if (out1) *out1 += b;
+    }
+}
+
+bool part_buffer()
+{
+    if (!g_part && cudaMalloc(&g_part, sizeof(double) * 2 * PART_MAX) != cudaSuccess) {
+        g_part = nullptr;
+        set_error(CASTRO_ERR_CUDA, "adjoint: partial-sum buffer");
+        return false;
+    }
+    return true;
+}
+
 template <class F>
 __global__ void k_box_sum(BoxRange r, F f, double* out)
 {
@@ -168,17 +206,91 @@ __global__ void k_box_sum(BoxRange r, F f, double* out)
     if (threadIdx.x == 0) {
         double s = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-        if (out && s != 0.0) atomicAdd(out, s);
+        out[2 * blockIdx.x] = s;
+        out[2 * blockIdx.x + 1] = 0.0;
+    }
+}
+
+// same with two sums: the body returns a double2
+template <class F>
+__global__ void k_box_sum2(BoxRange r, F f, double* out0)
+{
+    __shared__ double red[2][32];
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double2 v = make_double2(0.0, 0.0);
+    if (t < r.n) {
+        int i = r.lx + (int)(t % r.nx);
+        long long t2 = t / r.nx;
+        int j = r.ly + (int)(t2 % r.ny);
+        int k = r.lz + (int)(t2 / r.ny);
+        v = f(i, j, k);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = v.x; red[1][threadIdx.x >> 5] = v.y; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { s0 += red[0][w]; s1 += red[1][w]; }
+        out0[2 * blockIdx.x] = s0;
+        out0[2 * blockIdx.x + 1] = s1;
     }
 }
 
 template <class F>
+void launch_sum2(const char* what, const int* lo, const int* hi, F f, double* out0, double* out1)
+{
+    BoxRange r = make_range(lo, hi);
+    if (r.n == 0) return;
+    const int B = 128;
+    const long long nb = (r.n + B - 1) / B;
+    if (nb > PART_MAX || !part_buffer()) { set_error(CASTRO_ERR_ARG, "adjoint: box too large for the partial sums"); return; }
+    k_box_sum2<<<(unsigned)nb, B, 0, stream()>>>(r, f, g_part);
+    if (out0 || out1) k_finish_sum<<<1, 256, 0, stream()>>>(g_part, (int)nb, out0, out1);
+    check_launch(what);
+}
+
+// k_box_sum with a register budget for MINB resident blocks of 128 threads
+template <int MINB, class F>
+__global__ void __launch_bounds__(128, MINB) k_box_sum_lb(BoxRange r, F f, double* out)
+{
+    __shared__ double red[32];
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (t < r.n) {
+        int i = r.lx + (int)(t % r.nx);
+        long long t2 = t / r.nx;
+        int j = r.ly + (int)(t2 % r.ny);
+        int k = r.lz + (int)(t2 / r.ny);
+        v = f(i, j, k);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+        out[2 * blockIdx.x] = s;
+        out[2 * blockIdx.x + 1] = 0.0;
+    }
+}
+
+// MINB = 0: no register budget (the compiler's choice)
+template <int MINB = 0, class F>
 void launch_sum(const char* what, const int* lo, const int* hi, F f, double* out)
 {
     BoxRange r = make_range(lo, hi);
     if (r.n == 0) return;
     const int B = 128;
-    k_box_sum<<<(unsigned)((r.n + B - 1) / B), B, 0, stream()>>>(r, f, out);
+    const long long nb = (r.n + B - 1) / B;
+    if (nb > PART_MAX || !part_buffer()) { set_error(CASTRO_ERR_ARG, "adjoint: box too large for the partial sums"); return; }
+    if (MINB == 0) k_box_sum<<<(unsigned)nb, B, 0, stream()>>>(r, f, g_part);
+    else k_box_sum_lb<(MINB > 0 ? MINB : 1)><<<(unsigned)nb, B, 0, stream()>>>(r, f, g_part);
+    if (out) k_finish_sum<<<1, 256, 0, stream()>>>(g_part, (int)nb, out, nullptr);
     check_launch(what);
 }
 
@@ -242,7 +354,7 @@ template <int NS, int D>
 void trace_adj_dir(const int* lo, const int* hi, int vl, int vh, Fab Q, Fab QA, Fab QMB, Fab QPB, Fab QB, Fab QAB,
                    double dtdx, double* dtdxb)
 {
-    launch_sum("trace_ppm_adj", lo, hi, [=] __device__(int i, int j, int k) -> double {
+    launch_sum<4>("trace_ppm_adj", lo, hi, [=] __device__(int i, int j, int k) -> double {
         constexpr int NQS = Dims<NS>::NQS;
         QLoad ld{Q, QA};
         AtomicSink sk{QB, QAB};
@@ -344,9 +456,7 @@ void trans2_adj_impl(const int* lo, const int* hi, int idir1, int idir2, int idi
                      Fab F3, Fab G2, Fab G3, double cdtdx2, double cdtdx3, Fab QMOB, Fab QPOB, Fab QMB, Fab QPB, Fab QAB,
                      Fab F2B, Fab F3B, Fab G2B, Fab G3B, double* cdtdx2b, double* cdtdx3b)
 {
-    // two scalar adjoints: the block sum of each goes through its own launch
-    // slot, so the body returns the cdtdx2 part and adds the cdtdx3 part atomically
-    launch_sum("trans2_adj", lo, hi, [=] __device__(int i, int j, int k) -> double {
+    launch_sum2("trans2_adj", lo, hi, [=] __device__(int i, int j, int k) -> double2 {
         constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF;
         const int e1x = idir1 == 0, e1y = idir1 == 1, e1z = idir1 == 2;
         const int e2x = idir2 == 0, e2y = idir2 == 1, e2z = idir2 == 2;
@@ -377,9 +487,8 @@ void trans2_adj_impl(const int* lo, const int* hi, int idir1, int idir2, int idi
             aadd_tflux<NS>(F3B, G3B, il, jl, kl, idir3, f3lb);
             aadd(&QAB(il, jl, kl, QGAMC), gb);
         }
-        if (cdtdx3b) aadd(cdtdx3b, c3);
-        return c2;
-    }, cdtdx2b);
+        return make_double2(c2, c3);
+    }, cdtdx2b, cdtdx3b);
 }
 
 template <int NS>
@@ -666,6 +775,11 @@ __device__ __forceinline__ int map_bc_adj(int i, int lo, int hi, int bc)
 
 }  // namespace
 
+struct Prim {
+    Arr A, Bs, Cs, Sb, q, qaux, div, qint, qm[3][3], qp[3][3], F1[3], G1[3], F2[3][3], G2[3][3], ql[3], qr[3];
+    Arr Fav[3], flux[3], qe[3], src;
+};
+
 struct castro_adj {
     int ns = 2, nv = 9, qv = 10;
     IBx bx{}, obx{}, qbx{}, ebx[3], gebx[3], tbx[3][3];
@@ -677,14 +791,23 @@ struct castro_adj {
     double shell_r0 = 0.3, shell_r1 = 0.4;
     cudaStream_t st = nullptr;
     std::vector<char*> blocks;
+    std::vector<Arr> all;   // every allocation (size accounting)
     // primal
     std::vector<Arr> ckpts;   // V at steps 0, ckpt, 2 ckpt, ...
     std::vector<Arr> seg;     // V_n of the segment being reversed
-    Arr V, A, Bs, Cs, Sb, q, qaux, div, qint, qm[3][3], qp[3][3], F1[3], G1[3], F2[3][3], G2[3][3], ql[3], qr[3];
-    Arr Fav[3], flux[3], qe[3], area[3], vol, src, Vfinal;
+    // forward intermediates of one step; one set per step of a checkpoint
+    // segment when device memory allows (the reverse then reads the set the
+    // segment recomputation filled), else one set recomputed per step
+    std::vector<Prim> sets;
+    Prim* P = nullptr;
+    Arr V, area[3], vol, Vfinal;
     // adjoint
     Arr Vb, Ab, Sbb, qb, qab, divb, qmb[3][3], qpb[3][3], F1b[3], G1b[3], F2b[3][3], G2b[3][3], qlb[3], qrb[3];
     Arr fluxb[3], qeb[3], srcb;
+    // per-zone flux-record adjoints of the zone-based transverse reverses:
+    // T1L/T1R[d][t] for trans1 (flux d correcting states normal to t),
+    // T2L/T2R[d][0|1] for trans2 of direction d (fluxes t1|t2 and t2|t1)
+    Arr T1L[3][3], T1R[3][3], T2L[3][2], T2R[3][2];
     double* d_scal = nullptr;   // [32] scalar accumulators
     int* d_idx = nullptr;
     double* d_est = nullptr;
@@ -692,6 +815,7 @@ struct castro_adj {
     std::vector<char> limited, clamped;
     double J = 0.0;
     bool fwd_done = false;
+    bool last_seg_ready = false;   // the forward left the last segment's states and intermediates
     float ms_forward = 0.0f, ms_backward = 0.0f;
 };
 
@@ -712,6 +836,7 @@ bool alloc_arr(castro_adj* a, Arr& r, const IBx& b, int nc)
     if (cudaMalloc(&p, bytes) != cudaSuccess) return false;
     a->blocks.push_back(p);
     r.p = (double*)p;
+    a->all.push_back(r);
     return true;
 }
 
@@ -745,7 +870,7 @@ void clean(const IBx& b, const Arr& u)
 template <int NS>
 void fill_sborder(castro_adj* a)
 {
-    Fab S = a->Sb.fab(), A = a->A.fab();
+    Fab S = a->P->Sb.fab(), A = a->P->A.fab();
     const int bc = a->bc;
     const IBx bx = a->bx;
     launch_box("adj fill", a->qbx.lo, a->qbx.hi, [=] __device__(int i, int j, int k) {
@@ -761,7 +886,7 @@ void fill_sborder(castro_adj* a)
 template <int NS>
 void fill_clean_adj(castro_adj* a)
 {
-    Fab SB = a->Sbb.fab(), A = a->A.fab(), AB = a->Ab.fab();
+    Fab SB = a->Sbb.fab(), A = a->P->A.fab(), AB = a->Ab.fab();
     const int bc = a->bc;
     const IBx bx = a->bx;
     launch_box("adj fill_clean", a->qbx.lo, a->qbx.hi, [=] __device__(int i, int j, int k) {
@@ -806,6 +931,14 @@ int adj_check_level()
     return on;
 }
 bool adj_check_enabled() { return adj_check_level() > 0; }
+
+void adj_check(castro_adj* a, const char* stage);
+void adj_mark(castro_adj* a, const char* name);
+inline void adj_stage(castro_adj* a, const char* stage)
+{
+    adj_check(a, stage);
+    adj_mark(a, stage);
+}
 
 void adj_check(castro_adj* a, const char* stage)
 {
@@ -853,6 +986,54 @@ void adj_check(castro_adj* a, const char* stage)
     if (mags) fprintf(stderr, "[%s]%s\n", stage, line.c_str());
 }
 
+// stage timing: with CASTRO_ADJ_PROFILE set, CUDA events between the stages of
+// the reverse sweep; castro_adj_backward prints the accumulated table
+struct AdjProf {
+    std::vector<std::pair<std::string, cudaEvent_t>> marks;
+    std::vector<std::pair<std::string, double>> total;
+};
+AdjProf g_prof;
+bool adj_prof_enabled()
+{
+    static int on = -1;
+    if (on < 0) on = getenv("CASTRO_ADJ_PROFILE") ? 1 : 0;
+    return on == 1;
+}
+void adj_mark(castro_adj* a, const char* name)
+{
+    if (!adj_prof_enabled()) return;
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, a->st);
+    g_prof.marks.push_back({name, e});
+}
+void adj_prof_flush()
+{
+    if (!adj_prof_enabled() || g_prof.marks.empty()) return;
+    cudaEventSynchronize(g_prof.marks.back().second);
+    for (size_t i = 1; i < g_prof.marks.size(); ++i) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, g_prof.marks[i - 1].second, g_prof.marks[i].second);
+        const std::string& nm = g_prof.marks[i].first;
+        bool found = false;
+        for (auto& t : g_prof.total)
+            if (t.first == nm) { t.second += ms; found = true; break; }
+        if (!found) g_prof.total.push_back({nm, ms});
+    }
+    for (auto& m : g_prof.marks) cudaEventDestroy(m.second);
+    g_prof.marks.clear();
+}
+void adj_prof_report()
+{
+    if (!adj_prof_enabled()) return;
+    adj_prof_flush();
+    double sum = 0.0;
+    for (auto& t : g_prof.total) sum += t.second;
+    fprintf(stderr, "adjoint stage times (ms, summed over the sweep):\n");
+    for (auto& t : g_prof.total) fprintf(stderr, "  %-28s %9.3f  %5.1f%%\n", t.first.c_str(), t.second, 100.0 * t.second / sum);
+    g_prof.total.clear();
+}
+
 // B = A + dt*src (valid box); Saxpy of Source/Castro_advance.cpp:74
 __global__ void k_saxpy_adj(const double* a, const double* src, double* b, long long n, double dt)
 {
@@ -865,31 +1046,31 @@ template <int NS>
 void forward_step(castro_adj* a, const Arr& Vin, double dt)
 {
     cudaStream_t st = a->st;
-    copy(a->A, Vin, st);
-    clean(a->bx, a->A);                                        // clean_state(S_old)
+    copy(a->P->A, Vin, st);
+    clean(a->bx, a->P->A);                                        // clean_state(S_old)
     fill_sborder<NS>(a);
-    clean(a->qbx, a->Sb);                                      // clean_state(Sborder)
+    clean(a->qbx, a->P->Sb);                                      // clean_state(Sborder)
     const IBx &bx = a->bx, &obx = a->obx, &qbx = a->qbx;
-    ctoprim(qbx.lo, qbx.hi, a->Sb.p, qbx.lo, qbx.hi, a->q.p, qbx.lo, qbx.hi, a->qaux.p, qbx.lo, qbx.hi);
-    divu(obx.lo, obx.hi, a->q.p, qbx.lo, qbx.hi, a->dx, a->div.p, obx.lo, obx.hi);
+    ctoprim(qbx.lo, qbx.hi, a->P->Sb.p, qbx.lo, qbx.hi, a->P->q.p, qbx.lo, qbx.hi, a->P->qaux.p, qbx.lo, qbx.hi);
+    divu(obx.lo, obx.hi, a->P->q.p, qbx.lo, qbx.hi, a->dx, a->P->div.p, obx.lo, obx.hi);
     double hdtdx[3], cdtdx[3];
     for (int d = 0; d < 3; ++d) { hdtdx[d] = 0.5 * dt / a->dx[d]; cdtdx[d] = dt / a->dx[d] / 3.0; }
     for (int d = 0; d < 3; ++d)
-        trace_ppm(obx.lo, obx.hi, bx.lo, bx.hi, d + 1, a->q.p, qbx.lo, qbx.hi, a->qaux.p, qbx.lo, qbx.hi,
-                  a->qm[d][d].p, a->qm[d][d].b.lo, a->qm[d][d].b.hi, a->qp[d][d].p, a->qp[d][d].b.lo,
-                  a->qp[d][d].b.hi, bx.lo, bx.hi, a->dx, dt);
+        trace_ppm(obx.lo, obx.hi, bx.lo, bx.hi, d + 1, a->P->q.p, qbx.lo, qbx.hi, a->P->qaux.p, qbx.lo, qbx.hi,
+                  a->P->qm[d][d].p, a->P->qm[d][d].b.lo, a->P->qm[d][d].b.hi, a->P->qp[d][d].p, a->P->qp[d][d].b.lo,
+                  a->P->qp[d][d].b.hi, bx.lo, bx.hi, a->dx, dt);
     for (int d = 0; d < 3; ++d) {
         const IBx& b = a->tbx[d][d];
-        compute_flux(b.lo, b.hi, a->qm[d][d].p, a->qm[d][d].b.lo, a->qm[d][d].b.hi, a->qp[d][d].p, a->qp[d][d].b.lo,
-                     a->qp[d][d].b.hi, a->F1[d].p, obx.lo, obx.hi, a->qint.p, obx.lo, obx.hi, a->G1[d].p, obx.lo,
-                     obx.hi, a->qaux.p, qbx.lo, qbx.hi, d + 1);
+        compute_flux(b.lo, b.hi, a->P->qm[d][d].p, a->P->qm[d][d].b.lo, a->P->qm[d][d].b.hi, a->P->qp[d][d].p, a->P->qp[d][d].b.lo,
+                     a->P->qp[d][d].b.hi, a->P->F1[d].p, obx.lo, obx.hi, a->P->qint.p, obx.lo, obx.hi, a->P->G1[d].p, obx.lo,
+                     obx.hi, a->P->qaux.p, qbx.lo, qbx.hi, d + 1);
         for (int tt = 0; tt < 2; ++tt) {
             int t = (tt == 0) ? (d == 0 ? 1 : 0) : (d == 2 ? 1 : 2);
             const IBx& tb = a->tbx[t][d];
-            trans1(tb.lo, tb.hi, d + 1, t + 1, a->qm[t][t].p, a->qm[t][t].b.lo, a->qm[t][t].b.hi, a->qm[t][d].p,
-                   a->qm[t][d].b.lo, a->qm[t][d].b.hi, a->qp[t][t].p, a->qp[t][t].b.lo, a->qp[t][t].b.hi,
-                   a->qp[t][d].p, a->qp[t][d].b.lo, a->qp[t][d].b.hi, a->qaux.p, qbx.lo, qbx.hi, a->F1[d].p, obx.lo,
-                   obx.hi, a->G1[d].p, obx.lo, obx.hi, cdtdx[d]);
+            trans1(tb.lo, tb.hi, d + 1, t + 1, a->P->qm[t][t].p, a->P->qm[t][t].b.lo, a->P->qm[t][t].b.hi, a->P->qm[t][d].p,
+                   a->P->qm[t][d].b.lo, a->P->qm[t][d].b.hi, a->P->qp[t][t].p, a->P->qp[t][t].b.lo, a->P->qp[t][t].b.hi,
+                   a->P->qp[t][d].p, a->P->qp[t][d].b.lo, a->P->qp[t][d].b.hi, a->P->qaux.p, qbx.lo, qbx.hi, a->P->F1[d].p, obx.lo,
+                   obx.hi, a->P->G1[d].p, obx.lo, obx.hi, cdtdx[d]);
         }
     }
     for (int d = 0; d < 3; ++d) {
@@ -897,41 +1078,41 @@ void forward_step(castro_adj* a, const Arr& Vin, double dt)
         for (int pp = 0; pp < 2; ++pp) {
             int x = pp == 0 ? t1 : t2, y = pp == 0 ? t2 : t1;
             const IBx& b = a->tbx[x][y];
-            compute_flux(b.lo, b.hi, a->qm[x][y].p, a->qm[x][y].b.lo, a->qm[x][y].b.hi, a->qp[x][y].p,
-                         a->qp[x][y].b.lo, a->qp[x][y].b.hi, a->F2[x][y].p, obx.lo, obx.hi, a->qint.p, obx.lo, obx.hi,
-                         a->G2[x][y].p, obx.lo, obx.hi, a->qaux.p, qbx.lo, qbx.hi, x + 1);
+            compute_flux(b.lo, b.hi, a->P->qm[x][y].p, a->P->qm[x][y].b.lo, a->P->qm[x][y].b.hi, a->P->qp[x][y].p,
+                         a->P->qp[x][y].b.lo, a->P->qp[x][y].b.hi, a->P->F2[x][y].p, obx.lo, obx.hi, a->P->qint.p, obx.lo, obx.hi,
+                         a->P->G2[x][y].p, obx.lo, obx.hi, a->P->qaux.p, qbx.lo, qbx.hi, x + 1);
         }
-        trans2(a->ebx[d].lo, a->ebx[d].hi, d + 1, t1 + 1, t2 + 1, a->qm[d][d].p, a->qm[d][d].b.lo, a->qm[d][d].b.hi,
-               a->ql[d].p, obx.lo, obx.hi, a->qp[d][d].p, a->qp[d][d].b.lo, a->qp[d][d].b.hi, a->qr[d].p, obx.lo,
-               obx.hi, a->qaux.p, qbx.lo, qbx.hi, a->F2[t1][t2].p, obx.lo, obx.hi, a->F2[t2][t1].p, obx.lo, obx.hi,
-               a->G2[t1][t2].p, obx.lo, obx.hi, a->G2[t2][t1].p, obx.lo, obx.hi, hdtdx[d], hdtdx[t1], hdtdx[t2]);
-        compute_flux(a->ebx[d].lo, a->ebx[d].hi, a->ql[d].p, obx.lo, obx.hi, a->qr[d].p, obx.lo, obx.hi,
-                     a->flux[d].p, a->gebx[d].lo, a->gebx[d].hi, a->qint.p, obx.lo, obx.hi, a->qe[d].p,
-                     a->gebx[d].lo, a->gebx[d].hi, a->qaux.p, qbx.lo, qbx.hi, d + 1);
+        trans2(a->ebx[d].lo, a->ebx[d].hi, d + 1, t1 + 1, t2 + 1, a->P->qm[d][d].p, a->P->qm[d][d].b.lo, a->P->qm[d][d].b.hi,
+               a->P->ql[d].p, obx.lo, obx.hi, a->P->qp[d][d].p, a->P->qp[d][d].b.lo, a->P->qp[d][d].b.hi, a->P->qr[d].p, obx.lo,
+               obx.hi, a->P->qaux.p, qbx.lo, qbx.hi, a->P->F2[t1][t2].p, obx.lo, obx.hi, a->P->F2[t2][t1].p, obx.lo, obx.hi,
+               a->P->G2[t1][t2].p, obx.lo, obx.hi, a->P->G2[t2][t1].p, obx.lo, obx.hi, hdtdx[d], hdtdx[t1], hdtdx[t2]);
+        compute_flux(a->ebx[d].lo, a->ebx[d].hi, a->P->ql[d].p, obx.lo, obx.hi, a->P->qr[d].p, obx.lo, obx.hi,
+                     a->P->flux[d].p, a->gebx[d].lo, a->gebx[d].hi, a->P->qint.p, obx.lo, obx.hi, a->P->qe[d].p,
+                     a->gebx[d].lo, a->gebx[d].hi, a->P->qaux.p, qbx.lo, qbx.hi, d + 1);
     }
     for (int d = 0; d < 3; ++d) {
-        apply_av(a->ebx[d].lo, a->ebx[d].hi, d + 1, a->dx, a->div.p, obx.lo, obx.hi, a->Sb.p, qbx.lo, qbx.hi,
-                 a->flux[d].p, a->gebx[d].lo, a->gebx[d].hi);
-        copy(a->Fav[d], a->flux[d], st);
-        normalize_species_fluxes(a->ebx[d].lo, a->ebx[d].hi, a->flux[d].p, a->gebx[d].lo, a->gebx[d].hi);
+        apply_av(a->ebx[d].lo, a->ebx[d].hi, d + 1, a->dx, a->P->div.p, obx.lo, obx.hi, a->P->Sb.p, qbx.lo, qbx.hi,
+                 a->P->flux[d].p, a->gebx[d].lo, a->gebx[d].hi);
+        copy(a->P->Fav[d], a->P->flux[d], st);
+        normalize_species_fluxes(a->ebx[d].lo, a->ebx[d].hi, a->P->flux[d].p, a->gebx[d].lo, a->gebx[d].hi);
     }
-    zero(a->src, st);                                          // hydro_source.setVal(0)
-    fill_hydro_source(bx.lo, bx.hi, a->Sb.p, qbx.lo, qbx.hi, a->q.p, qbx.lo, qbx.hi, a->src.p, bx.lo, bx.hi,
-                      a->flux[0].p, a->gebx[0].lo, a->gebx[0].hi, a->flux[1].p, a->gebx[1].lo, a->gebx[1].hi,
-                      a->flux[2].p, a->gebx[2].lo, a->gebx[2].hi, a->qe[0].p, a->gebx[0].lo, a->gebx[0].hi,
-                      a->qe[1].p, a->gebx[1].lo, a->gebx[1].hi, a->qe[2].p, a->gebx[2].lo, a->gebx[2].hi,
+    zero(a->P->src, st);                                          // hydro_source.setVal(0)
+    fill_hydro_source(bx.lo, bx.hi, a->P->Sb.p, qbx.lo, qbx.hi, a->P->q.p, qbx.lo, qbx.hi, a->P->src.p, bx.lo, bx.hi,
+                      a->P->flux[0].p, a->gebx[0].lo, a->gebx[0].hi, a->P->flux[1].p, a->gebx[1].lo, a->gebx[1].hi,
+                      a->P->flux[2].p, a->gebx[2].lo, a->gebx[2].hi, a->P->qe[0].p, a->gebx[0].lo, a->gebx[0].hi,
+                      a->P->qe[1].p, a->gebx[1].lo, a->gebx[1].hi, a->P->qe[2].p, a->gebx[2].lo, a->gebx[2].hi,
                       a->area[0].p, a->gebx[0].lo, a->gebx[0].hi, a->area[1].p, a->gebx[1].lo, a->gebx[1].hi,
                       a->area[2].p, a->gebx[2].lo, a->gebx[2].hi, a->vol.p, bx.lo, bx.hi, a->dx, dt);
-    long long n = a->A.n();
-    k_saxpy_adj<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a->A.p, a->src.p, a->Bs.p, n, dt);
-    copy(a->Cs, a->Bs, st);
-    clean(bx, a->Cs);                                          // clean_state(S_new), Castro_advance.cpp
+    long long n = a->P->A.n();
+    k_saxpy_adj<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a->P->A.p, a->P->src.p, a->P->Bs.p, n, dt);
+    copy(a->P->Cs, a->P->Bs, st);
+    clean(bx, a->P->Cs);                                          // clean_state(S_new), Castro_advance.cpp
 }
 
 // V_{n+1} = clean(C)
 void finish_step(castro_adj* a, const Arr& Vout)
 {
-    copy(Vout, a->Cs, a->st);
+    copy(Vout, a->P->Cs, a->st);
     clean(a->bx, Vout);                                        // post_timestep clean_state, Castro.cpp:369
 }
 
@@ -1011,6 +1192,163 @@ void estdt_adj(castro_adj* a, const Arr& V, double minval, double scale, const A
     });
 }
 
+// ---- zone-based transverse reverses (no atomics on flux records) -----------
+__host__ __device__ inline bool in_box(const IBx& b, int i, int j, int k)
+{
+    return i >= b.lo[0] && i <= b.hi[0] && j >= b.lo[1] && j <= b.hi[1] && k >= b.lo[2] && k <= b.hi[2];
+}
+
+template <int NS>
+__device__ __forceinline__ void st_rec(const Fab& F, int i, int j, int k, const double* r)
+{
+#pragma unroll
+    for (int n = 0; n < Dims<NS>::NTF; ++n) F(i, j, k, n) = r[n];
+}
+
+// trans1 (flux direction d corrects the states normal to t) over the zones
+// that feed its face box fb = tbx[t][d]: zone z owns the minus state of face
+// z+e_t and the plus state of face z, and both use the flux records of faces
+// z and z+e_d; their adjoints go to L[z] and R[z]
+template <int NS>
+void trans1_adj_zones(castro_adj* a, int d, int t, double cdtdx, double* cdtdxb)
+{
+    const Prim& P = *a->P;
+    const IBx fb = a->tbx[t][d];
+    IBx zb = fb;
+    zb.lo[t] -= 1;
+    Fab Q2M = P.qm[t][t].fab(), Q2P = P.qp[t][t].fab(), QA = P.qaux.fab(), F1 = P.F1[d].fab(), Q1 = P.G1[d].fab();
+    Fab MOB = a->qmb[t][d].fab(), POB = a->qpb[t][d].fab(), MB = a->qmb[t][t].fab(), PB = a->qpb[t][t].fab();
+    Fab QAB = a->qab.fab(), LF = a->T1L[d][t].fab(), RF = a->T1R[d][t].fab();
+    launch_sum<4>("trans1_adj zones", zb.lo, zb.hi, [=] __device__(int i, int j, int k) -> double {
+        constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF;
+        const int etx = t == 0, ety = t == 1, etz = t == 2;
+        const int edx = d == 0, edy = d == 1, edz = d == 2;
+        double fr[NTF], fl[NTF], frb[NTF], flb[NTF];
+        ld_tflux<NS>(F1, Q1, i + edx, j + edy, k + edz, d, fr);
+        ld_tflux<NS>(F1, Q1, i, j, k, d, fl);
+#pragma unroll
+        for (int n = 0; n < NTF; ++n) { frb[n] = 0.0; flb[n] = 0.0; }
+        const double gamc = QA(i, j, k, QGAMC);
+        double gb = 0.0, cb = 0.0;
+        double lq[NQS], lqob[NQS], lqb[NQS];
+        if (in_box(fb, i + etx, j + ety, k + etz)) {   // minus state of face z+e_t
+            ld_state<NS>(Q2M, i + etx, j + ety, k + etz, lq);
+            ld_state<NS>(MOB, i + etx, j + ety, k + etz, lqob);
+#pragma unroll
+            for (int n = 0; n < NQS; ++n) lqb[n] = 0.0;
+            trans1_state_adj<NS>(lq, fr, fl, gamc, cdtdx, lqob, lqb, frb, flb, gb, cb);
+            add_state<NS>(MB, i + etx, j + ety, k + etz, lqb);
+        }
+        if (in_box(fb, i, j, k)) {                       // plus state of face z
+            ld_state<NS>(Q2P, i, j, k, lq);
+            ld_state<NS>(POB, i, j, k, lqob);
+#pragma unroll
+            for (int n = 0; n < NQS; ++n) lqb[n] = 0.0;
+            trans1_state_adj<NS>(lq, fr, fl, gamc, cdtdx, lqob, lqb, frb, flb, gb, cb);
+            add_state<NS>(PB, i, j, k, lqb);
+        }
+        st_rec<NS>(RF, i, j, k, frb);
+        st_rec<NS>(LF, i, j, k, flb);
+        QAB(i, j, k, QGAMC) += gb;
+        return cb;
+    }, cdtdxb);
+}
+
+// trans2 of direction d over the zones feeding ebx[d]: zone z owns the minus
+// state of face z+e_d and the plus state of face z; records of the t1 fluxes
+// (faces z, z+e_t1) go to T2L/T2R[d][0], of the t2 fluxes to [d][1]
+template <int NS>
+void trans2_adj_zones(castro_adj* a, int d, double c2, double c3, double* c2b, double* c3b)
+{
+    const Prim& P = *a->P;
+    const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+    const IBx fb = a->ebx[d];
+    IBx zb = fb;
+    zb.lo[d] -= 1;
+    Fab QM = P.qm[d][d].fab(), QP = P.qp[d][d].fab(), QA = P.qaux.fab();
+    Fab F2 = P.F2[t1][t2].fab(), G2 = P.G2[t1][t2].fab(), F3 = P.F2[t2][t1].fab(), G3 = P.G2[t2][t1].fab();
+    Fab MOB = a->qlb[d].fab(), POB = a->qrb[d].fab(), MB = a->qmb[d][d].fab(), PB = a->qpb[d][d].fab();
+    Fab QAB = a->qab.fab(), L2 = a->T2L[d][0].fab(), R2 = a->T2R[d][0].fab(), L3 = a->T2L[d][1].fab(),
+        R3 = a->T2R[d][1].fab();
+    launch_sum2("trans2_adj zones", zb.lo, zb.hi, [=] __device__(int i, int j, int k) -> double2 {
+        constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF;
+        const int e1x = d == 0, e1y = d == 1, e1z = d == 2;
+        const int e2x = t1 == 0, e2y = t1 == 1, e2z = t1 == 2;
+        const int e3x = t2 == 0, e3y = t2 == 1, e3z = t2 == 2;
+        double f2r[NTF], f2l[NTF], f3r[NTF], f3l[NTF], f2rb[NTF], f2lb[NTF], f3rb[NTF], f3lb[NTF];
+        ld_tflux<NS>(F2, G2, i + e2x, j + e2y, k + e2z, t1, f2r);
+        ld_tflux<NS>(F2, G2, i, j, k, t1, f2l);
+        ld_tflux<NS>(F3, G3, i + e3x, j + e3y, k + e3z, t2, f3r);
+        ld_tflux<NS>(F3, G3, i, j, k, t2, f3l);
+#pragma unroll
+        for (int n = 0; n < NTF; ++n) { f2rb[n] = 0.0; f2lb[n] = 0.0; f3rb[n] = 0.0; f3lb[n] = 0.0; }
+        const double gamc = QA(i, j, k, QGAMC);
+        double gb = 0.0, cb2 = 0.0, cb3 = 0.0;
+        double lq[NQS], lqob[NQS], lqb[NQS];
+        if (in_box(fb, i + e1x, j + e1y, k + e1z)) {     // minus state of face z+e_d
+            ld_state<NS>(QM, i + e1x, j + e1y, k + e1z, lq);
+            ld_state<NS>(MOB, i + e1x, j + e1y, k + e1z, lqob);
+#pragma unroll
+            for (int n = 0; n < NQS; ++n) lqb[n] = 0.0;
+            trans2_state_adj<NS>(lq, f2r, f2l, f3r, f3l, gamc, c2, c3, lqob, lqb, f2rb, f2lb, f3rb, f3lb, gb, cb2, cb3);
+            add_state<NS>(MB, i + e1x, j + e1y, k + e1z, lqb);
+        }
+        if (in_box(fb, i, j, k)) {                       // plus state of face z
+            ld_state<NS>(QP, i, j, k, lq);
+            ld_state<NS>(POB, i, j, k, lqob);
+#pragma unroll
+            for (int n = 0; n < NQS; ++n) lqb[n] = 0.0;
+            trans2_state_adj<NS>(lq, f2r, f2l, f3r, f3l, gamc, c2, c3, lqob, lqb, f2rb, f2lb, f3rb, f3lb, gb, cb2, cb3);
+            add_state<NS>(PB, i, j, k, lqb);
+        }
+        st_rec<NS>(R2, i, j, k, f2rb);
+        st_rec<NS>(L2, i, j, k, f2lb);
+        st_rec<NS>(R3, i, j, k, f3rb);
+        st_rec<NS>(L3, i, j, k, f3lb);
+        QAB(i, j, k, QGAMC) += gb;
+        return make_double2(cb2, cb3);
+    }, c2b, c3b);
+}
+
+// flux / qgdnv adjoints of the faces fb of direction n from up to two pairs of
+// zone records: sum over pairs of L[g] + R[g - e_n] (zones inside zb)
+template <int NS>
+void gather_records(const IBx& fb, int n, const IBx& zb0, Fab L0, Fab R0, bool two, const IBx& zb1, Fab L1, Fab R1,
+                    Fab FB, Fab GB)
+{
+    launch_box("adjoint record gather", fb.lo, fb.hi, [=] __device__(int i, int j, int k) {
+        using R = TF<NS>;
+        constexpr int NTF = Dims<NS>::NTF;
+        const int ex = n == 0, ey = n == 1, ez = n == 2;
+        double r[NTF];
+#pragma unroll
+        for (int m = 0; m < NTF; ++m) r[m] = 0.0;
+        if (in_box(zb0, i, j, k))
+#pragma unroll
+            for (int m = 0; m < NTF; ++m) r[m] += L0(i, j, k, m);
+        if (in_box(zb0, i - ex, j - ey, k - ez))
+#pragma unroll
+            for (int m = 0; m < NTF; ++m) r[m] += R0(i - ex, j - ey, k - ez, m);
+        if (two) {
+            if (in_box(zb1, i, j, k))
+#pragma unroll
+                for (int m = 0; m < NTF; ++m) r[m] += L1(i, j, k, m);
+            if (in_box(zb1, i - ex, j - ey, k - ez))
+#pragma unroll
+                for (int m = 0; m < NTF; ++m) r[m] += R1(i - ex, j - ey, k - ez, m);
+        }
+        FB(i, j, k, URHO) = r[R::RHO];
+        FB(i, j, k, UMX) = r[R::MX];
+        FB(i, j, k, UMY) = r[R::MY];
+        FB(i, j, k, UMZ) = r[R::MZ];
+        FB(i, j, k, UEDEN) = r[R::ED];
+#pragma unroll
+        for (int m = 0; m < NS; ++m) FB(i, j, k, UFS + m) = r[R::X + m];
+        GB(i, j, k, GDPRES) = r[R::PG];
+        GB(i, j, k, GDU + n) = r[R::UG];
+    });
+}
+
 // reverse of one step: a->Vb holds the adjoint of V_{n+1} on entry and of V_n
 // on exit; returns the adjoint of dt_n from this step's use of it
 template <int NS>
@@ -1020,19 +1358,24 @@ double reverse_step(castro_adj* a, const Arr& Vn, double dt)
     const IBx &bx = a->bx, &obx = a->obx, &qbx = a->qbx;
     for (Arr* r : {&a->Sbb, &a->qb, &a->qab, &a->divb, &a->srcb}) zero(*r, st);
     for (int d = 0; d < 3; ++d) {
-        for (Arr* r : {&a->F1b[d], &a->G1b[d], &a->qlb[d], &a->qrb[d], &a->fluxb[d], &a->qeb[d]}) zero(*r, st);
-        for (int e = 0; e < 3; ++e)
-            for (Arr* r : {&a->qmb[d][e], &a->qpb[d][e], &a->F2b[d][e], &a->G2b[d][e]}) zero(*r, st);
+        // F1b/G1b/F2b/G2b need no zeroing: the record gathers write every face
+        // the Riemann adjoints read (the other components stay zero from creation)
+        for (Arr* r : {&a->qlb[d], &a->qrb[d], &a->fluxb[d], &a->qeb[d]}) zero(*r, st);
+        for (int e = 0; e < 3; ++e) {
+            zero(a->qmb[d][e], st);
+            zero(a->qpb[d][e], st);
+        }
     }
     cudaMemsetAsync(a->d_scal, 0, 32 * sizeof(double), st);
     double* sc = a->d_scal;
+    adj_mark(a, "zero adjoint arrays");
     // V_{n+1} = clean(C), C = clean(B)
-    clean_state_adj_impl<NS>(bx.lo, bx.hi, a->Cs.fab(), a->Vb.fab(), true);
-    clean_state_adj_impl<NS>(bx.lo, bx.hi, a->Bs.fab(), a->Vb.fab(), true);
-    adj_check(a, "end cleans");
+    clean_state_adj_impl<NS>(bx.lo, bx.hi, a->P->Cs.fab(), a->Vb.fab(), true);
+    clean_state_adj_impl<NS>(bx.lo, bx.hi, a->P->Bs.fab(), a->Vb.fab(), true);
+    adj_stage(a, "end cleans");
     // B = A + dt*src: Ab = Bb, srcb = dt*Bb, dtb += sum(src*Bb)
     {
-        Fab BB = a->Vb.fab(), AB = a->Ab.fab(), SB = a->srcb.fab(), S = a->src.fab();
+        Fab BB = a->Vb.fab(), AB = a->Ab.fab(), SB = a->srcb.fab(), S = a->P->src.fab();
         launch_sum("adj saxpy", bx.lo, bx.hi, [=] __device__(int i, int j, int k) -> double {
             double s = 0.0;
 #pragma unroll
@@ -1045,65 +1388,69 @@ double reverse_step(castro_adj* a, const Arr& Vn, double dt)
             return s;
         }, sc + 9);
     }
-    adj_check(a, "saxpy");
-    fill_hydro_source_adj_impl<NS>(bx.lo, bx.hi, a->srcb.fab(), a->qe[0].fab(), a->qe[1].fab(), a->qe[2].fab(),
+    adj_stage(a, "saxpy");
+    fill_hydro_source_adj_impl<NS>(bx.lo, bx.hi, a->srcb.fab(), a->P->qe[0].fab(), a->P->qe[1].fab(), a->P->qe[2].fab(),
                                    a->area[0].fab(), a->area[1].fab(), a->area[2].fab(), a->vol.fab(), a->dx[0],
                                    a->dx[1], a->dx[2], a->fluxb[0].fab(), a->fluxb[1].fab(), a->fluxb[2].fab(),
                                    a->qeb[0].fab(), a->qeb[1].fab(), a->qeb[2].fab());
-    adj_check(a, "fill_hydro_source");
+    adj_stage(a, "fill_hydro_source");
     for (int d = 0; d < 3; ++d) {
-        normalize_species_fluxes_adj_impl<NS>(a->ebx[d].lo, a->ebx[d].hi, a->Fav[d].fab(), a->fluxb[d].fab());
-        apply_av_adj_impl<NS>(a->ebx[d].lo, a->ebx[d].hi, d, a->dx[d], a->div.fab(), a->Sb.fab(), a->fluxb[d].fab(),
+        normalize_species_fluxes_adj_impl<NS>(a->ebx[d].lo, a->ebx[d].hi, a->P->Fav[d].fab(), a->fluxb[d].fab());
+        apply_av_adj_impl<NS>(a->ebx[d].lo, a->ebx[d].hi, d, a->dx[d], a->P->div.fab(), a->P->Sb.fab(), a->fluxb[d].fab(),
                               a->divb.fab(), a->Sbb.fab());
-        compute_flux_adj_impl<NS>(a->ebx[d].lo, a->ebx[d].hi, a->ql[d].fab(), a->qr[d].fab(), a->qaux.fab(),
+        compute_flux_adj_impl<NS>(a->ebx[d].lo, a->ebx[d].hi, a->P->ql[d].fab(), a->P->qr[d].fab(), a->P->qaux.fab(),
                                   a->fluxb[d].fab(), a->qeb[d].fab(), a->qlb[d].fab(), a->qrb[d].fab(), a->qab.fab(), d);
     }
-    adj_check(a, "normalize/av/riemann3");
+    adj_stage(a, "normalize/av/riemann3");
     double hdtdx[3], cdtdx[3];
     for (int d = 0; d < 3; ++d) { hdtdx[d] = 0.5 * dt / a->dx[d]; cdtdx[d] = dt / a->dx[d] / 3.0; }
     for (int d = 0; d < 3; ++d) {
         int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
-        trans2_adj_impl<NS>(a->ebx[d].lo, a->ebx[d].hi, d, t1, t2, a->qm[d][d].fab(), a->qp[d][d].fab(), a->qaux.fab(),
-                            a->F2[t1][t2].fab(), a->F2[t2][t1].fab(), a->G2[t1][t2].fab(), a->G2[t2][t1].fab(),
-                            hdtdx[t1], hdtdx[t2], a->qlb[d].fab(), a->qrb[d].fab(), a->qmb[d][d].fab(),
-                            a->qpb[d][d].fab(), a->qab.fab(), a->F2b[t1][t2].fab(), a->F2b[t2][t1].fab(),
-                            a->G2b[t1][t2].fab(), a->G2b[t2][t1].fab(), sc + 6 + t1, sc + 6 + t2);
+        trans2_adj_zones<NS>(a, d, hdtdx[t1], hdtdx[t2], sc + 6 + t1, sc + 6 + t2);
+        IBx zb = a->ebx[d];
+        zb.lo[d] -= 1;
+        gather_records<NS>(a->tbx[t1][t2], t1, zb, a->T2L[d][0].fab(), a->T2R[d][0].fab(), false, zb,
+                           a->T2L[d][0].fab(), a->T2R[d][0].fab(), a->F2b[t1][t2].fab(), a->G2b[t1][t2].fab());
+        gather_records<NS>(a->tbx[t2][t1], t2, zb, a->T2L[d][1].fab(), a->T2R[d][1].fab(), false, zb,
+                           a->T2L[d][1].fab(), a->T2R[d][1].fab(), a->F2b[t2][t1].fab(), a->G2b[t2][t1].fab());
     }
-    adj_check(a, "trans2");
+    adj_stage(a, "trans2");
     for (int x = 0; x < 3; ++x)
         for (int y = 0; y < 3; ++y) {
             if (x == y) continue;
-            compute_flux_adj_impl<NS>(a->tbx[x][y].lo, a->tbx[x][y].hi, a->qm[x][y].fab(), a->qp[x][y].fab(),
-                                      a->qaux.fab(), a->F2b[x][y].fab(), a->G2b[x][y].fab(), a->qmb[x][y].fab(),
+            compute_flux_adj_impl<NS>(a->tbx[x][y].lo, a->tbx[x][y].hi, a->P->qm[x][y].fab(), a->P->qp[x][y].fab(),
+                                      a->P->qaux.fab(), a->F2b[x][y].fab(), a->G2b[x][y].fab(), a->qmb[x][y].fab(),
                                       a->qpb[x][y].fab(), a->qab.fab(), x);
         }
-    adj_check(a, "riemann2");
+    adj_stage(a, "riemann2");
+    for (int d = 0; d < 3; ++d) {
+        const int ta = d == 0 ? 1 : 0, tb = d == 2 ? 1 : 2;
+        trans1_adj_zones<NS>(a, d, ta, cdtdx[d], sc + 3 + d);
+        trans1_adj_zones<NS>(a, d, tb, cdtdx[d], sc + 3 + d);
+        IBx za = a->tbx[ta][d], zbb = a->tbx[tb][d];
+        za.lo[ta] -= 1;
+        zbb.lo[tb] -= 1;
+        gather_records<NS>(a->tbx[d][d], d, za, a->T1L[d][ta].fab(), a->T1R[d][ta].fab(), true, zbb,
+                           a->T1L[d][tb].fab(), a->T1R[d][tb].fab(), a->F1b[d].fab(), a->G1b[d].fab());
+    }
+    adj_stage(a, "trans1");
     for (int d = 0; d < 3; ++d)
-        for (int tt = 0; tt < 2; ++tt) {
-            int t = (tt == 0) ? (d == 0 ? 1 : 0) : (d == 2 ? 1 : 2);
-            trans1_adj_impl<NS>(a->tbx[t][d].lo, a->tbx[t][d].hi, d, t, a->qm[t][t].fab(), a->qp[t][t].fab(),
-                                a->qaux.fab(), a->F1[d].fab(), a->G1[d].fab(), cdtdx[d], a->qmb[t][d].fab(),
-                                a->qpb[t][d].fab(), a->qmb[t][t].fab(), a->qpb[t][t].fab(), a->qab.fab(),
-                                a->F1b[d].fab(), a->G1b[d].fab(), sc + 3 + d);
-        }
-    adj_check(a, "trans1");
-    for (int d = 0; d < 3; ++d)
-        compute_flux_adj_impl<NS>(a->tbx[d][d].lo, a->tbx[d][d].hi, a->qm[d][d].fab(), a->qp[d][d].fab(),
-                                  a->qaux.fab(), a->F1b[d].fab(), a->G1b[d].fab(), a->qmb[d][d].fab(),
+        compute_flux_adj_impl<NS>(a->tbx[d][d].lo, a->tbx[d][d].hi, a->P->qm[d][d].fab(), a->P->qp[d][d].fab(),
+                                  a->P->qaux.fab(), a->F1b[d].fab(), a->G1b[d].fab(), a->qmb[d][d].fab(),
                                   a->qpb[d][d].fab(), a->qab.fab(), d);
-    adj_check(a, "riemann1");
+    adj_stage(a, "riemann1");
     for (int d = 0; d < 3; ++d)
-        trace_adj_impl<NS>(obx.lo, obx.hi, bx.lo, bx.hi, d, a->q.fab(), a->qaux.fab(), a->qmb[d][d].fab(),
+        trace_adj_impl<NS>(obx.lo, obx.hi, bx.lo, bx.hi, d, a->P->q.fab(), a->P->qaux.fab(), a->qmb[d][d].fab(),
                            a->qpb[d][d].fab(), a->qb.fab(), a->qab.fab(), dt / a->dx[d], sc + d);
-    adj_check(a, "trace");
+    adj_stage(a, "trace");
     divu_adj_impl<NS>(obx.lo, obx.hi, a->divb.fab(), a->qb.fab(), a->dx[0], a->dx[1], a->dx[2]);
-    adj_check(a, "divu");
-    ctoprim_adj_impl<NS>(qbx.lo, qbx.hi, a->Sb.fab(), a->qb.fab(), a->qab.fab(), a->Sbb.fab());
-    adj_check(a, "ctoprim");
+    adj_stage(a, "divu");
+    ctoprim_adj_impl<NS>(qbx.lo, qbx.hi, a->P->Sb.fab(), a->qb.fab(), a->qab.fab(), a->Sbb.fab());
+    adj_stage(a, "ctoprim");
     fill_clean_adj<NS>(a);
-    adj_check(a, "sborder fill+clean");
+    adj_stage(a, "sborder fill+clean");
     clean_state_adj_impl<NS>(bx.lo, bx.hi, Vn.fab(), a->Ab.fab(), true);
-    adj_check(a, "start clean");
+    adj_stage(a, "start clean");
     copy(a->Vb, a->Ab, st);
     double h[16];
     cudaMemcpyAsync(h, sc, 16 * sizeof(double), cudaMemcpyDeviceToHost, st);
@@ -1121,6 +1468,7 @@ int adj_forward(castro_adj* a)
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, a->st);
+    a->P = &a->sets[0];
     castro_problem saved = castro::problem();
     castro_set_problem(&a->prob);
     initdata(a->bx.lo, a->bx.hi, a->V.p, a->bx.lo, a->bx.hi, a->dx, a->problo, a->probhi);
@@ -1129,8 +1477,17 @@ int adj_forward(castro_adj* a)
     a->dts.assign(N, 0.0); a->times.assign(N + 1, 0.0); a->ests.assign(N, 0.0); a->estmin.assign(N, 0.0);
     a->limited.assign(N, 0); a->clamped.assign(N, 0);
     double time = 0.0, dt_prev = 0.0;
+    // the last checkpoint segment keeps its states and intermediates, so the
+    // reverse sweep starts without recomputing it
+    const int K = a->ckpt;
+    const int n0_last = ((N - 1) / K) * K;
+    const bool keep_last = (int)a->sets.size() >= K;
     for (int n = 0; n < N; ++n) {
         if (n % a->ckpt == 0) copy(a->ckpts[n / a->ckpt], a->V, a->st);
+        if (keep_last && n >= n0_last) {
+            a->P = &a->sets[n - n0_last];
+            copy(a->seg[n - n0_last], a->V, a->st);
+        }
         // computeNewDt / computeInitialDt, Source/Castro.cpp:162-341
         double m = est_min(a, a->V);
         double est = m * cfl;
@@ -1156,6 +1513,7 @@ int adj_forward(castro_adj* a)
         dt_prev = dt;
     }
     a->times[N] = time;
+    a->last_seg_ready = keep_last;
     copy(a->Vfinal, a->V, a->st);
     a->J = objective<NS>(a, a->V, false, a->Vb);
     cudaEventRecord(e1, a->st);
@@ -1277,13 +1635,24 @@ int adj_backward(castro_adj* a, double* dE, double* drho, double* pertb)
     const int nseg = (N + K - 1) / K;
     for (int sgi = nseg - 1; sgi >= 0; --sgi) {
         const int n0 = sgi * K, n1 = std::min(N, n0 + K);
-        copy(a->seg[0], a->ckpts[sgi], a->st);
-        for (int n = n0; n < n1 - 1; ++n) {
+        adj_mark(a, "(segment start)");
+        const bool keep = (int)a->sets.size() >= K;
+        const bool ready = keep && a->last_seg_ready && sgi == nseg - 1;
+        if (!ready) copy(a->seg[0], a->ckpts[sgi], a->st);
+        for (int n = n0; n < (ready ? n0 : n1 - (keep ? 0 : 1)); ++n) {
+            a->P = &a->sets[keep ? n - n0 : 0];
             forward_step<NS>(a, a->seg[n - n0], a->dts[n]);
-            finish_step(a, a->seg[n - n0 + 1]);
+            if (n < n1 - 1) finish_step(a, a->seg[n - n0 + 1]);
         }
+        adj_mark(a, "segment recompute");
         for (int n = n1 - 1; n >= n0; --n) {
-            forward_step<NS>(a, a->seg[n - n0], a->dts[n]);
+            if (keep) {
+                a->P = &a->sets[n - n0];
+            } else {
+                a->P = &a->sets[0];
+                forward_step<NS>(a, a->seg[n - n0], a->dts[n]);
+            }
+            adj_mark(a, "step recompute");
             double dtb_n = reverse_step<NS>(a, a->seg[n - n0], a->dts[n]) + dtb[n] + timeb;
             // dt_n = rule(V_n, dt_{n-1}, time_n)
             if (a->clamped[n]) {
@@ -1294,9 +1663,16 @@ int adj_backward(castro_adj* a, double* dE, double* drho, double* pertb)
                 double scale = cfl * (n == 0 ? 0.01 : 1.0) * dtb_n;
                 estdt_adj<NS>(a, a->seg[n - n0], a->estmin[n], scale, a->Vb);
             }
+            adj_mark(a, "dt adjoint");
         }
+        adj_prof_flush();
     }
+    // earlier segments reused the sets: a second reverse sweep recomputes
+    a->last_seg_ready = a->last_seg_ready && nseg == 1;
+    adj_mark(a, "(init start)");
     initdata_adj<NS>(a, dE, drho, pertb);
+    adj_mark(a, "initdata adjoint");
+    adj_prof_report();
     cudaEventRecord(e1, a->st);
     cudaEventSynchronize(e1);
     cudaEventElapsedTime(&a->ms_backward, e0, e1);
@@ -1351,29 +1727,52 @@ castro_adj* castro_adj_create(const castro_instance_desc* desc, int nsteps, int 
     a->seg.resize(checkpoint_interval);
     for (auto& r : a->ckpts) ok = ok && alloc_arr(a, r, a->bx, NV);
     for (auto& r : a->seg) ok = ok && alloc_arr(a, r, a->bx, NV);
-    for (Arr* r : {&a->V, &a->A, &a->Bs, &a->Cs, &a->src, &a->Vfinal, &a->Vb, &a->Ab, &a->srcb}) ok = ok && alloc_arr(a, *r, a->bx, NV);
+    for (Arr* r : {&a->V, &a->Vfinal, &a->Vb, &a->Ab, &a->srcb}) ok = ok && alloc_arr(a, *r, a->bx, NV);
     ok = ok && alloc_arr(a, a->vol, a->bx, 1);
-    ok = ok && alloc_arr(a, a->Sb, a->qbx, NV) && alloc_arr(a, a->Sbb, a->qbx, NV);
-    ok = ok && alloc_arr(a, a->q, a->qbx, QV) && alloc_arr(a, a->qb, a->qbx, QV);
-    ok = ok && alloc_arr(a, a->qaux, a->qbx, NQAUX) && alloc_arr(a, a->qab, a->qbx, NQAUX);
-    ok = ok && alloc_arr(a, a->div, a->obx, 1) && alloc_arr(a, a->divb, a->obx, 1);
-    ok = ok && alloc_arr(a, a->qint, a->obx, QV);
+    ok = ok && alloc_arr(a, a->Sbb, a->qbx, NV) && alloc_arr(a, a->qb, a->qbx, QV) && alloc_arr(a, a->qab, a->qbx, NQAUX);
+    ok = ok && alloc_arr(a, a->divb, a->obx, 1);
     for (int d = 0; d < 3 && ok; ++d) {
         for (int e = 0; e < 3 && ok; ++e) {
-            ok = ok && alloc_arr(a, a->qm[d][e], a->obx, QV) && alloc_arr(a, a->qp[d][e], a->obx, QV);
             ok = ok && alloc_arr(a, a->qmb[d][e], a->obx, QV) && alloc_arr(a, a->qpb[d][e], a->obx, QV);
-            ok = ok && alloc_arr(a, a->F2[d][e], a->obx, NV) && alloc_arr(a, a->G2[d][e], a->obx, NGDNV);
-            ok = ok && alloc_arr(a, a->F2b[d][e], a->obx, NV) && alloc_arr(a, a->G2b[d][e], a->obx, NGDNV);
+            if (d != e) ok = ok && alloc_arr(a, a->F2b[d][e], a->obx, NV) && alloc_arr(a, a->G2b[d][e], a->obx, NGDNV);
         }
-        ok = ok && alloc_arr(a, a->F1[d], a->obx, NV) && alloc_arr(a, a->G1[d], a->obx, NGDNV);
         ok = ok && alloc_arr(a, a->F1b[d], a->obx, NV) && alloc_arr(a, a->G1b[d], a->obx, NGDNV);
-        ok = ok && alloc_arr(a, a->ql[d], a->obx, QV) && alloc_arr(a, a->qr[d], a->obx, QV);
         ok = ok && alloc_arr(a, a->qlb[d], a->obx, QV) && alloc_arr(a, a->qrb[d], a->obx, QV);
-        ok = ok && alloc_arr(a, a->Fav[d], a->gebx[d], NV) && alloc_arr(a, a->flux[d], a->gebx[d], NV);
-        ok = ok && alloc_arr(a, a->fluxb[d], a->gebx[d], NV);
-        ok = ok && alloc_arr(a, a->qe[d], a->gebx[d], NGDNV) && alloc_arr(a, a->qeb[d], a->gebx[d], NGDNV);
+        ok = ok && alloc_arr(a, a->fluxb[d], a->gebx[d], NV) && alloc_arr(a, a->qeb[d], a->gebx[d], NGDNV);
         ok = ok && alloc_arr(a, a->area[d], a->gebx[d], 1);
+        for (int e = 0; e < 3 && ok; ++e)
+            if (e != d) ok = ok && alloc_arr(a, a->T1L[d][e], a->obx, a->nv) && alloc_arr(a, a->T1R[d][e], a->obx, a->nv);
+        for (int e = 0; e < 2 && ok; ++e)
+            ok = ok && alloc_arr(a, a->T2L[d][e], a->obx, a->nv) && alloc_arr(a, a->T2R[d][e], a->obx, a->nv);
     }
+    // per-step forward intermediates: a set per segment step when they fit in
+    // 70% of the free device memory, else one set recomputed per step
+    auto set_bytes = [&]() {
+        long long n = 4 * nptsb(a->bx) * NV + nptsb(a->qbx) * (NV + QV + NQAUX) + nptsb(a->obx) * (1 + QV);
+        n += nptsb(a->obx) * (18LL * QV + 3LL * (NV + NGDNV) + 6LL * (NV + NGDNV) + 6LL * QV);
+        for (int d = 0; d < 3; ++d) n += nptsb(a->gebx[d]) * (2LL * NV + NGDNV);
+        return (size_t)n * sizeof(double);
+    };
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    int nsets = (ok && (size_t)checkpoint_interval * set_bytes() < (size_t)(0.7 * (double)fr)) ? checkpoint_interval : 1;
+    a->sets.resize(nsets);
+    for (Prim& P : a->sets) {
+        for (Arr* r : {&P.A, &P.Bs, &P.Cs, &P.src}) ok = ok && alloc_arr(a, *r, a->bx, NV);
+        ok = ok && alloc_arr(a, P.Sb, a->qbx, NV) && alloc_arr(a, P.q, a->qbx, QV) && alloc_arr(a, P.qaux, a->qbx, NQAUX);
+        ok = ok && alloc_arr(a, P.div, a->obx, 1) && alloc_arr(a, P.qint, a->obx, QV);
+        for (int d = 0; d < 3 && ok; ++d) {
+            for (int e = 0; e < 3 && ok; ++e) {
+                ok = ok && alloc_arr(a, P.qm[d][e], a->obx, QV) && alloc_arr(a, P.qp[d][e], a->obx, QV);
+                if (d != e) ok = ok && alloc_arr(a, P.F2[d][e], a->obx, NV) && alloc_arr(a, P.G2[d][e], a->obx, NGDNV);
+            }
+            ok = ok && alloc_arr(a, P.F1[d], a->obx, NV) && alloc_arr(a, P.G1[d], a->obx, NGDNV);
+            ok = ok && alloc_arr(a, P.ql[d], a->obx, QV) && alloc_arr(a, P.qr[d], a->obx, QV);
+            ok = ok && alloc_arr(a, P.Fav[d], a->gebx[d], NV) && alloc_arr(a, P.flux[d], a->gebx[d], NV);
+            ok = ok && alloc_arr(a, P.qe[d], a->gebx[d], NGDNV);
+        }
+    }
+    a->P = &a->sets[0];
     ok = ok && cudaMalloc(&a->d_scal, 32 * sizeof(double)) == cudaSuccess;
     ok = ok && cudaMalloc(&a->d_idx, sizeof(int)) == cudaSuccess;
     ok = ok && cudaMalloc(&a->d_est, sizeof(double)) == cudaSuccess;
@@ -1382,12 +1781,25 @@ castro_adj* castro_adj_create(const castro_instance_desc* desc, int nsteps, int 
         castro_adj_destroy(a);
         return nullptr;
     }
-    // zero every face array once: entries outside the forward's face boxes are never written
-    for (int d = 0; d < 3; ++d)
+    // components of the record-gather targets that no gather writes stay zero
+    for (int d = 0; d < 3; ++d) {
+        zero(a->F1b[d], a->st);
+        zero(a->G1b[d], a->st);
         for (int e = 0; e < 3; ++e)
-            for (Arr* r : {&a->qm[d][e], &a->qp[d][e], &a->F2[d][e], &a->G2[d][e]}) zero(*r, a->st);
-    for (int d = 0; d < 3; ++d)
-        for (Arr* r : {&a->F1[d], &a->G1[d], &a->ql[d], &a->qr[d], &a->Fav[d], &a->flux[d], &a->qe[d], &a->qint}) zero(*r, a->st);
+            if (e != d) { zero(a->F2b[d][e], a->st); zero(a->G2b[d][e], a->st); }
+    }
+    // zero every face array once: entries outside the forward's face boxes are never written
+    for (Prim& P : a->sets) {
+        for (int d = 0; d < 3; ++d) {
+            for (int e = 0; e < 3; ++e) {
+                zero(P.qm[d][e], a->st);
+                zero(P.qp[d][e], a->st);
+                if (d != e) { zero(P.F2[d][e], a->st); zero(P.G2[d][e], a->st); }
+            }
+            for (Arr* r : {&P.F1[d], &P.G1[d], &P.ql[d], &P.qr[d], &P.Fav[d], &P.flux[d], &P.qe[d]}) zero(*r, a->st);
+        }
+        zero(P.qint, a->st);
+    }
     const double ar[3] = {a->dx[1] * a->dx[2], a->dx[0] * a->dx[2], a->dx[0] * a->dx[1]};
     for (int d = 0; d < 3; ++d) fill_const(a->area[d], ar[d], a->st);
     fill_const(a->vol, a->dx[0] * a->dx[1] * a->dx[2], a->st);
@@ -1477,18 +1889,7 @@ size_t castro_adj_device_bytes(const castro_adj* a)
 {
     if (!a) return 0;
     size_t s = 0;
-    auto add = [&](const Arr& r) { s += (size_t)r.n() * sizeof(double); };
-    for (auto& r : a->ckpts) add(r);
-    for (auto& r : a->seg) add(r);
-    for (const Arr* r : {&a->V, &a->A, &a->Bs, &a->Cs, &a->src, &a->Vfinal, &a->Vb, &a->Ab, &a->srcb, &a->vol, &a->Sb,
-                         &a->Sbb, &a->q, &a->qb, &a->qaux, &a->qab, &a->div, &a->divb, &a->qint}) add(*r);
-    for (int d = 0; d < 3; ++d) {
-        for (int e = 0; e < 3; ++e)
-            for (const Arr* r : {&a->qm[d][e], &a->qp[d][e], &a->qmb[d][e], &a->qpb[d][e], &a->F2[d][e], &a->G2[d][e],
-                                 &a->F2b[d][e], &a->G2b[d][e]}) add(*r);
-        for (const Arr* r : {&a->F1[d], &a->G1[d], &a->F1b[d], &a->G1b[d], &a->ql[d], &a->qr[d], &a->qlb[d], &a->qrb[d],
-                             &a->Fav[d], &a->flux[d], &a->fluxb[d], &a->qe[d], &a->qeb[d], &a->area[d]}) add(*r);
-    }
+    for (const Arr& r : a->all) s += (size_t)r.n() * sizeof(double);
     return s;
 }
 
