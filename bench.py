@@ -285,12 +285,10 @@ def run_b200(args, pkg, rank, world):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic: Sedov blast, seeded Gaussian density perturbation (numpy PCG64), generated Helmholtz table",
-        "config": {"workload": f"{args.workload}: 128^3 zones in 64 boxes of 32^3, 2 species, outflow, "
-                               "rho=1*(1+1e-3 g), T=1e6 K, E=1e50 erg in r=4 zones, CFL 0.5, 50 coarse steps"
-                               + (f" (zone counts divided by {args.scale})" if args.scale > 1 else ""),
+        "config": {"workload": workload_text(args),
                    "zones": zones, "boxes": sum(len(i["boxes"]) for i in cfg["instances"]),
                    "path": "batched fused kernels, one CUDA graph per step",
-                   "l2": "no flush: state 151 MB plus ~3.6 GB of per-step intermediates exceed the 126 MB L2",
+                   "l2": "no flush: the state plus the per-step intermediates (~1.7 KB/zone) exceed the 126 MB L2",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": pkg.replicas.whole_job_rate(zones, args.steps, t_e2e * 1e3, world), "unit": "zone-updates/s",
                 "h2d_bytes_per_step": host_in.numel() * 8 / args.steps,
@@ -341,6 +339,23 @@ def run_batched_config(pkg, L, args):
         sim.close()
     out["speedup_batched_over_plain"] = out["batched"]["value"] / out["plain_per_box"]["value"]
     return out
+
+
+WORKLOAD_TEXT = {
+    "sedov128_pert": "128^3 zones in 64 boxes of 32^3, 2 species, outflow, rho=1*(1+1e-3 g), T=1e6 K, "
+                     "E=1e50 erg in r=4 zones, CFL 0.5, 50 coarse steps",
+    "sedov64": "one 64^3 box, 2 species, outflow, rho=1, T=1e6 K, E=1e50 erg in r=4 zones, 10 coarse steps",
+    "large": "384^3 zones in an uneven BoxArray of 32^3..64^3 boxes, 2 species, outflow, rho=1*(1+1e-3 g), "
+             "100 coarse steps",
+    "adjoint64": "one 64^3 box, 2 species, outflow, rho=1*(1+1e-3 g), 20 coarse steps",
+    "batched": "256^3 uneven BoxArray + 32 instances 32^3..96^3, 2 species, 20 coarse steps",
+    "reference": "Source/Prob.F90 problem: 128^3 in 64^3 boxes, 13 species, periodic, 1e9 cm, 10 coarse steps",
+}
+
+
+def workload_text(args) -> str:
+    t = f"{args.workload}: {WORKLOAD_TEXT.get(args.workload, '')}"
+    return t + (f" (zone counts divided by {args.scale})" if args.scale > 1 else "")
 
 
 def run_adjoint_config(pkg, args):
@@ -468,8 +483,7 @@ def run_reference(args, pkg):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: Sedov blast, seeded Gaussian density perturbation, generated Helmholtz table",
-        "config": {"workload": f"{args.workload}: 128^3 zones in 64 boxes of 32^3, 2 species, outflow, 50 coarse steps",
-                   "zones": zones},
+        "config": {"workload": workload_text(args), "zones": zones},
         "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "port",
                          "sample": f"{args.steps} full coarse steps after {args.warmup} warm-up steps; the reference "
                                    "(Fortran + AMReX) cannot be compiled in this image, so its C restatement runs, "

@@ -45,26 +45,50 @@ unsigned long long* eos_fail_counter();
 namespace {
 
 constexpr int NG = 4;   // ghost zones of Sborder, Source/Castro_advance.cpp:37
-constexpr int BLOCK = 128;
-// Minimum resident blocks per SM for the register allocator, chosen by a
-// timing sweep on B200: 4 blocks (128 registers) for the EOS kernels, whose
-// spills stay in L1, and 3 blocks for the final Riemann kernel; trace and the
-// other Riemann kernels keep the compiler's choice.  Override with -DCASTRO_MINB_*.
+// Launch shape of the fused kernels.  castro_tuned.h (written by autotune.py
+// from timings of the batched step on the target GPU) sets the block size
+// (= the zones of one work item) and the minimum resident blocks per SM given
+// to the register allocator per kernel group; 0 leaves it to the compiler.
+// The values below are the defaults without a tuned header (hand sweep on
+// B200: 4 blocks for the EOS kernels, whose spills stay in L1, 3 for the final
+// Riemann kernel).  Override with -DCASTRO_BLOCK / -DCASTRO_MINB_*.
+#if __has_include("castro_tuned.h")
+#include "castro_tuned.h"
+#endif
+#ifndef CASTRO_BLOCK
+#define CASTRO_BLOCK 128
+#endif
 #ifndef CASTRO_MINB_EOS
 #define CASTRO_MINB_EOS 4
 #endif
 #ifndef CASTRO_MINB_R3
 #define CASTRO_MINB_R3 3
 #endif
-#define LB_EOS __launch_bounds__(BLOCK, CASTRO_MINB_EOS)
-#define LB_R3 __launch_bounds__(BLOCK, CASTRO_MINB_R3)
-#ifdef CASTRO_MINB_TRACE
-#define LB_TRACE __launch_bounds__(BLOCK, CASTRO_MINB_TRACE)
+#ifndef CASTRO_MINB_TRACE
+#define CASTRO_MINB_TRACE 0
+#endif
+#ifndef CASTRO_MINB_RIEMANN
+#define CASTRO_MINB_RIEMANN 0
+#endif
+constexpr int BLOCK = CASTRO_BLOCK;
+#define CASTRO_LB(M) __launch_bounds__(BLOCK, ((M) > 0 ? (M) : 1))
+#if CASTRO_MINB_EOS > 0
+#define LB_EOS CASTRO_LB(CASTRO_MINB_EOS)
+#else
+#define LB_EOS __launch_bounds__(BLOCK)
+#endif
+#if CASTRO_MINB_R3 > 0
+#define LB_R3 CASTRO_LB(CASTRO_MINB_R3)
+#else
+#define LB_R3 __launch_bounds__(BLOCK)
+#endif
+#if CASTRO_MINB_TRACE > 0
+#define LB_TRACE CASTRO_LB(CASTRO_MINB_TRACE)
 #else
 #define LB_TRACE __launch_bounds__(BLOCK)
 #endif
-#ifdef CASTRO_MINB_RIEMANN
-#define LB_RIEMANN __launch_bounds__(BLOCK, CASTRO_MINB_RIEMANN)
+#if CASTRO_MINB_RIEMANN > 0
+#define LB_RIEMANN CASTRO_LB(CASTRO_MINB_RIEMANN)
 #else
 #define LB_RIEMANN __launch_bounds__(BLOCK)
 #endif
