@@ -281,6 +281,11 @@ int    castro_sim_steps(castro_sim* sim, int inst);
 double castro_sim_est_time_step(castro_sim* sim, int inst);
 /* blast radius diagnostic of Source/Castro.cpp:371-424, cm */
 double castro_sim_blast_radius(castro_sim* sim, int inst, double* blast_mass);
+/* AMReX native plotfile of instance inst in directory dir (Header,
+ * Level_0/Cell_H, Level_0/Cell_D_00000; one FAB per box of its BoxArray),
+ * readable by AMReX tools -- the layout Amr::writePlotFile produces (the
+ * reference never writes one by default: Source/main.cpp sets no plot_int) */
+int    castro_sim_write_plotfile(castro_sim* sim, int inst, const char* dir);
 /* the CUDA stream (cudaStream_t) every launch of this sim is issued on */
 void*  castro_sim_stream(castro_sim* sim);
 /* batched mode: one step with a CUDA event around each of the fused kernels

@@ -8,11 +8,12 @@ The product is the CUDA library ``lib/libcastro_b200.so`` (C-ABI in
 * ``helm_table`` -- writer of the Helmholtz table file read by ``eos_init``
 * ``replicas``   -- the multi-GPU (one replica per rank) reductions
 * ``adjoint``    -- gradients of a Sedov run (reverse sweep) and its torch.autograd wrapper
+* ``plotfile``   -- reader of the AMReX plotfiles the library writes
 * ``build``      -- nvcc recipe for the sm_100a libraries
 """
-from . import adjoint, castro, configs, helm_table, replicas  # noqa: F401
+from . import adjoint, castro, configs, helm_table, plotfile, replicas  # noqa: F401
 
-__all__ = ["adjoint", "castro", "configs", "helm_table", "replicas", "make_sim"]
+__all__ = ["adjoint", "castro", "configs", "helm_table", "plotfile", "replicas", "make_sim"]
 
 
 def make_sim(L, cfg, mode=castro.MODE_BATCHED):

@@ -79,7 +79,7 @@ ABI_SYMBOLS = [
     "apply_av_adj", "normalize_species_fluxes_adj", "fill_hydro_source_adj", "castro_adj_create",
     "castro_adj_destroy", "castro_adj_set_problem", "castro_adj_set_shell", "castro_adj_forward",
     "castro_adj_backward", "castro_adj_dt", "castro_adj_final_state", "castro_adj_initial_adjoint",
-    "castro_adj_time_ms", "castro_adj_device_bytes",
+    "castro_adj_time_ms", "castro_adj_device_bytes", "castro_sim_write_plotfile",
 ]
 
 
@@ -137,6 +137,7 @@ def load(exact: bool = False) -> C.CDLL:
     L.castro_measure_fp64_tflops.restype = C.c_double
     L.castro_sim_eos_failures.restype = C.c_longlong
     L.castro_sim_eos_failures.argtypes = [C.c_void_p]
+    L.castro_sim_write_plotfile.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
     L.castro_adj_create.restype = C.c_void_p
     L.castro_adj_create.argtypes = [C.POINTER(InstanceDesc), C.c_int, C.c_int]
     L.castro_adj_destroy.argtypes = [C.c_void_p]
@@ -331,6 +332,11 @@ class Sim:
 
     def est_time_step(self, inst: int = 0) -> float:
         return self.L.castro_sim_est_time_step(self.h, inst)
+
+    def write_plotfile(self, path: str, inst: int = 0):
+        """AMReX plotfile of instance inst (castro_sim_write_plotfile)."""
+        self.L.castro_sim_write_plotfile(self.h, inst, path.encode())
+        check(self.L, "castro_sim_write_plotfile")
 
     def blast_radius(self, inst: int = 0):
         m = C.c_double()

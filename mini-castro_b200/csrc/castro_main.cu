@@ -44,7 +44,8 @@ void usage()
     printf("max_level (0): The maximum adaptive mesh refinement level (zero-indexed).\n");
     printf("stop_time (0.01): The stopping time of the simulation, in seconds.\n");
     printf("max_step (10000000): The maximum number of timesteps to take.\n\n");
-    printf("B200 additions: problem=reference|sedov nspec=13|2 bc=periodic|outflow mode=batched|plain table=<path>\n\n");
+    printf("B200 additions: problem=reference|sedov nspec=13|2 bc=periodic|outflow mode=batched|plain table=<path>\n"
+           "               plot_file=<dir> (AMReX plotfile of the final state)\n\n");
 }
 
 }  // namespace
@@ -144,6 +145,9 @@ extern "C" int castro_main(int argc, char** argv)
         }
     }
     castro_sim_sync(sim);
+    const std::string plot = gets("plot_file", "");
+    if (!plot.empty() && castro_sim_write_plotfile(sim, 0, plot.c_str()) != CASTRO_OK)
+        fprintf(stderr, "plotfile: %s\n", castro_error_string());
     double zones = (double)n_cell * n_cell * n_cell;
     castro_sim_destroy(sim);
     auto t2 = std::chrono::steady_clock::now();

@@ -24,8 +24,11 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <sys/stat.h>
+
 #include <algorithm>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "castro_common.cuh"
@@ -1551,6 +1554,107 @@ double castro_sim_est_time_step(castro_sim* s, int inst)
     cuda_ok(cudaMemcpyAsync(&dt, s->d_dtloc, sizeof dt, cudaMemcpyDeviceToHost, s->st), "est read");
     cudaStreamSynchronize(s->st);
     return dt * cfl;
+}
+
+// AMReX native plotfile ("HyperCLaw-V1.1") of one instance's level: Header,
+// Level_0/Cell_H (the MultiFab header with every box, its offset in the data
+// file and per-component minima and maxima) and Level_0/Cell_D_00000 (every
+// FAB: a text header line, then the values in Fortran order, component
+// slowest, little-endian IEEE doubles).  Components are named as Castro's
+// state: density, xmom, ymom, zmom, rho_E, rho_e, Temp, rho_<species>.
+int castro_sim_write_plotfile(castro_sim* s, int inst, const char* dir)
+{
+    if (!s || !dir || inst < 0 || inst >= s->ninst) {
+        set_error(CASTRO_ERR_ARG, "castro_sim_write_plotfile: arguments");
+        return CASTRO_ERR_ARG;
+    }
+    const castro_instance_desc& D = s->desc[inst];
+    InstState hs;
+    if (!cuda_ok(cudaMemcpyAsync(&hs, s->dstate + inst, sizeof hs, cudaMemcpyDeviceToHost, s->st), "plotfile state") ||
+        !cuda_ok(cudaStreamSynchronize(s->st), "plotfile sync"))
+        return castro_last_error();
+    const std::string root(dir), lev = root + "/Level_0";
+    mkdir(root.c_str(), 0755);
+    mkdir(lev.c_str(), 0755);
+    const int nc = s->nvar;
+    std::vector<std::string> names = {"density", "xmom", "ymom", "zmom", "rho_E", "rho_e", "Temp"};
+    for (int n = 0; n < s->ns; ++n) names.push_back("rho_spec" + std::to_string(n));
+    const double* dx = &s->hdx[3 * inst];
+    const std::vector<int>& boxes = s->inst_boxes[inst];
+
+    // data file: one FAB per box
+    std::string dname = lev + "/Cell_D_00000";
+    FILE* fd = fopen(dname.c_str(), "wb");
+    if (!fd) {
+        set_error(CASTRO_ERR_ARG, ("castro_sim_write_plotfile: cannot write " + dname).c_str());
+        return CASTRO_ERR_ARG;
+    }
+    std::vector<long long> offsets;
+    std::vector<std::vector<double>> mins, maxs;
+    std::vector<double> h;
+    for (int b : boxes) {
+        const BoxDev& B = s->hboxes[b];
+        long long np = npts_reg(B.lo, B.hi, R_VALID, 0);
+        h.resize((size_t)(np * nc));
+        if (!cuda_ok(cudaMemcpy(h.data(), s->U + B.offU, h.size() * sizeof(double), cudaMemcpyDeviceToHost),
+                     "plotfile read")) {
+            fclose(fd);
+            return castro_last_error();
+        }
+        offsets.push_back((long long)ftell(fd));
+        fprintf(fd, "FAB ((8, (64 11 52 0 1 12 0 1023)),(8, (8 7 6 5 4 3 2 1)))((%d,%d,%d) (%d,%d,%d) (0,0,0)) %d\n",
+                B.lo[0], B.lo[1], B.lo[2], B.hi[0], B.hi[1], B.hi[2], nc);
+        fwrite(h.data(), sizeof(double), h.size(), fd);
+        std::vector<double> mn(nc), mx(nc);
+        for (int n = 0; n < nc; ++n) {
+            const double* c = h.data() + (size_t)np * n;
+            mn[n] = *std::min_element(c, c + np);
+            mx[n] = *std::max_element(c, c + np);
+        }
+        mins.push_back(mn);
+        maxs.push_back(mx);
+    }
+    fclose(fd);
+
+    // MultiFab header
+    FILE* fh = fopen((lev + "/Cell_H").c_str(), "w");
+    if (!fh) { set_error(CASTRO_ERR_ARG, "castro_sim_write_plotfile: Cell_H"); return CASTRO_ERR_ARG; }
+    fprintf(fh, "1\n0\n%d\n0\n(%d 0\n", nc, (int)boxes.size());
+    for (int b : boxes) {
+        const BoxDev& B = s->hboxes[b];
+        fprintf(fh, "((%d,%d,%d) (%d,%d,%d) (0,0,0))\n", B.lo[0], B.lo[1], B.lo[2], B.hi[0], B.hi[1], B.hi[2]);
+    }
+    fprintf(fh, ")\n%d\n", (int)boxes.size());
+    for (long long o : offsets) fprintf(fh, "FabOnDisk: Cell_D_00000 %lld\n", o);
+    for (int pass = 0; pass < 2; ++pass) {
+        fprintf(fh, "\n%d,%d\n", (int)boxes.size(), nc);
+        for (const auto& v : (pass == 0 ? mins : maxs)) {
+            for (double x : v) fprintf(fh, "%.17g,", x);
+            fprintf(fh, "\n");
+        }
+    }
+    fclose(fh);
+
+    // plotfile header
+    FILE* fp = fopen((root + "/Header").c_str(), "w");
+    if (!fp) { set_error(CASTRO_ERR_ARG, "castro_sim_write_plotfile: Header"); return CASTRO_ERR_ARG; }
+    fprintf(fp, "HyperCLaw-V1.1\n%d\n", nc);
+    for (const auto& nm : names) fprintf(fp, "%s\n", nm.c_str());
+    fprintf(fp, "3\n%.17g\n0\n", hs.time);
+    fprintf(fp, "%.17g %.17g %.17g\n", D.problo[0], D.problo[1], D.problo[2]);
+    fprintf(fp, "%.17g %.17g %.17g\n", D.probhi[0], D.probhi[1], D.probhi[2]);
+    fprintf(fp, "\n((%d,%d,%d) (%d,%d,%d) (0,0,0))\n", D.dom_lo[0], D.dom_lo[1], D.dom_lo[2], D.dom_hi[0], D.dom_hi[1],
+            D.dom_hi[2]);
+    fprintf(fp, "%d\n%.17g %.17g %.17g\n0\n0\n", hs.steps, dx[0], dx[1], dx[2]);
+    fprintf(fp, "0 %d %.17g\n%d\n", (int)boxes.size(), hs.time, hs.steps);
+    for (int b : boxes) {
+        const BoxDev& B = s->hboxes[b];
+        for (int d = 0; d < 3; ++d)
+            fprintf(fp, "%.17g %.17g\n", D.problo[d] + B.lo[d] * dx[d], D.problo[d] + (B.hi[d] + 1) * dx[d]);
+    }
+    fprintf(fp, "Level_0/Cell\n");
+    fclose(fp);
+    return castro_last_error();
 }
 
 double castro_sim_blast_radius(castro_sim* s, int inst, double* blast_mass)

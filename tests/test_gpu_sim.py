@@ -197,3 +197,29 @@ def test_construct_hydro_source_box(pkg, table, oracle, exact):
     bal = (fx[0][0].sum() - fx[0][-1].sum() + fx[1][:, 0].sum() - fx[1][:, -1].sum()
            + fx[2][:, :, 0].sum() - fx[2][:, :, -1].sum())
     assert abs(tot - bal) <= 1e-12 * max(abs(bal), abs(tot), area)
+
+
+def test_plotfile_roundtrip(pkg, table, tmp_path):
+    """castro_sim_write_plotfile: AMReX layout (Header, Level_0/Cell_H,
+    Level_0/Cell_D_00000) read back into the exact domain state, with the
+    instance's time, step count, geometry and BoxArray."""
+    cfg = pkg.configs.batched(scale=8, ninst=2)      # 32^3 uneven BoxArray + two instances
+    L = gpu_lib(pkg, table, cfg["network"], False)
+    sim = pkg.make_sim(L, cfg, 1)
+    sim.init_data()
+    sim.step(3)
+    states = sim.box_states()
+    for n, inst in enumerate(cfg["instances"]):
+        path = str(tmp_path / f"plt{n}")
+        sim.write_plotfile(path, n)
+        hdr, data = pkg.plotfile.read_plotfile(path)
+        G = pkg.castro.assemble(inst, states[n])
+        np.testing.assert_array_equal(data, G)
+        assert hdr["version"] == "HyperCLaw-V1.1"
+        assert hdr["names"][:7] == ["density", "xmom", "ymom", "zmom", "rho_E", "rho_e", "Temp"]
+        assert hdr["steps"] == 3 and hdr["time"] == sim.time(n)
+        assert hdr["domain"] == (tuple(inst["dom_lo"]), tuple(inst["dom_hi"]))
+        assert sorted(hdr["boxes"]) == sorted((tuple(a), tuple(b)) for a, b in inst["boxes"])
+        n_cell = inst["dom_hi"][0] - inst["dom_lo"][0] + 1
+        assert hdr["dx"][0] == pytest.approx((inst["probhi"][0] - inst["problo"][0]) / n_cell, rel=1e-15)
+    sim.close()
