@@ -212,6 +212,9 @@ __global__ void k_box_sum(BoxRange r, F f, double* out)
 }
 
 // same with two sums: the body returns a double2
+template <int MINB, class F>
+__global__ void __launch_bounds__(128, MINB) k_box_sum2_lb(BoxRange r, F f, double* out0);
+
 template <class F>
 __global__ void k_box_sum2(BoxRange r, F f, double* out0)
 {
@@ -240,7 +243,36 @@ __global__ void k_box_sum2(BoxRange r, F f, double* out0)
     }
 }
 
-template <class F>
+template <int MINB, class F>
+__global__ void __launch_bounds__(128, MINB) k_box_sum2_lb(BoxRange r, F f, double* out0)
+{
+    __shared__ double red[2][32];
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double2 v = make_double2(0.0, 0.0);
+    if (t < r.n) {
+        int i = r.lx + (int)(t % r.nx);
+        long long t2 = t / r.nx;
+        int j = r.ly + (int)(t2 % r.ny);
+        int k = r.lz + (int)(t2 / r.ny);
+        v = f(i, j, k);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    }
+    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = v.x; red[1][threadIdx.x >> 5] = v.y; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { s0 += red[0][w]; s1 += red[1][w]; }
+        out0[2 * blockIdx.x] = s0;
+        out0[2 * blockIdx.x + 1] = s1;
+    }
+}
+
+// MINB = 0: no register budget
+template <int MINB = 0, class F>
 void launch_sum2(const char* what, const int* lo, const int* hi, F f, double* out0, double* out1)
 {
     BoxRange r = make_range(lo, hi);
@@ -248,7 +280,8 @@ void launch_sum2(const char* what, const int* lo, const int* hi, F f, double* ou
     const int B = 128;
     const long long nb = (r.n + B - 1) / B;
     if (nb > PART_MAX || !part_buffer()) { set_error(CASTRO_ERR_ARG, "adjoint: box too large for the partial sums"); return; }
-    k_box_sum2<<<(unsigned)nb, B, 0, stream()>>>(r, f, g_part);
+    if (MINB == 0) k_box_sum2<<<(unsigned)nb, B, 0, stream()>>>(r, f, g_part);
+    else k_box_sum2_lb<(MINB > 0 ? MINB : 1)><<<(unsigned)nb, B, 0, stream()>>>(r, f, g_part);
     if (out0 || out1) k_finish_sum<<<1, 256, 0, stream()>>>(g_part, (int)nb, out0, out1);
     check_launch(what);
 }
@@ -380,7 +413,22 @@ void trace_adj_impl(const int* lo, const int* hi, const int* vlo, const int* vhi
     else trace_adj_dir<NS, 2>(lo, hi, vlo[2], vhi[2], Q, QA, QMB, QPB, QB, QAB, dtdx, dtdxb);
 }
 
-template <int NS, int D>
+template <int NS>
+__device__ __forceinline__ void put_state(const Fab& f, int i, int j, int k, const double* s)
+{
+    f(i, j, k, QRHO) = s[SRHO];
+    f(i, j, k, QU) = s[SU];
+    f(i, j, k, QV) = s[SV];
+    f(i, j, k, QW) = s[SW];
+    f(i, j, k, QPRES) = s[SPRES];
+    f(i, j, k, QREINT) = s[SREI];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) f(i, j, k, QFS + n) = s[SX + n];
+}
+
+// STORE: the face-state adjoints are written instead of accumulated (the
+// caller's first writer of those faces, so they need no zeroing)
+template <int NS, int D, bool STORE = false>
 void compute_flux_adj_dir(const int* lo, const int* hi, Fab QL, Fab QR, Fab QA, Fab FXB, Fab QGB, Fab QLB, Fab QRB,
                           Fab QAB)
 {
@@ -400,8 +448,13 @@ void compute_flux_adj_dir(const int* lo, const int* hi, Fab QL, Fab QR, Fab QA, 
         double gl = 0.0, gr = 0.0, cl = 0.0, cr = 0.0;
         riemann_cgf_adj<NS, D>(ql, qr, QA(i - ex, j - ey, k - ez, QGAMC), QA(i, j, k, QGAMC), QA(i - ex, j - ey, k - ez, QC),
                                QA(i, j, k, QC), flxb, qgb, qlb, qrb, gl, gr, cl, cr);
-        add_state<NS>(QLB, i, j, k, qlb);
-        add_state<NS>(QRB, i, j, k, qrb);
+        if (STORE) {
+            put_state<NS>(QLB, i, j, k, qlb);
+            put_state<NS>(QRB, i, j, k, qrb);
+        } else {
+            add_state<NS>(QLB, i, j, k, qlb);
+            add_state<NS>(QRB, i, j, k, qrb);
+        }
         aadd(&QAB(i - ex, j - ey, k - ez, QGAMC), gl);
         aadd(&QAB(i, j, k, QGAMC), gr);
         aadd(&QAB(i - ex, j - ey, k - ez, QC), cl);
@@ -411,8 +464,14 @@ void compute_flux_adj_dir(const int* lo, const int* hi, Fab QL, Fab QR, Fab QA, 
 
 template <int NS>
 void compute_flux_adj_impl(const int* lo, const int* hi, Fab QL, Fab QR, Fab QA, Fab FXB, Fab QGB, Fab QLB, Fab QRB,
-                           Fab QAB, int idir)
+                           Fab QAB, int idir, bool store = false)
 {
+    if (store) {
+        if (idir == 0) compute_flux_adj_dir<NS, 0, true>(lo, hi, QL, QR, QA, FXB, QGB, QLB, QRB, QAB);
+        else if (idir == 1) compute_flux_adj_dir<NS, 1, true>(lo, hi, QL, QR, QA, FXB, QGB, QLB, QRB, QAB);
+        else compute_flux_adj_dir<NS, 2, true>(lo, hi, QL, QR, QA, FXB, QGB, QLB, QRB, QAB);
+        return;
+    }
     if (idir == 0) compute_flux_adj_dir<NS, 0>(lo, hi, QL, QR, QA, FXB, QGB, QLB, QRB, QAB);
     else if (idir == 1) compute_flux_adj_dir<NS, 1>(lo, hi, QL, QR, QA, FXB, QGB, QLB, QRB, QAB);
     else compute_flux_adj_dir<NS, 2>(lo, hi, QL, QR, QA, FXB, QGB, QLB, QRB, QAB);
@@ -811,6 +870,7 @@ struct castro_adj {
     double* d_scal = nullptr;   // [32] scalar accumulators
     int* d_idx = nullptr;
     double* d_est = nullptr;
+    double* d_chain = nullptr;  // time-step adjoint chain of the reverse sweep
     std::vector<double> dts, times, ests, estmin;
     std::vector<char> limited, clamped;
     double J = 0.0;
@@ -1162,7 +1222,7 @@ double objective(castro_adj* a, const Arr& V, bool grad, const Arr& Vb)
 
 // adjoint of the CFL estimate at its arg-min zone: Vb(m) += scale * d(estdt_m)/dV
 template <int NS>
-void estdt_adj(castro_adj* a, const Arr& V, double minval, double scale, const Arr& Vb)
+void estdt_adj(castro_adj* a, const Arr& V, double minval, const double* scale, const Arr& Vb)
 {
     int big = 0x7fffffff;
     cudaMemcpyAsync(a->d_idx, &big, sizeof big, cudaMemcpyHostToDevice, a->st);
@@ -1182,12 +1242,13 @@ void estdt_adj(castro_adj* a, const Arr& V, double minval, double scale, const A
     const int one[3] = {0, 0, 0};
     launch_box<32>("adj estdt", one, one, [=] __device__(int, int, int) {
         int m = *idx;
-        if (m == 0x7fffffff) return;
+        const double sc_ = *scale;
+        if (m == 0x7fffffff || sc_ == 0.0) return;
         int i = bx.lo[0] + m % nx, j = bx.lo[1] + (m / nx) % ny, k = bx.lo[2] + m / (nx * ny);
         double u[Dims<NS>::NVAR], ub[Dims<NS>::NVAR];
         for (int n = 0; n < Dims<NS>::NVAR; ++n) { u[n] = U(i, j, k, n); ub[n] = 0.0; }
         const double dxs[3] = {dx0, dx1, dx2};
-        estdt_pt_adj<NS>(c_eos, c_net, u, dxs, scale, ub);
+        estdt_pt_adj<NS>(c_eos, c_net, u, dxs, sc_, ub);
         for (int n = 0; n < Dims<NS>::NVAR; ++n) UB(i, j, k, n) += ub[n];
     });
 }
@@ -1270,7 +1331,7 @@ void trans2_adj_zones(castro_adj* a, int d, double c2, double c3, double* c2b, d
     Fab MOB = a->qlb[d].fab(), POB = a->qrb[d].fab(), MB = a->qmb[d][d].fab(), PB = a->qpb[d][d].fab();
     Fab QAB = a->qab.fab(), L2 = a->T2L[d][0].fab(), R2 = a->T2R[d][0].fab(), L3 = a->T2L[d][1].fab(),
         R3 = a->T2R[d][1].fab();
-    launch_sum2("trans2_adj zones", zb.lo, zb.hi, [=] __device__(int i, int j, int k) -> double2 {
+    launch_sum2<3>("trans2_adj zones", zb.lo, zb.hi, [=] __device__(int i, int j, int k) -> double2 {
         constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF;
         const int e1x = d == 0, e1y = d == 1, e1z = d == 2;
         const int e2x = t1 == 0, e2y = t1 == 1, e2z = t1 == 2;
@@ -1350,9 +1411,10 @@ void gather_records(const IBx& fb, int n, const IBx& zb0, Fab L0, Fab R0, bool t
 }
 
 // reverse of one step: a->Vb holds the adjoint of V_{n+1} on entry and of V_n
-// on exit; returns the adjoint of dt_n from this step's use of it
+// on exit; slots 0..9 of a->d_scal receive the adjoint of dt_n from this
+// step's uses of it
 template <int NS>
-double reverse_step(castro_adj* a, const Arr& Vn, double dt)
+void reverse_step(castro_adj* a, const Arr& Vn, double dt)
 {
     cudaStream_t st = a->st;
     const IBx &bx = a->bx, &obx = a->obx, &qbx = a->qbx;
@@ -1360,11 +1422,12 @@ double reverse_step(castro_adj* a, const Arr& Vn, double dt)
     for (int d = 0; d < 3; ++d) {
         // F1b/G1b/F2b/G2b need no zeroing: the record gathers write every face
         // the Riemann adjoints read (the other components stay zero from creation)
-        for (Arr* r : {&a->qlb[d], &a->qrb[d], &a->fluxb[d], &a->qeb[d]}) zero(*r, st);
-        for (int e = 0; e < 3; ++e) {
-            zero(a->qmb[d][e], st);
-            zero(a->qpb[d][e], st);
-        }
+        // qlb/qrb and the cross face states qmb/qpb[a][b] (a != b) are stored, not
+        // accumulated, by their first writer (the riemann3 / riemann2 adjoints)
+        // on exactly the faces their readers use
+        for (Arr* r : {&a->fluxb[d], &a->qeb[d]}) zero(*r, st);
+        zero(a->qmb[d][d], st);
+        zero(a->qpb[d][d], st);
     }
     cudaMemsetAsync(a->d_scal, 0, 32 * sizeof(double), st);
     double* sc = a->d_scal;
@@ -1399,7 +1462,8 @@ double reverse_step(castro_adj* a, const Arr& Vn, double dt)
         apply_av_adj_impl<NS>(a->ebx[d].lo, a->ebx[d].hi, d, a->dx[d], a->P->div.fab(), a->P->Sb.fab(), a->fluxb[d].fab(),
                               a->divb.fab(), a->Sbb.fab());
         compute_flux_adj_impl<NS>(a->ebx[d].lo, a->ebx[d].hi, a->P->ql[d].fab(), a->P->qr[d].fab(), a->P->qaux.fab(),
-                                  a->fluxb[d].fab(), a->qeb[d].fab(), a->qlb[d].fab(), a->qrb[d].fab(), a->qab.fab(), d);
+                                  a->fluxb[d].fab(), a->qeb[d].fab(), a->qlb[d].fab(), a->qrb[d].fab(), a->qab.fab(), d,
+                                  true);
     }
     adj_stage(a, "normalize/av/riemann3");
     double hdtdx[3], cdtdx[3];
@@ -1420,7 +1484,7 @@ double reverse_step(castro_adj* a, const Arr& Vn, double dt)
             if (x == y) continue;
             compute_flux_adj_impl<NS>(a->tbx[x][y].lo, a->tbx[x][y].hi, a->P->qm[x][y].fab(), a->P->qp[x][y].fab(),
                                       a->P->qaux.fab(), a->F2b[x][y].fab(), a->G2b[x][y].fab(), a->qmb[x][y].fab(),
-                                      a->qpb[x][y].fab(), a->qab.fab(), x);
+                                      a->qpb[x][y].fab(), a->qab.fab(), x, true);
         }
     adj_stage(a, "riemann2");
     for (int d = 0; d < 3; ++d) {
@@ -1452,12 +1516,23 @@ double reverse_step(castro_adj* a, const Arr& Vn, double dt)
     clean_state_adj_impl<NS>(bx.lo, bx.hi, Vn.fab(), a->Ab.fab(), true);
     adj_stage(a, "start clean");
     copy(a->Vb, a->Ab, st);
-    double h[16];
-    cudaMemcpyAsync(h, sc, 16 * sizeof(double), cudaMemcpyDeviceToHost, st);
-    cudaStreamSynchronize(st);
-    double dtb = h[9];
-    for (int d = 0; d < 3; ++d) dtb += h[d] / a->dx[d] + h[3 + d] / a->dx[d] / 3.0 + h[6 + d] * 0.5 / a->dx[d];
-    return dtb;
+}
+
+// adjoint of dt_n: its uses in step n (slots 0..9 of sc), the growth-limit
+// chain from later steps (chain[n]) and the time adjoint (chain[N]); then the
+// rule that made dt_n: stop-time clamp (branch 1), 1.1x growth limit (2), or
+// the CFL estimate (0: chain[N+1] = scale handed to estdt_adj)
+__global__ void k_dt_chain(const double* sc, double dx0, double dx1, double dx2, double* chain, int n, int N,
+                           int branch, double fac)
+{
+    const double dx[3] = {dx0, dx1, dx2};
+    double dtb = sc[9];
+    for (int d = 0; d < 3; ++d) dtb += sc[d] / dx[d] + sc[3 + d] / dx[d] / 3.0 + sc[6 + d] * 0.5 / dx[d];
+    dtb += chain[n] + chain[N];
+    chain[N + 1] = 0.0;
+    if (branch == 1) chain[N] -= dtb;
+    else if (branch == 2) chain[n - 1] += 1.1e0 * dtb;
+    else chain[N + 1] = fac * dtb;
 }
 
 template <int NS>
@@ -1630,8 +1705,9 @@ int adj_backward(castro_adj* a, double* dE, double* drho, double* pertb)
     const int N = a->nsteps, K = a->ckpt;
     zero(a->Vb, a->st);
     objective<NS>(a, a->Vfinal, true, a->Vb);
-    std::vector<double> dtb(N, 0.0);
-    double timeb = 0.0;   // adjoint of the running time (stop-time clamp)
+    // chain[0..N-1]: adjoint of dt_n from the growth limit of later steps;
+    // chain[N]: adjoint of the running time (stop-time clamp); chain[N+1]: scale
+    cudaMemsetAsync(a->d_chain, 0, (N + 2) * sizeof(double), a->st);
     const int nseg = (N + K - 1) / K;
     for (int sgi = nseg - 1; sgi >= 0; --sgi) {
         const int n0 = sgi * K, n1 = std::min(N, n0 + K);
@@ -1653,16 +1729,12 @@ int adj_backward(castro_adj* a, double* dE, double* drho, double* pertb)
                 forward_step<NS>(a, a->seg[n - n0], a->dts[n]);
             }
             adj_mark(a, "step recompute");
-            double dtb_n = reverse_step<NS>(a, a->seg[n - n0], a->dts[n]) + dtb[n] + timeb;
-            // dt_n = rule(V_n, dt_{n-1}, time_n)
-            if (a->clamped[n]) {
-                timeb -= dtb_n;   // dt_n = stop_time - time_n
-            } else if (n > 0 && a->limited[n]) {
-                dtb[n - 1] += 1.1e0 * dtb_n;
-            } else if (dtb_n != 0.0) {
-                double scale = cfl * (n == 0 ? 0.01 : 1.0) * dtb_n;
-                estdt_adj<NS>(a, a->seg[n - n0], a->estmin[n], scale, a->Vb);
-            }
+            reverse_step<NS>(a, a->seg[n - n0], a->dts[n]);
+            // dt_n = rule(V_n, dt_{n-1}, time_n), reversed on the device
+            const int branch = a->clamped[n] ? 1 : (n > 0 && a->limited[n]) ? 2 : 0;
+            k_dt_chain<<<1, 1, 0, a->st>>>(a->d_scal, a->dx[0], a->dx[1], a->dx[2], a->d_chain, n, N, branch,
+                                           cfl * (n == 0 ? 0.01 : 1.0));
+            if (branch == 0) estdt_adj<NS>(a, a->seg[n - n0], a->estmin[n], a->d_chain + N + 1, a->Vb);
             adj_mark(a, "dt adjoint");
         }
         adj_prof_flush();
@@ -1776,6 +1848,7 @@ castro_adj* castro_adj_create(const castro_instance_desc* desc, int nsteps, int 
     ok = ok && cudaMalloc(&a->d_scal, 32 * sizeof(double)) == cudaSuccess;
     ok = ok && cudaMalloc(&a->d_idx, sizeof(int)) == cudaSuccess;
     ok = ok && cudaMalloc(&a->d_est, sizeof(double)) == cudaSuccess;
+    ok = ok && cudaMalloc(&a->d_chain, (nsteps + 2) * sizeof(double)) == cudaSuccess;
     if (!ok) {
         set_error(CASTRO_ERR_CUDA, "castro_adj_create: device allocation failed");
         castro_adj_destroy(a);
@@ -1819,6 +1892,7 @@ void castro_adj_destroy(castro_adj* a)
     if (a->d_scal) cudaFree(a->d_scal);
     if (a->d_idx) cudaFree(a->d_idx);
     if (a->d_est) cudaFree(a->d_est);
+    if (a->d_chain) cudaFree(a->d_chain);
     if (a->st) cudaStreamDestroy(a->st);
     delete a;
 }
