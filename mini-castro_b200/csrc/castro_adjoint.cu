@@ -152,9 +152,12 @@ __device__ __forceinline__ void aadd_tflux(const Fab& f, const Fab& qg, int i, i
 // same-address atomics from thousands of blocks); a one-block kernel then adds
 // their sum to the output scalar(s).
 constexpr int PART_MAX = 1 << 20;
-// PART_MAX x 2 doubles, allocated on first use; shared by every reduction of
-// this library, which are issued on the library stream one after another
-double* g_part = nullptr;
+// PART_MAX x 2 doubles per device, allocated on first use on that device;
+// shared by every reduction of this library on the device, which are issued on
+// the library stream one after another
+constexpr int MAX_DEVICES = 64;
+double* g_part_dev[MAX_DEVICES] = {};
+double* g_part = nullptr;   // the current device's buffer (set by part_buffer)
 
 __global__ void k_finish_sum(const double* part, int nb, double* out0, double* out1)
 {
@@ -178,11 +181,17 @@ __global__ void k_finish_sum(const double* part, int nb, double* out0, double* o
 
 bool part_buffer()
 {
-    if (!g_part && cudaMalloc(&g_part, sizeof(double) * 2 * PART_MAX) != cudaSuccess) {
-        g_part = nullptr;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) {
+        set_error(CASTRO_ERR_CUDA, "adjoint: current device");
+        return false;
+    }
+    if (!g_part_dev[dev] && cudaMalloc(&g_part_dev[dev], sizeof(double) * 2 * PART_MAX) != cudaSuccess) {
+        g_part_dev[dev] = nullptr;
         set_error(CASTRO_ERR_CUDA, "adjoint: partial-sum buffer");
         return false;
     }
+    g_part = g_part_dev[dev];
     return true;
 }
 
