@@ -245,8 +245,8 @@ def run_b200(args, pkg, rank, world):
         sim3.close()
 
     batched_cfg = None
-    if rank == 0 and args.batched_steps > 0:
-        batched_cfg = run_batched_config(pkg, L, args)
+    if args.batched_steps > 0:      # every rank: the instances are split over the ranks
+        batched_cfg = run_batched_config(pkg, L, args, rank, world)
     adjoint_cfg = None
     if rank == 0 and args.adjoint_reps > 0:
         adjoint_cfg = run_adjoint_config(pkg, args)
@@ -310,33 +310,46 @@ def run_b200(args, pkg, rank, world):
     return line
 
 
-def run_batched_config(pkg, L, args):
+def run_batched_config(pkg, L, args, rank=0, world=1):
     """a 256^3 Sedov domain on an uneven BoxArray (per-axis box sizes
     drawn from {16,24,32,48,64}) plus 32 independent instances of 32^3..96^3
-    zones, advanced together; batched fused path vs the per-box path."""
+    zones, advanced together; batched fused path vs the per-box path.  With N
+    ranks the instances are split over them by zone count (no data-path
+    collective: instances are independent; strong scaling)."""
     import torch
 
-    cfg = pkg.configs.batched()
-    zones = pkg.configs.zones(cfg)
+    full = pkg.configs.batched()
+    zones_all = [pkg.configs.zones(dict(full, instances=[i])) for i in full["instances"]]
+    mine = pkg.replicas.partition_by_zones(zones_all, world)[rank] if world > 1 else list(range(len(zones_all)))
+    cfg = dict(full, instances=[full["instances"][i] for i in mine])
+    zones = sum(zones_all)
     out = {"workload": "batched: 256^3 uneven BoxArray + 32 instances 32^3..96^3, E 1e49-1e51, rho 0.1-10, 2 species",
-           "zones": zones, "instances": len(cfg["instances"]),
-           "boxes": sum(len(i["boxes"]) for i in cfg["instances"])}
+           "zones": zones, "instances": len(full["instances"]),
+           "boxes": sum(len(i["boxes"]) for i in full["instances"]),
+           "sharding": (f"instances split over {world} ranks by zone count (largest first to the least-loaded "
+                        "rank); no data-path collective" if world > 1 else "one GPU"),
+           "scaling": "strong" if world > 1 else "single"}
     for mode, key, steps in ((pkg.castro.MODE_BATCHED, "batched", args.batched_steps),
                              (pkg.castro.MODE_PLAIN, "plain_per_box", 2)):
-        sim = pkg.make_sim(L, cfg, mode)
-        sim.init_data()
-        sim.step(2)
-        sim.sync()
-        st = torch.cuda.ExternalStream(sim.stream())
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        sim.step(steps)
-        e1.record(st)
-        e1.synchronize()
-        ms = e0.elapsed_time(e1)
+        ms = 0.0
+        launches = 0
+        if cfg["instances"]:
+            sim = pkg.make_sim(L, cfg, mode)
+            sim.init_data()
+            sim.step(2)
+            sim.sync()
+            st = torch.cuda.ExternalStream(sim.stream())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            sim.step(steps)
+            e1.record(st)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            launches = sim.launches_per_step()
+            sim.close()
+        ms = pkg.replicas.max_over_ranks(ms, device="cuda")
         out[key] = {"value": zones * steps / (ms * 1e-3), "ms_per_step": ms / steps, "steps": steps,
-                    "launches_per_step": sim.launches_per_step()}
-        sim.close()
+                    "launches_per_step": launches}
     out["speedup_batched_over_plain"] = out["batched"]["value"] / out["plain_per_box"]["value"]
     return out
 

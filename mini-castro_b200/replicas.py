@@ -1,5 +1,7 @@
-"""Multi-GPU host logic: one process per GPU, each advancing its own replica of
-the workload (independent Sedov instances need no data-path collective).
+"""Multi-GPU host logic: one process per GPU.  Independent Sedov instances
+need no data-path collective, so ranks either advance their own replica of a
+workload (weak scaling) or split a workload's instances between them
+(``partition_by_zones``, strong scaling).
 
 The only collectives are the timing reductions of the benchmark: the step time
 is the slowest rank's, and the whole-job rate counts every rank's zones.
@@ -23,3 +25,16 @@ def max_over_ranks(x: float, device=None) -> float:
 def whole_job_rate(zones_per_rank: int, steps: int, ms_max: float, world: int) -> float:
     """Zone-updates per second of the whole job under weak scaling."""
     return world * zones_per_rank * steps / (ms_max * 1e-3)
+
+
+def partition_by_zones(zones: list[int], world: int) -> list[list[int]]:
+    """Instance indices per rank, balanced by zone count: the largest remaining
+    instance goes to the least-loaded rank (longest-processing-time first).
+    Deterministic, so every rank computes the same split without communicating."""
+    parts = [[] for _ in range(world)]
+    load = [0] * world
+    for idx in sorted(range(len(zones)), key=lambda i: (-zones[i], i)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(idx)
+        load[r] += zones[idx]
+    return [sorted(p) for p in parts]

@@ -50,3 +50,17 @@ def test_two_rank_reductions(tmp_path):
 def test_single_process_is_identity(pkg):
     assert pkg.replicas.max_over_ranks(3.5) == 3.5
     assert pkg.replicas.whole_job_rate(10, 2, 1.0, 1) == pytest.approx(2e4)
+
+
+def test_partition_by_zones(pkg):
+    """Every instance on exactly one rank; loads within one instance of each other
+    (longest-processing-time bound); the batched configuration's 33 instances."""
+    cfg = pkg.configs.batched()
+    zones = [pkg.configs.zones(dict(cfg, instances=[i])) for i in cfg["instances"]]
+    for world in (1, 2, 3, 4, 8):
+        parts = pkg.replicas.partition_by_zones(zones, world)
+        assert len(parts) == world
+        assert sorted(i for p in parts for i in p) == list(range(len(zones)))
+        loads = [sum(zones[i] for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(zones)
+    assert pkg.replicas.partition_by_zones(zones, 2) == pkg.replicas.partition_by_zones(list(zones), 2)
