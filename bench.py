@@ -58,8 +58,8 @@ class ClockSampler:
     """SM clock and clock-event (throttle) reasons of this process's GPU, read
     through NVML every 10 ms on a background thread while the timed region
     runs (the GPU is found by its PCI bus id, so CUDA_VISIBLE_DEVICES does not
-    matter).  Readings only: no setting of the GPU is touched.  The samples go
-    to gpurun_out/clocks_rank<r>.csv as well."""
+    matter).  Readings only: no setting of the GPU is touched.  The samples are
+    also written as CSV to the file named by $CASTRO_CLOCKS_CSV, if set."""
 
     PERIOD_S = 0.01
 
@@ -67,7 +67,7 @@ class ClockSampler:
         self.cuda_index = cuda_index
         self.rows = []
         self.err = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{cuda_index}.csv")
+        self.path = os.environ.get("CASTRO_CLOCKS_CSV")
 
     def _handle(self):
         import pynvml as nv
@@ -117,8 +117,10 @@ class ClockSampler:
         if self.t:
             self.stop.set()
             self.t.join(timeout=5)
+        if not self.path:
+            return
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            os.makedirs(os.path.dirname(os.path.abspath(self.path)), exist_ok=True)
             with open(self.path, "w") as fp:
                 fp.write("unix_time,sm_mhz,sm_max_mhz,power_w,reasons\n")
                 for t, sm, pw, rs in self.rows:
@@ -311,7 +313,7 @@ def run_b200(args, pkg, rank, world):
 
 
 def run_batched_config(pkg, L, args, rank=0, world=1):
-    """a 256^3 Sedov domain on an uneven BoxArray (per-axis box sizes
+    """The batched configuration: a 256^3 Sedov domain on an uneven BoxArray (per-axis box sizes
     drawn from {16,24,32,48,64}) plus 32 independent instances of 32^3..96^3
     zones, advanced together; batched fused path vs the per-box path.  With N
     ranks the instances are split over them by zone count (no data-path
@@ -372,7 +374,7 @@ def workload_text(args) -> str:
 
 
 def run_adjoint_config(pkg, args):
-    """gradient of the shell kinetic energy (0.3 <= r/L <= 0.4) of a
+    """The gradient configuration: gradient of the shell kinetic energy (0.3 <= r/L <= 0.4) of a
     64^3 perturbed Sedov run over 20 steps with respect to the blast energy,
     the ambient density and the per-zone density perturbation, checkpoint every
     5 steps.  Reports forward and reverse device times (the forward is the

@@ -1,7 +1,8 @@
 // castro_device.cuh -- per-zone and per-face device stages of the CTU hydro
 // advance (Helmholtz EOS, state cleaning, conserved->primitive, PPM trace,
 // CGF Riemann, transverse corrections), shared by the per-routine C-ABI
-// kernels (castro_abi.cu) and the fused batched pipeline (castro_fused.cu).
+// kernels (castro_abi.cu), the fused batched pipeline (castro_sim.cu) and the
+// reverse-mode stages (castro_adjoint.cuh).
 //
 // FP64 throughout.  Statement order follows the reference Fortran so that a
 // build with -DCASTRO_EXACT --fmad=false reproduces a non-contracting CPU build
@@ -76,7 +77,7 @@ struct NetworkDev {
 };
 
 // Each translation unit holds its own copy; castro_upload_constants_<tu>()
-// fills it (see castro_host.cpp).
+// fills it (see castro_host.cu).
 static __constant__ EosTableDev c_eos;
 static __constant__ NetworkDev c_net;
 
