@@ -14,9 +14,11 @@ library, and times the batched step of the workload in a fresh process (CUDA
 events, after warm-up, best of three runs).  The knobs are searched by
 coordinate descent from the current defaults: the block size, then the
 register budget of the EOS kernels (front, update), of the final Riemann
-kernel, of trace, and of the first two Riemann kernels.  No knob changes any
-arithmetic, only register allocation and the distribution of zones over
-blocks, so every candidate computes the same results; the winner is written as
+kernel, of trace, and of the first two Riemann kernels, then the length of
+the zone segment one trace thread walks, and which operands riemann2 and
+riemann3 stage in shared memory.  No knob changes any arithmetic, only register
+allocation, the distribution of zones over threads and blocks and the path of
+the loads, so every candidate computes the same results; the winner is written as
 the header together with the timing table, and ``build.py`` compiles the
 library with it.
 """
@@ -40,9 +42,12 @@ KNOBS = [
     ("CASTRO_MINB_R3", [0, 2, 3, 4]),
     ("CASTRO_MINB_TRACE", [0, 2, 3, 4]),
     ("CASTRO_MINB_RIEMANN", [0, 2, 3, 4]),
+    ("CASTRO_TRACE_SEG", [3, 5, 7, 9]),
+    ("CASTRO_R2_STAGE", [0, 1, 2]),
+    ("CASTRO_R3_STAGE", [0, 1]),
 ]
-DEFAULTS = {"CASTRO_BLOCK": 128, "CASTRO_MINB_EOS": 4, "CASTRO_MINB_R3": 3, "CASTRO_MINB_TRACE": 0,
-            "CASTRO_MINB_RIEMANN": 0}
+DEFAULTS = {"CASTRO_BLOCK": 128, "CASTRO_MINB_EOS": 4, "CASTRO_MINB_R3": 0, "CASTRO_MINB_TRACE": 4,
+            "CASTRO_MINB_RIEMANN": 0, "CASTRO_TRACE_SEG": 5, "CASTRO_R2_STAGE": 1, "CASTRO_R3_STAGE": 0}
 
 
 def key(cfg: dict) -> str:

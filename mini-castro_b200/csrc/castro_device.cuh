@@ -619,29 +619,42 @@ CASTRO_HD double vl_slope(double sm1, double s0, double sp1)
     return 0.0;
 }
 
+// Interface value between a zone with value a and its right neighbour with
+// value b, from their van Leer slopes da, db (ppm.F90:171-180 for sm, :193-202
+// for sp).  The minus edge of a zone and the plus edge of its left neighbour
+// are this same expression on the same operands in the same order.
+CASTRO_HD double ppm_edge(double a, double b, double da, double db)
+{
+    double e = 0.5 * (b + a) - SIXTH * (db - da);
+    e = DMAX(e, DMIN(b, a));
+    return DMIN(e, DMAX(b, a));
+}
+
+// Flattening and monotonicity limiting of the edges of a zone with value s0,
+// ppm.F90:204-236
+CASTRO_HD void ppm_limit(double s0, double flatn, double& sm, double& sp)
+{
+    sm = flatn * sm + (1.0 - flatn) * s0;
+    sp = flatn * sp + (1.0 - flatn) * s0;
+    if ((sp - s0) * (s0 - sm) <= 0.0) {
+        sp = s0;
+        sm = s0;
+    } else if (fabs(sp - s0) >= 2.0 * fabs(sm - s0)) {
+        sp = 3.0 * s0 - 2.0 * sm;
+    } else if (fabs(sm - s0) >= 2.0 * fabs(sp - s0)) {
+        sm = 3.0 * s0 - 2.0 * sp;
+    }
+}
+
 // ppm_reconstruct, Source/ppm.F90:132-236; s[0..4] = s(-2..2)
 CASTRO_HD void ppm_reconstruct(const double* s, double flatn, double& smo, double& spo)
 {
     double dsvl_l = vl_slope(s[0], s[1], s[2]);
-    double dsvl_r = vl_slope(s[1], s[2], s[3]);
-    double sm = 0.5 * (s[2] + s[1]) - SIXTH * (dsvl_r - dsvl_l);
-    sm = DMAX(sm, DMIN(s[2], s[1]));
-    sm = DMIN(sm, DMAX(s[2], s[1]));
-    dsvl_l = dsvl_r;                       // same slope (ppm.F90:184-191 repeats :162-169)
-    dsvl_r = vl_slope(s[2], s[3], s[4]);
-    double sp = 0.5 * (s[3] + s[2]) - SIXTH * (dsvl_r - dsvl_l);
-    sp = DMAX(sp, DMIN(s[3], s[2]));
-    sp = DMIN(sp, DMAX(s[3], s[2]));
-    sm = flatn * sm + (1.0 - flatn) * s[2];
-    sp = flatn * sp + (1.0 - flatn) * s[2];
-    if ((sp - s[2]) * (s[2] - sm) <= 0.0) {
-        sp = s[2];
-        sm = s[2];
-    } else if (fabs(sp - s[2]) >= 2.0 * fabs(sm - s[2])) {
-        sp = 3.0 * s[2] - 2.0 * sm;
-    } else if (fabs(sm - s[2]) >= 2.0 * fabs(sp - s[2])) {
-        sm = 3.0 * s[2] - 2.0 * sp;
-    }
+    double dsvl_c = vl_slope(s[1], s[2], s[3]);
+    double dsvl_r = vl_slope(s[2], s[3], s[4]);   // ppm.F90:184-191 repeats :162-169 for the centre slope
+    double sm = ppm_edge(s[1], s[2], dsvl_l, dsvl_c);
+    double sp = ppm_edge(s[2], s[3], dsvl_c, dsvl_r);
+    ppm_limit(s[2], flatn, sm, sp);
     smo = sm;
     spo = sp;
 }

@@ -53,8 +53,9 @@ constexpr int NG = 4;   // ghost zones of Sborder, Source/Castro_advance.cpp:37
 // (= the zones of one work item) and the minimum resident blocks per SM given
 // to the register allocator per kernel group; 0 leaves it to the compiler.
 // The values below are the defaults without a tuned header (hand sweep on
-// B200: 4 blocks for the EOS kernels, whose spills stay in L1, 3 for the final
-// Riemann kernel).  Override with -DCASTRO_BLOCK / -DCASTRO_MINB_*.
+// B200: 4 blocks for the EOS kernels, whose spills stay in L1, and for trace,
+// segments of 5 zones per trace thread).  Override with -DCASTRO_BLOCK /
+// -DCASTRO_MINB_* / -DCASTRO_TRACE_SEG.
 #if __has_include("castro_tuned.h")
 #include "castro_tuned.h"
 #endif
@@ -65,15 +66,19 @@ constexpr int NG = 4;   // ghost zones of Sborder, Source/Castro_advance.cpp:37
 #define CASTRO_MINB_EOS 4
 #endif
 #ifndef CASTRO_MINB_R3
-#define CASTRO_MINB_R3 3
+#define CASTRO_MINB_R3 0
 #endif
 #ifndef CASTRO_MINB_TRACE
-#define CASTRO_MINB_TRACE 0
+#define CASTRO_MINB_TRACE 4
 #endif
 #ifndef CASTRO_MINB_RIEMANN
 #define CASTRO_MINB_RIEMANN 0
 #endif
+#ifndef CASTRO_TRACE_SEG
+#define CASTRO_TRACE_SEG 5
+#endif
 constexpr int BLOCK = CASTRO_BLOCK;
+constexpr int TSEG = CASTRO_TRACE_SEG;   // zones of grow(bx,1) one trace thread walks along its direction
 #define CASTRO_LB(M) __launch_bounds__(BLOCK, ((M) > 0 ? (M) : 1))
 #if CASTRO_MINB_EOS > 0
 #define LB_EOS CASTRO_LB(CASTRO_MINB_EOS)
@@ -124,7 +129,7 @@ struct InstState {
 
 struct Work { int box, sub, start, count; };
 
-enum Region { R_VALID = 0, R_G1, R_G4, R_TBX, R_EBX, R_GHOST };
+enum Region { R_VALID = 0, R_G1, R_G4, R_TBX, R_EBX, R_GHOST, R_SEG };
 
 struct Reg {
     int lx, ly, lz, nx, ny, nz;
@@ -144,6 +149,14 @@ __host__ __device__ __forceinline__ Reg make_reg(const int* lo, const int* hi, i
         for (int d = 0; d < a; ++d) { l[d] -= NG; h[d] += NG; }
         if (sub % 2 == 0) { h[a] = l[a] - 1; l[a] -= NG; }
         else { l[a] = h[a] + 1; h[a] += NG; }
+    }
+    else if (kind == R_SEG) {
+        // grow(bx,1) with the coordinate along direction sub replaced by the
+        // index of a segment of TSEG zones
+        for (int d = 0; d < 3; ++d) { l[d] -= 1; h[d] += 1; }
+        const int n = h[sub] - l[sub] + 1;
+        l[sub] = 0;
+        h[sub] = (n + TSEG - 1) / TSEG - 1;
     }
     else if (kind == R_TBX) {
         // sub = 3*a + b: faces normal to a; grown by 1 in the directions other
@@ -375,45 +388,168 @@ __global__ void __launch_bounds__(BLOCK) k_prep(SimDev S, const Work* wl)
     S.Div[B.offDiv + id + R.np] = uflatten(ld, i, j, k);
 }
 
+// trace_ppm (Source/ppm.F90:437-737) along one segment of up to TSEG zones of
+// grow(bx,1) in direction D, the other two coordinates fixed.  Each zone's
+// result equals trace_zone's bit for bit: the minus edge of zone z+1 and the
+// plus edge of zone z are ppm_edge on the same operands, and the van Leer slope
+// of zone z enters the edges of z-1, z and z+1 unchanged, so the thread forms
+// every slope and edge once and carries them along the segment in registers
+// (trace_zone forms three slopes and two edges per zone and variable).  Pass 1
+// walks rho, u_D, p, rhoe and gamma_c, which feed the characteristic
+// projection; pass 2 walks the transverse velocities and the species, one at a
+// time, each needing only the u_D wave.
 template <int NS, int D>
-__device__ __forceinline__ void trace_dir(const SimDev& S, const BoxDev& B, const QLoader<NS>& ld, const Reg& R1,
-                                          int i, int j, int k, double dtdx)
+__device__ __forceinline__ void trace_segment(const SimDev& S, const BoxDev& B, int i, int j, int k, double dtdx)
 {
+    using F = QF<NS>;
     constexpr int NQS = Dims<NS>::NQS;
-    double flatn = S.Div[B.offDiv + ridx(R1, i, j, k) + R1.np];
-    double qplus[NQS], qminus[NQS];
-    trace_zone<NS, D>(ld, i, j, k, dtdx, flatn, qplus, qminus);
-    Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * D);
-    double* T = S.Tr + B.offTr[D];
-    int idx = D == 0 ? i : D == 1 ? j : k;
-    if (idx >= B.lo[D]) {
-        long long f = ridx(RT, i, j, k);
+    constexpr int T1 = D == 0 ? 1 : D == 1 ? 2 : 0;   // qut - QU of trace_zone
+    constexpr int T2 = D == 0 ? 2 : D == 1 ? 0 : 1;   // qutt - QU
+    const Reg R4 = make_reg(B.lo, B.hi, R_G4, 0);
+    const Reg R1 = make_reg(B.lo, B.hi, R_G1, 0);
+    const Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * D);
+    int p[3] = {i, j, k};
+    const int z0 = B.lo[D] - 1 + p[D] * TSEG;          // first zone of the segment
+    const int n = min(TSEG, B.hi[D] + 2 - z0);           // zones in the segment
+    p[D] = z0;
+    const int zlo = B.lo[D] - z0, zhi = B.hi[D] - z0;    // zone offsets with a plus / minus face in tbx[D][D]
+    const double* Q = S.Q + B.offQ;
+    const double* Fl = S.Div + B.offDiv + R1.np;        // flatn
+    double* Tr = S.Tr + B.offTr[D];
+    // linear indices of zone z0 (Q, flatn) and of its low face (face states);
+    // the face of zone lo-1 lies one stride below tbx[D][D] and is never stored
+    const long long q0 = ridx(R4, p[0], p[1], p[2]);
+    const long long f0 = ridx(R1, p[0], p[1], p[2]);
+    const long long t0 = ridx(RT, p[0], p[1], p[2]);
+    const long long sq = D == 0 ? 1 : D == 1 ? (long long)R4.nx : (long long)R4.nx * R4.ny;
+    const long long sf = D == 0 ? 1 : D == 1 ? (long long)R1.nx : (long long)R1.nx * R1.ny;
+    const long long st = D == 0 ? 1 : D == 1 ? (long long)RT.nx : (long long)RT.nx * RT.ny;
+    const long long nq = R4.np, nt = RT.np;
+
+    // pass 1: rho, u_D, p, rhoe, gamma_c.  Window of variable v at zone z:
+    // wa = s(z), wb = s(z+1), wd = slope(z), we = edge(z) (minus edge of z).
+    // The loads of zone z+1 (s(z+3), flatn, c) are issued while zone z is
+    // computed: s(z+3) lies at most at hi+4 and c at hi+2, inside grow(bx,4);
+    // flatn exists up to hi+1 and is fetched only for a zone of the segment.
+    constexpr int NW = 5;
+    constexpr int cw[NW] = {F::RHO, F::U + D, F::P, F::RE, F::GAMC};
+    double wa[NW], wb[NW], wd[NW], we[NW], nxt[NW];
 #pragma unroll
-        for (int c = 0; c < NQS; ++c) T[f + RT.np * (NQS + c)] = qplus[c];
+    for (int v = 0; v < NW; ++v) {
+        const double* c = Q + q0 + (long long)cw[v] * nq;
+        double sm2 = c[-2 * sq], sm1 = c[-sq], s0 = c[0], sp1 = c[sq];
+        nxt[v] = c[2 * sq];
+        double dm = vl_slope(sm2, sm1, s0);
+        wd[v] = vl_slope(sm1, s0, sp1);
+        we[v] = ppm_edge(sm1, s0, dm, wd[v]);
+        wa[v] = s0;
+        wb[v] = sp1;
     }
-    if (idx <= B.hi[D]) {
-        long long f = ridx(RT, i + (D == 0), j + (D == 1), k + (D == 2));
+    double flatn_n = Fl[f0], cc_n = Q[q0 + (long long)F::C * nq];
+#pragma unroll 1
+    for (int z = 0; z < n; ++z) {
+        const double flatn = flatn_n;
+        const double cc = cc_n;
+        const double un = wa[1];
+        double cur[NW];
 #pragma unroll
-        for (int c = 0; c < NQS; ++c) T[f + RT.np * c] = qminus[c];
+        for (int v = 0; v < NW; ++v) {
+            cur[v] = nxt[v];
+            nxt[v] = Q[q0 + (z + 3) * sq + (long long)cw[v] * nq];
+        }
+        cc_n = Q[q0 + (z + 1) * sq + (long long)F::C * nq];
+        if (z + 1 < n) flatn_n = Fl[f0 + (z + 1) * sf];
+        double Ip[3][4], Im[3][4], gp0, gm0, gp2, gm2;
+#pragma unroll
+        for (int v = 0; v < NW; ++v) {
+            const double s2 = cur[v];
+            const double dn = vl_slope(wa[v], wb[v], s2);
+            const double en = ppm_edge(wa[v], wb[v], wd[v], dn);
+            double sm = we[v], sp = en;
+            ppm_limit(wa[v], flatn, sm, sp);
+            const double s6 = 6.0 * wa[v] - 3.0 * (sm + sp);
+            if (v < 4) {
+                ppm_int_wave(sm, sp, s6, un - cc, dtdx, Ip[0][v], Im[0][v]);
+                ppm_int_wave(sm, sp, s6, un, dtdx, Ip[1][v], Im[1][v]);
+                ppm_int_wave(sm, sp, s6, un + cc, dtdx, Ip[2][v], Im[2][v]);
+            } else {
+                ppm_int_wave(sm, sp, s6, un - cc, dtdx, gp0, gm0);
+                ppm_int_wave(sm, sp, s6, un + cc, dtdx, gp2, gm2);
+            }
+            wa[v] = wb[v];
+            wb[v] = s2;
+            wd[v] = dn;
+            we[v] = en;
+        }
+        if (z >= zlo) {
+            double r, u, re, pr;
+            trace_project(Im, gm0, un, cc, true, r, u, re, pr);
+            double* t = Tr + (t0 + z * st);
+            t[nt * (NQS + SRHO)] = r;
+            t[nt * (NQS + SU + D)] = u;
+            t[nt * (NQS + SREI)] = re;
+            t[nt * (NQS + SPRES)] = pr;
+        }
+        if (z <= zhi) {
+            double r, u, re, pr;
+            trace_project(Ip, gp2, un, cc, false, r, u, re, pr);
+            double* t = Tr + (t0 + (z + 1) * st);
+            t[nt * SRHO] = r;
+            t[nt * (SU + D)] = u;
+            t[nt * SREI] = re;
+            t[nt * SPRES] = pr;
+        }
+    }
+
+    // pass 2: transverse velocities and species, the u_D wave only
+#pragma unroll 1
+    for (int v = 0; v < 2 + NS; ++v) {
+        const int comp = v == 0 ? F::U + T1 : v == 1 ? F::U + T2 : F::X + (v - 2);
+        const int slot = v == 0 ? SU + T1 : v == 1 ? SU + T2 : SX + (v - 2);
+        const double* c = Q + q0 + (long long)comp * nq;
+        const double* cu = Q + q0 + (long long)(F::U + D) * nq;
+        double sm2 = c[-2 * sq], sm1 = c[-sq], a = c[0], bq = c[sq];
+        double nxt2 = c[2 * sq], un_n = cu[0], flatn_n2 = Fl[f0];
+        double d = vl_slope(sm1, a, bq);
+        double e = ppm_edge(sm1, a, vl_slope(sm2, sm1, a), d);
+#pragma unroll 1
+        for (int z = 0; z < n; ++z) {
+            const double flatn = flatn_n2;
+            const double un = un_n;
+            const double s2 = nxt2;
+            nxt2 = c[(z + 3) * sq];
+            un_n = cu[(z + 1) * sq];
+            if (z + 1 < n) flatn_n2 = Fl[f0 + (z + 1) * sf];
+            const double dn = vl_slope(a, bq, s2);
+            const double en = ppm_edge(a, bq, d, dn);
+            double sm = e, sp = en;
+            ppm_limit(a, flatn, sm, sp);
+            const double s6 = 6.0 * a - 3.0 * (sm + sp);
+            double ip, im;
+            ppm_int_wave(sm, sp, s6, un, dtdx, ip, im);
+            if (z >= zlo) Tr[t0 + z * st + nt * (NQS + slot)] = im;
+            if (z <= zhi) Tr[t0 + (z + 1) * st + nt * slot] = ip;
+            a = bq;
+            bq = s2;
+            d = dn;
+            e = en;
+        }
     }
 }
 
-// trace: trace_ppm of one zone of grow(bx,1) in one direction (work sub = direction)
+// trace: one segment of grow(bx,1) in one direction per thread (work sub = direction)
 template <int NS>
 __global__ void LB_TRACE k_trace(SimDev S, const Work* wl)
 {
     int b, d, i, j, k;
     Reg R;
-    if (!work_point(wl, S, R_G1, -1, b, d, R, i, j, k)) return;
+    if (!work_point(wl, S, R_SEG, -1, b, d, R, i, j, k)) return;
     const BoxDev& B = S.boxes[b];
     const InstDev& I = S.inst[B.inst];
     const double dt = S.st[B.inst].dt;
-    QLoader<NS> ld;
-    ld.base = S.Q + B.offQ;
-    ld.R = make_reg(B.lo, B.hi, R_G4, 0);
-    if (d == 0) trace_dir<NS, 0>(S, B, ld, R, i, j, k, dt / I.dx[0]);
-    else if (d == 1) trace_dir<NS, 1>(S, B, ld, R, i, j, k, dt / I.dx[1]);
-    else trace_dir<NS, 2>(S, B, ld, R, i, j, k, dt / I.dx[2]);
+    if (d == 0) trace_segment<NS, 0>(S, B, i, j, k, dt / I.dx[0]);
+    else if (d == 1) trace_segment<NS, 1>(S, B, i, j, k, dt / I.dx[1]);
+    else trace_segment<NS, 2>(S, B, i, j, k, dt / I.dx[2]);
 }
 
 // compute_flux on the face (i,j,k) normal to D: left zone i-e_D, right zone i
@@ -517,6 +653,120 @@ __device__ __forceinline__ void cross_flux(const SimDev& S, const BoxDev& B, con
     rec[T_::UG] = g.y;
 }
 
+// 8-byte asynchronous global -> shared copies (cp.async, Ampere and later):
+// the copies of one thread are in flight together without holding registers,
+// and the thread waits for all of them once
+__device__ __forceinline__ void cp_async8(double* dst, const double* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Per-thread shared-memory slot of riemann2: the face's two A-normal trace
+// states, the Bd normal-flux records on the faces of both side zones, and the
+// two zones' gamma_1.  The stride is odd, so that the 64-bit accesses of a
+// half-warp fall in distinct bank pairs.
+// CASTRO_R2_STAGE: 0 plain loads, 1 the face states and gamma_1 staged, 2 the
+// flux records too (measured on B200: 1 is fastest; the flux records are each
+// read by about four neighbouring threads and are best served from L1).
+// CASTRO_R2_CARVEOUT: preferred shared-memory carveout in percent, -1 leaves
+// it to the driver (fastest: a larger carveout shrinks L1).
+#ifndef CASTRO_R2_STAGE
+#define CASTRO_R2_STAGE 1
+#endif
+#ifndef CASTRO_R2_CARVEOUT
+#define CASTRO_R2_CARVEOUT -1
+#endif
+template <int NS>
+struct R2Slot {
+    static constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF;
+    static constexpr bool F1 = CASTRO_R2_STAGE >= 2;   // flux records staged too
+    static constexpr int LQ = 0;                   // 2 x NQS: minus (left) state, plus (right) state
+    static constexpr int G = 2 * NQS;              // gamma_1 of the left and right zones
+    static constexpr int FR = G + 2;               // 4 x NTF: fr, fl of the left zone, fr, fl of the right zone
+    static constexpr int USED = FR + (F1 ? 4 * NTF : 0);
+    static constexpr int STRIDE = USED | 1;
+    // staging pays while four blocks of BLOCK threads still fit on an SM
+    static constexpr bool ON = CASTRO_R2_STAGE > 0 && STRIDE * BLOCK * 8 * 4 + 4 * 1024 <= 228 * 1024;
+    static constexpr int BYTES = ON ? STRIDE * BLOCK * 8 : 0;
+};
+
+// cross_flux with its operands staged in the thread's shared-memory slot sm;
+// the arithmetic is cross_flux's
+template <int NS, int A, int Bd>
+__device__ __forceinline__ void cross_flux_staged(const SimDev& S, const BoxDev& B, const QLoader<NS>& ld, int i,
+                                                  int j, int k, double cdtdx, double* rec, double* sm)
+{
+    using SL = R2Slot<NS>;
+    constexpr int NQS = SL::NQS, NTF = SL::NTF, NVAR = Dims<NS>::NVAR;
+    constexpr int eax = A == 0, eay = A == 1, eaz = A == 2;
+    constexpr int ebx_ = Bd == 0, eby = Bd == 1, ebz = Bd == 2;
+    const Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * A);
+    const Reg RF = make_reg(B.lo, B.hi, R_TBX, 4 * Bd);
+    const double* T = S.Tr + B.offTr[A];
+    const double* F = S.F1 + B.offF1[Bd];
+    const long long ft = ridx(RT, i, j, k);
+#pragma unroll
+    for (int c = 0; c < 2 * NQS; ++c) cp_async8(sm + SL::LQ + c, T + ft + RT.np * c);
+    double frec[SL::F1 ? 1 : 4 * NTF];
+#pragma unroll
+    for (int D = -1; D <= 0; ++D) {
+        const int il = i + D * eax, jl = j + D * eay, kl = k + D * eaz;
+        const long long fr = ridx(RF, il + ebx_, jl + eby, kl + ebz), fl = ridx(RF, il, jl, kl);
+        if constexpr (SL::F1) {
+            double* o = sm + SL::FR + (D + 1) * 2 * NTF;
+#pragma unroll
+            for (int c = 0; c < NTF; ++c) {
+                cp_async8(o + c, F + fr + RF.np * c);
+                cp_async8(o + NTF + c, F + fl + RF.np * c);
+            }
+        } else {
+            load_tf<NS>(F, RF, fr, frec + (D + 1) * 2 * NTF);
+            load_tf<NS>(F, RF, fl, frec + (D + 1) * 2 * NTF + NTF);
+        }
+    }
+    const long long zl = ridx(ld.R, i - eax, j - eay, k - eaz), zr = ridx(ld.R, i, j, k);
+    cp_async8(sm + SL::G, ld.base + zl + ld.R.np * QF<NS>::GAMC);
+    cp_async8(sm + SL::G + 1, ld.base + zr + ld.R.np * QF<NS>::GAMC);
+    const double cl = ld.base[zl + ld.R.np * QF<NS>::C], cr = ld.base[zr + ld.R.np * QF<NS>::C];
+    cp_async_wait_all();
+    const double* fb = SL::F1 ? sm + SL::FR : frec;
+    double st2[2][NQS];
+#pragma unroll
+    for (int D = 0; D < 2; ++D)
+        trans1_state<NS>(sm + SL::LQ + D * NQS, fb + D * 2 * NTF, fb + D * 2 * NTF + NTF, sm[SL::G + D], cdtdx,
+                         st2[D]);
+    double flx[NVAR], qg[NGDNV];
+    riemann_cgf<NS, A>(st2[0], st2[1], sm[SL::G], sm[SL::G + 1], cl, cr, flx, qg, nullptr);
+    using T_ = TF<NS>;
+    rec[T_::RHO] = flx[URHO];
+    rec[T_::MX] = flx[UMX];
+    rec[T_::MY] = flx[UMY];
+    rec[T_::MZ] = flx[UMZ];
+    rec[T_::ED] = flx[UEDEN];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) rec[T_::X + n] = flx[UFS + n];
+    rec[T_::PG] = qg[GDPRES];
+    rec[T_::UG] = qg[GDU + A];
+}
+
+template <int NS, int A, int Bd>
+__device__ __forceinline__ void cross_flux_any(const SimDev& S, const BoxDev& B, const QLoader<NS>& ld, int i, int j,
+                                               int k, double cdtdx, double* rec)
+{
+    if constexpr (R2Slot<NS>::ON) {
+        extern __shared__ double r2_smem[];
+        cross_flux_staged<NS, A, Bd>(S, B, ld, i, j, k, cdtdx, rec, r2_smem + threadIdx.x * R2Slot<NS>::STRIDE);
+    } else {
+        cross_flux<NS, A, Bd>(S, B, ld, i, j, k, cdtdx, rec);
+    }
+}
+
 // riemann2: F^{a|b} on tbx[a][b] for the six ordered pairs
 template <int NS>
 __global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
@@ -533,12 +783,12 @@ __global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
     ld.R = make_reg(B.lo, B.hi, R_G4, 0);
     double rec[NTF];
     switch (p) {   // pair_index order: (0,1) (0,2) (1,0) (1,2) (2,0) (2,1)
-    case 0: cross_flux<NS, 0, 1>(S, B, ld, i, j, k, dt / I.dx[1] / 3.0, rec); break;
-    case 1: cross_flux<NS, 0, 2>(S, B, ld, i, j, k, dt / I.dx[2] / 3.0, rec); break;
-    case 2: cross_flux<NS, 1, 0>(S, B, ld, i, j, k, dt / I.dx[0] / 3.0, rec); break;
-    case 3: cross_flux<NS, 1, 2>(S, B, ld, i, j, k, dt / I.dx[2] / 3.0, rec); break;
-    case 4: cross_flux<NS, 2, 0>(S, B, ld, i, j, k, dt / I.dx[0] / 3.0, rec); break;
-    default: cross_flux<NS, 2, 1>(S, B, ld, i, j, k, dt / I.dx[1] / 3.0, rec); break;
+    case 0: cross_flux_any<NS, 0, 1>(S, B, ld, i, j, k, dt / I.dx[1] / 3.0, rec); break;
+    case 1: cross_flux_any<NS, 0, 2>(S, B, ld, i, j, k, dt / I.dx[2] / 3.0, rec); break;
+    case 2: cross_flux_any<NS, 1, 0>(S, B, ld, i, j, k, dt / I.dx[0] / 3.0, rec); break;
+    case 3: cross_flux_any<NS, 1, 2>(S, B, ld, i, j, k, dt / I.dx[2] / 3.0, rec); break;
+    case 4: cross_flux_any<NS, 2, 0>(S, B, ld, i, j, k, dt / I.dx[0] / 3.0, rec); break;
+    default: cross_flux_any<NS, 2, 1>(S, B, ld, i, j, k, dt / I.dx[1] / 3.0, rec); break;
     }
     double* out = S.F2 + B.offF2[p];
     long long f = ridx(R, i, j, k);
@@ -546,15 +796,44 @@ __global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
     for (int c = 0; c < NTF; ++c) out[f + R.np * c] = rec[c];
 }
 
+// CASTRO_R3_STAGE: 0 plain loads, 1 the per-face operands of riemann3 that no
+// neighbouring thread reads (both trace states, gamma_1, the two zones'
+// Sborder values and the four divu nodes of apply_av) staged in shared memory
+// by cp.async; the cross-flux records stay plain loads served from L1
+// (measured on B200: 0 is faster, 0.85 against 0.90 ms for the 128^3 step).
+#ifndef CASTRO_R3_STAGE
+#define CASTRO_R3_STAGE 0
+#endif
+template <int NS>
+struct R3Slot {
+    static constexpr int NQS = Dims<NS>::NQS, NVAR = Dims<NS>::NVAR;
+    static constexpr int LQ = 0;              // 2 x NQS: minus (left) state, plus (right) state
+    static constexpr int G = 2 * NQS;         // gamma_1 of the left and right zones
+    static constexpr int UB = G + 2;          // Sborder of the right zone, then of the left zone (NVAR each)
+    static constexpr int DV = UB + 2 * NVAR;  // the four divu nodes of apply_av
+    static constexpr int USED = DV + 4;
+    static constexpr int STRIDE = USED | 1;   // odd: conflict-free 64-bit accesses
+    static constexpr bool ON = CASTRO_R3_STAGE > 0 && STRIDE * BLOCK * 8 * 4 + 4 * 1024 <= 228 * 1024;
+    static constexpr int BYTES = ON ? STRIDE * BLOCK * 8 : 0;
+};
+
+// divu nodes summed by apply_av on a D-normal face, offsets from (i,j,k) in the
+// order of Castro_hydro_nd.F90:207-237 (the x and y sums repeat a node there)
+__device__ constexpr int AV_NODE[3][4][3] = {{{0, 0, 0}, {0, 1, 0}, {0, 0, 1}, {0, 1, 0}},
+                                             {{0, 0, 0}, {1, 0, 0}, {0, 0, 1}, {1, 0, 0}},
+                                             {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0}}};
+
 // The final flux on the D-normal face (i,j,k) of ebx[D]: trans2 of the face's
 // two D-normal trace states with the cross fluxes F^{t1|t2} (f12) and
 // F^{t2|t1} (f21), compute_flux, apply_av, normalize_species_fluxes
 // (Castro_hydro.cpp:307-359), written to the final-flux record of ebx[D].
-// f12(i,j,k,rec) / f21(i,j,k,rec) load the cross-flux record at a face.
-template <int NS, int D, class L12, class L21>
+// f12(i,j,k,rec) / f21(i,j,k,rec) load the cross-flux record at a face.  With
+// STG the face's own operands come from the thread's shared-memory slot sm.
+template <int NS, int D, bool STG, class L12, class L21>
 __device__ __forceinline__ void final_flux(const SimDev& S, const BoxDev& B, const InstDev& I, const QLoader<NS>& ld,
-                                           int i, int j, int k, double dt, const L12& f12, const L21& f21)
+                                           int i, int j, int k, double dt, const L12& f12, const L21& f21, double* sm)
 {
+    using SL = R3Slot<NS>;
     constexpr int T1 = (D == 0) ? 1 : 0;
     constexpr int T2 = (D == 2) ? 1 : 2;
     constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF, NVAR = Dims<NS>::NVAR;
@@ -562,42 +841,73 @@ __device__ __forceinline__ void final_flux(const SimDev& S, const BoxDev& B, con
     constexpr int e1x = T1 == 0, e1y = T1 == 1, e1z = T1 == 2;
     constexpr int e2x = T2 == 0, e2y = T2 == 1, e2z = T2 == 2;
     const double hdt1 = 0.5 * dt / I.dx[T1], hdt2 = 0.5 * dt / I.dx[T2];
-    Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * D);
+    const Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * D);
+    const Reg R1 = make_reg(B.lo, B.hi, R_G1, 0);
     const double* T = S.Tr + B.offTr[D];
-    long long ft = ridx(RT, i, j, k);
+    const double* Dv = S.Div + B.offDiv;
+    const double* Ub = S.Ub + B.offUb;
+    const long long ft = ridx(RT, i, j, k);
+    const long long c0 = ridx(R1, i, j, k), cm = ridx(R1, i - ex, j - ey, k - ez);
+    const long long zl = ridx(ld.R, i - ex, j - ey, k - ez), zr = ridx(ld.R, i, j, k);
+    if constexpr (STG) {
+#pragma unroll
+        for (int c = 0; c < 2 * NQS; ++c) cp_async8(sm + SL::LQ + c, T + ft + RT.np * c);
+        cp_async8(sm + SL::G, ld.base + zl + ld.R.np * QF<NS>::GAMC);
+        cp_async8(sm + SL::G + 1, ld.base + zr + ld.R.np * QF<NS>::GAMC);
+#pragma unroll
+        for (int n = 0; n < NVAR; ++n) {
+            if (n == UTEMP) continue;
+            cp_async8(sm + SL::UB + n, Ub + c0 + R1.np * n);
+            cp_async8(sm + SL::UB + NVAR + n, Ub + cm + R1.np * n);
+        }
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+            cp_async8(sm + SL::DV + m, Dv + ridx(R1, i + AV_NODE[D][m][0], j + AV_NODE[D][m][1], k + AV_NODE[D][m][2]));
+    }
+    const double cl = ld.base[zl + ld.R.np * QF<NS>::C], cr = ld.base[zr + ld.R.np * QF<NS>::C];
     double st2[2][NQS];
 #pragma unroll
     for (int Dm = -1; Dm <= 0; ++Dm) {
-        double lq[NQS], f2r[NTF], f2l[NTF], f3r[NTF], f3l[NTF];
+        double lqr[STG ? 1 : NQS], f2r[NTF], f2l[NTF], f3r[NTF], f3l[NTF];
         const int off = (Dm == -1) ? 0 : NQS;
+        if constexpr (!STG) {
 #pragma unroll
-        for (int c = 0; c < NQS; ++c) lq[c] = T[ft + RT.np * (off + c)];
+            for (int c = 0; c < NQS; ++c) lqr[c] = T[ft + RT.np * (off + c)];
+        }
         int il = i + Dm * ex, jl = j + Dm * ey, kl = k + Dm * ez;
         f12(il + e1x, jl + e1y, kl + e1z, f2r);
         f12(il, jl, kl, f2l);
         f21(il + e2x, jl + e2y, kl + e2z, f3r);
         f21(il, jl, kl, f3l);
-        trans2_state<NS>(lq, f2r, f2l, f3r, f3l, ld.gamc(il, jl, kl), hdt1, hdt2, st2[Dm + 1]);
+        if constexpr (STG) {
+            if (Dm == -1) cp_async_wait_all();
+        }
+        const double* lq = STG ? sm + SL::LQ + off : lqr;
+        const double gam = STG ? sm[SL::G + Dm + 1] : ld.gamc(il, jl, kl);
+        trans2_state<NS>(lq, f2r, f2l, f3r, f3l, gam, hdt1, hdt2, st2[Dm + 1]);
     }
-    double flx[NVAR];
-    double2 g = riemann_at<NS, D>(ld, i, j, k, st2[0], st2[1], flx);
-
-    // apply_av, Castro_hydro_nd.F90:207-237 (the x and y four-node sums as written there)
+    double flx[NVAR], qg[NGDNV];
     {
-        Reg R1 = make_reg(B.lo, B.hi, R_G1, 0);
-        const double* Dv = S.Div + B.offDiv;
-        auto dv = [&](int a, int bq, int c) { return Dv[ridx(R1, a, bq, c)]; };
-        double ds;
-        if (D == 0) ds = dv(i, j, k) + dv(i, j + 1, k) + dv(i, j, k + 1) + dv(i, j + 1, k);
-        else if (D == 1) ds = dv(i, j, k) + dv(i + 1, j, k) + dv(i, j, k + 1) + dv(i + 1, j, k);
-        else ds = dv(i, j, k) + dv(i + 1, j, k) + dv(i, j + 1, k) + dv(i + 1, j + 1, k);
-        const double* Ub = S.Ub + B.offUb;
-        long long c0 = ridx(R1, i, j, k), cm = ridx(R1, i - ex, j - ey, k - ez);
+        const double gl = STG ? sm[SL::G] : ld.gamc(i - ex, j - ey, k - ez);
+        const double gr = STG ? sm[SL::G + 1] : ld.gamc(i, j, k);
+        riemann_cgf<NS, D>(st2[0], st2[1], gl, gr, cl, cr, flx, qg, nullptr);
+    }
+    const double2 g = make_double2(qg[GDPRES], qg[GDU + D]);
+
+    // apply_av, Castro_hydro_nd.F90:207-237
+    {
+        double dvn[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+            dvn[m] = STG ? sm[SL::DV + m] : Dv[ridx(R1, i + AV_NODE[D][m][0], j + AV_NODE[D][m][1], k + AV_NODE[D][m][2])];
+        const double ds = dvn[0] + dvn[1] + dvn[2] + dvn[3];
         const double dxd = I.dx[D];
 #pragma unroll
         for (int n = 0; n < NVAR; ++n) {
             if (n == UTEMP) continue;
-            double div1 = av_term(ds, Ub[c0 + R1.np * n] - Ub[cm + R1.np * n]);
+            const double u0 = STG ? sm[SL::UB + n] : Ub[c0 + R1.np * n];
+            const double um = STG ? sm[SL::UB + NVAR + n] : Ub[cm + R1.np * n];
+            double div1 = av_term(ds, u0 - um);
             flx[n] = flx[n] + dxd * div1;
         }
     }
@@ -638,7 +948,12 @@ __device__ __forceinline__ void riemann3_dir(const SimDev& S, const BoxDev& B, c
     constexpr int T2 = (D == 2) ? 1 : 2;
     GlobalTF<NS> f12{S.F2 + B.offF2[pair_index(T1, T2)], make_reg(B.lo, B.hi, R_TBX, 3 * T1 + T2)};
     GlobalTF<NS> f21{S.F2 + B.offF2[pair_index(T2, T1)], make_reg(B.lo, B.hi, R_TBX, 3 * T2 + T1)};
-    final_flux<NS, D>(S, B, I, ld, i, j, k, dt, f12, f21);
+    if constexpr (R3Slot<NS>::ON) {
+        extern __shared__ double r3_smem[];
+        final_flux<NS, D, true>(S, B, I, ld, i, j, k, dt, f12, f21, r3_smem + threadIdx.x * R3Slot<NS>::STRIDE);
+    } else {
+        final_flux<NS, D, false>(S, B, I, ld, i, j, k, dt, f12, f21, nullptr);
+    }
 }
 
 // riemann3: the final fluxes on ebx[d] from the F2 pool
@@ -937,9 +1252,9 @@ struct castro_sim {
     double *Tr = nullptr, *F1 = nullptr, *F2 = nullptr, *Fx = nullptr;
     long long nU = 0;
     // work lists
-    Work *w_valid = nullptr, *w_g4 = nullptr, *w_g1 = nullptr, *w_g1x3 = nullptr, *w_tbx = nullptr, *w_pair = nullptr,
+    Work *w_valid = nullptr, *w_g4 = nullptr, *w_g1 = nullptr, *w_trace = nullptr, *w_tbx = nullptr, *w_pair = nullptr,
          *w_ebx = nullptr, *w_ghost = nullptr;
-    int n_valid = 0, n_g4 = 0, n_g1 = 0, n_g1x3 = 0, n_tbx = 0, n_pair = 0, n_ebx = 0, n_ghost = 0;
+    int n_valid = 0, n_g4 = 0, n_g1 = 0, n_trace = 0, n_tbx = 0, n_pair = 0, n_ebx = 0, n_ghost = 0;
     bool dt_ready = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -1018,6 +1333,24 @@ void build_work(castro_sim* s, int kind, int nsub, int tbx_mode, Work** out, int
         cuda_ok(cudaMemcpy(*out, w.data(), w.size() * sizeof(Work), cudaMemcpyHostToDevice), "work list copy");
 }
 
+// Shared-memory sizing of the kernels that stage operands (set outside any
+// graph capture, before the first launch on the current device)
+template <int NS>
+bool set_kernel_attributes()
+{
+    if (R3Slot<NS>::BYTES > 48 * 1024 &&
+        !cuda_ok(cudaFuncSetAttribute(k_riemann3<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, R3Slot<NS>::BYTES),
+                 "riemann3 shared memory"))
+        return false;
+    if (!R2Slot<NS>::ON) return true;
+    return cuda_ok(cudaFuncSetAttribute(k_riemann2<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, R2Slot<NS>::BYTES),
+                   "riemann2 shared memory") &&
+           (CASTRO_R2_CARVEOUT < 0 ||
+            cuda_ok(cudaFuncSetAttribute(k_riemann2<NS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         CASTRO_R2_CARVEOUT),
+                    "riemann2 carveout"));
+}
+
 template <int NS>
 void batched_step_kernels(castro_sim* s)
 {
@@ -1026,10 +1359,10 @@ void batched_step_kernels(castro_sim* s)
     k_front<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid);
     k_ghost<NS><<<s->n_ghost, BLOCK, 0, st>>>(S, s->w_ghost);
     k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(S, s->w_g1);
-    k_trace<NS><<<s->n_g1x3, BLOCK, 0, st>>>(S, s->w_g1x3);
+    k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(S, s->w_trace);
     k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(S, s->w_tbx);
-    k_riemann2<NS><<<s->n_pair, BLOCK, 0, st>>>(S, s->w_pair);
-    k_riemann3<NS><<<s->n_ebx, BLOCK, 0, st>>>(S, s->w_ebx);
+    k_riemann2<NS><<<s->n_pair, BLOCK, R2Slot<NS>::BYTES, st>>>(S, s->w_pair);
+    k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, st>>>(S, s->w_ebx);
     k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid);
     k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0);
 }
@@ -1042,10 +1375,10 @@ void profile_kernel(castro_sim* s, const SimDev& S, int k)
     case 0: k_front<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid); break;
     case 1: k_ghost<NS><<<s->n_ghost, BLOCK, 0, st>>>(S, s->w_ghost); break;
     case 2: k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(S, s->w_g1); break;
-    case 3: k_trace<NS><<<s->n_g1x3, BLOCK, 0, st>>>(S, s->w_g1x3); break;
+    case 3: k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(S, s->w_trace); break;
     case 4: k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(S, s->w_tbx); break;
-    case 5: k_riemann2<NS><<<s->n_pair, BLOCK, 0, st>>>(S, s->w_pair); break;
-    case 6: k_riemann3<NS><<<s->n_ebx, BLOCK, 0, st>>>(S, s->w_ebx); break;
+    case 5: k_riemann2<NS><<<s->n_pair, BLOCK, R2Slot<NS>::BYTES, st>>>(S, s->w_pair); break;
+    case 6: k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, st>>>(S, s->w_ebx); break;
     case 7: k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid); break;
     default: k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0); break;
     }
@@ -1314,6 +1647,7 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
     if (ninst < 1 || !desc) { set_error(CASTRO_ERR_ARG, "castro_sim_create: no instances"); return nullptr; }
     int ns = nspec();
     if (ns != 2 && ns != 13) { set_error(CASTRO_ERR_NSPEC, "castro_sim_create: nspec"); return nullptr; }
+    if (!(ns == 2 ? set_kernel_attributes<2>() : set_kernel_attributes<13>())) return nullptr;
     castro_sim* s = new castro_sim();
     s->mode = mode;
     s->ns = ns;
@@ -1407,7 +1741,7 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
         build_work(s, R_VALID, 1, -1, &s->w_valid, &s->n_valid);
         build_work(s, R_G4, 1, -1, &s->w_g4, &s->n_g4);
         build_work(s, R_G1, 1, -1, &s->w_g1, &s->n_g1);
-        build_work(s, R_G1, 3, -1, &s->w_g1x3, &s->n_g1x3);
+        build_work(s, R_SEG, 3, -1, &s->w_trace, &s->n_trace);
         build_work(s, R_TBX, 3, 0, &s->w_tbx, &s->n_tbx);
         build_work(s, R_TBX, 6, 1, &s->w_pair, &s->n_pair);
         build_work(s, R_EBX, 3, -1, &s->w_ebx, &s->n_ebx);
@@ -1440,7 +1774,7 @@ void castro_sim_destroy(castro_sim* s)
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     if (s->graph) cudaGraphDestroy(s->graph);
     void* ptrs[] = {s->dboxes, s->dinst, s->dstate, s->downer, s->U, s->Ub, s->Q, s->Div, s->Tr, s->F1, s->F2, s->Fx,
-                    s->w_valid, s->w_g4, s->w_g1, s->w_g1x3, s->w_tbx, s->w_pair, s->w_ebx, s->w_ghost, s->sb, s->src, s->scratch,
+                    s->w_valid, s->w_g4, s->w_g1, s->w_trace, s->w_tbx, s->w_pair, s->w_ebx, s->w_ghost, s->sb, s->src, s->scratch,
                     s->d_dtloc, s->d_dtbox};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1746,10 +2080,10 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
     SimDev S = s->dev();
     k_box_prim<NS><<<s->n_g4, BLOCK, 0, cs>>>(S, s->w_g4, make_fab(sb, sb_lo, sb_hi));
     k_prep<NS><<<s->n_g1, BLOCK, 0, cs>>>(S, s->w_g1);
-    k_trace<NS><<<s->n_g1x3, BLOCK, 0, cs>>>(S, s->w_g1x3);
+    k_trace<NS><<<s->n_trace, BLOCK, 0, cs>>>(S, s->w_trace);
     k_riemann1<NS><<<s->n_tbx, BLOCK, 0, cs>>>(S, s->w_tbx);
-    k_riemann2<NS><<<s->n_pair, BLOCK, 0, cs>>>(S, s->w_pair);
-    k_riemann3<NS><<<s->n_ebx, BLOCK, 0, cs>>>(S, s->w_ebx);
+    k_riemann2<NS><<<s->n_pair, BLOCK, R2Slot<NS>::BYTES, cs>>>(S, s->w_pair);
+    k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, cs>>>(S, s->w_ebx);
     k_box_source<NS><<<s->n_valid, BLOCK, 0, cs>>>(S, s->w_valid, make_fab(source, sr_lo, sr_hi));
     if (fo) {
         Fab F[3];
@@ -1787,7 +2121,7 @@ static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
 // device address of g_noalloc_scratch per device, from cudaGetSymbolAddress
 double* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
 
-enum { NL_VALID = 0, NL_G4, NL_G1, NL_G1X3, NL_TBX, NL_PAIR, NL_EBX, NL_COUNT };
+enum { NL_VALID = 0, NL_G4, NL_G1, NL_TRACE, NL_TBX, NL_PAIR, NL_EBX, NL_COUNT };
 
 struct NoallocLists {
     int nsub[NL_COUNT];
@@ -1837,6 +2171,7 @@ int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const
         }
     int dev = 0;
     if (!cuda_ok(cudaGetDevice(&dev), "castro_construct_hydro_source_box_noalloc: cudaGetDevice")) return CASTRO_ERR_CUDA;
+    if (!set_kernel_attributes<NS>()) return CASTRO_ERR_CUDA;
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
         set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box_noalloc: device index beyond 63");
         return CASTRO_ERR_ARG;
@@ -1874,7 +2209,7 @@ int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const
 
     NoallocLists NLs;
     memset(&NLs, 0, sizeof NLs);
-    const int kinds[NL_COUNT] = {R_VALID, R_G4, R_G1, R_G1, R_TBX, R_TBX, R_EBX};
+    const int kinds[NL_COUNT] = {R_VALID, R_G4, R_G1, R_SEG, R_TBX, R_TBX, R_EBX};
     const int nsubs[NL_COUNT] = {1, 1, 1, 3, 3, 6, 3};
     int total = 0;
     int nblocks[NL_COUNT];
@@ -1929,10 +2264,10 @@ int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const
     const Work* W = work;
     k_box_prim<NS><<<nblocks[NL_G4], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G4], make_fab(sb, sb_lo, sb_hi));
     k_prep<NS><<<nblocks[NL_G1], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G1]);
-    k_trace<NS><<<nblocks[NL_G1X3], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G1X3]);
+    k_trace<NS><<<nblocks[NL_TRACE], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TRACE]);
     k_riemann1<NS><<<nblocks[NL_TBX], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TBX]);
-    k_riemann2<NS><<<nblocks[NL_PAIR], BLOCK, 0, cs>>>(S, W + NLs.first[NL_PAIR]);
-    k_riemann3<NS><<<nblocks[NL_EBX], BLOCK, 0, cs>>>(S, W + NLs.first[NL_EBX]);
+    k_riemann2<NS><<<nblocks[NL_PAIR], BLOCK, R2Slot<NS>::BYTES, cs>>>(S, W + NLs.first[NL_PAIR]);
+    k_riemann3<NS><<<nblocks[NL_EBX], BLOCK, R3Slot<NS>::BYTES, cs>>>(S, W + NLs.first[NL_EBX]);
     k_box_source<NS><<<nblocks[NL_VALID], BLOCK, 0, cs>>>(S, W + NLs.first[NL_VALID], make_fab(source, sr_lo, sr_hi));
     if (fo) {
         Fab F[3];
