@@ -169,7 +169,8 @@ def kernel_bytes(cfg, nspec):
             tot["ghost"] += 8 * ((g4 - v) * NQF * 2 + (g1 - v) * NV * 2)
             tot["trace"] += 8 * (g4 * NQF + tdd * 2 * NQS + g1)
             tot["riemann1"] += 8 * (tdd * 2 * NQS + g4 * 2 + tdd * NTF)
-            tot["riemann2"] += 8 * (2 * tab * 2 * NQS // 2 + tdd * NTF + g4 * 2 + tab * NTF)
+            # one thread per face of tbx[a][a] reads its two trace states once for both cross fluxes
+            tot["riemann2"] += 8 * (tdd * 2 * NQS + tdd * NTF + g4 * 2 + tab * NTF)
             tot["riemann3"] += 8 * (eb * 2 * NQS + tab * NTF + g1 * NV + g1 + g4 * 2 + eb * (NV + 1))
             tot["update"] += 8 * (v * NV * 2 + eb * (NV + 1))
     return tot

@@ -41,17 +41,17 @@ KNOBS = [
     ("CASTRO_MINB_EOS", [0, 2, 3, 4]),
     ("CASTRO_MINB_R3", [0, 2, 3, 4]),
     ("CASTRO_MINB_TRACE", [0, 2, 3, 4]),
-    ("CASTRO_MINB_RIEMANN", [0, 2, 3, 4]),
+    ("CASTRO_MINB_RIEMANN", [0, 3, 4, 5, 6]),
     ("CASTRO_TRACE_SEG", [3, 5, 7, 9]),
-    ("CASTRO_R2_STAGE", [0, 1, 2]),
+    ("CASTRO_R2_STAGE", [0, 1]),
     ("CASTRO_R3_STAGE", [0, 1]),
 ]
 DEFAULTS = {"CASTRO_BLOCK": 128, "CASTRO_MINB_EOS": 4, "CASTRO_MINB_R3": 0, "CASTRO_MINB_TRACE": 4,
-            "CASTRO_MINB_RIEMANN": 0, "CASTRO_TRACE_SEG": 5, "CASTRO_R2_STAGE": 1, "CASTRO_R3_STAGE": 0}
+            "CASTRO_MINB_RIEMANN": 5, "CASTRO_TRACE_SEG": 5, "CASTRO_R2_STAGE": 1, "CASTRO_R3_STAGE": 0}
 
 
 def key(cfg: dict) -> str:
-    return "_".join(f"{k.split('_')[-1].lower()}{cfg[k]}" for k in sorted(cfg))
+    return "_".join(f"{k.replace('CASTRO_', '').replace('_', '').lower()}{cfg[k]}" for k in sorted(cfg))
 
 
 def compile_variant(cfg: dict, workdir: str) -> str:
@@ -123,7 +123,7 @@ def write_header(path: str, cfg: dict, table: list, workload: str) -> None:
              "// mini-castro_b200/autotune.py from timings of the batched step",
              f"// ({workload}) on the GPU it ran on.  Timing table (ms per step):"]
     for c, ms in table:
-        lines.append(f"//   {key(c):40s} {ms:8.3f}")
+        lines.append(f"//   {key(c):72s} {ms:8.3f}")
     lines.append("#pragma once")
     lines.append("#ifndef CASTRO_NO_TUNED_HEADER")
     for k in sorted(cfg):

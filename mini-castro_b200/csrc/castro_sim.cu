@@ -12,7 +12,7 @@
 //   ghost   : Q / Sborder ghost zones gathered from the owning boxes (periodic or outflow)
 //   trace   : uflatten once, trace_ppm in x, y, z, divu                (per zone of grow(bx,1))
 //   riemann1: compute_flux on tbx[d][d]                                 (normal fluxes)
-//   riemann2: trans1 + compute_flux on tbx[a][b], a != b                (cross fluxes)
+//   riemann2: trans1 + compute_flux on tbx[a][b], both b != a per face of tbx[a][a] (cross fluxes)
 //   riemann3: trans2 + compute_flux + apply_av + normalize_species_fluxes on ebx[d]
 //   update  : fill_hydro_source + Saxpy + clean_state x2 + estdt        (per valid zone)
 //   dt      : computeNewDt (change_max 1.1, stop_time clamp) on the device
@@ -72,7 +72,7 @@ constexpr int NG = 4;   // ghost zones of Sborder, Source/Castro_advance.cpp:37
 #define CASTRO_MINB_TRACE 4
 #endif
 #ifndef CASTRO_MINB_RIEMANN
-#define CASTRO_MINB_RIEMANN 0
+#define CASTRO_MINB_RIEMANN 5
 #endif
 #ifndef CASTRO_TRACE_SEG
 #define CASTRO_TRACE_SEG 5
@@ -204,11 +204,6 @@ __device__ __forceinline__ bool work_point(const Work* wl, const SimDev& S, int 
     const BoxDev& B = S.boxes[b];
     int rs = sub;
     if (kind == R_TBX && subkind_tbx == 0) rs = 4 * sub;   // tbx[d][d]
-    if (kind == R_TBX && subkind_tbx == 1) {               // pair index -> (a,b)
-        int a = sub / 2, r2 = sub % 2;
-        int bb = (r2 < a) ? r2 : r2 + 1;
-        rs = 3 * a + bb;
-    }
     R = make_reg(B.lo, B.hi, kind, rs);
     long long t = (long long)w.start + threadIdx.x;
     i = R.lx + (int)(t % R.nx);
@@ -612,47 +607,6 @@ __global__ void LB_RIEMANN k_riemann1(SimDev S, const Work* wl)
     store_tf<NS>(S.F1 + B.offF1[d], R, f, flx, g.x, g.y);
 }
 
-// F^{A|Bd} on the A-normal face (i,j,k) of tbx[A][Bd]: trans1 of the face's
-// two A-normal trace states with the Bd normal fluxes, then compute_flux
-// (Castro_hydro.cpp:228-255, 280-304).  rec receives the transverse-flux record.
-template <int NS, int A, int Bd>
-__device__ __forceinline__ void cross_flux(const SimDev& S, const BoxDev& B, const QLoader<NS>& ld, int i, int j,
-                                           int k, double cdtdx, double* rec)
-{
-    constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF, NVAR = Dims<NS>::NVAR;
-    constexpr int eax = A == 0, eay = A == 1, eaz = A == 2;
-    constexpr int ebx_ = Bd == 0, eby = Bd == 1, ebz = Bd == 2;
-    Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * A);
-    Reg RF = make_reg(B.lo, B.hi, R_TBX, 4 * Bd);
-    const double* T = S.Tr + B.offTr[A];
-    const double* F = S.F1 + B.offF1[Bd];
-    long long ft = ridx(RT, i, j, k);
-    double st2[2][NQS];
-#pragma unroll
-    for (int D = -1; D <= 0; ++D) {
-        double lq[NQS], fr[NTF], fl[NTF];
-        const int off = (D == -1) ? 0 : NQS;
-#pragma unroll
-        for (int c = 0; c < NQS; ++c) lq[c] = T[ft + RT.np * (off + c)];
-        int il = i + D * eax, jl = j + D * eay, kl = k + D * eaz;
-        load_tf<NS>(F, RF, ridx(RF, il + ebx_, jl + eby, kl + ebz), fr);
-        load_tf<NS>(F, RF, ridx(RF, il, jl, kl), fl);
-        trans1_state<NS>(lq, fr, fl, ld.gamc(il, jl, kl), cdtdx, st2[D + 1]);
-    }
-    double flx[NVAR];
-    double2 g = riemann_at<NS, A>(ld, i, j, k, st2[0], st2[1], flx);
-    using T_ = TF<NS>;
-    rec[T_::RHO] = flx[URHO];
-    rec[T_::MX] = flx[UMX];
-    rec[T_::MY] = flx[UMY];
-    rec[T_::MZ] = flx[UMZ];
-    rec[T_::ED] = flx[UEDEN];
-#pragma unroll
-    for (int n = 0; n < NS; ++n) rec[T_::X + n] = flx[UFS + n];
-    rec[T_::PG] = g.x;
-    rec[T_::UG] = g.y;
-}
-
 // 8-byte asynchronous global -> shared copies (cp.async, Ampere and later):
 // the copies of one thread are in flight together without holding registers,
 // and the thread waits for all of them once
@@ -668,132 +622,125 @@ __device__ __forceinline__ void cp_async_wait_all()
 }
 
 // Per-thread shared-memory slot of riemann2: the face's two A-normal trace
-// states, the Bd normal-flux records on the faces of both side zones, and the
-// two zones' gamma_1.  The stride is odd, so that the 64-bit accesses of a
-// half-warp fall in distinct bank pairs.
-// CASTRO_R2_STAGE: 0 plain loads, 1 the face states and gamma_1 staged, 2 the
-// flux records too (measured on B200: 1 is fastest; the flux records are each
-// read by about four neighbouring threads and are best served from L1).
-// CASTRO_R2_CARVEOUT: preferred shared-memory carveout in percent, -1 leaves
-// it to the driver (fastest: a larger carveout shrinks L1).
+// states and the two side zones' gamma_1, read once for both cross fluxes of
+// the face.  The stride is odd, so that the 64-bit accesses of a half-warp
+// fall in distinct bank pairs.  CASTRO_R2_STAGE 0 keeps them in registers
+// (measured on B200: staging is faster; staging the normal-flux records too
+// was slower, as each is read by about four neighbouring threads and is best
+// served from L1).
 #ifndef CASTRO_R2_STAGE
 #define CASTRO_R2_STAGE 1
 #endif
-#ifndef CASTRO_R2_CARVEOUT
-#define CASTRO_R2_CARVEOUT -1
-#endif
 template <int NS>
 struct R2Slot {
-    static constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF;
-    static constexpr bool F1 = CASTRO_R2_STAGE >= 2;   // flux records staged too
+    static constexpr int NQS = Dims<NS>::NQS;
     static constexpr int LQ = 0;                   // 2 x NQS: minus (left) state, plus (right) state
     static constexpr int G = 2 * NQS;              // gamma_1 of the left and right zones
-    static constexpr int FR = G + 2;               // 4 x NTF: fr, fl of the left zone, fr, fl of the right zone
-    static constexpr int USED = FR + (F1 ? 4 * NTF : 0);
+    static constexpr int USED = G + 2;
     static constexpr int STRIDE = USED | 1;
-    // staging pays while four blocks of BLOCK threads still fit on an SM
-    static constexpr bool ON = CASTRO_R2_STAGE > 0 && STRIDE * BLOCK * 8 * 4 + 4 * 1024 <= 228 * 1024;
+    static constexpr bool ON = CASTRO_R2_STAGE > 0;
     static constexpr int BYTES = ON ? STRIDE * BLOCK * 8 : 0;
 };
 
-// cross_flux with its operands staged in the thread's shared-memory slot sm;
-// the arithmetic is cross_flux's
+// F^{A|Bd} on the A-normal face (i,j,k) from its two trace states lq (minus
+// then plus, 2 x NQS), the side zones' gamma_1 (gl, gr) and sound speeds (cl,
+// cr): cross_flux's arithmetic, the record written to the F2 pool
 template <int NS, int A, int Bd>
-__device__ __forceinline__ void cross_flux_staged(const SimDev& S, const BoxDev& B, const QLoader<NS>& ld, int i,
-                                                  int j, int k, double cdtdx, double* rec, double* sm)
+__device__ __forceinline__ void cross_flux_store(const SimDev& S, const BoxDev& B, int i, int j, int k, double cdtdx,
+                                                 const double* lq, double gl, double gr, double cl, double cr)
 {
-    using SL = R2Slot<NS>;
-    constexpr int NQS = SL::NQS, NTF = SL::NTF, NVAR = Dims<NS>::NVAR;
+    constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF, NVAR = Dims<NS>::NVAR;
     constexpr int eax = A == 0, eay = A == 1, eaz = A == 2;
     constexpr int ebx_ = Bd == 0, eby = Bd == 1, ebz = Bd == 2;
-    const Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * A);
     const Reg RF = make_reg(B.lo, B.hi, R_TBX, 4 * Bd);
-    const double* T = S.Tr + B.offTr[A];
     const double* F = S.F1 + B.offF1[Bd];
-    const long long ft = ridx(RT, i, j, k);
-#pragma unroll
-    for (int c = 0; c < 2 * NQS; ++c) cp_async8(sm + SL::LQ + c, T + ft + RT.np * c);
-    double frec[SL::F1 ? 1 : 4 * NTF];
-#pragma unroll
-    for (int D = -1; D <= 0; ++D) {
-        const int il = i + D * eax, jl = j + D * eay, kl = k + D * eaz;
-        const long long fr = ridx(RF, il + ebx_, jl + eby, kl + ebz), fl = ridx(RF, il, jl, kl);
-        if constexpr (SL::F1) {
-            double* o = sm + SL::FR + (D + 1) * 2 * NTF;
-#pragma unroll
-            for (int c = 0; c < NTF; ++c) {
-                cp_async8(o + c, F + fr + RF.np * c);
-                cp_async8(o + NTF + c, F + fl + RF.np * c);
-            }
-        } else {
-            load_tf<NS>(F, RF, fr, frec + (D + 1) * 2 * NTF);
-            load_tf<NS>(F, RF, fl, frec + (D + 1) * 2 * NTF + NTF);
-        }
-    }
-    const long long zl = ridx(ld.R, i - eax, j - eay, k - eaz), zr = ridx(ld.R, i, j, k);
-    cp_async8(sm + SL::G, ld.base + zl + ld.R.np * QF<NS>::GAMC);
-    cp_async8(sm + SL::G + 1, ld.base + zr + ld.R.np * QF<NS>::GAMC);
-    const double cl = ld.base[zl + ld.R.np * QF<NS>::C], cr = ld.base[zr + ld.R.np * QF<NS>::C];
-    cp_async_wait_all();
-    const double* fb = SL::F1 ? sm + SL::FR : frec;
     double st2[2][NQS];
 #pragma unroll
-    for (int D = 0; D < 2; ++D)
-        trans1_state<NS>(sm + SL::LQ + D * NQS, fb + D * 2 * NTF, fb + D * 2 * NTF + NTF, sm[SL::G + D], cdtdx,
-                         st2[D]);
-    double flx[NVAR], qg[NGDNV];
-    riemann_cgf<NS, A>(st2[0], st2[1], sm[SL::G], sm[SL::G + 1], cl, cr, flx, qg, nullptr);
-    using T_ = TF<NS>;
-    rec[T_::RHO] = flx[URHO];
-    rec[T_::MX] = flx[UMX];
-    rec[T_::MY] = flx[UMY];
-    rec[T_::MZ] = flx[UMZ];
-    rec[T_::ED] = flx[UEDEN];
-#pragma unroll
-    for (int n = 0; n < NS; ++n) rec[T_::X + n] = flx[UFS + n];
-    rec[T_::PG] = qg[GDPRES];
-    rec[T_::UG] = qg[GDU + A];
-}
-
-template <int NS, int A, int Bd>
-__device__ __forceinline__ void cross_flux_any(const SimDev& S, const BoxDev& B, const QLoader<NS>& ld, int i, int j,
-                                               int k, double cdtdx, double* rec)
-{
-    if constexpr (R2Slot<NS>::ON) {
-        extern __shared__ double r2_smem[];
-        cross_flux_staged<NS, A, Bd>(S, B, ld, i, j, k, cdtdx, rec, r2_smem + threadIdx.x * R2Slot<NS>::STRIDE);
-    } else {
-        cross_flux<NS, A, Bd>(S, B, ld, i, j, k, cdtdx, rec);
+    for (int D = -1; D <= 0; ++D) {
+        double fr[NTF], fl[NTF];
+        const int il = i + D * eax, jl = j + D * eay, kl = k + D * eaz;
+        load_tf<NS>(F, RF, ridx(RF, il + ebx_, jl + eby, kl + ebz), fr);
+        load_tf<NS>(F, RF, ridx(RF, il, jl, kl), fl);
+        trans1_state<NS>(lq + (D + 1) * NQS, fr, fl, D == -1 ? gl : gr, cdtdx, st2[D + 1]);
     }
+    double flx[NVAR], qg[NGDNV];
+    riemann_cgf<NS, A>(st2[0], st2[1], gl, gr, cl, cr, flx, qg, nullptr);
+    const Reg R = make_reg(B.lo, B.hi, R_TBX, 3 * A + Bd);
+    double* out = S.F2 + B.offF2[pair_index(A, Bd)];
+    const long long f = ridx(R, i, j, k);
+    using T_ = TF<NS>;
+    out[f + R.np * T_::RHO] = flx[URHO];
+    out[f + R.np * T_::MX] = flx[UMX];
+    out[f + R.np * T_::MY] = flx[UMY];
+    out[f + R.np * T_::MZ] = flx[UMZ];
+    out[f + R.np * T_::ED] = flx[UEDEN];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) out[f + R.np * (T_::X + n)] = flx[UFS + n];
+    out[f + R.np * T_::PG] = qg[GDPRES];
+    out[f + R.np * T_::UG] = qg[GDU + A];
 }
 
-// riemann2: F^{a|b} on tbx[a][b] for the six ordered pairs
+// Both cross fluxes of the A-normal face (i,j,k) of tbx[A][A]: F^{A|B1} where
+// the face lies in tbx[A][B1] (its B1 coordinate inside the box), F^{A|B2}
+// likewise.  The face's trace states, gamma_1 and sound speeds are read once
+// for the two.
+template <int NS, int A>
+__device__ __forceinline__ void cross_flux_both(const SimDev& S, const BoxDev& B, const InstDev& I,
+                                                const QLoader<NS>& ld, int i, int j, int k, double dt)
+{
+    using SL = R2Slot<NS>;
+    constexpr int NQS = Dims<NS>::NQS;
+    constexpr int B1 = A == 0 ? 1 : 0, B2 = A == 2 ? 1 : 2;
+    constexpr int eax = A == 0, eay = A == 1, eaz = A == 2;
+    const Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * A);
+    const double* T = S.Tr + B.offTr[A];
+    const long long ft = ridx(RT, i, j, k);
+    const long long zl = ridx(ld.R, i - eax, j - eay, k - eaz), zr = ridx(ld.R, i, j, k);
+    double lqr[SL::ON ? 1 : 2 * NQS];
+    const double* lq;
+    double gl, gr;
+    if constexpr (SL::ON) {
+        extern __shared__ double r2_smem[];
+        double* sm = r2_smem + threadIdx.x * SL::STRIDE;
+#pragma unroll
+        for (int c = 0; c < 2 * NQS; ++c) cp_async8(sm + SL::LQ + c, T + ft + RT.np * c);
+        cp_async8(sm + SL::G, ld.base + zl + ld.R.np * QF<NS>::GAMC);
+        cp_async8(sm + SL::G + 1, ld.base + zr + ld.R.np * QF<NS>::GAMC);
+        lq = sm + SL::LQ;
+        cp_async_wait_all();
+        gl = sm[SL::G];
+        gr = sm[SL::G + 1];
+    } else {
+#pragma unroll
+        for (int c = 0; c < 2 * NQS; ++c) lqr[c] = T[ft + RT.np * c];
+        lq = lqr;
+        gl = ld.base[zl + ld.R.np * QF<NS>::GAMC];
+        gr = ld.base[zr + ld.R.np * QF<NS>::GAMC];
+    }
+    const double cl = ld.base[zl + ld.R.np * QF<NS>::C], cr = ld.base[zr + ld.R.np * QF<NS>::C];
+    const int p[3] = {i, j, k};
+    if (p[B1] >= B.lo[B1] && p[B1] <= B.hi[B1])
+        cross_flux_store<NS, A, B1>(S, B, i, j, k, dt / I.dx[B1] / 3.0, lq, gl, gr, cl, cr);
+    if (p[B2] >= B.lo[B2] && p[B2] <= B.hi[B2])
+        cross_flux_store<NS, A, B2>(S, B, i, j, k, dt / I.dx[B2] / 3.0, lq, gl, gr, cl, cr);
+}
+
+// riemann2: one thread per face of tbx[a][a] (Castro_hydro.cpp:228-304)
 template <int NS>
 __global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
 {
-    int bx, p, i, j, k;
+    int bx, a, i, j, k;
     Reg R;
-    if (!work_point(wl, S, R_TBX, 1, bx, p, R, i, j, k)) return;
+    if (!work_point(wl, S, R_TBX, 0, bx, a, R, i, j, k)) return;
     const BoxDev& B = S.boxes[bx];
     const InstDev& I = S.inst[B.inst];
     const double dt = S.st[B.inst].dt;
-    constexpr int NTF = Dims<NS>::NTF;
     QLoader<NS> ld;
     ld.base = S.Q + B.offQ;
     ld.R = make_reg(B.lo, B.hi, R_G4, 0);
-    double rec[NTF];
-    switch (p) {   // pair_index order: (0,1) (0,2) (1,0) (1,2) (2,0) (2,1)
-    case 0: cross_flux_any<NS, 0, 1>(S, B, ld, i, j, k, dt / I.dx[1] / 3.0, rec); break;
-    case 1: cross_flux_any<NS, 0, 2>(S, B, ld, i, j, k, dt / I.dx[2] / 3.0, rec); break;
-    case 2: cross_flux_any<NS, 1, 0>(S, B, ld, i, j, k, dt / I.dx[0] / 3.0, rec); break;
-    case 3: cross_flux_any<NS, 1, 2>(S, B, ld, i, j, k, dt / I.dx[2] / 3.0, rec); break;
-    case 4: cross_flux_any<NS, 2, 0>(S, B, ld, i, j, k, dt / I.dx[0] / 3.0, rec); break;
-    default: cross_flux_any<NS, 2, 1>(S, B, ld, i, j, k, dt / I.dx[1] / 3.0, rec); break;
-    }
-    double* out = S.F2 + B.offF2[p];
-    long long f = ridx(R, i, j, k);
-#pragma unroll
-    for (int c = 0; c < NTF; ++c) out[f + R.np * c] = rec[c];
+    if (a == 0) cross_flux_both<NS, 0>(S, B, I, ld, i, j, k, dt);
+    else if (a == 1) cross_flux_both<NS, 1>(S, B, I, ld, i, j, k, dt);
+    else cross_flux_both<NS, 2>(S, B, I, ld, i, j, k, dt);
 }
 
 // CASTRO_R3_STAGE: 0 plain loads, 1 the per-face operands of riemann3 that no
@@ -1252,9 +1199,9 @@ struct castro_sim {
     double *Tr = nullptr, *F1 = nullptr, *F2 = nullptr, *Fx = nullptr;
     long long nU = 0;
     // work lists
-    Work *w_valid = nullptr, *w_g4 = nullptr, *w_g1 = nullptr, *w_trace = nullptr, *w_tbx = nullptr, *w_pair = nullptr,
+    Work *w_valid = nullptr, *w_g4 = nullptr, *w_g1 = nullptr, *w_trace = nullptr, *w_tbx = nullptr,
          *w_ebx = nullptr, *w_ghost = nullptr;
-    int n_valid = 0, n_g4 = 0, n_g1 = 0, n_trace = 0, n_tbx = 0, n_pair = 0, n_ebx = 0, n_ghost = 0;
+    int n_valid = 0, n_g4 = 0, n_g1 = 0, n_trace = 0, n_tbx = 0, n_ebx = 0, n_ghost = 0;
     bool dt_ready = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -1305,18 +1252,14 @@ bool dalloc(T** p, size_t n, const char* what)
 
 void build_work(castro_sim* s, int kind, int nsub, int tbx_mode, Work** out, int* count)
 {
-    // sub-major order: every box's items of one direction (or pair) before the
-    // next, so the blocks resident on an SM run the same code path
+    // sub-major order: every box's items of one direction before the next, so
+    // the blocks resident on an SM run the same code path
     std::vector<Work> w;
     for (int sub = 0; sub < nsub; ++sub) {
         for (size_t b = 0; b < s->hboxes.size(); ++b) {
             const BoxDev& B = s->hboxes[b];
             int rs = sub;
             if (kind == R_TBX && tbx_mode == 0) rs = 4 * sub;
-            if (kind == R_TBX && tbx_mode == 1) {
-                int a = sub / 2, r2 = sub % 2;
-                rs = 3 * a + ((r2 < a) ? r2 : r2 + 1);
-            }
             long long np = npts_reg(B.lo, B.hi, kind, rs);
             for (long long st = 0; st < np; st += BLOCK) {
                 Work it;
@@ -1342,13 +1285,11 @@ bool set_kernel_attributes()
         !cuda_ok(cudaFuncSetAttribute(k_riemann3<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, R3Slot<NS>::BYTES),
                  "riemann3 shared memory"))
         return false;
-    if (!R2Slot<NS>::ON) return true;
-    return cuda_ok(cudaFuncSetAttribute(k_riemann2<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, R2Slot<NS>::BYTES),
-                   "riemann2 shared memory") &&
-           (CASTRO_R2_CARVEOUT < 0 ||
-            cuda_ok(cudaFuncSetAttribute(k_riemann2<NS>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                         CASTRO_R2_CARVEOUT),
-                    "riemann2 carveout"));
+    if (R2Slot<NS>::BYTES > 48 * 1024 &&
+        !cuda_ok(cudaFuncSetAttribute(k_riemann2<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, R2Slot<NS>::BYTES),
+                 "riemann2 shared memory"))
+        return false;
+    return true;
 }
 
 template <int NS>
@@ -1361,7 +1302,7 @@ void batched_step_kernels(castro_sim* s)
     k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(S, s->w_g1);
     k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(S, s->w_trace);
     k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(S, s->w_tbx);
-    k_riemann2<NS><<<s->n_pair, BLOCK, R2Slot<NS>::BYTES, st>>>(S, s->w_pair);
+    k_riemann2<NS><<<s->n_tbx, BLOCK, R2Slot<NS>::BYTES, st>>>(S, s->w_tbx);
     k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, st>>>(S, s->w_ebx);
     k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid);
     k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0);
@@ -1377,7 +1318,7 @@ void profile_kernel(castro_sim* s, const SimDev& S, int k)
     case 2: k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(S, s->w_g1); break;
     case 3: k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(S, s->w_trace); break;
     case 4: k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(S, s->w_tbx); break;
-    case 5: k_riemann2<NS><<<s->n_pair, BLOCK, R2Slot<NS>::BYTES, st>>>(S, s->w_pair); break;
+    case 5: k_riemann2<NS><<<s->n_tbx, BLOCK, R2Slot<NS>::BYTES, st>>>(S, s->w_tbx); break;
     case 6: k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, st>>>(S, s->w_ebx); break;
     case 7: k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid); break;
     default: k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0); break;
@@ -1743,7 +1684,6 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
         build_work(s, R_G1, 1, -1, &s->w_g1, &s->n_g1);
         build_work(s, R_SEG, 3, -1, &s->w_trace, &s->n_trace);
         build_work(s, R_TBX, 3, 0, &s->w_tbx, &s->n_tbx);
-        build_work(s, R_TBX, 6, 1, &s->w_pair, &s->n_pair);
         build_work(s, R_EBX, 3, -1, &s->w_ebx, &s->n_ebx);
         build_work(s, R_GHOST, 6, -1, &s->w_ghost, &s->n_ghost);
     }
@@ -1774,7 +1714,7 @@ void castro_sim_destroy(castro_sim* s)
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     if (s->graph) cudaGraphDestroy(s->graph);
     void* ptrs[] = {s->dboxes, s->dinst, s->dstate, s->downer, s->U, s->Ub, s->Q, s->Div, s->Tr, s->F1, s->F2, s->Fx,
-                    s->w_valid, s->w_g4, s->w_g1, s->w_trace, s->w_tbx, s->w_pair, s->w_ebx, s->w_ghost, s->sb, s->src, s->scratch,
+                    s->w_valid, s->w_g4, s->w_g1, s->w_trace, s->w_tbx, s->w_ebx, s->w_ghost, s->sb, s->src, s->scratch,
                     s->d_dtloc, s->d_dtbox};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -2082,7 +2022,7 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
     k_prep<NS><<<s->n_g1, BLOCK, 0, cs>>>(S, s->w_g1);
     k_trace<NS><<<s->n_trace, BLOCK, 0, cs>>>(S, s->w_trace);
     k_riemann1<NS><<<s->n_tbx, BLOCK, 0, cs>>>(S, s->w_tbx);
-    k_riemann2<NS><<<s->n_pair, BLOCK, R2Slot<NS>::BYTES, cs>>>(S, s->w_pair);
+    k_riemann2<NS><<<s->n_tbx, BLOCK, R2Slot<NS>::BYTES, cs>>>(S, s->w_tbx);
     k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, cs>>>(S, s->w_ebx);
     k_box_source<NS><<<s->n_valid, BLOCK, 0, cs>>>(S, s->w_valid, make_fab(source, sr_lo, sr_hi));
     if (fo) {
@@ -2121,7 +2061,7 @@ static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
 // device address of g_noalloc_scratch per device, from cudaGetSymbolAddress
 double* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
 
-enum { NL_VALID = 0, NL_G4, NL_G1, NL_TRACE, NL_TBX, NL_PAIR, NL_EBX, NL_COUNT };
+enum { NL_VALID = 0, NL_G4, NL_G1, NL_TRACE, NL_TBX, NL_EBX, NL_COUNT };
 
 struct NoallocLists {
     int nsub[NL_COUNT];
@@ -2209,8 +2149,8 @@ int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const
 
     NoallocLists NLs;
     memset(&NLs, 0, sizeof NLs);
-    const int kinds[NL_COUNT] = {R_VALID, R_G4, R_G1, R_SEG, R_TBX, R_TBX, R_EBX};
-    const int nsubs[NL_COUNT] = {1, 1, 1, 3, 3, 6, 3};
+    const int kinds[NL_COUNT] = {R_VALID, R_G4, R_G1, R_SEG, R_TBX, R_EBX};
+    const int nsubs[NL_COUNT] = {1, 1, 1, 3, 3, 3};
     int total = 0;
     int nblocks[NL_COUNT];
     for (int l = 0; l < NL_COUNT; ++l) {
@@ -2220,7 +2160,6 @@ int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const
         for (int sub = 0; sub < nsubs[l]; ++sub) {
             int rs = sub;
             if (l == NL_TBX) rs = 4 * sub;
-            if (l == NL_PAIR) { int a = sub / 2, r2 = sub % 2; rs = 3 * a + ((r2 < a) ? r2 : r2 + 1); }
             NLs.np[l][sub] = npts_reg(B.lo, B.hi, kinds[l], rs);
             nb += (int)((NLs.np[l][sub] + BLOCK - 1) / BLOCK);
         }
@@ -2266,7 +2205,7 @@ int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const
     k_prep<NS><<<nblocks[NL_G1], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G1]);
     k_trace<NS><<<nblocks[NL_TRACE], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TRACE]);
     k_riemann1<NS><<<nblocks[NL_TBX], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TBX]);
-    k_riemann2<NS><<<nblocks[NL_PAIR], BLOCK, R2Slot<NS>::BYTES, cs>>>(S, W + NLs.first[NL_PAIR]);
+    k_riemann2<NS><<<nblocks[NL_TBX], BLOCK, R2Slot<NS>::BYTES, cs>>>(S, W + NLs.first[NL_TBX]);
     k_riemann3<NS><<<nblocks[NL_EBX], BLOCK, R3Slot<NS>::BYTES, cs>>>(S, W + NLs.first[NL_EBX]);
     k_box_source<NS><<<nblocks[NL_VALID], BLOCK, 0, cs>>>(S, W + NLs.first[NL_VALID], make_fab(source, sr_lo, sr_hi));
     if (fo) {
