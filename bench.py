@@ -143,6 +143,12 @@ def kernel_bytes(cfg, nspec):
     NV, NQF, NQS, NTF = 7 + nspec, 8 + nspec, 6 + nspec, 7 + nspec
     tot = dict(front=0, ghost=0, trace=0, riemann1=0, riemann2=0, riemann3=0, update=0)
     for inst in cfg["instances"]:
+        # Q and Sborder live per instance on grow(domain,4) / grow(domain,1): the ghost kernel fills the domain halo
+        nd = [h - l + 1 for l, h in zip(inst["dom_lo"], inst["dom_hi"])]
+        vd = nd[0] * nd[1] * nd[2]
+        g4d = (nd[0] + 8) * (nd[1] + 8) * (nd[2] + 8)
+        g1d = (nd[0] + 2) * (nd[1] + 2) * (nd[2] + 2)
+        tot["ghost"] += 8 * ((g4d - vd) * NQF * 2 + (g1d - vd) * NV * 2)
         for lo, hi in inst["boxes"]:
             n = [h - l + 1 for l, h in zip(lo, hi)]
             v = n[0] * n[1] * n[2]
@@ -166,7 +172,6 @@ def kernel_bytes(cfg, nspec):
             tab = sum(tbx(a, b) for a in range(3) for b in range(3) if a != b)
             eb = sum(ebx(d) for d in range(3))
             tot["front"] += 8 * (v * NV * 2 + v * NV + v * NQF)
-            tot["ghost"] += 8 * ((g4 - v) * NQF * 2 + (g1 - v) * NV * 2)
             tot["trace"] += 8 * (g4 * NQF + tdd * 2 * NQS + g1)
             tot["riemann1"] += 8 * (tdd * 2 * NQS + g4 * 2 + tdd * NTF)
             # one thread per face of tbx[a][a] reads its two trace states once for both cross fluxes

@@ -213,6 +213,14 @@ __device__ __forceinline__ bool work_point(const Work* wl, const SimDev& S, int 
     return true;
 }
 
+// Q lives on grow(domain,4) and Sborder on grow(domain,1) of the box's
+// instance: one array each per instance, written at every zone by the box that
+// owns it, so the halo zones of a box that lie inside the domain are the
+// neighbouring boxes' zones themselves and only the domain's own halo needs a
+// fill (k_ghost).  On the single-box entry points the instance domain is the box.
+__host__ __device__ __forceinline__ Reg q_region(const InstDev& I) { return make_reg(I.dom_lo, I.dom_hi, R_G4, 0); }
+__host__ __device__ __forceinline__ Reg u_region(const InstDev& I) { return make_reg(I.dom_lo, I.dom_hi, R_G1, 0); }
+
 // Q record: rho, u, v, w, p, rhoe, X[NS], gamc, c
 template <int NS>
 struct QF {
@@ -283,14 +291,15 @@ __global__ void LB_EOS k_front(SimDev S, const Work* wl)
 #pragma unroll
     for (int n = 0; n < NVAR; ++n) U[id + R.np * n] = u[n];
     clean_state_pt<NS>(u);                          // Castro_advance.cpp:66 (valid part of Sborder)
-    Reg R1 = make_reg(B.lo, B.hi, R_G1, 0);
+    const InstDev& I = S.inst[B.inst];
+    const Reg R1 = u_region(I);
     double* Ub = S.Ub + B.offUb;
     long long id1 = ridx(R1, i, j, k);
 #pragma unroll
     for (int n = 0; n < NVAR; ++n) Ub[id1 + R1.np * n] = u[n];
     double q[QVAR], qa[NQAUX];
     ctoprim_pt<NS>(u, q, qa);                       // Castro_hydro.cpp:64-70
-    Reg R4 = make_reg(B.lo, B.hi, R_G4, 0);
+    const Reg R4 = q_region(I);
     double* Q = S.Q + B.offQ;
     long long id4 = ridx(R4, i, j, k);
     using F = QF<NS>;
@@ -317,36 +326,39 @@ __device__ __forceinline__ int map_bc(int i, int lo, int hi, int bc)
     return i < lo ? lo : (i > hi ? hi : i);
 }
 
-// ghost: Q on grow(bx,4) and Sborder on grow(bx,1) outside the valid box,
-// one thread per ghost zone (the work list walks the six slabs)
+// ghost: Q on grow(domain,4) and Sborder on grow(domain,1) outside the domain
+// of each instance, from the domain zone the boundary condition maps to
+// (periodic wrap or outflow nearest zone), one thread per halo zone.  Work item:
+// box = any box of the instance (for its arrays), sub = slab of the domain halo.
+// Sources are domain zones, written by k_front, never halo zones.
 template <int NS>
 __global__ void __launch_bounds__(BLOCK) k_ghost(SimDev S, const Work* wl)
 {
-    int b, sub, i, j, k;
-    Reg RS;
-    if (!work_point(wl, S, R_GHOST, -1, b, sub, RS, i, j, k)) return;
-    const BoxDev& B = S.boxes[b];
-    const Reg R = make_reg(B.lo, B.hi, R_G4, 0);
+    const Work w = wl[blockIdx.x];
+    if ((int)threadIdx.x >= w.count) return;
+    const BoxDev& B = S.boxes[w.box];
     const InstDev& I = S.inst[B.inst];
-    int ii = map_bc(i, I.dom_lo[0], I.dom_hi[0], I.bc);
-    int jj = map_bc(j, I.dom_lo[1], I.dom_hi[1], I.bc);
-    int kk = map_bc(k, I.dom_lo[2], I.dom_hi[2], I.bc);
-    int ob = S.owner[I.owner_off + (long long)((ii - I.dom_lo[0]) / I.g) +
-                     (long long)I.on[0] * ((long long)((jj - I.dom_lo[1]) / I.g) + (long long)I.on[1] * ((kk - I.dom_lo[2]) / I.g))];
-    const BoxDev& O = S.boxes[ob];
-    Reg RO4 = make_reg(O.lo, O.hi, R_G4, 0);
-    const double* Qs = S.Q + O.offQ;
-    double* Qd = S.Q + B.offQ;
-    long long is = ridx(RO4, ii, jj, kk), id = ridx(R, i, j, k);
+    const Reg RS = make_reg(I.dom_lo, I.dom_hi, R_GHOST, w.sub);
+    const long long t = (long long)w.start + threadIdx.x;
+    const int i = RS.lx + (int)(t % RS.nx);
+    const long long t2 = t / RS.nx;
+    const int j = RS.ly + (int)(t2 % RS.ny);
+    const int k = RS.lz + (int)(t2 / RS.ny);
+    const int ii = map_bc(i, I.dom_lo[0], I.dom_hi[0], I.bc);
+    const int jj = map_bc(j, I.dom_lo[1], I.dom_hi[1], I.bc);
+    const int kk = map_bc(k, I.dom_lo[2], I.dom_hi[2], I.bc);
+    const Reg R = q_region(I);
+    double* Q = S.Q + B.offQ;
+    const long long is = ridx(R, ii, jj, kk), id = ridx(R, i, j, k);
 #pragma unroll
-    for (int c = 0; c < QF<NS>::N; ++c) Qd[id + R.np * c] = Qs[is + RO4.np * c];
-    if (i >= B.lo[0] - 1 && i <= B.hi[0] + 1 && j >= B.lo[1] - 1 && j <= B.hi[1] + 1 && k >= B.lo[2] - 1 && k <= B.hi[2] + 1) {
-        Reg R1 = make_reg(B.lo, B.hi, R_G1, 0), RO1 = make_reg(O.lo, O.hi, R_G1, 0);
-        const double* Us = S.Ub + O.offUb;
-        double* Ud = S.Ub + B.offUb;
-        long long is1 = ridx(RO1, ii, jj, kk), id1 = ridx(R1, i, j, k);
+    for (int c = 0; c < QF<NS>::N; ++c) Q[id + R.np * c] = Q[is + R.np * c];
+    if (i >= I.dom_lo[0] - 1 && i <= I.dom_hi[0] + 1 && j >= I.dom_lo[1] - 1 && j <= I.dom_hi[1] + 1 &&
+        k >= I.dom_lo[2] - 1 && k <= I.dom_hi[2] + 1) {
+        const Reg R1 = u_region(I);
+        double* Ub = S.Ub + B.offUb;
+        const long long is1 = ridx(R1, ii, jj, kk), id1 = ridx(R1, i, j, k);
 #pragma unroll
-        for (int n = 0; n < Dims<NS>::NVAR; ++n) Ud[id1 + R1.np * n] = Us[is1 + RO1.np * n];
+        for (int n = 0; n < Dims<NS>::NVAR; ++n) Ub[id1 + R1.np * n] = Ub[is1 + R1.np * n];
     }
 }
 
@@ -363,7 +375,7 @@ __global__ void __launch_bounds__(BLOCK) k_prep(SimDev S, const Work* wl)
     const InstDev& I = S.inst[B.inst];
     QLoader<NS> ld;
     ld.base = S.Q + B.offQ;
-    ld.R = make_reg(B.lo, B.hi, R_G4, 0);
+    ld.R = q_region(S.inst[B.inst]);
     double dxinv = 1.0 / I.dx[0], dyinv = 1.0 / I.dx[1], dzinv = 1.0 / I.dx[2];
     auto Qv = [&](int a, int bq, int c, int n) { return ld.at(a, bq, c, QF<NS>::U + n); };
     double ux = 0.25 * (+Qv(i, j, k, 0) - Qv(i - 1, j, k, 0)
@@ -400,7 +412,7 @@ __device__ __forceinline__ void trace_segment(const SimDev& S, const BoxDev& B, 
     constexpr int NQS = Dims<NS>::NQS;
     constexpr int T1 = D == 0 ? 1 : D == 1 ? 2 : 0;   // qut - QU of trace_zone
     constexpr int T2 = D == 0 ? 2 : D == 1 ? 0 : 1;   // qutt - QU
-    const Reg R4 = make_reg(B.lo, B.hi, R_G4, 0);
+    const Reg R4 = q_region(S.inst[B.inst]);
     const Reg R1 = make_reg(B.lo, B.hi, R_G1, 0);
     const Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * D);
     int p[3] = {i, j, k};
@@ -598,7 +610,7 @@ __global__ void LB_RIEMANN k_riemann1(SimDev S, const Work* wl)
     for (int c = 0; c < NQS; ++c) { ql[c] = T[f + R.np * c]; qr[c] = T[f + R.np * (NQS + c)]; }
     QLoader<NS> ld;
     ld.base = S.Q + B.offQ;
-    ld.R = make_reg(B.lo, B.hi, R_G4, 0);
+    ld.R = q_region(S.inst[B.inst]);
     double flx[NVAR];
     double2 g;
     if (d == 0) g = riemann_at<NS, 0>(ld, i, j, k, ql, qr, flx);
@@ -737,7 +749,7 @@ __global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
     const double dt = S.st[B.inst].dt;
     QLoader<NS> ld;
     ld.base = S.Q + B.offQ;
-    ld.R = make_reg(B.lo, B.hi, R_G4, 0);
+    ld.R = q_region(S.inst[B.inst]);
     if (a == 0) cross_flux_both<NS, 0>(S, B, I, ld, i, j, k, dt);
     else if (a == 1) cross_flux_both<NS, 1>(S, B, I, ld, i, j, k, dt);
     else cross_flux_both<NS, 2>(S, B, I, ld, i, j, k, dt);
@@ -789,12 +801,13 @@ __device__ __forceinline__ void final_flux(const SimDev& S, const BoxDev& B, con
     constexpr int e2x = T2 == 0, e2y = T2 == 1, e2z = T2 == 2;
     const double hdt1 = 0.5 * dt / I.dx[T1], hdt2 = 0.5 * dt / I.dx[T2];
     const Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * D);
-    const Reg R1 = make_reg(B.lo, B.hi, R_G1, 0);
+    const Reg R1 = make_reg(B.lo, B.hi, R_G1, 0);   // divu nodes
+    const Reg RU = u_region(I);                         // Sborder
     const double* T = S.Tr + B.offTr[D];
     const double* Dv = S.Div + B.offDiv;
     const double* Ub = S.Ub + B.offUb;
     const long long ft = ridx(RT, i, j, k);
-    const long long c0 = ridx(R1, i, j, k), cm = ridx(R1, i - ex, j - ey, k - ez);
+    const long long c0 = ridx(RU, i, j, k), cm = ridx(RU, i - ex, j - ey, k - ez);
     const long long zl = ridx(ld.R, i - ex, j - ey, k - ez), zr = ridx(ld.R, i, j, k);
     if constexpr (STG) {
 #pragma unroll
@@ -804,8 +817,8 @@ __device__ __forceinline__ void final_flux(const SimDev& S, const BoxDev& B, con
 #pragma unroll
         for (int n = 0; n < NVAR; ++n) {
             if (n == UTEMP) continue;
-            cp_async8(sm + SL::UB + n, Ub + c0 + R1.np * n);
-            cp_async8(sm + SL::UB + NVAR + n, Ub + cm + R1.np * n);
+            cp_async8(sm + SL::UB + n, Ub + c0 + RU.np * n);
+            cp_async8(sm + SL::UB + NVAR + n, Ub + cm + RU.np * n);
         }
 #pragma unroll
         for (int m = 0; m < 4; ++m)
@@ -852,8 +865,8 @@ __device__ __forceinline__ void final_flux(const SimDev& S, const BoxDev& B, con
 #pragma unroll
         for (int n = 0; n < NVAR; ++n) {
             if (n == UTEMP) continue;
-            const double u0 = STG ? sm[SL::UB + n] : Ub[c0 + R1.np * n];
-            const double um = STG ? sm[SL::UB + NVAR + n] : Ub[cm + R1.np * n];
+            const double u0 = STG ? sm[SL::UB + n] : Ub[c0 + RU.np * n];
+            const double um = STG ? sm[SL::UB + NVAR + n] : Ub[cm + RU.np * n];
             double div1 = av_term(ds, u0 - um);
             flx[n] = flx[n] + dxd * div1;
         }
@@ -915,7 +928,7 @@ __global__ void LB_R3 k_riemann3(SimDev S, const Work* wl)
     const double dt = S.st[B.inst].dt;
     QLoader<NS> ld;
     ld.base = S.Q + B.offQ;
-    ld.R = make_reg(B.lo, B.hi, R_G4, 0);
+    ld.R = q_region(S.inst[B.inst]);
     if (d == 0) riemann3_dir<NS, 0>(S, B, I, ld, i, j, k, dt);
     else if (d == 1) riemann3_dir<NS, 1>(S, B, I, ld, i, j, k, dt);
     else riemann3_dir<NS, 2>(S, B, I, ld, i, j, k, dt);
@@ -1073,21 +1086,23 @@ __global__ void __launch_bounds__(BLOCK) k_box_prim(SimDev S, const Work* wl, Fa
 #pragma unroll
     for (int n = 0; n < NVAR; ++n) u[n] = SB(i, j, k, n);
     ctoprim_pt<NS>(u, q, qa);
+    const InstDev& I = S.inst[B.inst];
+    const Reg RQ = q_region(I);   // grow(bx,4): the instance domain is the box here
     double* Q = S.Q + B.offQ;
-    long long id = ridx(R, i, j, k);
+    long long id = ridx(RQ, i, j, k);
     using F = QF<NS>;
-    Q[id + R.np * F::RHO] = q[QRHO];
-    Q[id + R.np * (F::U + 0)] = q[QU];
-    Q[id + R.np * (F::U + 1)] = q[QV];
-    Q[id + R.np * (F::U + 2)] = q[QW];
-    Q[id + R.np * F::P] = q[QPRES];
-    Q[id + R.np * F::RE] = q[QREINT];
+    Q[id + RQ.np * F::RHO] = q[QRHO];
+    Q[id + RQ.np * (F::U + 0)] = q[QU];
+    Q[id + RQ.np * (F::U + 1)] = q[QV];
+    Q[id + RQ.np * (F::U + 2)] = q[QW];
+    Q[id + RQ.np * F::P] = q[QPRES];
+    Q[id + RQ.np * F::RE] = q[QREINT];
 #pragma unroll
-    for (int n = 0; n < NS; ++n) Q[id + R.np * (F::X + n)] = q[QFS + n];
-    Q[id + R.np * F::GAMC] = qa[QGAMC];
-    Q[id + R.np * F::C] = qa[QC];
+    for (int n = 0; n < NS; ++n) Q[id + RQ.np * (F::X + n)] = q[QFS + n];
+    Q[id + RQ.np * F::GAMC] = qa[QGAMC];
+    Q[id + RQ.np * F::C] = qa[QC];
     if (i >= B.lo[0] - 1 && i <= B.hi[0] + 1 && j >= B.lo[1] - 1 && j <= B.hi[1] + 1 && k >= B.lo[2] - 1 && k <= B.hi[2] + 1) {
-        Reg R1 = make_reg(B.lo, B.hi, R_G1, 0);
+        const Reg R1 = u_region(I);
         double* Ub = S.Ub + B.offUb;
         long long i1 = ridx(R1, i, j, k);
 #pragma unroll
@@ -1290,6 +1305,29 @@ bool set_kernel_attributes()
                  "riemann2 shared memory"))
         return false;
     return true;
+}
+
+// work list of k_ghost: the six slabs of grow(domain,4) \ domain of every
+// instance, items naming the instance's first box
+void build_ghost_work(castro_sim* s)
+{
+    std::vector<Work> w;
+    for (int sub = 0; sub < 6; ++sub)
+        for (int in = 0; in < s->ninst; ++in) {
+            const InstDev& I = s->hinst[in];
+            const long long np = npts_reg(I.dom_lo, I.dom_hi, R_GHOST, sub);
+            for (long long st = 0; st < np; st += BLOCK) {
+                Work it;
+                it.box = s->inst_boxes[in][0];
+                it.sub = sub;
+                it.start = (int)st;
+                it.count = (int)std::min<long long>(BLOCK, np - st);
+                w.push_back(it);
+            }
+        }
+    s->n_ghost = (int)w.size();
+    if (dalloc(&s->w_ghost, w.size(), "ghost work list"))
+        cuda_ok(cudaMemcpy(s->w_ghost, w.data(), w.size() * sizeof(Work), cudaMemcpyHostToDevice), "ghost work list copy");
 }
 
 template <int NS>
@@ -1624,6 +1662,10 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
         I.g = g;
         for (int d = 0; d < 3; ++d) I.on[d] = (D.dom_hi[d] - D.dom_lo[d] + 1) / g;
         I.owner_off = (long long)owner_all.size();
+        // Q and Sborder of the instance: one array each over grow(domain,4) / grow(domain,1)
+        const long long offQ_inst = oQ, offUb_inst = oUb;
+        oQ += npts_reg(I.dom_lo, I.dom_hi, R_G4, 0) * NQF;
+        oUb += npts_reg(I.dom_lo, I.dom_hi, R_G1, 0) * NV;
         size_t nown = (size_t)I.on[0] * I.on[1] * I.on[2];
         owner_all.resize(owner_all.size() + nown, -1);
         for (int b = 0; b < D.nbox; ++b) {
@@ -1632,8 +1674,8 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
             for (int d = 0; d < 3; ++d) { B.lo[d] = D.box_lo[3 * b + d]; B.hi[d] = D.box_hi[3 * b + d]; }
             B.inst = in;
             B.offU = oU; oU += npts_reg(B.lo, B.hi, R_VALID, 0) * NV;
-            B.offUb = oUb; oUb += npts_reg(B.lo, B.hi, R_G1, 0) * NV;
-            B.offQ = oQ; oQ += npts_reg(B.lo, B.hi, R_G4, 0) * NQF;
+            B.offUb = offUb_inst;
+            B.offQ = offQ_inst;
             B.offDiv = oDiv; oDiv += npts_reg(B.lo, B.hi, R_G1, 0) * 2;   // divu, flatn
             for (int d = 0; d < 3; ++d) {
                 B.offTr[d] = oTr; oTr += npts_reg(B.lo, B.hi, R_TBX, 4 * d) * 2 * NQS;
@@ -1685,7 +1727,7 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
         build_work(s, R_SEG, 3, -1, &s->w_trace, &s->n_trace);
         build_work(s, R_TBX, 3, 0, &s->w_tbx, &s->n_tbx);
         build_work(s, R_EBX, 3, -1, &s->w_ebx, &s->n_ebx);
-        build_work(s, R_GHOST, 6, -1, &s->w_ghost, &s->n_ghost);
+        build_ghost_work(s);
     }
     if (ok && mode == CASTRO_MODE_PLAIN) {
         long long nsb = 0, nsrc = 0, mx = 0;
