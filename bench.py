@@ -139,45 +139,49 @@ class ClockSampler:
 
 def kernel_bytes(cfg, nspec):
     """Compulsory HBM bytes of one launch of each fused kernel (every array the
-    kernel reads or writes touched once), from the BoxArray geometry."""
+    kernel reads or writes touched once).  front and update walk the boxes of
+    the BoxArray; ghost fills each instance's domain halo; prep, trace and the
+    three Riemann kernels walk each instance's domain as one region."""
     NV, NQF, NQS, NTF = 7 + nspec, 8 + nspec, 6 + nspec, 7 + nspec
     tot = dict(front=0, ghost=0, trace=0, riemann1=0, riemann2=0, riemann3=0, update=0)
+
+    def regions(n):
+        v = n[0] * n[1] * n[2]
+        g1 = (n[0] + 2) * (n[1] + 2) * (n[2] + 2)
+        g4 = (n[0] + 8) * (n[1] + 8) * (n[2] + 8)
+
+        def tbx(a, b):
+            m = list(n)
+            m[a] += 1
+            for c in range(3):
+                if c != a and c != b:
+                    m[c] += 2
+            return m[0] * m[1] * m[2]
+
+        def ebx(d):
+            m = list(n)
+            m[d] += 1
+            return m[0] * m[1] * m[2]
+
+        tdd = sum(tbx(d, d) for d in range(3))
+        tab = sum(tbx(a, b) for a in range(3) for b in range(3) if a != b)
+        eb = sum(ebx(d) for d in range(3))
+        return v, g1, g4, tdd, tab, eb
+
     for inst in cfg["instances"]:
-        # Q and Sborder live per instance on grow(domain,4) / grow(domain,1): the ghost kernel fills the domain halo
         nd = [h - l + 1 for l, h in zip(inst["dom_lo"], inst["dom_hi"])]
-        vd = nd[0] * nd[1] * nd[2]
-        g4d = (nd[0] + 8) * (nd[1] + 8) * (nd[2] + 8)
-        g1d = (nd[0] + 2) * (nd[1] + 2) * (nd[2] + 2)
+        vd, g1d, g4d, tdd, tab, eb = regions(nd)
         tot["ghost"] += 8 * ((g4d - vd) * NQF * 2 + (g1d - vd) * NV * 2)
+        tot["trace"] += 8 * (g4d * NQF + tdd * 2 * NQS + g1d)
+        tot["riemann1"] += 8 * (tdd * 2 * NQS + g4d * 2 + tdd * NTF)
+        # one thread per face of tbx[a][a] reads its two trace states once for both cross fluxes
+        tot["riemann2"] += 8 * (tdd * 2 * NQS + tdd * NTF + g4d * 2 + tab * NTF)
+        tot["riemann3"] += 8 * (eb * 2 * NQS + tab * NTF + g1d * NV + g1d + g4d * 2 + eb * (NV + 1))
+        tot["update"] += 8 * eb * (NV + 1)   # every final-flux record of the domain read once
         for lo, hi in inst["boxes"]:
-            n = [h - l + 1 for l, h in zip(lo, hi)]
-            v = n[0] * n[1] * n[2]
-            g1 = (n[0] + 2) * (n[1] + 2) * (n[2] + 2)
-            g4 = (n[0] + 8) * (n[1] + 8) * (n[2] + 8)
-
-            def tbx(a, b):
-                m = list(n)
-                m[a] += 1
-                for c in range(3):
-                    if c != a and c != b:
-                        m[c] += 2
-                return m[0] * m[1] * m[2]
-
-            def ebx(d):
-                m = list(n)
-                m[d] += 1
-                return m[0] * m[1] * m[2]
-
-            tdd = sum(tbx(d, d) for d in range(3))
-            tab = sum(tbx(a, b) for a in range(3) for b in range(3) if a != b)
-            eb = sum(ebx(d) for d in range(3))
+            v = regions([h - l + 1 for l, h in zip(lo, hi)])[0]
             tot["front"] += 8 * (v * NV * 2 + v * NV + v * NQF)
-            tot["trace"] += 8 * (g4 * NQF + tdd * 2 * NQS + g1)
-            tot["riemann1"] += 8 * (tdd * 2 * NQS + g4 * 2 + tdd * NTF)
-            # one thread per face of tbx[a][a] reads its two trace states once for both cross fluxes
-            tot["riemann2"] += 8 * (tdd * 2 * NQS + tdd * NTF + g4 * 2 + tab * NTF)
-            tot["riemann3"] += 8 * (eb * 2 * NQS + tab * NTF + g1 * NV + g1 + g4 * 2 + eb * (NV + 1))
-            tot["update"] += 8 * (v * NV * 2 + eb * (NV + 1))
+            tot["update"] += 8 * v * NV * 2
     return tot
 
 

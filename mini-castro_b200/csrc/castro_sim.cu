@@ -180,6 +180,7 @@ __device__ __forceinline__ long long ridx(const Reg& r, int i, int j, int k)
 
 struct SimDev {
     const BoxDev* boxes;
+    const BoxDev* dom;        // per instance: the domain box whose stage arrays hold the final fluxes
     const InstDev* inst;
     InstState* st;
     double* U;
@@ -954,10 +955,11 @@ __global__ void LB_EOS k_update(SimDev S, const Work* wl)
         Reg RX[3];
         const double* X[3];
         long long f0[3], f1[3];
+        const BoxDev& DB = S.dom[B.inst];   // final fluxes live on the domain's faces
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            RX[d] = make_reg(B.lo, B.hi, R_EBX, d);
-            X[d] = S.Fx + B.offFx[d];
+            RX[d] = make_reg(DB.lo, DB.hi, R_EBX, d);
+            X[d] = S.Fx + DB.offFx[d];
             f0[d] = ridx(RX[d], i, j, k);
             f1[d] = ridx(RX[d], i + (d == 0), j + (d == 1), k + (d == 2));
         }
@@ -1204,9 +1206,11 @@ struct castro_sim {
     std::vector<castro_problem> probs;
     std::vector<std::vector<int>> inst_boxes;   // global box ids per instance
     std::vector<BoxDev> hboxes;
+    std::vector<BoxDev> hdom;     // per instance: the domain as one box (stage arrays)
     std::vector<InstDev> hinst;
     std::vector<double> hdx;                    // 3 per instance
     BoxDev* dboxes = nullptr;
+    BoxDev* ddom = nullptr;
     InstDev* dinst = nullptr;
     InstState* dstate = nullptr;
     int* downer = nullptr;
@@ -1232,9 +1236,16 @@ struct castro_sim {
     SimDev dev() const
     {
         SimDev S;
-        S.boxes = dboxes; S.inst = dinst; S.st = dstate;
+        S.boxes = dboxes; S.dom = ddom; S.inst = dinst; S.st = dstate;
         S.U = U; S.Ub = Ub; S.Q = Q; S.Div = Div; S.Tr = Tr; S.F1 = F1; S.F2 = F2; S.Fx = Fx;
         S.owner = downer;
+        return S;
+    }
+    // the stage kernels' view: their work items name domain boxes
+    SimDev dev_dom() const
+    {
+        SimDev S = dev();
+        S.boxes = ddom;
         return S;
     }
 };
@@ -1265,17 +1276,22 @@ bool dalloc(T** p, size_t n, const char* what)
     return cuda_ok(cudaMalloc((void**)p, n * sizeof(T)), what);
 }
 
-void build_work(castro_sim* s, int kind, int nsub, int tbx_mode, Work** out, int* count)
+void build_work(const std::vector<BoxDev>& boxes, int kind, int nsub, int tbx_mode, Work** out, int* count)
 {
     // sub-major order: every box's items of one direction before the next, so
     // the blocks resident on an SM run the same code path
     std::vector<Work> w;
     for (int sub = 0; sub < nsub; ++sub) {
-        for (size_t b = 0; b < s->hboxes.size(); ++b) {
-            const BoxDev& B = s->hboxes[b];
+        for (size_t b = 0; b < boxes.size(); ++b) {
+            const BoxDev& B = boxes[b];
             int rs = sub;
             if (kind == R_TBX && tbx_mode == 0) rs = 4 * sub;
             long long np = npts_reg(B.lo, B.hi, kind, rs);
+            if (np > 2147483647LL - BLOCK) {   // work items carry 32-bit offsets
+                set_error(CASTRO_ERR_ARG, "castro_sim_create: a domain region exceeds 2^31 points");
+                *count = 0;
+                return;
+            }
             for (long long st = 0; st < np; st += BLOCK) {
                 Work it;
                 it.box = (int)b;
@@ -1333,15 +1349,15 @@ void build_ghost_work(castro_sim* s)
 template <int NS>
 void batched_step_kernels(castro_sim* s)
 {
-    SimDev S = s->dev();
+    SimDev S = s->dev(), Sd = s->dev_dom();
     cudaStream_t st = s->st;
     k_front<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid);
     k_ghost<NS><<<s->n_ghost, BLOCK, 0, st>>>(S, s->w_ghost);
-    k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(S, s->w_g1);
-    k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(S, s->w_trace);
-    k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(S, s->w_tbx);
-    k_riemann2<NS><<<s->n_tbx, BLOCK, R2Slot<NS>::BYTES, st>>>(S, s->w_tbx);
-    k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, st>>>(S, s->w_ebx);
+    k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(Sd, s->w_g1);
+    k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace);
+    k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(Sd, s->w_tbx);
+    k_riemann2<NS><<<s->n_tbx, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_tbx);
+    k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_ebx);
     k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid);
     k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0);
 }
@@ -1350,14 +1366,16 @@ template <int NS>
 void profile_kernel(castro_sim* s, const SimDev& S, int k)
 {
     cudaStream_t st = s->st;
+    SimDev Sd = S;
+    Sd.boxes = S.dom;
     switch (k) {
     case 0: k_front<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid); break;
     case 1: k_ghost<NS><<<s->n_ghost, BLOCK, 0, st>>>(S, s->w_ghost); break;
-    case 2: k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(S, s->w_g1); break;
-    case 3: k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(S, s->w_trace); break;
-    case 4: k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(S, s->w_tbx); break;
-    case 5: k_riemann2<NS><<<s->n_tbx, BLOCK, R2Slot<NS>::BYTES, st>>>(S, s->w_tbx); break;
-    case 6: k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, st>>>(S, s->w_ebx); break;
+    case 2: k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(Sd, s->w_g1); break;
+    case 3: k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace); break;
+    case 4: k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(Sd, s->w_tbx); break;
+    case 5: k_riemann2<NS><<<s->n_tbx, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_tbx); break;
+    case 6: k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_ebx); break;
     case 7: k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid); break;
     default: k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0); break;
     }
@@ -1662,10 +1680,24 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
         I.g = g;
         for (int d = 0; d < 3; ++d) I.on[d] = (D.dom_hi[d] - D.dom_lo[d] + 1) / g;
         I.owner_off = (long long)owner_all.size();
-        // Q and Sborder of the instance: one array each over grow(domain,4) / grow(domain,1)
-        const long long offQ_inst = oQ, offUb_inst = oUb;
-        oQ += npts_reg(I.dom_lo, I.dom_hi, R_G4, 0) * NQF;
-        oUb += npts_reg(I.dom_lo, I.dom_hi, R_G1, 0) * NV;
+        // The instance's domain box: Q and Sborder over grow(domain,4) / grow(domain,1),
+        // and the stage arrays of prep, trace and the three Riemann kernels over the
+        // domain's regions, so that each face is computed once for the whole domain
+        BoxDev P;
+        memset(&P, 0, sizeof P);
+        for (int d = 0; d < 3; ++d) { P.lo[d] = I.dom_lo[d]; P.hi[d] = I.dom_hi[d]; }
+        P.inst = in;
+        P.offQ = oQ; oQ += npts_reg(P.lo, P.hi, R_G4, 0) * NQF;
+        P.offUb = oUb; oUb += npts_reg(P.lo, P.hi, R_G1, 0) * NV;
+        P.offDiv = oDiv; oDiv += npts_reg(P.lo, P.hi, R_G1, 0) * 2;   // divu, flatn
+        for (int d = 0; d < 3; ++d) {
+            P.offTr[d] = oTr; oTr += npts_reg(P.lo, P.hi, R_TBX, 4 * d) * 2 * NQS;
+            P.offF1[d] = oF1; oF1 += npts_reg(P.lo, P.hi, R_TBX, 4 * d) * NTF;
+            P.offFx[d] = oFx; oFx += npts_reg(P.lo, P.hi, R_EBX, d) * (NV + 1);
+        }
+        for (int a = 0; a < 3; ++a)
+            for (int bb = 0; bb < 3; ++bb)
+                if (a != bb) { P.offF2[pair_index(a, bb)] = oF2; oF2 += npts_reg(P.lo, P.hi, R_TBX, 3 * a + bb) * NTF; }
         size_t nown = (size_t)I.on[0] * I.on[1] * I.on[2];
         owner_all.resize(owner_all.size() + nown, -1);
         for (int b = 0; b < D.nbox; ++b) {
@@ -1674,20 +1706,15 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
             for (int d = 0; d < 3; ++d) { B.lo[d] = D.box_lo[3 * b + d]; B.hi[d] = D.box_hi[3 * b + d]; }
             B.inst = in;
             B.offU = oU; oU += npts_reg(B.lo, B.hi, R_VALID, 0) * NV;
-            B.offUb = offUb_inst;
-            B.offQ = offQ_inst;
-            B.offDiv = oDiv; oDiv += npts_reg(B.lo, B.hi, R_G1, 0) * 2;   // divu, flatn
-            for (int d = 0; d < 3; ++d) {
-                B.offTr[d] = oTr; oTr += npts_reg(B.lo, B.hi, R_TBX, 4 * d) * 2 * NQS;
-                B.offF1[d] = oF1; oF1 += npts_reg(B.lo, B.hi, R_TBX, 4 * d) * NTF;
-                B.offFx[d] = oFx; oFx += npts_reg(B.lo, B.hi, R_EBX, d) * (NV + 1);
-            }
-            for (int a = 0; a < 3; ++a)
-                for (int bb = 0; bb < 3; ++bb) {
-                    if (a == bb) continue;
-                    int p = pair_index(a, bb);
-                    B.offF2[p] = oF2; oF2 += npts_reg(B.lo, B.hi, R_TBX, 3 * a + bb) * NTF;
-                }
+            // the instance's arrays; the stage-array offsets describe the domain's
+            // regions and are read through the domain box (a box's own only when
+            // it is the whole domain)
+            B.offUb = P.offUb;
+            B.offQ = P.offQ;
+            B.offDiv = P.offDiv;
+            for (int d = 0; d < 3; ++d) { B.offTr[d] = P.offTr[d]; B.offF1[d] = P.offF1[d]; B.offFx[d] = P.offFx[d]; }
+            for (int q = 0; q < 6; ++q) B.offF2[q] = P.offF2[q];
+            if (b == 0) P.offU = B.offU;
             int gid = (int)s->hboxes.size();
             ids.push_back(gid);
             s->hboxes.push_back(B);
@@ -1701,13 +1728,16 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
             if (owner_all[m] < 0) { set_error(CASTRO_ERR_ARG, "castro_sim_create: boxes do not cover the domain"); delete s; return nullptr; }
         s->inst_boxes.push_back(ids);
         s->hinst.push_back(I);
+        s->hdom.push_back(P);
     }
     s->nU = oU;
-    bool ok = dalloc(&s->dboxes, s->hboxes.size(), "boxes") && dalloc(&s->dinst, s->hinst.size(), "instances") &&
+    bool ok = dalloc(&s->dboxes, s->hboxes.size(), "boxes") && dalloc(&s->ddom, s->hdom.size(), "domain boxes") &&
+              dalloc(&s->dinst, s->hinst.size(), "instances") &&
               dalloc(&s->dstate, ninst, "state") && dalloc(&s->downer, owner_all.size(), "owner") &&
               dalloc(&s->U, oU, "U") && dalloc(&s->d_dtloc, 1, "dtloc") && dalloc(&s->d_dtbox, 1, "dtbox");
     if (ok) {
         cuda_ok(cudaMemcpy(s->dboxes, s->hboxes.data(), s->hboxes.size() * sizeof(BoxDev), cudaMemcpyHostToDevice), "boxes");
+        cuda_ok(cudaMemcpy(s->ddom, s->hdom.data(), s->hdom.size() * sizeof(BoxDev), cudaMemcpyHostToDevice), "domain boxes");
         cuda_ok(cudaMemcpy(s->dinst, s->hinst.data(), s->hinst.size() * sizeof(InstDev), cudaMemcpyHostToDevice), "inst");
         cuda_ok(cudaMemcpy(s->downer, owner_all.data(), owner_all.size() * sizeof(int), cudaMemcpyHostToDevice), "owner");
         std::vector<InstState> hs(ninst);
@@ -1721,12 +1751,13 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
     if (ok && mode == CASTRO_MODE_BATCHED) {
         ok = dalloc(&s->Ub, oUb, "Ub") && dalloc(&s->Q, oQ, "Q") && dalloc(&s->Div, oDiv, "Div") &&
              dalloc(&s->Tr, oTr, "Tr") && dalloc(&s->F1, oF1, "F1") && dalloc(&s->F2, oF2, "F2") && dalloc(&s->Fx, oFx, "Fx");
-        build_work(s, R_VALID, 1, -1, &s->w_valid, &s->n_valid);
-        build_work(s, R_G4, 1, -1, &s->w_g4, &s->n_g4);
-        build_work(s, R_G1, 1, -1, &s->w_g1, &s->n_g1);
-        build_work(s, R_SEG, 3, -1, &s->w_trace, &s->n_trace);
-        build_work(s, R_TBX, 3, 0, &s->w_tbx, &s->n_tbx);
-        build_work(s, R_EBX, 3, -1, &s->w_ebx, &s->n_ebx);
+        build_work(s->hboxes, R_VALID, 1, -1, &s->w_valid, &s->n_valid);
+        build_work(s->hboxes, R_G4, 1, -1, &s->w_g4, &s->n_g4);
+        // the stage kernels walk the domain boxes (launched with dev_dom())
+        build_work(s->hdom, R_G1, 1, -1, &s->w_g1, &s->n_g1);
+        build_work(s->hdom, R_SEG, 3, -1, &s->w_trace, &s->n_trace);
+        build_work(s->hdom, R_TBX, 3, 0, &s->w_tbx, &s->n_tbx);
+        build_work(s->hdom, R_EBX, 3, -1, &s->w_ebx, &s->n_ebx);
         build_ghost_work(s);
     }
     if (ok && mode == CASTRO_MODE_PLAIN) {
@@ -1742,7 +1773,7 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
         s->scratch_n = mx;
         ok = dalloc(&s->sb, nsb, "Sborder") && dalloc(&s->src, nsrc, "hydro_source") && dalloc(&s->scratch, mx, "scratch");
         // the work list of the valid region is still used by estdt of the sim API
-        build_work(s, R_VALID, 1, -1, &s->w_valid, &s->n_valid);
+        build_work(s->hboxes, R_VALID, 1, -1, &s->w_valid, &s->n_valid);
     }
     s->probs.resize(ninst);
     for (int in = 0; in < ninst; ++in) s->probs[in] = desc[in].prob;
@@ -1755,7 +1786,7 @@ void castro_sim_destroy(castro_sim* s)
     if (!s) return;
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     if (s->graph) cudaGraphDestroy(s->graph);
-    void* ptrs[] = {s->dboxes, s->dinst, s->dstate, s->downer, s->U, s->Ub, s->Q, s->Div, s->Tr, s->F1, s->F2, s->Fx,
+    void* ptrs[] = {s->dboxes, s->ddom, s->dinst, s->dstate, s->downer, s->U, s->Ub, s->Q, s->Div, s->Tr, s->F1, s->F2, s->Fx,
                     s->w_valid, s->w_g4, s->w_g1, s->w_trace, s->w_tbx, s->w_ebx, s->w_ghost, s->sb, s->src, s->scratch,
                     s->d_dtloc, s->d_dtbox};
     for (void* p : ptrs)
@@ -2059,13 +2090,13 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
     cudaStream_t cs = castro::stream();
     cuda_ok(cudaMemcpyAsync(s->dinst, &I, sizeof I, cudaMemcpyHostToDevice, cs), "box geometry");
     cuda_ok(cudaMemcpyAsync(s->dstate, &st, sizeof st, cudaMemcpyHostToDevice, cs), "box dt");
-    SimDev S = s->dev();
+    SimDev S = s->dev(), Sd = s->dev_dom();   // one box, which is the instance domain
     k_box_prim<NS><<<s->n_g4, BLOCK, 0, cs>>>(S, s->w_g4, make_fab(sb, sb_lo, sb_hi));
-    k_prep<NS><<<s->n_g1, BLOCK, 0, cs>>>(S, s->w_g1);
-    k_trace<NS><<<s->n_trace, BLOCK, 0, cs>>>(S, s->w_trace);
-    k_riemann1<NS><<<s->n_tbx, BLOCK, 0, cs>>>(S, s->w_tbx);
-    k_riemann2<NS><<<s->n_tbx, BLOCK, R2Slot<NS>::BYTES, cs>>>(S, s->w_tbx);
-    k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, cs>>>(S, s->w_ebx);
+    k_prep<NS><<<s->n_g1, BLOCK, 0, cs>>>(Sd, s->w_g1);
+    k_trace<NS><<<s->n_trace, BLOCK, 0, cs>>>(Sd, s->w_trace);
+    k_riemann1<NS><<<s->n_tbx, BLOCK, 0, cs>>>(Sd, s->w_tbx);
+    k_riemann2<NS><<<s->n_tbx, BLOCK, R2Slot<NS>::BYTES, cs>>>(Sd, s->w_tbx);
+    k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, cs>>>(Sd, s->w_ebx);
     k_box_source<NS><<<s->n_valid, BLOCK, 0, cs>>>(S, s->w_valid, make_fab(source, sr_lo, sr_hi));
     if (fo) {
         Fab F[3];
@@ -2240,7 +2271,7 @@ int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const
     k_noalloc_setup<<<(total + 127) / 128, 128, 0, cs>>>(B, I, st, NLs, dB, dI, dS, work);
     SimDev S;
     memset(&S, 0, sizeof S);
-    S.boxes = dB; S.inst = dI; S.st = dS;
+    S.boxes = dB; S.dom = dB; S.inst = dI; S.st = dS;   // the box is the instance domain
     S.Ub = pools; S.Q = pools; S.Div = pools; S.Tr = pools; S.F1 = pools; S.F2 = pools; S.Fx = pools;
     const Work* W = work;
     k_box_prim<NS><<<nblocks[NL_G4], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G4], make_fab(sb, sb_lo, sb_hi));
