@@ -79,6 +79,15 @@ constexpr int NG = 4;   // ghost zones of Sborder, Source/Castro_advance.cpp:37
 #endif
 constexpr int BLOCK = CASTRO_BLOCK;
 constexpr int TSEG = CASTRO_TRACE_SEG;   // zones of grow(bx,1) one trace thread walks along its direction
+// Passes of BLOCK consecutive faces one block of riemann2 / riemann3 makes in
+// turn on the batched path: the next pass's faces are the next row, whose
+// flux records the previous pass has brought into this SM's L1
+#ifndef CASTRO_R2_ROWS
+#define CASTRO_R2_ROWS 1
+#endif
+#ifndef CASTRO_R3_ROWS
+#define CASTRO_R3_ROWS 2
+#endif
 #define CASTRO_LB(M) __launch_bounds__(BLOCK, ((M) > 0 ? (M) : 1))
 #if CASTRO_MINB_EOS > 0
 #define LB_EOS CASTRO_LB(CASTRO_MINB_EOS)
@@ -194,24 +203,33 @@ struct SimDev {
     const int* owner;
 };
 
-// item of a work list -> (box, zone index); returns false for idle threads
-__device__ __forceinline__ bool work_point(const Work* wl, const SimDev& S, int kind, int subkind_tbx,
-                                          int& b, int& sub, Reg& R, int& i, int& j, int& k)
+// item of a work list -> (box, zone index) of the thread's point in pass rep
+// of the item (an item holds up to BLOCK points per pass); returns false for
+// idle threads
+__device__ __forceinline__ bool work_point_rep(const Work* wl, const SimDev& S, int kind, int subkind_tbx, int rep,
+                                              int& b, int& sub, Reg& R, int& i, int& j, int& k)
 {
     const Work w = wl[blockIdx.x];
-    if ((int)threadIdx.x >= w.count) return false;
+    const int tp = rep * BLOCK + (int)threadIdx.x;
+    if (tp >= w.count) return false;
     b = w.box;
     sub = w.sub;
     const BoxDev& B = S.boxes[b];
     int rs = sub;
     if (kind == R_TBX && subkind_tbx == 0) rs = 4 * sub;   // tbx[d][d]
     R = make_reg(B.lo, B.hi, kind, rs);
-    long long t = (long long)w.start + threadIdx.x;
+    long long t = (long long)w.start + tp;
     i = R.lx + (int)(t % R.nx);
     long long t2 = t / R.nx;
     j = R.ly + (int)(t2 % R.ny);
     k = R.lz + (int)(t2 / R.ny);
     return true;
+}
+
+__device__ __forceinline__ bool work_point(const Work* wl, const SimDev& S, int kind, int subkind_tbx, int& b, int& sub,
+                                          Reg& R, int& i, int& j, int& k)
+{
+    return work_point_rep(wl, S, kind, subkind_tbx, 0, b, sub, R, i, j, k);
 }
 
 // Q lives on grow(domain,4) and Sborder on grow(domain,1) of the box's
@@ -744,16 +762,18 @@ __global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
 {
     int bx, a, i, j, k;
     Reg R;
-    if (!work_point(wl, S, R_TBX, 0, bx, a, R, i, j, k)) return;
-    const BoxDev& B = S.boxes[bx];
-    const InstDev& I = S.inst[B.inst];
-    const double dt = S.st[B.inst].dt;
-    QLoader<NS> ld;
-    ld.base = S.Q + B.offQ;
-    ld.R = q_region(S.inst[B.inst]);
-    if (a == 0) cross_flux_both<NS, 0>(S, B, I, ld, i, j, k, dt);
-    else if (a == 1) cross_flux_both<NS, 1>(S, B, I, ld, i, j, k, dt);
-    else cross_flux_both<NS, 2>(S, B, I, ld, i, j, k, dt);
+    for (int rp = 0; rp < CASTRO_R2_ROWS; ++rp) {
+        if (!work_point_rep(wl, S, R_TBX, 0, rp, bx, a, R, i, j, k)) return;
+        const BoxDev& B = S.boxes[bx];
+        const InstDev& I = S.inst[B.inst];
+        const double dt = S.st[B.inst].dt;
+        QLoader<NS> ld;
+        ld.base = S.Q + B.offQ;
+        ld.R = q_region(S.inst[B.inst]);
+        if (a == 0) cross_flux_both<NS, 0>(S, B, I, ld, i, j, k, dt);
+        else if (a == 1) cross_flux_both<NS, 1>(S, B, I, ld, i, j, k, dt);
+        else cross_flux_both<NS, 2>(S, B, I, ld, i, j, k, dt);
+    }
 }
 
 // CASTRO_R3_STAGE: 0 plain loads, 1 the per-face operands of riemann3 that no
@@ -923,16 +943,18 @@ __global__ void LB_R3 k_riemann3(SimDev S, const Work* wl)
 {
     int bx, d, i, j, k;
     Reg R;
-    if (!work_point(wl, S, R_EBX, -1, bx, d, R, i, j, k)) return;
-    const BoxDev& B = S.boxes[bx];
-    const InstDev& I = S.inst[B.inst];
-    const double dt = S.st[B.inst].dt;
-    QLoader<NS> ld;
-    ld.base = S.Q + B.offQ;
-    ld.R = q_region(S.inst[B.inst]);
-    if (d == 0) riemann3_dir<NS, 0>(S, B, I, ld, i, j, k, dt);
-    else if (d == 1) riemann3_dir<NS, 1>(S, B, I, ld, i, j, k, dt);
-    else riemann3_dir<NS, 2>(S, B, I, ld, i, j, k, dt);
+    for (int rp = 0; rp < CASTRO_R3_ROWS; ++rp) {
+        if (!work_point_rep(wl, S, R_EBX, -1, rp, bx, d, R, i, j, k)) return;
+        const BoxDev& B = S.boxes[bx];
+        const InstDev& I = S.inst[B.inst];
+        const double dt = S.st[B.inst].dt;
+        QLoader<NS> ld;
+        ld.base = S.Q + B.offQ;
+        ld.R = q_region(S.inst[B.inst]);
+        if (d == 0) riemann3_dir<NS, 0>(S, B, I, ld, i, j, k, dt);
+        else if (d == 1) riemann3_dir<NS, 1>(S, B, I, ld, i, j, k, dt);
+        else riemann3_dir<NS, 2>(S, B, I, ld, i, j, k, dt);
+    }
 }
 
 // update: fill_hydro_source, Saxpy, clean_state (advance), clean_state
@@ -1219,8 +1241,8 @@ struct castro_sim {
     long long nU = 0;
     // work lists
     Work *w_valid = nullptr, *w_g4 = nullptr, *w_g1 = nullptr, *w_trace = nullptr, *w_tbx = nullptr,
-         *w_ebx = nullptr, *w_ghost = nullptr;
-    int n_valid = 0, n_g4 = 0, n_g1 = 0, n_trace = 0, n_tbx = 0, n_ebx = 0, n_ghost = 0;
+         *w_ebx = nullptr, *w_r2 = nullptr, *w_r3 = nullptr, *w_ghost = nullptr;
+    int n_valid = 0, n_g4 = 0, n_g1 = 0, n_trace = 0, n_tbx = 0, n_ebx = 0, n_r2 = 0, n_r3 = 0, n_ghost = 0;
     bool dt_ready = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -1276,7 +1298,8 @@ bool dalloc(T** p, size_t n, const char* what)
     return cuda_ok(cudaMalloc((void**)p, n * sizeof(T)), what);
 }
 
-void build_work(const std::vector<BoxDev>& boxes, int kind, int nsub, int tbx_mode, Work** out, int* count)
+void build_work(const std::vector<BoxDev>& boxes, int kind, int nsub, int tbx_mode, Work** out, int* count,
+                int passes = 1)
 {
     // sub-major order: every box's items of one direction before the next, so
     // the blocks resident on an SM run the same code path
@@ -1292,12 +1315,13 @@ void build_work(const std::vector<BoxDev>& boxes, int kind, int nsub, int tbx_mo
                 *count = 0;
                 return;
             }
-            for (long long st = 0; st < np; st += BLOCK) {
+            const long long chunk = (long long)BLOCK * passes;
+            for (long long st = 0; st < np; st += chunk) {
                 Work it;
                 it.box = (int)b;
                 it.sub = sub;
                 it.start = (int)st;
-                it.count = (int)std::min<long long>(BLOCK, np - st);
+                it.count = (int)std::min<long long>(chunk, np - st);
                 w.push_back(it);
             }
         }
@@ -1356,8 +1380,8 @@ void batched_step_kernels(castro_sim* s)
     k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(Sd, s->w_g1);
     k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace);
     k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(Sd, s->w_tbx);
-    k_riemann2<NS><<<s->n_tbx, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_tbx);
-    k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_ebx);
+    k_riemann2<NS><<<s->n_r2, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_r2);
+    k_riemann3<NS><<<s->n_r3, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_r3);
     k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid);
     k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0);
 }
@@ -1374,8 +1398,8 @@ void profile_kernel(castro_sim* s, const SimDev& S, int k)
     case 2: k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(Sd, s->w_g1); break;
     case 3: k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace); break;
     case 4: k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(Sd, s->w_tbx); break;
-    case 5: k_riemann2<NS><<<s->n_tbx, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_tbx); break;
-    case 6: k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_ebx); break;
+    case 5: k_riemann2<NS><<<s->n_r2, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_r2); break;
+    case 6: k_riemann3<NS><<<s->n_r3, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_r3); break;
     case 7: k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid); break;
     default: k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0); break;
     }
@@ -1758,6 +1782,8 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
         build_work(s->hdom, R_SEG, 3, -1, &s->w_trace, &s->n_trace);
         build_work(s->hdom, R_TBX, 3, 0, &s->w_tbx, &s->n_tbx);
         build_work(s->hdom, R_EBX, 3, -1, &s->w_ebx, &s->n_ebx);
+        build_work(s->hdom, R_TBX, 3, 0, &s->w_r2, &s->n_r2, CASTRO_R2_ROWS);
+        build_work(s->hdom, R_EBX, 3, -1, &s->w_r3, &s->n_r3, CASTRO_R3_ROWS);
         build_ghost_work(s);
     }
     if (ok && mode == CASTRO_MODE_PLAIN) {
@@ -1787,7 +1813,7 @@ void castro_sim_destroy(castro_sim* s)
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     if (s->graph) cudaGraphDestroy(s->graph);
     void* ptrs[] = {s->dboxes, s->ddom, s->dinst, s->dstate, s->downer, s->U, s->Ub, s->Q, s->Div, s->Tr, s->F1, s->F2, s->Fx,
-                    s->w_valid, s->w_g4, s->w_g1, s->w_trace, s->w_tbx, s->w_ebx, s->w_ghost, s->sb, s->src, s->scratch,
+                    s->w_valid, s->w_g4, s->w_g1, s->w_trace, s->w_tbx, s->w_ebx, s->w_r2, s->w_r3, s->w_ghost, s->sb, s->src, s->scratch,
                     s->d_dtloc, s->d_dtbox};
     for (void* p : ptrs)
         if (p) cudaFree(p);
