@@ -50,7 +50,7 @@ KNOBS = [
     ("CASTRO_R3_ROWS", [1, 2, 4]),
 ]
 DEFAULTS = {"CASTRO_BLOCK": 128, "CASTRO_MINB_EOS": 4, "CASTRO_MINB_R3": 0, "CASTRO_MINB_TRACE": 4,
-            "CASTRO_MINB_RIEMANN": 5, "CASTRO_TRACE_SEG": 5, "CASTRO_R2_STAGE": 1, "CASTRO_R3_STAGE": 0,
+            "CASTRO_MINB_RIEMANN": 5, "CASTRO_TRACE_SEG": 5, "CASTRO_R2_STAGE": 1, "CASTRO_R3_STAGE": 1,
             "CASTRO_R2_ROWS": 1, "CASTRO_R3_ROWS": 2}
 
 

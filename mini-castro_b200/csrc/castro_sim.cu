@@ -675,7 +675,9 @@ struct R2Slot {
 
 // F^{A|Bd} on the A-normal face (i,j,k) from its two trace states lq (minus
 // then plus, 2 x NQS), the side zones' gamma_1 (gl, gr) and sound speeds (cl,
-// cr): cross_flux's arithmetic, the record written to the F2 pool
+// cr): trans1 of each state with the Bd normal fluxes of its zone, then
+// compute_flux (Castro_hydro.cpp:228-255, 280-304); the record is written to
+// the F2 pool
 template <int NS, int A, int Bd>
 __device__ __forceinline__ void cross_flux_store(const SimDev& S, const BoxDev& B, int i, int j, int k, double cdtdx,
                                                  const double* lq, double gl, double gr, double cl, double cr)
