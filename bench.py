@@ -310,7 +310,8 @@ def run_b200(args, pkg, rank, world):
                    "zones": zones, "boxes": sum(len(i["boxes"]) for i in cfg["instances"]),
                    "path": "batched fused kernels, one CUDA graph per step",
                    "l2": "no flush: the state plus the per-step intermediates (~1.7 KB/zone) exceed the 126 MB L2",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}",
+                   "helm_table_sha256": pkg.helm_table.sha256(table)},
         "e2e": {"value": pkg.replicas.whole_job_rate(zones, args.steps, t_e2e * 1e3, world), "unit": "zone-updates/s",
                 "h2d_bytes_per_step": host_in.numel() * 8 / args.steps,
                 "d2h_bytes_per_step": host_out.numel() * 8 / args.steps,
@@ -517,7 +518,8 @@ def run_reference(args, pkg):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: Sedov blast, seeded Gaussian density perturbation, generated Helmholtz table",
-        "config": {"workload": workload_text(args), "zones": zones},
+        "config": {"workload": workload_text(args), "zones": zones,
+                   "helm_table_sha256": pkg.helm_table.sha256(table)},
         "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "port",
                          "sample": f"{args.steps} full coarse steps after {args.warmup} warm-up steps; the reference "
                                    "(Fortran + AMReX) cannot be compiled in this image, so its C restatement runs, "
