@@ -164,8 +164,15 @@ struct EosConst {   // per-call constants of the Newton loop
 
 // The electron-positron part plus radiation and ions at temperature temp,
 // eos.F90:195-518 (entropy, eta and xne are not formed: no hydro consumer).
-__device__ __forceinline__ void eos_eval(double temp, const EosConst& K, const DensityBasis& B, EosEval& r)
+// ENERGY_ONLY forms r.e and r.dedT alone -- all that a Newton iteration on e
+// (EOS_RE) reads -- skipping the density derivatives, the pressure-derivative
+// table and gamma_1; every quantity it does form is the full evaluation's,
+// operation for operation.
+enum { EVAL_FULL = 0, EVAL_ENERGY_ONLY = 1 };
+template <int WHAT>
+__device__ __forceinline__ void eos_eval_part(double temp, const EosConst& K, const DensityBasis& B, EosEval& r)
 {
+    constexpr bool FULL = WHAT == EVAL_FULL;
     const double den = K.den, deni = K.deni, ytot1 = K.ytot1, ye = K.ye, din = K.din;
     double tempi = 1.0 / temp;
     // radiation, :207-213
@@ -173,14 +180,14 @@ __device__ __forceinline__ void eos_eval(double temp, const EosConst& K, const D
     double dpraddd = 0.0;
     double dpraddt = 4.0 * prad * tempi;
     double erad = 3.0 * prad * deni;
-    double deraddd = -erad * deni;
+    double deraddd = FULL ? -erad * deni : 0.0;
     double deraddt = 3.0 * dpraddt * deni;
     // ions, :220-226
     double pion = c_eos.kergavo * ytot1 * den * temp;
-    double dpiondd = c_eos.kergavo * ytot1 * temp;
+    double dpiondd = FULL ? c_eos.kergavo * ytot1 * temp : 0.0;
     double dpiondt = c_eos.kergavo * ytot1 * den;
     double eion = 1.5 * pion * deni;
-    double deiondd = (1.5 * dpiondd - eion) * deni;
+    double deiondd = FULL ? (1.5 * dpiondd - eion) * deni : 0.0;
     double deiondt = 1.5 * dpiondt * deni;
 
     // temperature cell, :242-243
@@ -255,10 +262,10 @@ __device__ __forceinline__ void eos_eval(double temp, const EosConst& K, const D
              + fi[34] * w2d * w2mt + fi[35] * w2md * w2mt;
     };
     free_e = h5(st, B.si);
-    df_d = h5(st, B.dsi);
+    df_d = FULL ? h5(st, B.dsi) : 0.0;
     df_t = h5(dst, B.si);
     df_tt = h5(ddst, B.si);
-    df_dt = h5(dst, B.dsi);
+    df_dt = FULL ? h5(dst, B.dsi) : 0.0;
     (void)slot;
 #else
     // Factored biquintic: contract the temperature direction first for each of
@@ -287,12 +294,22 @@ __device__ __forceinline__ void eos_eval(double temp, const EosConst& K, const D
 #pragma unroll
         for (int di = 0; di < 2; ++di) {
             free_e = fma(g0[a][di], B.si.w[a][di], free_e);
-            df_d = fma(g0[a][di], B.dsi.w[a][di], df_d);
+            if (FULL) df_d = fma(g0[a][di], B.dsi.w[a][di], df_d);
             df_t = fma(g1[a][di], B.si.w[a][di], df_t);
             df_tt = fma(g2[a][di], B.si.w[a][di], df_tt);
-            df_dt = fma(g1[a][di], B.dsi.w[a][di], df_dt);
+            if (FULL) df_dt = fma(g1[a][di], B.dsi.w[a][di], df_dt);
         }
 #endif
+    if constexpr (!FULL) {
+        // :468-472, :476-478 for e and de/dT
+        double sele = -df_t * ye;
+        double dsepdt = -df_tt * ye;
+        double eele = ye * free_e + temp * sele;
+        double deepdt = temp * dsepdt;
+        r.e = erad + eion + eele;
+        r.dedT = deraddt + deiondt + deepdt;
+        return;
+    }
 
     // cubic pressure-derivative interpolation, :362-409
     double xs0t = xpsi0(xt), xs1t = xpsi1(xt) * dt, xs0mt = xpsi0(mxt), xs1mt = -xpsi1(mxt) * dt;
@@ -349,6 +366,11 @@ __device__ __forceinline__ void eos_eval(double temp, const EosConst& K, const D
     r.dedr = denerdd;
 }
 
+__device__ __forceinline__ void eos_eval(double temp, const EosConst& K, const DensityBasis& B, EosEval& r)
+{
+    eos_eval_part<EVAL_FULL>(temp, K, B, r);
+}
+
 struct EosResult {
     double T, p, e, gam1, cs, dedT, dpdT, dpde, dpdr_e;
 };
@@ -371,10 +393,22 @@ __device__ __forceinline__ EosResult eos_solve(double rho, double T, double v_wa
 
     bool converged = (MODE == EOS_RT);
     EosEval r;
+    // The reference evaluates the full EOS at the top of every iteration and
+    // leaves the loop right after the evaluation that follows convergence
+    // (eos.F90:520-552), so only that last evaluation's outputs are used; for
+    // EOS_RE the iterations before it form only e and de/dT.
+    bool full = false;
+    double temp_last = T;
     for (int iter = 1; iter <= 100; ++iter) {
         double temp = T;
-        eos_eval(temp, K, B, r);
-        if (converged) break;
+        temp_last = temp;
+        if (MODE != EOS_RE || converged) {
+            eos_eval(temp, K, B, r);
+            full = true;
+            if (converged) break;
+        } else {
+            eos_eval_part<EVAL_ENERGY_ONLY>(temp, K, B, r);
+        }
         double temp_old = temp;
         double v = (MODE == EOS_RE) ? r.e : r.p;
         double dvdx = (MODE == EOS_RE) ? r.dedT : r.dpdT;
@@ -385,6 +419,8 @@ __device__ __forceinline__ EosResult eos_solve(double rho, double T, double v_wa
         double error = fabs((temp - temp_old) / temp_old);
         if (error < 1.e-8) converged = true;
     }
+    // ended by the iteration limit: the last evaluation was a light one
+    if (MODE == EOS_RE && !(full && converged)) eos_eval(temp_last, K, B, r);
     if (!converged && c_eos.fail_count) atomicAdd(c_eos.fail_count, 1ULL);
     EosResult o;
     o.T = T;
