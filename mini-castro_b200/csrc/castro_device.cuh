@@ -378,8 +378,10 @@ struct EosResult {
 enum { EOS_RT = 1, EOS_RE = 2, EOS_RP = 3 };   // eos.F90:11-13
 
 // eos(input, state): the Newton inversion of eos.F90:181-574.  v_want is e for
-// EOS_RE and p for EOS_RP (ignored for EOS_RT).
-template <int MODE>
+// EOS_RE and p for EOS_RP (ignored for EOS_RT).  OUTPUTS = false when the
+// caller reads only T (and the input e or p back): the evaluation after
+// convergence, which only forms the other outputs, is then not made.
+template <int MODE, bool OUTPUTS = true>
 __device__ __forceinline__ EosResult eos_solve(double rho, double T, double v_want, double abar, double zbar)
 {
     EosConst K;
@@ -397,18 +399,21 @@ __device__ __forceinline__ EosResult eos_solve(double rho, double T, double v_wa
     // leaves the loop right after the evaluation that follows convergence
     // (eos.F90:520-552), so only that last evaluation's outputs are used; for
     // EOS_RE the iterations before it form only e and de/dT.
+    static_assert(OUTPUTS || MODE != EOS_RT, "an EOS_RT call exists for its outputs");
     bool full = false;
     double temp_last = T;
     for (int iter = 1; iter <= 100; ++iter) {
         double temp = T;
-        temp_last = temp;
-        if (MODE != EOS_RE || converged) {
-            eos_eval(temp, K, B, r);
-            full = true;
-            if (converged) break;
-        } else {
-            eos_eval_part<EVAL_ENERGY_ONLY>(temp, K, B, r);
+        if (converged) {
+            if (OUTPUTS) {
+                eos_eval(temp, K, B, r);
+                full = true;
+            }
+            break;
         }
+        temp_last = temp;
+        if (MODE == EOS_RE) eos_eval_part<EVAL_ENERGY_ONLY>(temp, K, B, r);
+        else eos_eval(temp, K, B, r);
         double temp_old = temp;
         double v = (MODE == EOS_RE) ? r.e : r.p;
         double dvdx = (MODE == EOS_RE) ? r.dedT : r.dpdT;
@@ -419,11 +424,17 @@ __device__ __forceinline__ EosResult eos_solve(double rho, double T, double v_wa
         double error = fabs((temp - temp_old) / temp_old);
         if (error < 1.e-8) converged = true;
     }
-    // ended by the iteration limit: the last evaluation was a light one
-    if (MODE == EOS_RE && !(full && converged)) eos_eval(temp_last, K, B, r);
+    // ended by the iteration limit: the reference's outputs are those of the
+    // last iteration's evaluation, here a light one
+    if (OUTPUTS && MODE == EOS_RE && !full) eos_eval(temp_last, K, B, r);
     if (!converged && c_eos.fail_count) atomicAdd(c_eos.fail_count, 1ULL);
     EosResult o;
     o.T = T;
+    if (!OUTPUTS) {
+        o.e = v_want;
+        o.p = o.gam1 = o.cs = o.dedT = o.dpdT = o.dpde = o.dpdr_e = 0.0;
+        return o;
+    }
     o.p = (MODE == EOS_RP) ? v_want : r.p;
     o.e = (MODE == EOS_RE) ? v_want : r.e;
     o.gam1 = r.gam1;
@@ -523,7 +534,7 @@ __device__ __forceinline__ void compute_temp_pt(double* u)
     double rhoInv = 1.0 / u[URHO];                                     // :280-291
     double abar, zbar;
     abar_zbar_cons<NS>(u, rhoInv, abar, zbar);
-    EosResult r = eos_solve<EOS_RE>(u[URHO], u[UTEMP], u[UEINT] * rhoInv, abar, zbar);
+    EosResult r = eos_solve<EOS_RE, false>(u[URHO], u[UTEMP], u[UEINT] * rhoInv, abar, zbar);   // reads T only
     u[UTEMP] = r.T;
     u[UEINT] = u[URHO] * r.e;
 }
