@@ -15,8 +15,9 @@ events, after warm-up, best of three runs).  The knobs are searched by
 coordinate descent from the current defaults: the block size, then the
 register budget of the EOS kernels (front, update), of the final Riemann
 kernel, of trace, and of the first two Riemann kernels, then the length of
-the zone segment one trace thread walks, which operands riemann2 and riemann3
-stage in shared memory, and how many passes of consecutive faces one block of
+the zone segment one trace thread walks, whether trace's second pass
+(transverse velocities and species) runs as a kernel of its own and its
+register budget, which operands riemann2 and riemann3 stage in shared memory, and how many passes of consecutive faces one block of
 riemann2 / riemann3 makes.  No knob changes any arithmetic, only register
 allocation, the distribution of zones over threads and blocks and the path of
 the loads, so every candidate computes the same results; the winner is written as
@@ -44,14 +45,17 @@ KNOBS = [
     ("CASTRO_MINB_TRACE", [0, 2, 3, 4]),
     ("CASTRO_MINB_RIEMANN", [0, 3, 4, 5, 6]),
     ("CASTRO_TRACE_SEG", [3, 5, 7, 9]),
+    ("CASTRO_TRACE_SPLIT", [0, 1]),
+    ("CASTRO_MINB_TRACE2", [0, 6, 8]),
     ("CASTRO_R2_STAGE", [0, 1]),
     ("CASTRO_R3_STAGE", [0, 1]),
     ("CASTRO_R2_ROWS", [1, 2, 4]),
     ("CASTRO_R3_ROWS", [1, 2, 4]),
 ]
-DEFAULTS = {"CASTRO_BLOCK": 128, "CASTRO_MINB_EOS": 4, "CASTRO_MINB_R3": 0, "CASTRO_MINB_TRACE": 4,
+DEFAULTS = {"CASTRO_BLOCK": 128, "CASTRO_MINB_EOS": 4, "CASTRO_MINB_R3": 0, "CASTRO_MINB_TRACE": 3,
             "CASTRO_MINB_RIEMANN": 5, "CASTRO_TRACE_SEG": 5, "CASTRO_R2_STAGE": 1, "CASTRO_R3_STAGE": 1,
-            "CASTRO_R2_ROWS": 1, "CASTRO_R3_ROWS": 2}
+            "CASTRO_R2_ROWS": 1, "CASTRO_R3_ROWS": 2,
+            "CASTRO_TRACE_SPLIT": 1, "CASTRO_MINB_TRACE2": 0}
 
 
 def key(cfg: dict) -> str:

@@ -69,7 +69,7 @@ constexpr int NG = 4;   // ghost zones of Sborder, Source/Castro_advance.cpp:37
 #define CASTRO_MINB_R3 0
 #endif
 #ifndef CASTRO_MINB_TRACE
-#define CASTRO_MINB_TRACE 4
+#define CASTRO_MINB_TRACE 3
 #endif
 #ifndef CASTRO_MINB_RIEMANN
 #define CASTRO_MINB_RIEMANN 5
@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(BLOCK) k_prep(SimDev S, const Work* wl)
 // walks rho, u_D, p, rhoe and gamma_c, which feed the characteristic
 // projection; pass 2 walks the transverse velocities and the species, one at a
 // time, each needing only the u_D wave.
-template <int NS, int D>
+template <int NS, int D, int PASSES>   // bit 0: pass 1, bit 1: pass 2
 __device__ __forceinline__ void trace_segment(const SimDev& S, const BoxDev& B, int i, int j, int k, double dtdx)
 {
     using F = QF<NS>;
@@ -457,6 +457,7 @@ __device__ __forceinline__ void trace_segment(const SimDev& S, const BoxDev& B, 
     // The loads of zone z+1 (s(z+3), flatn, c) are issued while zone z is
     // computed: s(z+3) lies at most at hi+4 and c at hi+2, inside grow(bx,4);
     // flatn exists up to hi+1 and is fetched only for a zone of the segment.
+    if constexpr ((PASSES & 1) != 0) {
     constexpr int NW = 5;
     constexpr int cw[NW] = {F::RHO, F::U + D, F::P, F::RE, F::GAMC};
     double wa[NW], wb[NW], wd[NW], we[NW], nxt[NW];
@@ -527,7 +528,10 @@ __device__ __forceinline__ void trace_segment(const SimDev& S, const BoxDev& B, 
         }
     }
 
+    }
+
     // pass 2: transverse velocities and species, the u_D wave only
+    if constexpr ((PASSES & 2) != 0) {
 #pragma unroll 1
     for (int v = 0; v < 2 + NS; ++v) {
         const int comp = v == 0 ? F::U + T1 : v == 1 ? F::U + T2 : F::X + (v - 2);
@@ -561,11 +565,11 @@ __device__ __forceinline__ void trace_segment(const SimDev& S, const BoxDev& B, 
             e = en;
         }
     }
+    }
 }
 
-// trace: one segment of grow(bx,1) in one direction per thread (work sub = direction)
-template <int NS>
-__global__ void LB_TRACE k_trace(SimDev S, const Work* wl)
+template <int NS, int PASSES>
+__device__ __forceinline__ void trace_item(const SimDev& S, const Work* wl)
 {
     int b, d, i, j, k;
     Reg R;
@@ -573,9 +577,36 @@ __global__ void LB_TRACE k_trace(SimDev S, const Work* wl)
     const BoxDev& B = S.boxes[b];
     const InstDev& I = S.inst[B.inst];
     const double dt = S.st[B.inst].dt;
-    if (d == 0) trace_segment<NS, 0>(S, B, i, j, k, dt / I.dx[0]);
-    else if (d == 1) trace_segment<NS, 1>(S, B, i, j, k, dt / I.dx[1]);
-    else trace_segment<NS, 2>(S, B, i, j, k, dt / I.dx[2]);
+    if (d == 0) trace_segment<NS, 0, PASSES>(S, B, i, j, k, dt / I.dx[0]);
+    else if (d == 1) trace_segment<NS, 1, PASSES>(S, B, i, j, k, dt / I.dx[1]);
+    else trace_segment<NS, 2, PASSES>(S, B, i, j, k, dt / I.dx[2]);
+}
+
+// trace: one segment of grow(bx,1) in one direction per thread (work sub =
+// direction).  With CASTRO_TRACE_SPLIT, pass 2 (transverse velocities and
+// species, a few registers per variable) runs as its own kernel k_trace2 at
+// the occupancy its registers allow instead of pass 1's.
+#ifndef CASTRO_TRACE_SPLIT
+#define CASTRO_TRACE_SPLIT 1
+#endif
+#ifndef CASTRO_MINB_TRACE2
+#define CASTRO_MINB_TRACE2 0
+#endif
+#if CASTRO_MINB_TRACE2 > 0
+#define LB_TRACE2 CASTRO_LB(CASTRO_MINB_TRACE2)
+#else
+#define LB_TRACE2 __launch_bounds__(BLOCK)
+#endif
+template <int NS>
+__global__ void LB_TRACE k_trace(SimDev S, const Work* wl)
+{
+    trace_item<NS, CASTRO_TRACE_SPLIT ? 1 : 3>(S, wl);
+}
+
+template <int NS>
+__global__ void LB_TRACE2 k_trace2(SimDev S, const Work* wl)
+{
+    trace_item<NS, 2>(S, wl);
 }
 
 // compute_flux on the face (i,j,k) normal to D: left zone i-e_D, right zone i
@@ -1381,6 +1412,7 @@ void batched_step_kernels(castro_sim* s)
     k_ghost<NS><<<s->n_ghost, BLOCK, 0, st>>>(S, s->w_ghost);
     k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(Sd, s->w_g1);
     k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace);
+    if (CASTRO_TRACE_SPLIT) k_trace2<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace);
     k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(Sd, s->w_tbx);
     k_riemann2<NS><<<s->n_r2, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_r2);
     k_riemann3<NS><<<s->n_r3, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_r3);
@@ -1399,6 +1431,7 @@ void profile_kernel(castro_sim* s, const SimDev& S, int k)
     case 1: k_ghost<NS><<<s->n_ghost, BLOCK, 0, st>>>(S, s->w_ghost); break;
     case 2: k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(Sd, s->w_g1); break;
     case 3: k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace); break;
+    case 9: k_trace2<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace); break;
     case 4: k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(Sd, s->w_tbx); break;
     case 5: k_riemann2<NS><<<s->n_r2, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_r2); break;
     case 6: k_riemann3<NS><<<s->n_r3, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_r3); break;
@@ -1653,7 +1686,7 @@ int step_impl(castro_sim* s)
         if (!cuda_ok(cudaGraphInstantiate(&s->gexec, s->graph, 0), "graph instantiate")) return castro_last_error();
     }
     cuda_ok(cudaGraphLaunch(s->gexec, s->st), "graph launch");
-    s->launches = 9;
+    s->launches = 9 + (CASTRO_TRACE_SPLIT ? 1 : 0);
     return castro_last_error();
 }
 
@@ -2122,6 +2155,7 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
     k_box_prim<NS><<<s->n_g4, BLOCK, 0, cs>>>(S, s->w_g4, make_fab(sb, sb_lo, sb_hi));
     k_prep<NS><<<s->n_g1, BLOCK, 0, cs>>>(Sd, s->w_g1);
     k_trace<NS><<<s->n_trace, BLOCK, 0, cs>>>(Sd, s->w_trace);
+    if (CASTRO_TRACE_SPLIT) k_trace2<NS><<<s->n_trace, BLOCK, 0, cs>>>(Sd, s->w_trace);
     k_riemann1<NS><<<s->n_tbx, BLOCK, 0, cs>>>(Sd, s->w_tbx);
     k_riemann2<NS><<<s->n_tbx, BLOCK, R2Slot<NS>::BYTES, cs>>>(Sd, s->w_tbx);
     k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, cs>>>(Sd, s->w_ebx);
@@ -2305,6 +2339,7 @@ int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const
     k_box_prim<NS><<<nblocks[NL_G4], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G4], make_fab(sb, sb_lo, sb_hi));
     k_prep<NS><<<nblocks[NL_G1], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G1]);
     k_trace<NS><<<nblocks[NL_TRACE], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TRACE]);
+    if (CASTRO_TRACE_SPLIT) k_trace2<NS><<<nblocks[NL_TRACE], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TRACE]);
     k_riemann1<NS><<<nblocks[NL_TBX], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TBX]);
     k_riemann2<NS><<<nblocks[NL_TBX], BLOCK, R2Slot<NS>::BYTES, cs>>>(S, W + NLs.first[NL_TBX]);
     k_riemann3<NS><<<nblocks[NL_EBX], BLOCK, R3Slot<NS>::BYTES, cs>>>(S, W + NLs.first[NL_EBX]);
@@ -2366,9 +2401,20 @@ void* castro_sim_stream(castro_sim* s) { return (void*)s->st; }
 int castro_sim_profile_step(castro_sim* s, double* ms, const char** names)
 {
     if (s->mode != CASTRO_MODE_BATCHED) { set_error(CASTRO_ERR_ARG, "castro_sim_profile_step: batched mode only"); return 0; }
-    static const char* kn[9] = {"front", "ghost", "prep", "trace", "riemann1", "riemann2", "riemann3", "update", "dt"};
-    cudaEvent_t ev[10];
-    for (int k = 0; k < 10; ++k) cudaEventCreate(&ev[k]);
+    // profile_kernel ids in step order; 9 = trace's pass 2 when it is a kernel of its own
+    static const int ids[10] = {0, 1, 2, 3, 9, 4, 5, 6, 7, 8};
+    static const char* kn[10] = {"front", "ghost", "prep", "trace", "trace2", "riemann1", "riemann2", "riemann3", "update",
+                                 "dt"};
+    const int NK = CASTRO_TRACE_SPLIT ? 10 : 9;
+    int order[10], m = 0;
+    const char* nm[10];
+    for (int q = 0; q < 10; ++q) {
+        if (ids[q] == 9 && !CASTRO_TRACE_SPLIT) continue;
+        order[m] = ids[q];
+        nm[m++] = kn[q];
+    }
+    cudaEvent_t ev[11];
+    for (int k = 0; k < 11; ++k) cudaEventCreate(&ev[k]);
     if (!s->dt_ready) {
         if (s->ns == 2) initial_dt_kernels<2>(s); else initial_dt_kernels<13>(s);
         s->dt_ready = true;
@@ -2376,20 +2422,20 @@ int castro_sim_profile_step(castro_sim* s, double* ms, const char** names)
     SimDev S = s->dev();
     cudaStream_t st = s->st;
     cudaEventRecord(ev[0], st);
-    for (int k = 0; k < 9; ++k) {
-        if (s->ns == 2) profile_kernel<2>(s, S, k); else profile_kernel<13>(s, S, k);
+    for (int k = 0; k < NK; ++k) {
+        if (s->ns == 2) profile_kernel<2>(s, S, order[k]); else profile_kernel<13>(s, S, order[k]);
         cudaEventRecord(ev[k + 1], st);
     }
-    cudaEventSynchronize(ev[9]);
-    for (int k = 0; k < 9; ++k) {
+    cudaEventSynchronize(ev[NK]);
+    for (int k = 0; k < NK; ++k) {
         float t = 0.f;
         cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
         ms[k] = t;
-        names[k] = kn[k];
+        names[k] = nm[k];
     }
-    for (int k = 0; k < 10; ++k) cudaEventDestroy(ev[k]);
+    for (int k = 0; k < 11; ++k) cudaEventDestroy(ev[k]);
     check_launch("castro_sim_profile_step");
-    return 9;
+    return NK;
 }
 
 long long castro_sim_eos_failures(castro_sim* s)

@@ -2,7 +2,7 @@
 against the oracle's level driver, through the C-ABI castro_sim_* entry points.
 
 * plain   : the reference's per-box launch sequence of the per-routine kernels;
-* batched : the fused nine-kernel step over every box of every instance,
+* batched : the fused ten-kernel step over every box of every instance,
             replayed as a CUDA graph.
 The exact build must reproduce the oracle bit for bit, dt included; the
 production build within the tolerances of gpu_harness (1e-12 per zone after
@@ -19,7 +19,7 @@ pytestmark = pytest.mark.gpu
 
 # front, ghost, prep, trace, riemann1, riemann2, riemann3, update, dt -- for
 # any number of boxes and instances
-FUSED_KERNELS_PER_STEP = 9
+FUSED_KERNELS_PER_STEP = 10
 
 _current = {}
 
