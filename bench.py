@@ -143,7 +143,7 @@ def kernel_bytes(cfg, nspec):
     the BoxArray; ghost fills each instance's domain halo; prep, trace and the
     three Riemann kernels walk each instance's domain as one region."""
     NV, NQF, NQS, NTF = 7 + nspec, 8 + nspec, 6 + nspec, 7 + nspec
-    tot = dict(front=0, ghost=0, trace=0, riemann1=0, riemann2=0, riemann3=0, update=0)
+    tot = dict(front=0, ghost=0, trace=0, trace2=0, riemann1=0, riemann2=0, riemann3=0, update=0)
 
     def regions(n):
         v = n[0] * n[1] * n[2]
@@ -172,7 +172,10 @@ def kernel_bytes(cfg, nspec):
         nd = [h - l + 1 for l, h in zip(inst["dom_lo"], inst["dom_hi"])]
         vd, g1d, g4d, tdd, tab, eb = regions(nd)
         tot["ghost"] += 8 * ((g4d - vd) * NQF * 2 + (g1d - vd) * NV * 2)
-        tot["trace"] += 8 * (g4d * NQF + tdd * 2 * NQS + g1d)
+        # trace pass 1: rho, u_D, p, rhoe, gamma_1, c and flatn -> 4 face-state components on each side;
+        # pass 2 (trace2): the two transverse velocities and the species (+ u_D, flatn) -> the rest
+        tot["trace"] += 8 * (g4d * 6 + tdd * 2 * 4 + g1d)
+        tot["trace2"] += 8 * (g4d * (3 + nspec) + tdd * 2 * (2 + nspec) + g1d)
         tot["riemann1"] += 8 * (tdd * 2 * NQS + g4d * 2 + tdd * NTF)
         # one thread per face of tbx[a][a] reads its two trace states once for both cross fluxes
         tot["riemann2"] += 8 * (tdd * 2 * NQS + tdd * NTF + g4d * 2 + tab * NTF)
