@@ -88,27 +88,28 @@ constexpr int TSEG = CASTRO_TRACE_SEG;   // zones of grow(bx,1) one trace thread
 #ifndef CASTRO_R3_ROWS
 #define CASTRO_R3_ROWS 2
 #endif
-#define CASTRO_LB(M) __launch_bounds__(BLOCK, ((M) > 0 ? (M) : 1))
-#if CASTRO_MINB_EOS > 0
-#define LB_EOS CASTRO_LB(CASTRO_MINB_EOS)
-#else
-#define LB_EOS __launch_bounds__(BLOCK)
+// The 13-species instantiations carry larger records and take their own
+// register budgets (CASTRO_MINB13_*, 0 = the compiler's choice; measured on the
+// 13-species reference problem): the budgets tuned for 2 species make the
+// Riemann kernels spill.
+#ifndef CASTRO_MINB13_EOS
+#define CASTRO_MINB13_EOS 4
 #endif
-#if CASTRO_MINB_R3 > 0
-#define LB_R3 CASTRO_LB(CASTRO_MINB_R3)
-#else
-#define LB_R3 __launch_bounds__(BLOCK)
+#ifndef CASTRO_MINB13_R3
+#define CASTRO_MINB13_R3 0
 #endif
-#if CASTRO_MINB_TRACE > 0
-#define LB_TRACE CASTRO_LB(CASTRO_MINB_TRACE)
-#else
-#define LB_TRACE __launch_bounds__(BLOCK)
+#ifndef CASTRO_MINB13_TRACE
+#define CASTRO_MINB13_TRACE 0
 #endif
-#if CASTRO_MINB_RIEMANN > 0
-#define LB_RIEMANN CASTRO_LB(CASTRO_MINB_RIEMANN)
-#else
-#define LB_RIEMANN __launch_bounds__(BLOCK)
+#ifndef CASTRO_MINB13_RIEMANN
+#define CASTRO_MINB13_RIEMANN 3
 #endif
+// minimum resident blocks per SM of a kernel templated on NS (0 = no bound)
+#define CASTRO_LB_NS(M2, M13) __launch_bounds__(BLOCK, (NS == 2 ? ((M2) > 0 ? (M2) : 0) : ((M13) > 0 ? (M13) : 0)))
+#define LB_EOS CASTRO_LB_NS(CASTRO_MINB_EOS, CASTRO_MINB13_EOS)
+#define LB_R3 CASTRO_LB_NS(CASTRO_MINB_R3, CASTRO_MINB13_R3)
+#define LB_TRACE CASTRO_LB_NS(CASTRO_MINB_TRACE, CASTRO_MINB13_TRACE)
+#define LB_RIEMANN CASTRO_LB_NS(CASTRO_MINB_RIEMANN, CASTRO_MINB13_RIEMANN)
 
 // ordered pair (a,b), a != b -> 0..5
 __host__ __device__ __forceinline__ int pair_index(int a, int b) { return a * 2 + (b > a ? b - 1 : b); }
@@ -592,11 +593,7 @@ __device__ __forceinline__ void trace_item(const SimDev& S, const Work* wl)
 #ifndef CASTRO_MINB_TRACE2
 #define CASTRO_MINB_TRACE2 0
 #endif
-#if CASTRO_MINB_TRACE2 > 0
-#define LB_TRACE2 CASTRO_LB(CASTRO_MINB_TRACE2)
-#else
-#define LB_TRACE2 __launch_bounds__(BLOCK)
-#endif
+#define LB_TRACE2 CASTRO_LB_NS(CASTRO_MINB_TRACE2, 0)
 template <int NS>
 __global__ void LB_TRACE k_trace(SimDev S, const Work* wl)
 {
