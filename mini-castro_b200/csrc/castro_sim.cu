@@ -814,6 +814,9 @@ __global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
 #ifndef CASTRO_R3_STAGE
 #define CASTRO_R3_STAGE 0
 #endif
+#ifndef CASTRO_R3_STAGE13
+#define CASTRO_R3_STAGE13 1
+#endif
 template <int NS>
 struct R3Slot {
     static constexpr int NQS = Dims<NS>::NQS, NVAR = Dims<NS>::NVAR;
@@ -823,7 +826,11 @@ struct R3Slot {
     static constexpr int DV = UB + 2 * NVAR;  // the four divu nodes of apply_av
     static constexpr int USED = DV + 4;
     static constexpr int STRIDE = USED | 1;   // odd: conflict-free 64-bit accesses
-    static constexpr bool ON = CASTRO_R3_STAGE > 0 && STRIDE * BLOCK * 8 * 4 + 4 * 1024 <= 228 * 1024;
+    // 2 species: while four blocks fit; 13 species (255 registers, two blocks
+    // per SM either way): while two blocks fit
+    static constexpr int FIT = NS == 2 ? 4 : 2;
+    static constexpr bool ON = (NS == 2 ? CASTRO_R3_STAGE > 0 : CASTRO_R3_STAGE13 > 0) &&
+                               STRIDE * BLOCK * 8 * FIT + FIT * 1024 <= 228 * 1024;
     static constexpr int BYTES = ON ? STRIDE * BLOCK * 8 : 0;
 };
 
