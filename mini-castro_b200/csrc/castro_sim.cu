@@ -1261,6 +1261,10 @@ struct castro_sim {
     int nvar = 9;
     int ninst = 0;
     cudaStream_t st = nullptr;
+    // second stream and events of the captured step: the two trace kernels,
+    // independent of each other, become parallel graph nodes
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::vector<castro_instance_desc> desc;
     std::vector<castro_problem> probs;
     std::vector<std::vector<int>> inst_boxes;   // global box ids per instance
@@ -1415,8 +1419,17 @@ void batched_step_kernels(castro_sim* s)
     k_front<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid);
     k_ghost<NS><<<s->n_ghost, BLOCK, 0, st>>>(S, s->w_ghost);
     k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(Sd, s->w_g1);
-    k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace);
-    if (CASTRO_TRACE_SPLIT) k_trace2<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace);
+    if (CASTRO_TRACE_SPLIT) {
+        // pass 2 writes face-state components pass 1 does not, from the same inputs
+        cudaEventRecord(s->ev_fork, st);
+        cudaStreamWaitEvent(s->st2, s->ev_fork, 0);
+        k_trace2<NS><<<s->n_trace, BLOCK, 0, s->st2>>>(Sd, s->w_trace);
+        k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace);
+        cudaEventRecord(s->ev_join, s->st2);
+        cudaStreamWaitEvent(st, s->ev_join, 0);
+    } else {
+        k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace);
+    }
     k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(Sd, s->w_tbx);
     k_riemann2<NS><<<s->n_r2, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_r2);
     k_riemann3<NS><<<s->n_r3, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_r3);
@@ -1715,6 +1728,9 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
     s->ninst = ninst;
     s->desc.assign(desc, desc + ninst);
     cuda_ok(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking), "stream create");
+    cuda_ok(cudaStreamCreateWithFlags(&s->st2, cudaStreamNonBlocking), "stream create");
+    cuda_ok(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming), "event create");
+    cuda_ok(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming), "event create");
     const int NQS = 6 + ns, NTF = 7 + ns, NQF = 8 + ns, NV = 7 + ns;
 
     long long oU = 0, oUb = 0, oQ = 0, oDiv = 0, oTr = 0, oF1 = 0, oF2 = 0, oFx = 0;
@@ -1857,6 +1873,9 @@ void castro_sim_destroy(castro_sim* s)
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->st) cudaStreamDestroy(s->st);
+    if (s->st2) cudaStreamDestroy(s->st2);
+    if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+    if (s->ev_join) cudaEventDestroy(s->ev_join);
     delete s;
 }
 
