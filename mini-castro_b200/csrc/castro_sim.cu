@@ -4,13 +4,18 @@
 // the per-routine entry points (Castro::advance, Source/Castro_advance.cpp:12-100,
 // with construct_hydro_source's 36 launches per box, Source/Castro_hydro.cpp:31-397).
 //
-// CASTRO_MODE_BATCHED advances every box of every instance with eight fused
+// CASTRO_MODE_BATCHED advances every box of every instance with ten fused
 // kernels per step, each walking a static work list of (box, region, chunk)
-// items built once per BoxArray, and replays the step as one CUDA graph:
+// items built once per BoxArray, and replays the step as one CUDA graph.
+// front and update walk the boxes (the state U keeps the reference's per-box
+// FABs); the stages in between walk each instance's domain as one region, so
+// every face state and flux is formed once for the whole domain:
 //
 //   front   : clean_state(S_old) -> clean_state(Sborder) -> ctoprim   (per valid zone)
-//   ghost   : Q / Sborder ghost zones gathered from the owning boxes (periodic or outflow)
-//   trace   : uflatten once, trace_ppm in x, y, z, divu                (per zone of grow(bx,1))
+//   ghost   : the domain halo of Q / Sborder by the boundary condition (periodic or outflow)
+//   prep    : divu at the nodes and uflatten per zone of grow(domain,1)
+//   trace   : trace_ppm pass 1 (rho, u_D, p, rhoe, gamma_1)  | two parallel graph nodes,
+//   trace2  : trace_ppm pass 2 (transverse u, species)       | segments of zones along x, y, z
 //   riemann1: compute_flux on tbx[d][d]                                 (normal fluxes)
 //   riemann2: trans1 + compute_flux on tbx[a][b], both b != a per face of tbx[a][a] (cross fluxes)
 //   riemann3: trans2 + compute_flux + apply_av + normalize_species_fluxes on ebx[d]
@@ -19,7 +24,8 @@
 //
 // Because clean_state, ctoprim and estdt are pointwise, a ghost zone's value
 // equals its source zone's value bit for bit, so primitive variables are formed
-// once per zone and gathered instead of recomputed in every box's halo.
+// once per zone and stored once per instance (Q over grow(domain,4)), where the
+// box halos read them in place.
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
