@@ -280,6 +280,18 @@ __global__ void __launch_bounds__(128, MINB) k_box_sum2_lb(BoxRange r, F f, doub
     }
 }
 
+// Register budgets (minimum resident blocks of 128 per SM) of the three
+// heaviest reverse kernels, chosen by timing the reverse sweep on B200
+#ifndef CASTRO_ADJ_MINB_TRACE
+#define CASTRO_ADJ_MINB_TRACE 4
+#endif
+#ifndef CASTRO_ADJ_MINB_TRANS1
+#define CASTRO_ADJ_MINB_TRANS1 4
+#endif
+#ifndef CASTRO_ADJ_MINB_TRANS2
+#define CASTRO_ADJ_MINB_TRANS2 3
+#endif
+
 // MINB = 0: no register budget
 template <int MINB = 0, class F>
 void launch_sum2(const char* what, const int* lo, const int* hi, F f, double* out0, double* out1)
@@ -396,7 +408,7 @@ template <int NS, int D>
 void trace_adj_dir(const int* lo, const int* hi, int vl, int vh, Fab Q, Fab QA, Fab QMB, Fab QPB, Fab QB, Fab QAB,
                    double dtdx, double* dtdxb)
 {
-    launch_sum<4>("trace_ppm_adj", lo, hi, [=] __device__(int i, int j, int k) -> double {
+    launch_sum<CASTRO_ADJ_MINB_TRACE>("trace_ppm_adj", lo, hi, [=] __device__(int i, int j, int k) -> double {
         constexpr int NQS = Dims<NS>::NQS;
         QLoad ld{Q, QA};
         AtomicSink sk{QB, QAB};
@@ -1289,7 +1301,7 @@ void trans1_adj_zones(castro_adj* a, int d, int t, double cdtdx, double* cdtdxb)
     Fab Q2M = P.qm[t][t].fab(), Q2P = P.qp[t][t].fab(), QA = P.qaux.fab(), F1 = P.F1[d].fab(), Q1 = P.G1[d].fab();
     Fab MOB = a->qmb[t][d].fab(), POB = a->qpb[t][d].fab(), MB = a->qmb[t][t].fab(), PB = a->qpb[t][t].fab();
     Fab QAB = a->qab.fab(), LF = a->T1L[d][t].fab(), RF = a->T1R[d][t].fab();
-    launch_sum<4>("trans1_adj zones", zb.lo, zb.hi, [=] __device__(int i, int j, int k) -> double {
+    launch_sum<CASTRO_ADJ_MINB_TRANS1>("trans1_adj zones", zb.lo, zb.hi, [=] __device__(int i, int j, int k) -> double {
         constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF;
         const int etx = t == 0, ety = t == 1, etz = t == 2;
         const int edx = d == 0, edy = d == 1, edz = d == 2;
@@ -1340,7 +1352,7 @@ void trans2_adj_zones(castro_adj* a, int d, double c2, double c3, double* c2b, d
     Fab MOB = a->qlb[d].fab(), POB = a->qrb[d].fab(), MB = a->qmb[d][d].fab(), PB = a->qpb[d][d].fab();
     Fab QAB = a->qab.fab(), L2 = a->T2L[d][0].fab(), R2 = a->T2R[d][0].fab(), L3 = a->T2L[d][1].fab(),
         R3 = a->T2R[d][1].fab();
-    launch_sum2<3>("trans2_adj zones", zb.lo, zb.hi, [=] __device__(int i, int j, int k) -> double2 {
+    launch_sum2<CASTRO_ADJ_MINB_TRANS2>("trans2_adj zones", zb.lo, zb.hi, [=] __device__(int i, int j, int k) -> double2 {
         constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF;
         const int e1x = d == 0, e1y = d == 1, e1z = d == 2;
         const int e2x = t1 == 0, e2y = t1 == 1, e2z = t1 == 2;
