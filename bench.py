@@ -241,10 +241,11 @@ def run_b200(args, pkg, rank, world):
     sim2.close()
     t_e2e = pkg.replicas.max_over_ranks(t_e2e, device="cuda")
 
-    # plain per-box path (the reference's launch structure), a few steps
-    plain = None
-    if rank == 0 and args.plain_steps > 0:
-        sim3 = pkg.make_sim(L, cfg, pkg.castro.MODE_PLAIN)
+    # the per-box paths, a few steps: the reference's launch structure through the per-routine
+    # entry points (plain), and the same host sequence with each box's hydro source from the
+    # coarse drop-in castro_construct_hydro_source_box (plain_box)
+    def time_per_box(mode):
+        sim3 = pkg.make_sim(L, cfg, mode)
         sim3.init_data()
         sim3.step(2)
         sim3.sync()
@@ -255,9 +256,15 @@ def run_b200(args, pkg, rank, world):
         p1.record(s3)
         p1.synchronize()
         pms = p0.elapsed_time(p1)
-        plain = {"value": zones * args.plain_steps / (pms * 1e-3), "ms_per_step": pms / args.plain_steps,
-                 "steps": args.plain_steps, "launches_per_step": sim3.launches_per_step()}
+        out = {"value": zones * args.plain_steps / (pms * 1e-3), "ms_per_step": pms / args.plain_steps,
+               "steps": args.plain_steps, "launches_per_step": sim3.launches_per_step()}
         sim3.close()
+        return out
+
+    plain = plain_box = None
+    if rank == 0 and args.plain_steps > 0:
+        plain = time_per_box(pkg.castro.MODE_PLAIN)
+        plain_box = time_per_box(pkg.castro.MODE_PLAIN_BOX)
 
     batched_cfg = None
     if args.batched_steps > 0:      # every rank: the instances are split over the ranks
@@ -326,6 +333,7 @@ def run_b200(args, pkg, rank, world):
                      "algorithmic_bytes_per_launch": kb[dom], "fp64_of_kernel": dom_fp64},
         "fp64": fp64,
         "plain_per_box": plain,
+        "plain_box_drop_in": plain_box,
         "batched_config": batched_cfg,
         "adjoint_config": adjoint_cfg,
         "adjoint_forward_ratio": adjoint_cfg["adjoint_forward_ratio"] if adjoint_cfg else None,

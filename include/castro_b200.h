@@ -240,8 +240,11 @@ int castro_construct_hydro_source_box_noalloc(const int* lo, const int* hi,
 typedef struct castro_sim castro_sim;
 
 enum { CASTRO_BC_PERIODIC = 0, CASTRO_BC_OUTFLOW = 1 };
-enum { CASTRO_MODE_PLAIN = 0,     /* per-box launches of the per-routine kernels, reference call sequence */
-       CASTRO_MODE_BATCHED = 1 }; /* fused kernels over every box of every instance, CUDA-graph replay */
+enum { CASTRO_MODE_PLAIN = 0,      /* per-box launches of the per-routine kernels, reference call sequence */
+       CASTRO_MODE_BATCHED = 1,    /* fused kernels over every box of every instance, CUDA-graph replay */
+       CASTRO_MODE_PLAIN_BOX = 2 };/* the reference call sequence per box, each box's hydro source from
+                                    * castro_construct_hydro_source_box (what a Castro host calling the
+                                    * coarse entry point from its MFIter loop runs) */
 
 typedef struct {
     int dom_lo[3], dom_hi[3];

@@ -17,7 +17,7 @@ LIBDIR = os.path.join(HERE, "lib")
 MAX_SPEC = 13
 
 BC_PERIODIC, BC_OUTFLOW = 0, 1
-MODE_PLAIN, MODE_BATCHED = 0, 1
+MODE_PLAIN, MODE_BATCHED, MODE_PLAIN_BOX = 0, 1, 2
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)

@@ -1663,7 +1663,13 @@ void plain_step(castro_sim* s)
             IBox bx{{B.lo[0], B.lo[1], B.lo[2]}, {B.hi[0], B.hi[1], B.hi[2]}};
             long long n = npts(bx) * s->nvar;
             cudaMemsetAsync(s->src + s->offSrc[b], 0, n * sizeof(double), s->st);   // hydro_source.setVal(0)
-            plain_hydro_box(s, bx, s->sb + s->offSb[b], s->src + s->offSrc[b], D.dom_lo, D.dom_hi, dx, dt);
+            if (s->mode == CASTRO_MODE_PLAIN_BOX) {
+                IBox g = grow(bx, NG, NG, NG);
+                castro_construct_hydro_source_box(bx.lo, bx.hi, s->sb + s->offSb[b], g.lo, g.hi, s->src + s->offSrc[b],
+                                                  bx.lo, bx.hi, nullptr, nullptr, nullptr, D.dom_lo, D.dom_hi, dx, dt);
+            } else {
+                plain_hydro_box(s, bx, s->sb + s->offSb[b], s->src + s->offSrc[b], D.dom_lo, D.dom_hi, dx, dt);
+            }
         }
         cudaMemcpyAsync(s->d_dtbox, &hs.dt, sizeof(double), cudaMemcpyHostToDevice, s->st);
         for (int b : s->inst_boxes[in]) {
@@ -1692,10 +1698,13 @@ void plain_step(castro_sim* s)
 template <int NS>
 int step_impl(castro_sim* s)
 {
-    if (s->mode == CASTRO_MODE_PLAIN) {
+    if (s->mode == CASTRO_MODE_PLAIN || s->mode == CASTRO_MODE_PLAIN_BOX) {
         plain_step<NS>(s);
+        // per box: estdt, fill_sborder, Saxpy and 4 x 4 clean kernels, plus construct_hydro_source's
+        // 36 per-routine launches or the fused box path's kernels (prim, prep, trace (x2), riemann1-3, source)
+        const int per_box = 19 + (s->mode == CASTRO_MODE_PLAIN ? 36 : 6 + (CASTRO_TRACE_SPLIT ? 2 : 1));
         s->launches = 0;
-        for (int in = 0; in < s->ninst; ++in) s->launches += 55 * (int)s->inst_boxes[in].size();
+        for (int in = 0; in < s->ninst; ++in) s->launches += per_box * (int)s->inst_boxes[in].size();
         return castro_last_error();
     }
     if (!s->dt_ready) {
@@ -1724,6 +1733,10 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
 {
     if (!table_ready()) { set_error(CASTRO_ERR_NO_TABLE, "castro_sim_create: eos_init has not run"); return nullptr; }
     if (ninst < 1 || !desc) { set_error(CASTRO_ERR_ARG, "castro_sim_create: no instances"); return nullptr; }
+    if (mode != CASTRO_MODE_PLAIN && mode != CASTRO_MODE_BATCHED && mode != CASTRO_MODE_PLAIN_BOX) {
+        set_error(CASTRO_ERR_ARG, "castro_sim_create: unknown mode");
+        return nullptr;
+    }
     int ns = nspec();
     if (ns != 2 && ns != 13) { set_error(CASTRO_ERR_NSPEC, "castro_sim_create: nspec"); return nullptr; }
     if (!(ns == 2 ? set_kernel_attributes<2>() : set_kernel_attributes<13>())) return nullptr;
@@ -1847,7 +1860,7 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
         build_work(s->hdom, R_EBX, 3, -1, &s->w_r3, &s->n_r3, CASTRO_R3_ROWS);
         build_ghost_work(s);
     }
-    if (ok && mode == CASTRO_MODE_PLAIN) {
+    if (ok && (mode == CASTRO_MODE_PLAIN || mode == CASTRO_MODE_PLAIN_BOX)) {
         long long nsb = 0, nsrc = 0, mx = 0;
         for (const BoxDev& B : s->hboxes) {
             s->offSb.push_back(nsb);
@@ -2147,8 +2160,11 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
             set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box: Sborder needs 4 ghost zones");
             return CASTRO_ERR_ARG;
         }
+    // the cached arrays and work lists depend on the box's shape only; its
+    // position is uploaded with every call, so that a host walking the boxes of
+    // a BoxArray reuses them
     bool same = g_box.s && g_box.ns == NS;
-    for (int d = 0; d < 3 && same; ++d) same = g_box.lo[d] == lo[d] && g_box.hi[d] == hi[d];
+    for (int d = 0; d < 3 && same; ++d) same = g_box.hi[d] - g_box.lo[d] == hi[d] - lo[d];
     if (!same) {
         if (g_box.s) castro_sim_destroy(g_box.s);
         g_box.s = nullptr;
@@ -2170,14 +2186,21 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
         g_box.ns = NS;
     }
     castro_sim* s = g_box.s;
-    // geometry and dt of this call
+    // position, geometry and dt of this call (the box is its own instance domain)
+    BoxDev B = s->hboxes[0];
     InstDev I = s->hinst[0];
-    for (int d = 0; d < 3; ++d) I.dx[d] = dx[d];
+    for (int d = 0; d < 3; ++d) {
+        B.lo[d] = lo[d]; B.hi[d] = hi[d];
+        I.dom_lo[d] = lo[d]; I.dom_hi[d] = hi[d];
+        I.dx[d] = dx[d];
+    }
     InstState st;
     memset(&st, 0, sizeof st);
     st.dt = dt;
     st.stop_time = -1.0;
     cudaStream_t cs = castro::stream();
+    cuda_ok(cudaMemcpyAsync(s->dboxes, &B, sizeof B, cudaMemcpyHostToDevice, cs), "box position");
+    cuda_ok(cudaMemcpyAsync(s->ddom, &B, sizeof B, cudaMemcpyHostToDevice, cs), "box position");
     cuda_ok(cudaMemcpyAsync(s->dinst, &I, sizeof I, cudaMemcpyHostToDevice, cs), "box geometry");
     cuda_ok(cudaMemcpyAsync(s->dstate, &st, sizeof st, cudaMemcpyHostToDevice, cs), "box dt");
     SimDev S = s->dev(), Sd = s->dev_dom();   // one box, which is the instance domain

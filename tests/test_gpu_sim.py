@@ -3,7 +3,9 @@ against the oracle's level driver, through the C-ABI castro_sim_* entry points.
 
 * plain   : the reference's per-box launch sequence of the per-routine kernels;
 * batched : the fused ten-kernel step over every box of every instance,
-            replayed as a CUDA graph.
+            replayed as a CUDA graph;
+* plain_box: the plain host sequence with each box's hydro source from the
+            coarse drop-in castro_construct_hydro_source_box.
 The exact build must reproduce the oracle bit for bit, dt included; the
 production build within the tolerances of gpu_harness (1e-12 per zone after
 one step, 1e-9 relative L1 after a run, dt within 1e-14).
@@ -70,7 +72,7 @@ WORKLOADS = {
 
 
 @pytest.mark.parametrize("exact", [True, False], ids=["exact", "fast"])
-@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "batched"])
+@pytest.mark.parametrize("mode", [0, 1, 2], ids=["plain", "batched", "plain_box"])
 @pytest.mark.parametrize("wl", list(WORKLOADS))
 def test_steps_match_oracle(pkg, table, oracle, wl, mode, exact):
     cfg = WORKLOADS[wl](pkg.configs)
