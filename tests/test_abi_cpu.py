@@ -31,6 +31,16 @@ def test_header_and_binding_agree(pkg):
     assert sorted(pkg.castro.ABI_SYMBOLS) == decl
 
 
+def test_enum_constants_agree(pkg):
+    """The binding's mode and boundary-condition constants are the header's enum values."""
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    enums = {k: int(v) for k, v in re.findall(r"(CASTRO_(?:MODE|BC)_\w+)\s*=\s*(\d+)", src)}
+    assert enums["CASTRO_MODE_PLAIN"] == pkg.castro.MODE_PLAIN
+    assert enums["CASTRO_MODE_BATCHED"] == pkg.castro.MODE_BATCHED
+    assert enums["CASTRO_MODE_PLAIN_BOX"] == pkg.castro.MODE_PLAIN_BOX
+    assert len({v for k, v in enums.items() if k.startswith("CASTRO_MODE_")}) == 3
+
+
 @pytest.mark.parametrize("exact", [False, True])
 def test_library_exports_every_symbol(pkg, exact):
     import importlib
