@@ -404,9 +404,12 @@ void divu_adj_impl(const int* lo, const int* hi, Fab DIVB, Fab QB, double dx0, d
     });
 }
 
+// FLB: when given, the adjoint of the zone's flattening coefficient is left in
+// FLB (stored by direction 0, added by the others) for one uflatten reverse
+// after the three directions (uflatten_adj_zones); else it is reversed here
 template <int NS, int D>
 void trace_adj_dir(const int* lo, const int* hi, int vl, int vh, Fab Q, Fab QA, Fab QMB, Fab QPB, Fab QB, Fab QAB,
-                   double dtdx, double* dtdxb)
+                   double dtdx, double* dtdxb, Fab FLB)
 {
     launch_sum<CASTRO_ADJ_MINB_TRACE>("trace_ppm_adj", lo, hi, [=] __device__(int i, int j, int k) -> double {
         constexpr int NQS = Dims<NS>::NQS;
@@ -420,18 +423,35 @@ void trace_adj_dir(const int* lo, const int* hi, int vl, int vh, Fab Q, Fab QA, 
         double flatn = uflatten(ld, i, j, k);
         double dtdxb_l = 0.0;
         double fb = trace_zone_adj<NS, D>(ld, sk, i, j, k, dtdx, flatn, hp ? qpb : nullptr, hm ? qmb : nullptr, dtdxb_l);
-        uflatten_adj(ld, sk, i, j, k, fb);
+        if (FLB.p) {
+            if (D == 0) FLB(i, j, k, 0) = fb;
+            else FLB(i, j, k, 0) += fb;
+        } else {
+            uflatten_adj(ld, sk, i, j, k, fb);
+        }
         return dtdxb_l;
     }, dtdxb);
 }
 
+// the flattening reverse of every zone with the adjoint summed over the three
+// trace directions (uflatten_adj is linear in that adjoint)
+template <int NS>
+void uflatten_adj_zones(const int* lo, const int* hi, Fab Q, Fab QA, Fab QB, Fab QAB, Fab FLB)
+{
+    launch_box("uflatten_adj zones", lo, hi, [=] __device__(int i, int j, int k) {
+        QLoad ld{Q, QA};
+        AtomicSink sk{QB, QAB};
+        uflatten_adj(ld, sk, i, j, k, FLB(i, j, k, 0));
+    });
+}
+
 template <int NS>
 void trace_adj_impl(const int* lo, const int* hi, const int* vlo, const int* vhi, int idir, Fab Q, Fab QA, Fab QMB,
-                    Fab QPB, Fab QB, Fab QAB, double dtdx, double* dtdxb)
+                    Fab QPB, Fab QB, Fab QAB, double dtdx, double* dtdxb, Fab FLB = Fab{})
 {
-    if (idir == 0) trace_adj_dir<NS, 0>(lo, hi, vlo[0], vhi[0], Q, QA, QMB, QPB, QB, QAB, dtdx, dtdxb);
-    else if (idir == 1) trace_adj_dir<NS, 1>(lo, hi, vlo[1], vhi[1], Q, QA, QMB, QPB, QB, QAB, dtdx, dtdxb);
-    else trace_adj_dir<NS, 2>(lo, hi, vlo[2], vhi[2], Q, QA, QMB, QPB, QB, QAB, dtdx, dtdxb);
+    if (idir == 0) trace_adj_dir<NS, 0>(lo, hi, vlo[0], vhi[0], Q, QA, QMB, QPB, QB, QAB, dtdx, dtdxb, FLB);
+    else if (idir == 1) trace_adj_dir<NS, 1>(lo, hi, vlo[1], vhi[1], Q, QA, QMB, QPB, QB, QAB, dtdx, dtdxb, FLB);
+    else trace_adj_dir<NS, 2>(lo, hi, vlo[2], vhi[2], Q, QA, QMB, QPB, QB, QAB, dtdx, dtdxb, FLB);
 }
 
 template <int NS>
@@ -882,6 +902,7 @@ struct castro_adj {
     Prim* P = nullptr;
     Arr V, area[3], vol, Vfinal;
     // adjoint
+    Arr flb;   // adjoint of the flattening coefficient, summed over the trace directions
     Arr Vb, Ab, Sbb, qb, qab, divb, qmb[3][3], qpb[3][3], F1b[3], G1b[3], F2b[3][3], G2b[3][3], qlb[3], qrb[3];
     Arr fluxb[3], qeb[3], srcb;
     // per-zone flux-record adjoints of the zone-based transverse reverses:
@@ -1026,8 +1047,7 @@ void adj_check(castro_adj* a, const char* stage)
     if (!adj_check_enabled()) return;
     std::vector<std::pair<const char*, const Arr*>> arrs = {
         {"Vb", &a->Vb}, {"Ab", &a->Ab}, {"Sbb", &a->Sbb}, {"qb", &a->qb}, {"qab", &a->qab}, {"divb", &a->divb},
-        {"srcb", &a->srcb}};
-    static const char* nm3[3] = {"x", "y", "z"};
+        {"srcb", &a->srcb}, {"flb", &a->flb}};
     for (int d = 0; d < 3; ++d) {
         arrs.push_back({"F1b", &a->F1b[d]}); arrs.push_back({"G1b", &a->G1b[d]});
         arrs.push_back({"qlb", &a->qlb[d]}); arrs.push_back({"qrb", &a->qrb[d]});
@@ -1526,7 +1546,8 @@ void reverse_step(castro_adj* a, const Arr& Vn, double dt)
     adj_stage(a, "riemann1");
     for (int d = 0; d < 3; ++d)
         trace_adj_impl<NS>(obx.lo, obx.hi, bx.lo, bx.hi, d, a->P->q.fab(), a->P->qaux.fab(), a->qmb[d][d].fab(),
-                           a->qpb[d][d].fab(), a->qb.fab(), a->qab.fab(), dt / a->dx[d], sc + d);
+                           a->qpb[d][d].fab(), a->qb.fab(), a->qab.fab(), dt / a->dx[d], sc + d, a->flb.fab());
+    uflatten_adj_zones<NS>(obx.lo, obx.hi, a->P->q.fab(), a->P->qaux.fab(), a->qb.fab(), a->qab.fab(), a->flb.fab());
     adj_stage(a, "trace");
     divu_adj_impl<NS>(obx.lo, obx.hi, a->divb.fab(), a->qb.fab(), a->dx[0], a->dx[1], a->dx[2]);
     adj_stage(a, "divu");
@@ -1823,7 +1844,7 @@ castro_adj* castro_adj_create(const castro_instance_desc* desc, int nsteps, int 
     for (Arr* r : {&a->V, &a->Vfinal, &a->Vb, &a->Ab, &a->srcb}) ok = ok && alloc_arr(a, *r, a->bx, NV);
     ok = ok && alloc_arr(a, a->vol, a->bx, 1);
     ok = ok && alloc_arr(a, a->Sbb, a->qbx, NV) && alloc_arr(a, a->qb, a->qbx, QV) && alloc_arr(a, a->qab, a->qbx, NQAUX);
-    ok = ok && alloc_arr(a, a->divb, a->obx, 1);
+    ok = ok && alloc_arr(a, a->divb, a->obx, 1) && alloc_arr(a, a->flb, a->obx, 1);
     for (int d = 0; d < 3 && ok; ++d) {
         for (int e = 0; e < 3 && ok; ++e) {
             ok = ok && alloc_arr(a, a->qmb[d][e], a->obx, QV) && alloc_arr(a, a->qpb[d][e], a->obx, QV);
