@@ -1057,7 +1057,6 @@ void adj_check(castro_adj* a, const char* stage)
             arrs.push_back({"F2b", &a->F2b[d][e]}); arrs.push_back({"G2b", &a->G2b[d][e]});
         }
     }
-    (void)nm3;
     const bool mags = adj_check_level() >= 2;
     std::string line;
     for (auto& pr : arrs) {
