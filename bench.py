@@ -188,6 +188,29 @@ def kernel_bytes(cfg, nspec):
     return tot
 
 
+def algorithmic_bytes_per_zone(nspec: int) -> int:
+    """HBM bytes one zone-update must move: the conserved state read once and
+    written once, 2 x NVAR x 8 B (144 B for 2 species, 320 B for 13)."""
+    return 2 * (7 + nspec) * 8
+
+
+def fp64_block(flops: float, ms: float, peak: float) -> dict:
+    ach = flops / (ms * 1e-3) / 1e12
+    return {"achieved": ach, "frac": ach / peak if peak else None}
+
+
+def path_roofline(zones, ms_per_step, bpz, hbm, flops_per_zone, fp64_peak) -> dict:
+    """Step-level roofline of a whole path: algorithmic bytes and the counted
+    FP64 work of the batched step per zone-update, over the path's step time."""
+    gbs = zones * bpz / (ms_per_step * 1e-3) / 1e9
+    out = {"hbm": {"achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                   "algorithmic_bytes_per_zone_update": bpz}}
+    if flops_per_zone:
+        out["fp64"] = dict(fp64_block(zones * flops_per_zone, ms_per_step, fp64_peak), peak=fp64_peak,
+                           unit="TFLOP/s", flops_per_zone_update=flops_per_zone)
+    return out
+
+
 def run_b200(args, pkg, rank, world):
     import numpy as np
     import torch
@@ -275,34 +298,49 @@ def run_b200(args, pkg, rank, world):
 
     value = pkg.replicas.whole_job_rate(zones, args.steps, ms, world)
     hbm, peak_kind = peaks()
+    fp64_peak = float(L.castro_measure_fp64_tflops())
+    step_ms = ms / args.steps
+    # algorithmic bytes per zone-update: the state read once and written once, 2 x NVAR x 8 B
+    alg_bpz = algorithmic_bytes_per_zone(nspec)
     kb = kernel_bytes(cfg, nspec)
     dom = max((k for k in prof if k in kb), key=lambda k: prof[k])
-    achieved = kb[dom] / (prof[dom] * 1e-3) / 1e9
-    fp64_peak = float(L.castro_measure_fp64_tflops())
-    flops_per_zone = None
+    fpz = {}
     fpz_path = os.path.join(ROOT, "profiles", "fp64_flops_per_zone.json")
     if os.path.exists(fpz_path):
         with open(fpz_path) as fp:
-            flops_per_zone = json.load(fp).get(args.workload)
-    fp64 = None
-    dom_fp64 = None   # the dominant kernel's own FP64 rate: what bounds the latency-bound stencil kernels
-    if os.path.exists(fpz_path):
-        with open(fpz_path) as fp:
-            per_kernel = json.load(fp).get(args.workload + "_per_kernel", {})
-        if per_kernel.get(dom):
-            ach = zones * per_kernel[dom] / (prof[dom] * 1e-3) / 1e12
-            dom_fp64 = {"achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
-                        "frac": ach / fp64_peak if fp64_peak else None,
-                        "flops_per_zone_update": per_kernel[dom]}
-    if flops_per_zone:
-        ach = zones * flops_per_zone / (ms / args.steps * 1e-3) / 1e12
-        fp64 = {"achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s", "frac": ach / fp64_peak if fp64_peak else None,
-                "flops_per_zone_update": flops_per_zone, "peak_kind": "measured (DFMA chain kernel, this run)"}
+            fpz = json.load(fp)
+    flops_per_zone = fpz.get(args.workload)
+    per_kernel = fpz.get(args.workload + "_per_kernel", {})
     traffic = None
     tr_path = os.path.join(ROOT, "profiles", "kernel_traffic.json")
     if os.path.exists(tr_path):
         with open(tr_path) as fp:
             traffic = json.load(fp).get(args.workload, {}).get(dom)
+    roof_fp64 = None
+    if flops_per_zone:
+        roof_fp64 = {"bound": "fp64", "kernel": dom, "unit": "TFLOP/s", "peak": fp64_peak,
+                     "peak_kind": "measured (DFMA-chain probe kernel, this run)",
+                     "flops_per_zone_update": flops_per_zone,
+                     "step": fp64_block(zones * flops_per_zone, step_ms, fp64_peak)}
+        if per_kernel.get(dom):
+            roof_fp64.update(fp64_block(zones * per_kernel[dom], prof[dom], fp64_peak))
+            roof_fp64["kernel_flops_per_zone_update"] = per_kernel[dom]
+    alg = zones * alg_bpz
+    roof = {"bound": "hbm", "kernel": dom, "unit": "GB/s", "peak": hbm, "peak_kind": peak_kind,
+            "algorithmic_bytes_per_zone_update": alg_bpz, "algorithmic_bytes_per_launch": alg,
+            "achieved": alg / (prof[dom] * 1e-3) / 1e9, "frac": alg / (prof[dom] * 1e-3) / 1e9 / hbm,
+            "traffic": traffic,
+            "step": {"achieved": alg / (step_ms * 1e-3) / 1e9, "frac": alg / (step_ms * 1e-3) / 1e9 / hbm},
+            "kernel_compulsory": {
+                "bytes_per_launch": kb[dom], "achieved": kb[dom] / (prof[dom] * 1e-3) / 1e9,
+                "frac": kb[dom] / (prof[dom] * 1e-3) / 1e9 / hbm,
+                "traffic_over_compulsory": traffic / kb[dom] if traffic else None,
+                "traffic_over_algorithmic": traffic / alg if traffic else None,
+                "note": "bytes of every array the kernel itself reads or writes, touched once (its "
+                        "intermediates included): how well it streams what the design keeps in HBM"}}
+    for leg in (plain, plain_box):
+        if leg:
+            leg["roofline"] = path_roofline(zones, leg["ms_per_step"], alg_bpz, hbm, flops_per_zone, fp64_peak)
     line = {
         "metric": METRIC,
         "value": value,
@@ -328,10 +366,8 @@ def run_b200(args, pkg, rank, world):
                 "call": "castro_sim_run_host (upload state, K steps, download state)"},
         "gpu_launches": launches,
         "kernel_ms": prof,
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": kb[dom], "fp64_of_kernel": dom_fp64},
-        "fp64": fp64,
+        "roofline_fp64": roof_fp64,
+        "roofline": roof,
         "plain_per_box": plain,
         "plain_box_drop_in": plain_box,
         "batched_config": batched_cfg,
@@ -479,51 +515,55 @@ def run_adjoint_config(pkg, args):
     return out
 
 
-def cpu_baseline(pkg, args, steps=2):
+ORACLE_BUILDS = {
+    "fast": "C oracle timing build (gcc -O3 -march=native, FMA contraction)",
+    "parity": "C oracle parity build (gcc -O2 -ffp-contract=off)",
+}
+
+
+def time_oracle(pkg, workload, steps, warmup, variant):
+    """Zone-updates/s of the oracle's level driver on all host cores: OpenMP
+    over MFIter-style (1024,16,16) tiles as Source/Castro.cpp:26."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
-    cfg = pkg.configs.WORKLOADS[args.workload]()
+    cfg = pkg.configs.WORKLOADS[workload]()
     A, Z = cfg["network"]
     table = pkg.helm_table.ensure_table()
-    O.network_init(A, Z)
-    O.eos_init(table)
+    O.network_init(A, Z, variant)
+    O.eos_init(table, variant)
     inst = cfg["instances"][0]
-    lev, prob = O.level_from_instance(inst, pkg.configs.nvar(cfg))
+    lev, prob = O.level_from_instance(inst, pkg.configs.nvar(cfg), variant)
     cores = os.cpu_count() or 1
     lev.set_threads(cores)
-    lev.coarse_step(-1.0)          # first step (initial dt) untimed
+    for _ in range(warmup):
+        lev.coarse_step(-1.0)
     t0 = time.perf_counter()
     for _ in range(steps):
         lev.coarse_step(-1.0)
     t = time.perf_counter() - t0
-    zones = pkg.configs.zones(cfg)
-    return {"value": zones * steps / t, "unit": "zone-updates/s", "cores": cores, "kind": "port",
-            "sample": f"{steps} coarse steps of the full {args.workload} level after the first step "
-                      f"({t:.1f} s), C oracle -O2, OpenMP over (1024,16,16) tiles"}
+    del lev
+    return pkg.configs.zones(cfg) * steps / t, t, cores
+
+
+def cpu_baseline(pkg, args, steps=5):
+    """Both oracle builds on the full workload: the timing build is the baseline's value."""
+    out = {}
+    for variant in ("fast", "parity"):
+        v, t, cores = time_oracle(pkg, args.workload, steps, 1, variant)
+        out[variant] = {"value": v, "seconds": t}
+    return {"value": out["fast"]["value"], "unit": "zone-updates/s", "cores": cores, "kind": "port",
+            "sample": f"{steps} coarse steps of the full {args.workload} level after one untimed step, "
+                      f"{ORACLE_BUILDS['fast']} ({out['fast']['seconds']:.1f} s); OpenMP over (1024,16,16) tiles",
+            "parity_build": {"value": out["parity"]["value"], "unit": "zone-updates/s",
+                             "sample": f"the same {steps} steps, {ORACLE_BUILDS['parity']} "
+                                       f"({out['parity']['seconds']:.1f} s)"}}
 
 
 def run_reference(args, pkg):
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-
-    cfg = pkg.configs.WORKLOADS[args.workload]()
-    A, Z = cfg["network"]
+    v, t, cores = time_oracle(pkg, args.workload, args.steps, args.warmup, "fast")
+    zones = pkg.configs.zones(pkg.configs.WORKLOADS[args.workload]())
     table = pkg.helm_table.ensure_table()
-    O.network_init(A, Z)
-    O.eos_init(table)
-    inst = cfg["instances"][0]
-    lev, prob = O.level_from_instance(inst, pkg.configs.nvar(cfg))
-    cores = os.cpu_count() or 1
-    lev.set_threads(cores)
-    for _ in range(args.warmup):
-        lev.coarse_step(-1.0)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        lev.coarse_step(-1.0)
-    t = time.perf_counter() - t0
-    zones = pkg.configs.zones(cfg)
-    v = zones * args.steps / t
     return {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "zone-updates/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
@@ -533,8 +573,8 @@ def run_reference(args, pkg):
                    "helm_table_sha256": pkg.helm_table.sha256(table)},
         "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": "port",
                          "sample": f"{args.steps} full coarse steps after {args.warmup} warm-up steps; the reference "
-                                   "(Fortran + AMReX) cannot be compiled in this image, so its C restatement runs, "
-                                   "OpenMP over MFIter-style (1024,16,16) tiles"},
+                                   "(Fortran + AMReX) cannot be compiled in this image, so its C restatement runs: "
+                                   f"{ORACLE_BUILDS['fast']}, OpenMP over MFIter-style (1024,16,16) tiles"},
         "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 

@@ -10,7 +10,7 @@
  *    Fortran order, component slowest; lo/hi/dx pointers are host pointers.
  *    The reference calls these per zone from inside an AMReX device lambda
  *    (Source/Castro.H:23-27); a host replacing the Fortran objects calls them
- *    once per box instead (see INTEGRATION.md).  Like the reference they
+ *    once per box instead.  Like the reference they
  *    return void; errors are reported through castro_last_error().
  *
  * 2. Coarse entry points with no reference counterpart at the ABI level but
@@ -205,7 +205,10 @@ int  castro_set_problem(const castro_problem* p);
  * fused: Sborder (grow(box,4), NVAR comps, already cleaned) -> source on the box
  * (accumulated into 'source', which the caller zeroes like hydro_source.setVal(0)).
  * fluxes_out[d] (optional, may be NULL): dt*F*A on the faces of the box
- * (store_flux).  Uses library-managed scratch. */
+ * (store_flux).  Uses library-managed scratch: one set per device, allocated on
+ * the first call and again when the box shape changes (so do not capture such a
+ * call in a CUDA graph); the box position, geometry and dt travel as kernel
+ * arguments, so calls for boxes of one shape allocate nothing. */
 int castro_construct_hydro_source_box(const int* lo, const int* hi,
                                       const double* sborder, const int* sb_lo, const int* sb_hi,
                                       double* source, const int* sr_lo, const int* sr_hi,
@@ -222,10 +225,13 @@ int castro_construct_hydro_source_box(const int* lo, const int* hi,
  * loads the library until the process exits), which fits a box of at most
  * 16^3 zones with 13 species or 21^3 zones with 2 species; larger boxes are
  * rejected with CASTRO_ERR_ARG before anything is launched.  The first call
- * on each device looks up the array's device address (cudaGetSymbolAddress);
- * make that first call before any stream capture.  Every call shares the
- * array and overwrites it: calls that overlap on the GPU (two streams, two
- * host threads) race and must be serialized by the caller.  Kernels launch on
+ * on each device (and species count) looks up the array's device address
+ * (cudaGetSymbolAddress) and sets the Riemann kernels' shared-memory limits,
+ * once, even when host threads make that first call together; make it before
+ * any stream capture.  Later calls make no CUDA runtime call but the kernel
+ * launches.  Every call shares the array and overwrites it: calls that overlap
+ * on the GPU (two streams, two host threads) race and must be serialized by
+ * the caller.  Kernels launch on
  * the library stream (castro_set_stream); allocates neither device nor host
  * memory on its success path. */
 int castro_construct_hydro_source_box_noalloc(const int* lo, const int* hi,

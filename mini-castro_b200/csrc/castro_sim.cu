@@ -33,6 +33,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -2141,14 +2142,28 @@ double castro_sim_blast_radius(castro_sim* s, int inst, double* blast_mass)
 
 }  // extern "C"
 
-// Library-managed scratch of castro_construct_hydro_source_box, reused while
-// the box shape does not change.
+// Library-managed scratch of castro_construct_hydro_source_box, one per
+// device, reused while the box shape does not change.
 struct BoxScratch {
     int lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
     int ns = 0;
     castro_sim* s = nullptr;
 };
-static BoxScratch g_box;
+constexpr int BOX_MAX_DEVICES = 64;
+static BoxScratch g_box[BOX_MAX_DEVICES];
+
+// Position, geometry and dt of one castro_construct_hydro_source_box call,
+// passed by value (kernel arguments are copied at launch, also into a graph
+// node under stream capture) into the cached sim's records.
+__global__ void k_box_setup(BoxDev B, InstDev I, InstState st, BoxDev* dB, BoxDev* dDom, InstDev* dI, InstState* dS)
+{
+    if (threadIdx.x == 0) {
+        *dB = B;
+        *dDom = B;
+        *dI = I;
+        *dS = st;
+    }
+}
 
 template <int NS>
 static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const int* sb_lo, const int* sb_hi,
@@ -2160,14 +2175,21 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
             set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box: Sborder needs 4 ghost zones");
             return CASTRO_ERR_ARG;
         }
+    int dev = 0;
+    if (!cuda_ok(cudaGetDevice(&dev), "castro_construct_hydro_source_box: cudaGetDevice")) return CASTRO_ERR_CUDA;
+    if (dev < 0 || dev >= BOX_MAX_DEVICES) {
+        set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box: device index beyond 63");
+        return CASTRO_ERR_ARG;
+    }
+    BoxScratch& gb = g_box[dev];
     // the cached arrays and work lists depend on the box's shape only; its
-    // position is uploaded with every call, so that a host walking the boxes of
+    // position is passed with every call, so that a host walking the boxes of
     // a BoxArray reuses them
-    bool same = g_box.s && g_box.ns == NS;
-    for (int d = 0; d < 3 && same; ++d) same = g_box.hi[d] - g_box.lo[d] == hi[d] - lo[d];
+    bool same = gb.s && gb.ns == NS;
+    for (int d = 0; d < 3 && same; ++d) same = gb.hi[d] - gb.lo[d] == hi[d] - lo[d];
     if (!same) {
-        if (g_box.s) castro_sim_destroy(g_box.s);
-        g_box.s = nullptr;
+        if (gb.s) castro_sim_destroy(gb.s);
+        gb.s = nullptr;
         castro_instance_desc D;
         memset(&D, 0, sizeof D);
         for (int d = 0; d < 3; ++d) {
@@ -2180,12 +2202,12 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
         D.box_hi = hi;
         castro_problem_defaults(&D.prob);
         D.stop_time = -1.0;
-        g_box.s = castro_sim_create(1, &D, CASTRO_MODE_BATCHED);
-        if (!g_box.s) return castro_last_error();
-        for (int d = 0; d < 3; ++d) { g_box.lo[d] = lo[d]; g_box.hi[d] = hi[d]; }
-        g_box.ns = NS;
+        gb.s = castro_sim_create(1, &D, CASTRO_MODE_BATCHED);
+        if (!gb.s) return castro_last_error();
+        for (int d = 0; d < 3; ++d) { gb.lo[d] = lo[d]; gb.hi[d] = hi[d]; }
+        gb.ns = NS;
     }
-    castro_sim* s = g_box.s;
+    castro_sim* s = gb.s;
     // position, geometry and dt of this call (the box is its own instance domain)
     BoxDev B = s->hboxes[0];
     InstDev I = s->hinst[0];
@@ -2199,10 +2221,7 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
     st.dt = dt;
     st.stop_time = -1.0;
     cudaStream_t cs = castro::stream();
-    cuda_ok(cudaMemcpyAsync(s->dboxes, &B, sizeof B, cudaMemcpyHostToDevice, cs), "box position");
-    cuda_ok(cudaMemcpyAsync(s->ddom, &B, sizeof B, cudaMemcpyHostToDevice, cs), "box position");
-    cuda_ok(cudaMemcpyAsync(s->dinst, &I, sizeof I, cudaMemcpyHostToDevice, cs), "box geometry");
-    cuda_ok(cudaMemcpyAsync(s->dstate, &st, sizeof st, cudaMemcpyHostToDevice, cs), "box dt");
+    k_box_setup<<<1, 32, 0, cs>>>(B, I, st, s->dboxes, s->ddom, s->dinst, s->dstate);
     SimDev S = s->dev(), Sd = s->dev_dom();   // one box, which is the instance domain
     k_box_prim<NS><<<s->n_g4, BLOCK, 0, cs>>>(S, s->w_g4, make_fab(sb, sb_lo, sb_hi));
     k_prep<NS><<<s->n_g1, BLOCK, 0, cs>>>(Sd, s->w_g1);
@@ -2245,8 +2264,13 @@ constexpr long long NOALLOC_META_BYTES = 65536;   // BoxDev, InstDev, InstState,
 // Every GPU that loads the library holds this array until the process exits.
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
 
-// device address of g_noalloc_scratch per device, from cudaGetSymbolAddress
+// device address of g_noalloc_scratch per device, from cudaGetSymbolAddress,
+// looked up once per device together with the kernel attributes of each
+// species count (std::call_once: host threads making their first call on a
+// device together do it once and all see the result)
 double* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+std::once_flag g_noalloc_once[NOALLOC_MAX_DEVICES][2];
+int g_noalloc_setup_rc[NOALLOC_MAX_DEVICES][2] = {};
 
 enum { NL_VALID = 0, NL_G4, NL_G1, NL_TRACE, NL_TBX, NL_EBX, NL_COUNT };
 
@@ -2298,18 +2322,26 @@ int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const
         }
     int dev = 0;
     if (!cuda_ok(cudaGetDevice(&dev), "castro_construct_hydro_source_box_noalloc: cudaGetDevice")) return CASTRO_ERR_CUDA;
-    if (!set_kernel_attributes<NS>()) return CASTRO_ERR_CUDA;
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
         set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box_noalloc: device index beyond 63");
         return CASTRO_ERR_ARG;
     }
-    if (!g_noalloc_addr[dev]) {
-        // once per device: the host-side name of a __device__ array is only a
-        // stand-in; kernels need its device address
+    const int nsi = NS == 2 ? 0 : 1;
+    std::call_once(g_noalloc_once[dev][nsi], [dev, nsi]() {
+        // the host-side name of a __device__ array is only a stand-in; kernels
+        // need its device address on this device
         void* p = nullptr;
-        if (!cuda_ok(cudaGetSymbolAddress(&p, g_noalloc_scratch), "castro_construct_hydro_source_box_noalloc: cudaGetSymbolAddress"))
-            return CASTRO_ERR_CUDA;
+        if (!set_kernel_attributes<NS>() ||
+            !cuda_ok(cudaGetSymbolAddress(&p, g_noalloc_scratch),
+                     "castro_construct_hydro_source_box_noalloc: cudaGetSymbolAddress")) {
+            g_noalloc_setup_rc[dev][nsi] = CASTRO_ERR_CUDA;
+            return;
+        }
         g_noalloc_addr[dev] = static_cast<double*>(p);
+    });
+    if (g_noalloc_setup_rc[dev][nsi] != 0 || !g_noalloc_addr[dev]) {
+        set_error(CASTRO_ERR_CUDA, "castro_construct_hydro_source_box_noalloc: device set-up failed on this device");
+        return CASTRO_ERR_CUDA;
     }
     double* base = g_noalloc_addr[dev];
 

@@ -14,6 +14,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+# the two builds of oracle/Makefile: "parity" (non-contracting, the checker) and
+# "fast" (-O3 -march=native with FMA contraction: the timed CPU baseline, and an
+# independent rounding of the same algorithm for the noise classification)
+LIB_PATHS = {"parity": LIB_PATH, "fast": os.path.join(HERE, "_build", "liboracle_fast.so")}
 
 MAX_SPEC = 13
 EOS_INPUT_RT, EOS_INPUT_RE, EOS_INPUT_RP = 1, 2, 3
@@ -48,46 +52,59 @@ class ProbT(C.Structure):
 
 def build(force: bool = False) -> str:
     src = os.path.join(HERE, "castro_oracle.c")
-    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+    stale = [p for p in LIB_PATHS.values()
+             if not os.path.exists(p) or os.path.getmtime(p) < os.path.getmtime(src)]
+    if force or stale:
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
 
 
 _lib = None
+_variants: dict = {}
 
 
-def lib():
+def lib(variant: str = "parity"):
+    """The oracle library: the parity build (default) or the "fast" timing build."""
     global _lib
+    if variant != "parity":
+        if variant not in _variants:
+            build()
+            _variants[variant] = _bind(C.CDLL(LIB_PATHS[variant]))
+        return _variants[variant]
     if _lib is None:
         build()
-        L = C.CDLL(LIB_PATH)
-        L.oracle_network_init.argtypes = [C.c_int, _dp, _dp]
-        L.oracle_eos_init.argtypes = [C.c_char_p]
-        L.oracle_eos.argtypes = [C.c_int, C.POINTER(EosT)]
-        L.oracle_set_problem.argtypes = [C.POINTER(ProbT)]
-        L.oracle_level_create.restype = C.c_void_p
-        L.oracle_level_create.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _dp, _dp, C.c_int]
-        L.oracle_level_destroy.argtypes = [C.c_void_p]
-        L.oracle_level_state.restype = _dp
-        L.oracle_level_state.argtypes = [C.c_void_p, C.c_int]
-        L.oracle_level_set_threads.argtypes = [C.c_void_p, C.c_int]
-        L.oracle_level_init_data.argtypes = [C.c_void_p]
-        L.oracle_level_est_time_step.restype = C.c_double
-        L.oracle_level_est_time_step.argtypes = [C.c_void_p]
-        L.oracle_level_clean_state.argtypes = [C.c_void_p]
-        L.oracle_level_advance.argtypes = [C.c_void_p, C.c_double]
-        L.oracle_level_coarse_step.restype = C.c_double
-        L.oracle_level_coarse_step.argtypes = [C.c_void_p, C.c_double]
-        L.oracle_level_time.restype = C.c_double
-        L.oracle_level_time.argtypes = [C.c_void_p]
-        L.oracle_level_dt.restype = C.c_double
-        L.oracle_level_dt.argtypes = [C.c_void_p]
-        L.oracle_level_steps.restype = C.c_int
-        L.oracle_level_steps.argtypes = [C.c_void_p]
-        L.oracle_level_blast_radius.restype = C.c_double
-        L.oracle_level_blast_radius.argtypes = [C.c_void_p, _dp]
-        _lib = L
+        _lib = _bind(C.CDLL(LIB_PATH))
     return _lib
+
+
+def _bind(L):
+    """Argument and result types of the entry points the bindings call."""
+    L.oracle_network_init.argtypes = [C.c_int, _dp, _dp]
+    L.oracle_eos_init.argtypes = [C.c_char_p]
+    L.oracle_eos.argtypes = [C.c_int, C.POINTER(EosT)]
+    L.oracle_set_problem.argtypes = [C.POINTER(ProbT)]
+    L.oracle_level_create.restype = C.c_void_p
+    L.oracle_level_create.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _dp, _dp, C.c_int]
+    L.oracle_level_destroy.argtypes = [C.c_void_p]
+    L.oracle_level_state.restype = _dp
+    L.oracle_level_state.argtypes = [C.c_void_p, C.c_int]
+    L.oracle_level_set_threads.argtypes = [C.c_void_p, C.c_int]
+    L.oracle_level_init_data.argtypes = [C.c_void_p]
+    L.oracle_level_est_time_step.restype = C.c_double
+    L.oracle_level_est_time_step.argtypes = [C.c_void_p]
+    L.oracle_level_clean_state.argtypes = [C.c_void_p]
+    L.oracle_level_advance.argtypes = [C.c_void_p, C.c_double]
+    L.oracle_level_coarse_step.restype = C.c_double
+    L.oracle_level_coarse_step.argtypes = [C.c_void_p, C.c_double]
+    L.oracle_level_time.restype = C.c_double
+    L.oracle_level_time.argtypes = [C.c_void_p]
+    L.oracle_level_dt.restype = C.c_double
+    L.oracle_level_dt.argtypes = [C.c_void_p]
+    L.oracle_level_steps.restype = C.c_int
+    L.oracle_level_steps.argtypes = [C.c_void_p]
+    L.oracle_level_blast_radius.restype = C.c_double
+    L.oracle_level_blast_radius.argtypes = [C.c_void_p, _dp]
+    return L
 
 
 def ptr(a: np.ndarray):
@@ -103,14 +120,14 @@ def dvec(v):
     return (C.c_double * len(v))(*[float(x) for x in v])
 
 
-def network_init(aion, zion):
+def network_init(aion, zion, variant: str = "parity"):
     a = np.ascontiguousarray(aion, dtype=np.float64)
     z = np.ascontiguousarray(zion, dtype=np.float64)
-    assert lib().oracle_network_init(len(a), ptr(a), ptr(z)) == 0
+    assert lib(variant).oracle_network_init(len(a), ptr(a), ptr(z)) == 0
 
 
-def eos_init(path: str):
-    rc = lib().oracle_eos_init(path.encode())
+def eos_init(path: str, variant: str = "parity"):
+    rc = lib(variant).oracle_eos_init(path.encode())
     if rc != 0:
         raise RuntimeError(f"oracle_eos_init({path}) failed: {rc}")
 
@@ -182,78 +199,81 @@ class Problem:
                 self.s.pert_hi[d] = pert_lo[d] + self.pert.shape[d] - 1
             self.s.pert_amp = pert_amp
 
-    def install(self):
-        lib().oracle_set_problem(C.byref(self.s))
+    def install(self, variant: str = "parity"):
+        lib(variant).oracle_set_problem(C.byref(self.s))
 
 
 class Level:
     """A single AMR level (BoxArray + state) advanced by the oracle."""
 
-    def __init__(self, boxes, dom_lo, dom_hi, problo, probhi, bc, nvar):
+    def __init__(self, boxes, dom_lo, dom_hi, problo, probhi, bc, nvar, variant: str = "parity"):
         self.boxes = [(tuple(l), tuple(h)) for l, h in boxes]
         los = np.array([b[0] for b in self.boxes], dtype=np.int32).reshape(-1)
         his = np.array([b[1] for b in self.boxes], dtype=np.int32).reshape(-1)
         self.nvar = nvar
-        self.h = lib().oracle_level_create(len(self.boxes), los.ctypes.data_as(_ip), his.ctypes.data_as(_ip),
+        self.L = lib(variant)
+        self.h = self.L.oracle_level_create(len(self.boxes), los.ctypes.data_as(_ip), his.ctypes.data_as(_ip),
                                            ivec(dom_lo), ivec(dom_hi), dvec(problo), dvec(probhi), int(bc))
 
     def __del__(self):
-        if getattr(self, "h", None) and _lib is not None:
-            _lib.oracle_level_destroy(self.h)
+        if getattr(self, "h", None) and getattr(self, "L", None) is not None:
+            self.L.oracle_level_destroy(self.h)
             self.h = None
 
     def state(self, b) -> np.ndarray:
         lo, hi = self.boxes[b]
         shape = tuple(h - l + 1 for l, h in zip(lo, hi)) + (self.nvar,)
         n = int(np.prod(shape))
-        p = lib().oracle_level_state(self.h, b)
+        p = self.L.oracle_level_state(self.h, b)
         return np.ctypeslib.as_array(p, shape=(n,)).reshape(shape, order="F")
 
     def set_threads(self, n):
-        lib().oracle_level_set_threads(self.h, n)
+        self.L.oracle_level_set_threads(self.h, n)
 
     def init_data(self):
-        lib().oracle_level_init_data(self.h)
+        self.L.oracle_level_init_data(self.h)
 
     def est_time_step(self):
-        return lib().oracle_level_est_time_step(self.h)
+        return self.L.oracle_level_est_time_step(self.h)
 
     def clean_state(self):
-        lib().oracle_level_clean_state(self.h)
+        self.L.oracle_level_clean_state(self.h)
 
     def advance(self, dt):
-        lib().oracle_level_advance(self.h, dt)
+        self.L.oracle_level_advance(self.h, dt)
 
     def coarse_step(self, stop_time=-1.0):
-        return lib().oracle_level_coarse_step(self.h, stop_time)
+        return self.L.oracle_level_coarse_step(self.h, stop_time)
 
     @property
     def time(self):
-        return lib().oracle_level_time(self.h)
+        return self.L.oracle_level_time(self.h)
 
     @property
     def dt(self):
-        return lib().oracle_level_dt(self.h)
+        return self.L.oracle_level_dt(self.h)
 
     @property
     def steps(self):
-        return lib().oracle_level_steps(self.h)
+        return self.L.oracle_level_steps(self.h)
 
     def blast_radius(self):
         m = C.c_double()
-        r = lib().oracle_level_blast_radius(self.h, C.byref(m))
+        r = self.L.oracle_level_blast_radius(self.h, C.byref(m))
         return r, m.value
 
 
-def level_from_instance(inst: dict, nvar: int) -> tuple["Level", "Problem"]:
-    """An oracle Level + Problem for one instance of a workload description."""
+def level_from_instance(inst: dict, nvar: int, variant: str = "parity") -> tuple["Level", "Problem"]:
+    """An oracle Level + Problem for one instance of a workload description
+    (on the given build of the oracle; its network and table must be initialised)."""
     p = dict(inst["problem"])
     prob = Problem(ambient_from_T=p["ambient_from_T"], dens_ambient=p["dens_ambient"], p_ambient=p["p_ambient"],
                    T_ambient=p["T_ambient"], exp_energy=p["exp_energy"], r_init=p["r_init"], X=p["X"],
                    nsub=p["nsub"], T_init=p["T_init"], pert=p.get("pert"), pert_lo=inst["dom_lo"],
                    pert_amp=p.get("pert_amp", 0.0))
-    prob.install()
-    L = Level(inst["boxes"], inst["dom_lo"], inst["dom_hi"], inst["problo"], inst["probhi"], inst["bc"], nvar)
+    prob.install(variant)
+    L = Level(inst["boxes"], inst["dom_lo"], inst["dom_hi"], inst["problo"], inst["probhi"], inst["bc"], nvar,
+              variant)
     L.init_data()
     return L, prob
 

@@ -1,0 +1,132 @@
+"""Parity at the benchmark configurations' own sizes (Castro::advance + dt
+control, Source/Castro_advance.cpp:32-97, Source/Castro.cpp:218-295), through
+the C-ABI castro_sim_* entry points on the batched path, against the oracle's
+level driver on the same inputs:
+
+* C1  one 64^3 box, outflow, 2 species, 10 steps;
+* C2  128^3 in 64 boxes of 32^3, perturbed density, 50 steps (the full run);
+* C3  256^3 on the uneven BoxArray plus the 32 instances of 32^3..96^3, one step;
+* R   the Source/Prob.F90 problem, 128^3 in 64^3 boxes, 13 species, periodic, 10 steps.
+
+The oracle, the exact build and the production build advance in lockstep.
+Exact build: state and dt bit for bit after every step.  Production build:
+dt within 1e-14 every step; after the first step every zone within 1e-12
+relative (no floor beyond the smallest normal double) except the round-off
+noise zones, which are identified by the oracle's own contracting build and
+reported apart (gpu_harness); relative L1 per component <= 1e-9 after the full
+run.  R (periodic) also conserves mass and total energy to 1e-13.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from gpu_harness import RTOL_L1, assert_strict, noise_mask, rel_l1
+
+pytestmark = pytest.mark.gpu
+
+CONFIGS = {
+    "C1_sedov64": (lambda c: c.sedov64(), 10),
+    "C2_sedov128_pert": (lambda c: c.sedov128_pert(), 50),
+    "C3_batched": (lambda c: c.batched(), 1),
+    "R_reference128": (lambda c: c.reference(), 10),
+}
+
+
+def _report(name, data):
+    path = os.environ.get("CASTRO_PARITY_REPORT")
+    if not path:
+        return
+    rep = {}
+    if os.path.exists(path):
+        with open(path) as fp:
+            rep = json.load(fp)
+    rep[name] = data
+    with open(path, "w") as fp:
+        json.dump(rep, fp, indent=1)
+
+
+def _oracle_levels(oracle, pkg, table, cfg, variant):
+    A, Z = cfg["network"]
+    oracle.network_init(A, Z, variant)
+    oracle.eos_init(table, variant)
+    levs = []
+    for inst in cfg["instances"]:
+        lev, prob = oracle.level_from_instance(inst, pkg.configs.nvar(cfg), variant)
+        lev.set_threads(os.cpu_count() or 1)
+        levs.append((lev, prob))
+    return levs
+
+
+def _gpu_sim(pkg, table, cfg, exact):
+    L = pkg.castro.init(cfg["network"][0], cfg["network"][1], table, exact=exact)
+    sim = pkg.make_sim(L, cfg, pkg.castro.MODE_BATCHED)
+    sim.init_data()
+    return sim
+
+
+def _states(pkg, cfg, sim):
+    st = sim.box_states()
+    return [pkg.castro.assemble(inst, st[i]) for i, inst in enumerate(cfg["instances"])]
+
+
+@pytest.mark.parametrize("name", list(CONFIGS))
+def test_config_parity(pkg, table, oracle, name):
+    make, steps = CONFIGS[name]
+    cfg = make(pkg.configs)
+    insts = cfg["instances"]
+    levs = _oracle_levels(oracle, pkg, table, cfg, "parity")
+    ex = _gpu_sim(pkg, table, cfg, True)
+    pr = _gpu_sim(pkg, table, cfg, False)
+    periodic = all(i["bc"] == pkg.castro.BC_PERIODIC for i in insts)
+    if periodic:
+        G0 = _states(pkg, cfg, pr)
+        tot0 = [(g[..., 0].sum(), g[..., 4].sum()) for g in G0]
+    report = {"steps": steps, "instances": len(insts), "zones": pkg.configs.zones(cfg)}
+    for s in range(steps):
+        dto = [lev.coarse_step(i.get("stop_time", -1.0)) for (lev, _), i in zip(levs, insts)]
+        ex.step(1)
+        pr.step(1)
+        for n in range(len(insts)):
+            assert ex.dt(n) == dto[n], f"{name} step {s + 1} instance {n}: exact dt {ex.dt(n)!r} != {dto[n]!r}"
+            assert abs(pr.dt(n) / dto[n] - 1) <= 1e-14, f"{name} step {s + 1} instance {n}: dt {pr.dt(n)!r} vs {dto[n]!r}"
+        Gx = _states(pkg, cfg, ex)
+        Go = [oracle.assemble(lev, i) for (lev, _), i in zip(levs, insts)]
+        for n in range(len(insts)):
+            assert np.array_equal(Gx[n], Go[n]), f"{name} step {s + 1} instance {n}: exact build differs from the oracle"
+        del Gx
+        if s == 0:
+            # one step: the strict per-zone check, noise zones from the contracting oracle build
+            fast = _oracle_levels(oracle, pkg, table, cfg, "fast")
+            for (lev, _), i in zip(fast, insts):
+                lev.coarse_step(i.get("stop_time", -1.0))
+            Gp = _states(pkg, cfg, pr)
+            per = []
+            for n, ((lev, _), i) in enumerate(zip(fast, insts)):
+                noise = noise_mask(Go[n], oracle.assemble(lev, i))
+                per.append(assert_strict(Gp[n], Go[n], noise, what=f"{name} step 1 instance {n}"))
+            del fast, Gp
+            report["one_step"] = {
+                "max_rel_non_noise": max(r["max_rel"] for p in per for r in p),
+                "noise_zones_per_component": [sum(p[c]["noise_zones"] for p in per) for c in range(len(per[0]))],
+                "noise_max_abs_over_scale": max(r["noise_max_abs_over_scale"] for p in per for r in p),
+            }
+        if s == steps - 1:
+            Gp = _states(pkg, cfg, pr)
+            l1 = [rel_l1(Gp[n], Go[n]) for n in range(len(insts))]
+            worst = max(float(x.max()) for x in l1)
+            report["full_run_rel_l1_max"] = worst
+            assert worst <= RTOL_L1, f"{name}: relative L1 after {steps} steps {worst:.3e}"
+            if periodic:
+                for n, g in enumerate(Gp):
+                    m0, e0 = tot0[n]
+                    dm, de = abs(g[..., 0].sum() / m0 - 1), abs(g[..., 4].sum() / e0 - 1)
+                    report["mass_rel_change"], report["energy_rel_change"] = dm, de
+                    assert dm <= 1e-13 and de <= 1e-13, f"{name}: mass {dm:.2e} / energy {de:.2e} not conserved"
+    assert ex.eos_failures() == 0 and pr.eos_failures() == 0
+    ex.close()
+    pr.close()
+    _report(name, report)

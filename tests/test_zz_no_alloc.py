@@ -103,3 +103,43 @@ def test_noalloc_rejects_oversized_box(pkg, table):
     L.castro_clear_error()
     torch.cuda.synchronize()
     assert float(src.abs().max()) == 0.0         # nothing was launched
+
+
+def test_noalloc_shape_changes_and_capacity(pkg, table):
+    """Calls in a row whose box shapes differ (8x8x16, then 21^3, then 8^3), so the
+    layout carved out of the static array moves between calls, each against the
+    allocating entry point; 21^3 with 2 species is the largest cube the array
+    holds and 22^3 is refused."""
+    cfg = pkg.configs.sedov64(scale=2)               # one 32^3 box, 2 species, outflow
+    A, Z = cfg["network"]
+    L = pkg.castro.init(A, Z, table)
+    K = pkg.castro
+    sim = pkg.make_sim(L, cfg, K.MODE_BATCHED)
+    sim.init_data()
+    sim.step(3)
+    inst = cfg["instances"][0]
+    G = K.assemble(inst, sim.box_states()[0])
+    dt = sim.est_time_step()
+    sim.close()
+    nv = pkg.configs.nvar(cfg)
+    dx = [1.0 / 32] * 3
+    for lo, hi, dtc in (((4, 4, 4), (11, 11, 19), dt), ((5, 5, 5), (25, 25, 25), 0.7 * dt), ((12, 12, 12), (19, 19, 19), dt)):
+        sblo, sbhi = [l - 4 for l in lo], [h + 4 for h in hi]
+        sb = to_dev(sborder_from_domain(G, inst["dom_lo"], lo, hi, inst["bc"]))
+        for name in ("enforce_minimum_density", "normalize_species", "reset_internal_e", "compute_temp"):
+            K.call(L, name, sblo, sbhi, sb, sblo, sbhi)
+        rc0, src0, fo0 = _call(L, K, "castro_construct_hydro_source_box", lo, hi, sb, sblo, sbhi, nv, dx, dtc)
+        rc1, src1, fo1 = _call(L, K, "castro_construct_hydro_source_box_noalloc", lo, hi, sb, sblo, sbhi, nv, dx, dtc)
+        assert rc0 == 0 and rc1 == 0, L.castro_error_string()
+        assert np.isfinite(src1).all()
+        assert_match(src1, src0, False, rtol=RTOL_KERNEL, what=f"noalloc source, box {lo}-{hi}")
+        for d in range(3):
+            assert_match(fo1[d], fo0[d], False, rtol=RTOL_KERNEL, what=f"noalloc store_flux d={d}, box {lo}-{hi}")
+    lo, hi = (4, 4, 4), (25, 25, 25)                 # 22^3 with 2 species: one zone per side too many
+    sblo, sbhi = [l - 4 for l in lo], [h + 4 for h in hi]
+    sb = to_dev(sborder_from_domain(G, inst["dom_lo"], lo, hi, inst["bc"]))
+    L.castro_clear_error()
+    rc, src, _ = _call(L, K, "castro_construct_hydro_source_box_noalloc", lo, hi, sb, sblo, sbhi, nv, dx, dt)
+    assert rc == 5 and b"static array" in L.castro_error_string()
+    L.castro_clear_error()
+    assert float(np.abs(src).max()) == 0.0
