@@ -50,7 +50,8 @@ enum {
     CASTRO_ERR_TABLE_IO = 3,    /* helm_table.dat missing or malformed */
     CASTRO_ERR_NSPEC = 4,       /* network size other than 2 or 13 */
     CASTRO_ERR_ARG = 5,         /* invalid argument */
-    CASTRO_ERR_EOS = 6          /* EOS Newton iteration did not converge */
+    CASTRO_ERR_EOS = 6,         /* EOS Newton iteration did not converge */
+    CASTRO_ERR_IO = 7           /* a checkpoint or plotfile could not be read or written */
 };
 int         castro_last_error(void);          /* sticky: first error since castro_clear_error */
 void        castro_clear_error(void);
@@ -263,6 +264,10 @@ typedef struct {
     double stop_time;             /* < 0: none (Source/main.cpp:66 default is 0.01) */
 } castro_instance_desc;
 
+/* Creates the sim; NULL with CASTRO_ERR_ARG when an instance's domain is empty,
+ * its zones are not cubic (the reference aborts on dx != dy != dz,
+ * Source/Castro.cpp:95-100), its boundary condition is unknown, or its boxes are
+ * empty, leave the domain, overlap or leave a gap: nothing is allocated then. */
 castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int mode);
 void   castro_sim_destroy(castro_sim* sim);
 int    castro_sim_nbox(const castro_sim* sim, int inst);
@@ -282,6 +287,9 @@ int    castro_sim_run(castro_sim* sim, int nsteps);
 /* host <-> device whole-run call: upload 'host_in', nsteps coarse steps,
  * download into 'host_out' (may alias host_in) */
 int    castro_sim_run_host(castro_sim* sim, const double* host_in, int nsteps, double* host_out);
+/* waits for the sim's stream; also reports, as CASTRO_ERR_EOS, EOS Newton
+ * solves that hit their 100-iteration limit since the sim's last sync (a
+ * non-finite or unphysical state: silent in the reference) */
 int    castro_sim_sync(castro_sim* sim);
 double castro_sim_time(castro_sim* sim, int inst);
 double castro_sim_dt(castro_sim* sim, int inst);
@@ -295,6 +303,16 @@ double castro_sim_blast_radius(castro_sim* sim, int inst, double* blast_mass);
  * readable by AMReX tools -- the layout Amr::writePlotFile produces (the
  * reference never writes one by default: Source/main.cpp sets no plot_int) */
 int    castro_sim_write_plotfile(castro_sim* sim, int inst, const char* dir);
+/* Checkpoint / restart (the reference's State_Type checkpoint,
+ * Source/Castro_setup.cpp:50-53, in a format of this library's own): dir/Header
+ * (text: nspec, per instance its domain, BoxArray, time, completed steps, last dt
+ * and stop time as exact hexadecimal floats) and dir/State_<n> (instance n's box
+ * FABs, raw doubles in the castro_sim_download layout).  Reading needs a sim of
+ * the same species count, domains and BoxArrays (CASTRO_ERR_ARG otherwise) and
+ * checks the files completely before installing anything (CASTRO_ERR_IO); the
+ * run then continues bit for bit as if it had not stopped, in any mode. */
+int    castro_sim_write_checkpoint(castro_sim* sim, const char* dir);
+int    castro_sim_read_checkpoint(castro_sim* sim, const char* dir);
 /* the CUDA stream (cudaStream_t) every launch of this sim is issued on */
 void*  castro_sim_stream(castro_sim* sim);
 /* batched mode: one step with a CUDA event around each of the fused kernels
@@ -303,7 +321,7 @@ void*  castro_sim_stream(castro_sim* sim);
 int    castro_sim_profile_step(castro_sim* sim, double* ms, const char** names);
 /* kernel launches issued by the last castro_sim_step (graph nodes for the batched mode) */
 int    castro_sim_launches_per_step(const castro_sim* sim);
-/* per-step EOS Newton failures seen so far (non-converged zones) */
+/* EOS Newton solves that hit their iteration limit since the sim was created */
 long long castro_sim_eos_failures(castro_sim* sim);
 
 /* FP64 fused-multiply-add throughput of the current device in TFLOP/s,

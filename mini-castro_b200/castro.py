@@ -80,6 +80,7 @@ ABI_SYMBOLS = [
     "castro_adj_destroy", "castro_adj_set_problem", "castro_adj_set_shell", "castro_adj_forward",
     "castro_adj_backward", "castro_adj_dt", "castro_adj_final_state", "castro_adj_initial_adjoint",
     "castro_adj_time_ms", "castro_adj_device_bytes", "castro_sim_write_plotfile",
+    "castro_sim_write_checkpoint", "castro_sim_read_checkpoint",
 ]
 
 
@@ -138,6 +139,8 @@ def load(exact: bool = False) -> C.CDLL:
     L.castro_sim_eos_failures.restype = C.c_longlong
     L.castro_sim_eos_failures.argtypes = [C.c_void_p]
     L.castro_sim_write_plotfile.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
+    L.castro_sim_write_checkpoint.argtypes = [C.c_void_p, C.c_char_p]
+    L.castro_sim_read_checkpoint.argtypes = [C.c_void_p, C.c_char_p]
     L.castro_adj_create.restype = C.c_void_p
     L.castro_adj_create.argtypes = [C.POINTER(InstanceDesc), C.c_int, C.c_int]
     L.castro_adj_destroy.argtypes = [C.c_void_p]
@@ -337,6 +340,16 @@ class Sim:
         """AMReX plotfile of instance inst (castro_sim_write_plotfile)."""
         self.L.castro_sim_write_plotfile(self.h, inst, path.encode())
         check(self.L, "castro_sim_write_plotfile")
+
+    def write_checkpoint(self, path: str):
+        """Checkpoint of every instance (castro_sim_write_checkpoint)."""
+        self.L.castro_sim_write_checkpoint(self.h, path.encode())
+        check(self.L, "castro_sim_write_checkpoint")
+
+    def read_checkpoint(self, path: str):
+        """Restart from a checkpoint of a sim with the same instances (castro_sim_read_checkpoint)."""
+        self.L.castro_sim_read_checkpoint(self.h, path.encode())
+        check(self.L, "castro_sim_read_checkpoint")
 
     def blast_radius(self, inst: int = 0):
         m = C.c_double()

@@ -1956,6 +1956,7 @@ int castro_adj_set_shell(castro_adj* a, double r0, double r1)
 
 int castro_adj_forward(castro_adj* a, double* J)
 {
+    NvtxRange r("castro_adj_forward");
     if (!a) { set_error(CASTRO_ERR_ARG, "castro_adj_forward: null"); return CASTRO_ERR_ARG; }
     int rc = CASTRO_ERR_NSPEC;
     if (a->ns == 2) rc = adj_forward<2>(a);
@@ -1966,6 +1967,7 @@ int castro_adj_forward(castro_adj* a, double* J)
 
 int castro_adj_backward(castro_adj* a, double* dJ_dE, double* dJ_drho, double* dJ_dpert)
 {
+    NvtxRange r("castro_adj_backward");
     if (!a || !dJ_dE || !dJ_drho) { set_error(CASTRO_ERR_ARG, "castro_adj_backward: arguments"); return CASTRO_ERR_ARG; }
     if (a->ns == 2) return adj_backward<2>(a, dJ_dE, dJ_drho, dJ_dpert);
     if (a->ns == 13) return adj_backward<13>(a, dJ_dE, dJ_drho, dJ_dpert);

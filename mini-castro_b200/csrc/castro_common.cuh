@@ -8,7 +8,29 @@
 
 #include "castro_device.cuh"
 
+// NVTX ranges around the host routines (the counterpart of the reference's
+// BL_PROFILE regions, e.g. Source/Castro_advance.cpp:28,
+// Source/Castro_hydro.cpp:10); header-only NVTX v3, inert unless a profiler
+// attaches.  -DCASTRO_NVTX=0 compiles them out.
+#ifndef CASTRO_NVTX
+#define CASTRO_NVTX 1
+#endif
+#if CASTRO_NVTX
+#include <nvtx3/nvToolsExt.h>
+#endif
+
 namespace castro {
+
+struct NvtxRange {
+#if CASTRO_NVTX
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+#else
+    explicit NvtxRange(const char*) {}
+#endif
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // A FAB view in BL_FORT_FAB_ARG_3D form: Fortran order, component slowest.
 struct Fab {

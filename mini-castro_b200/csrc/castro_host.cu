@@ -143,6 +143,7 @@ int castro_nspec(void) { return nspec(); }
 
 int castro_eos_init_path(const char* path)
 {
+    NvtxRange r("eos_init");
     HostTable T;
     int rc = read_helm_table(path, T);
     if (rc == 1) {

@@ -1087,8 +1087,11 @@ __global__ void __launch_bounds__(BLOCK) k_estdt_state(SimDev S, const Work* wl)
     if (threadIdx.x == 0) atomic_min_pos(&S.st[B.inst].dt_est, m);
 }
 
-// computeInitialDt (first) or, after a step, time/step bookkeeping and
-// computeNewDt (Source/Castro.cpp:162-341)
+// computeInitialDt (DT_FIRST) or, after a step, time/step bookkeeping and
+// computeNewDt (DT_STEP; Source/Castro.cpp:162-341).  DT_RESTART is
+// computeNewDt alone, for a state restored from a checkpoint whose st.dt holds
+// the last step's dt: the same dt the uninterrupted run formed at that step's end.
+enum { DT_STEP = 0, DT_FIRST = 1, DT_RESTART = 2 };
 __global__ void k_dt(SimDev S, int ninst, int first)
 {
     int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1096,12 +1099,14 @@ __global__ void k_dt(SimDev S, int ninst, int first)
     InstState& st = S.st[n];
     double est = st.dt_est * cfl;                       // estTimeStep, Castro.cpp:212-213
     double dt_0;
-    if (first) {
+    if (first == DT_FIRST) {
         dt_0 = DMIN(1.0e+100, 0.01 * est);               // initialTimeStep, Castro.cpp:168-170
     } else {
-        st.time = st.time + st.dt;
-        st.steps = st.steps + 1;
-        st.dt_last = st.dt;
+        if (first == DT_STEP) {
+            st.time = st.time + st.dt;
+            st.steps = st.steps + 1;
+            st.dt_last = st.dt;
+        }
         double dt_min = DMIN(est, 1.1e0 * st.dt);        // Castro.cpp:264-267
         dt_0 = DMIN(1.0e+100, dt_min);
     }
@@ -1295,6 +1300,10 @@ struct castro_sim {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     int launches = 0;
+    // EOS Newton non-convergences (library-wide counter) already reported
+    // through castro_last_error when this sim last synchronized
+    unsigned long long eos_seen = 0;
+    unsigned long long eos_base = 0;   // the counter when this sim was created
     // plain-path scratch (largest box)
     double* sb = nullptr;      // Sborder per box (grow 4) for all boxes
     double* src = nullptr;     // hydro_source per box for all boxes
@@ -1447,6 +1456,9 @@ void batched_step_kernels(castro_sim* s)
 template <int NS>
 void profile_kernel(castro_sim* s, const SimDev& S, int k)
 {
+    static const char* names[10] = {"front", "ghost", "prep", "trace", "riemann1", "riemann2", "riemann3", "update", "dt",
+                                    "trace2"};
+    NvtxRange r(k >= 0 && k < 10 ? names[k] : "kernel");
     cudaStream_t st = s->st;
     SimDev Sd = S;
     Sd.boxes = S.dom;
@@ -1625,6 +1637,7 @@ void plain_step(castro_sim* s)
         const double* dx = &s->hdx[3 * in];
         // computeInitialDt / computeNewDt, Source/Castro.cpp:175-341
         {
+            NvtxRange r("computeNewDt: estTimeStep");
             double big = 1.79769313486231570e+308;
             cudaMemcpyAsync(s->d_dtloc, &big, sizeof big, cudaMemcpyHostToDevice, s->st);
             for (int b : s->inst_boxes[in]) {
@@ -1644,10 +1657,15 @@ void plain_step(castro_sim* s)
         }
         const double dt = hs.dt;
         // Castro::advance, Source/Castro_advance.cpp:32-97
-        for (int b : s->inst_boxes[in]) {
-            const BoxDev& B = s->hboxes[b];
-            plain_clean(B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
+        NvtxRange adv("Castro::advance");
+        {
+            NvtxRange r("clean_state(S_old)");
+            for (int b : s->inst_boxes[in]) {
+                const BoxDev& B = s->hboxes[b];
+                plain_clean(B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
+            }
         }
+        NvtxRange fp("FillPatch(Sborder) + clean_state(Sborder)");
         for (int b : s->inst_boxes[in]) {
             const BoxDev& B = s->hboxes[b];
             long long n = npts_reg(B.lo, B.hi, R_G4, 0);
@@ -1659,6 +1677,7 @@ void plain_step(castro_sim* s)
             IBox g = grow(bx, NG, NG, NG);
             plain_clean(g.lo, g.hi, s->sb + s->offSb[b], g.lo, g.hi);
         }
+        NvtxRange hs_r("construct_hydro_source");
         for (int b : s->inst_boxes[in]) {
             const BoxDev& B = s->hboxes[b];
             IBox bx{{B.lo[0], B.lo[1], B.lo[2]}, {B.hi[0], B.hi[1], B.hi[2]}};
@@ -1723,6 +1742,52 @@ int step_impl(castro_sim* s)
     return castro_last_error();
 }
 
+// The BoxArray and geometry of one instance, checked before anything is
+// allocated: a non-empty domain with cubic zones (the reference aborts on
+// dx != dy != dz, Source/Castro.cpp:95-100), a known boundary condition, and
+// non-empty boxes inside the domain that cover it without overlapping (the
+// owner map then assigns every zone exactly once).  Returns false with msg set.
+bool validate_instance(const castro_instance_desc& D, int in, char* msg, size_t nmsg)
+{
+    long long dvol = 1;
+    for (int d = 0; d < 3; ++d) {
+        if (D.dom_hi[d] < D.dom_lo[d]) { snprintf(msg, nmsg, "castro_sim_create: instance %d: empty domain", in); return false; }
+        if (!(D.probhi[d] > D.problo[d])) { snprintf(msg, nmsg, "castro_sim_create: instance %d: probhi <= problo", in); return false; }
+        dvol *= (long long)(D.dom_hi[d] - D.dom_lo[d] + 1);
+    }
+    double dx[3];
+    for (int d = 0; d < 3; ++d) dx[d] = (D.probhi[d] - D.problo[d]) / (double)(D.dom_hi[d] - D.dom_lo[d] + 1);
+    if (fabs(dx[0] - dx[1]) > 1.e-13 * dx[0] || fabs(dx[0] - dx[2]) > 1.e-13 * dx[0]) {
+        snprintf(msg, nmsg, "castro_sim_create: instance %d: zones are not cubic (dx != dy != dz)", in);
+        return false;
+    }
+    if (D.bc != CASTRO_BC_PERIODIC && D.bc != CASTRO_BC_OUTFLOW) {
+        snprintf(msg, nmsg, "castro_sim_create: instance %d: unknown boundary condition %d", in, D.bc);
+        return false;
+    }
+    if (D.nbox < 1 || !D.box_lo || !D.box_hi) { snprintf(msg, nmsg, "castro_sim_create: instance %d: no boxes", in); return false; }
+    long long vol = 0;
+    for (int b = 0; b < D.nbox; ++b) {
+        long long v = 1;
+        for (int d = 0; d < 3; ++d) {
+            const int l = D.box_lo[3 * b + d], h = D.box_hi[3 * b + d];
+            if (h < l) { snprintf(msg, nmsg, "castro_sim_create: instance %d box %d: empty box", in, b); return false; }
+            if (l < D.dom_lo[d] || h > D.dom_hi[d]) {
+                snprintf(msg, nmsg, "castro_sim_create: instance %d box %d: outside the domain", in, b);
+                return false;
+            }
+            v *= (long long)(h - l + 1);
+        }
+        vol += v;
+    }
+    if (vol != dvol) {
+        snprintf(msg, nmsg, "castro_sim_create: instance %d: boxes hold %lld zones, the domain %lld (overlap or gap)",
+                 in, vol, dvol);
+        return false;
+    }
+    return true;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1740,6 +1805,10 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
     }
     int ns = nspec();
     if (ns != 2 && ns != 13) { set_error(CASTRO_ERR_NSPEC, "castro_sim_create: nspec"); return nullptr; }
+    for (int in = 0; in < ninst; ++in) {
+        char msg[200];
+        if (!validate_instance(desc[in], in, msg, sizeof msg)) { set_error(CASTRO_ERR_ARG, msg); return nullptr; }
+    }
     if (!(ns == 2 ? set_kernel_attributes<2>() : set_kernel_attributes<13>())) return nullptr;
     castro_sim* s = new castro_sim();
     s->mode = mode;
@@ -1817,14 +1886,19 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
             int gid = (int)s->hboxes.size();
             ids.push_back(gid);
             s->hboxes.push_back(B);
+            bool overlap = false;
             for (int k = B.lo[2]; k <= B.hi[2]; k += g)
                 for (int j = B.lo[1]; j <= B.hi[1]; j += g)
-                    for (int i = B.lo[0]; i <= B.hi[0]; i += g)
-                        owner_all[I.owner_off + (i - D.dom_lo[0]) / g +
-                                  (long long)I.on[0] * ((j - D.dom_lo[1]) / g + (long long)I.on[1] * ((k - D.dom_lo[2]) / g))] = gid;
+                    for (int i = B.lo[0]; i <= B.hi[0]; i += g) {
+                        int& o = owner_all[I.owner_off + (i - D.dom_lo[0]) / g +
+                                           (long long)I.on[0] * ((j - D.dom_lo[1]) / g + (long long)I.on[1] * ((k - D.dom_lo[2]) / g))];
+                        overlap = overlap || o >= 0;
+                        o = gid;
+                    }
+            if (overlap) { set_error(CASTRO_ERR_ARG, "castro_sim_create: boxes overlap"); castro_sim_destroy(s); return nullptr; }
         }
         for (size_t m = I.owner_off; m < owner_all.size(); ++m)
-            if (owner_all[m] < 0) { set_error(CASTRO_ERR_ARG, "castro_sim_create: boxes do not cover the domain"); delete s; return nullptr; }
+            if (owner_all[m] < 0) { set_error(CASTRO_ERR_ARG, "castro_sim_create: boxes do not cover the domain"); castro_sim_destroy(s); return nullptr; }
         s->inst_boxes.push_back(ids);
         s->hinst.push_back(I);
         s->hdom.push_back(P);
@@ -1878,6 +1952,9 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
     }
     s->probs.resize(ninst);
     for (int in = 0; in < ninst; ++in) s->probs[in] = desc[in].prob;
+    if (ok && eos_fail_counter())
+        cuda_ok(cudaMemcpy(&s->eos_seen, eos_fail_counter(), sizeof s->eos_seen, cudaMemcpyDeviceToHost), "eos counter");
+    s->eos_base = s->eos_seen;
     if (!ok || castro_last_error()) { castro_sim_destroy(s); return nullptr; }
     return s;
 }
@@ -1916,6 +1993,7 @@ size_t castro_sim_total_size(const castro_sim* s) { return (size_t)s->nU; }
 
 int castro_sim_init_data(castro_sim* s)
 {
+    NvtxRange r("castro_sim_init_data: Castro::initData");
     cudaStream_t saved = castro::stream();
     castro_set_stream(s->st);
     for (int in = 0; in < s->ninst; ++in) {
@@ -1945,6 +2023,8 @@ int castro_sim_download(castro_sim* s, double* host)
 
 int castro_sim_step(castro_sim* s)
 {
+    NvtxRange r(s->mode == CASTRO_MODE_BATCHED ? "castro_sim_step: Castro::advance (batched step graph)"
+                                                : "castro_sim_step: Castro::advance (per-box sequence)");
     if (s->ns == 2) return step_impl<2>(s);
     return step_impl<13>(s);
 }
@@ -1969,7 +2049,18 @@ int castro_sim_run_host(castro_sim* s, const double* host_in, int nsteps, double
 
 int castro_sim_sync(castro_sim* s)
 {
-    cuda_ok(cudaStreamSynchronize(s->st), "sync");
+    if (!cuda_ok(cudaStreamSynchronize(s->st), "sync")) return castro_last_error();
+    // an EOS Newton iteration that reached its 100-iteration limit (a NaN or
+    // otherwise unphysical state) is silent in the reference; here it is an error
+    unsigned long long v = 0;
+    if (eos_fail_counter() && cuda_ok(cudaMemcpy(&v, eos_fail_counter(), sizeof v, cudaMemcpyDeviceToHost), "eos counter") &&
+        v > s->eos_seen) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "castro_sim: %llu EOS Newton solves did not converge (non-finite or unphysical state)",
+                 v - s->eos_seen);
+        s->eos_seen = v;
+        set_error(CASTRO_ERR_EOS, msg);
+    }
     return castro_last_error();
 }
 
@@ -1992,6 +2083,7 @@ int castro_sim_steps(castro_sim* s, int inst) { return read_state(s, inst).steps
 
 double castro_sim_est_time_step(castro_sim* s, int inst)
 {
+    NvtxRange r("castro_sim_est_time_step: Castro::estTimeStep");
     double big = 1.79769313486231570e+308;
     cuda_ok(cudaMemcpyAsync(s->d_dtloc, &big, sizeof big, cudaMemcpyHostToDevice, s->st), "est");
     cudaStream_t saved = castro::stream();
@@ -2015,6 +2107,7 @@ double castro_sim_est_time_step(castro_sim* s, int inst)
 // state: density, xmom, ymom, zmom, rho_E, rho_e, Temp, rho_<species>.
 int castro_sim_write_plotfile(castro_sim* s, int inst, const char* dir)
 {
+    NvtxRange r("castro_sim_write_plotfile");
     if (!s || !dir || inst < 0 || inst >= s->ninst) {
         set_error(CASTRO_ERR_ARG, "castro_sim_write_plotfile: arguments");
         return CASTRO_ERR_ARG;
@@ -2108,6 +2201,171 @@ int castro_sim_write_plotfile(castro_sim* s, int inst, const char* dir)
     return castro_last_error();
 }
 
+// Checkpoint / restart of every instance (the reference registers State_Type for
+// AMReX checkpoints, Source/Castro_setup.cpp:50-53).  dir/Header is text: the
+// format line, nspec, nvar, then per instance its domain, BoxArray, time,
+// completed steps, last dt and stop time (floating-point values as C99
+// hexadecimal, so they round-trip exactly); dir/State_<n> holds instance n's box
+// FABs in box order as raw doubles (the castro_sim_download layout).
+int castro_sim_write_checkpoint(castro_sim* s, const char* dir)
+{
+    NvtxRange r("castro_sim_write_checkpoint");
+    if (!s || !dir) { set_error(CASTRO_ERR_ARG, "castro_sim_write_checkpoint: arguments"); return CASTRO_ERR_ARG; }
+    if (!cuda_ok(cudaStreamSynchronize(s->st), "checkpoint sync")) return castro_last_error();
+    mkdir(dir, 0755);
+    const std::string root(dir);
+    FILE* fp = fopen((root + "/Header").c_str(), "w");
+    if (!fp) { set_error(CASTRO_ERR_IO, ("castro_sim_write_checkpoint: cannot write " + root + "/Header").c_str()); return CASTRO_ERR_IO; }
+    fprintf(fp, "castro_b200_checkpoint 1\nnspec %d\nnvar %d\nninst %d\n", s->ns, s->nvar, s->ninst);
+    std::vector<double> h;
+    bool ok = true;
+    for (int in = 0; in < s->ninst && ok; ++in) {
+        const castro_instance_desc& D = s->desc[in];
+        InstState hs;
+        ok = cuda_ok(cudaMemcpy(&hs, s->dstate + in, sizeof hs, cudaMemcpyDeviceToHost), "checkpoint state");
+        // the plain mode keeps the last step's dt in dt as well
+        fprintf(fp, "instance %d\ndomain %d %d %d %d %d %d\nnbox %d\n", in, D.dom_lo[0], D.dom_lo[1], D.dom_lo[2],
+                D.dom_hi[0], D.dom_hi[1], D.dom_hi[2], (int)s->inst_boxes[in].size());
+        for (int b : s->inst_boxes[in]) {
+            const BoxDev& B = s->hboxes[b];
+            fprintf(fp, "box %d %d %d %d %d %d\n", B.lo[0], B.lo[1], B.lo[2], B.hi[0], B.hi[1], B.hi[2]);
+        }
+        fprintf(fp, "time %a\nsteps %d\ndt_last %a\nstop_time %a\n", hs.time, hs.steps, hs.dt_last, hs.stop_time);
+        char name[32];
+        snprintf(name, sizeof name, "/State_%05d", in);
+        FILE* fd = fopen((root + name).c_str(), "wb");
+        if (!fd) { set_error(CASTRO_ERR_IO, ("castro_sim_write_checkpoint: cannot write " + root + name).c_str()); ok = false; break; }
+        for (int b : s->inst_boxes[in]) {
+            const BoxDev& B = s->hboxes[b];
+            h.resize((size_t)(npts_reg(B.lo, B.hi, R_VALID, 0) * s->nvar));
+            ok = cuda_ok(cudaMemcpy(h.data(), s->U + B.offU, h.size() * sizeof(double), cudaMemcpyDeviceToHost), "checkpoint read");
+            if (ok && fwrite(h.data(), sizeof(double), h.size(), fd) != h.size()) {
+                set_error(CASTRO_ERR_IO, "castro_sim_write_checkpoint: short write");
+                ok = false;
+            }
+            if (!ok) break;
+        }
+        fclose(fd);
+    }
+    fprintf(fp, "end\n");
+    if (fclose(fp) != 0 && ok) { set_error(CASTRO_ERR_IO, "castro_sim_write_checkpoint: cannot close Header"); ok = false; }
+    return castro_last_error();
+}
+
+}  // extern "C"
+
+namespace {
+
+bool ck_expect(FILE* fp, const char* key)
+{
+    char w[64];
+    return fscanf(fp, "%63s", w) == 1 && strcmp(w, key) == 0;
+}
+
+template <int NS>
+void restart_dt_kernels(castro_sim* s)
+{
+    SimDev S = s->dev();
+    k_estdt_state<NS><<<s->n_valid, BLOCK, 0, s->st>>>(S, s->w_valid);
+    k_dt<<<(s->ninst + 63) / 64, 64, 0, s->st>>>(S, s->ninst, DT_RESTART);
+}
+
+}  // namespace
+
+extern "C" {
+
+int castro_sim_read_checkpoint(castro_sim* s, const char* dir)
+{
+    NvtxRange r("castro_sim_read_checkpoint");
+    if (!s || !dir) { set_error(CASTRO_ERR_ARG, "castro_sim_read_checkpoint: arguments"); return CASTRO_ERR_ARG; }
+    const std::string root(dir);
+    FILE* fp = fopen((root + "/Header").c_str(), "r");
+    if (!fp) { set_error(CASTRO_ERR_IO, ("castro_sim_read_checkpoint: cannot open " + root + "/Header").c_str()); return CASTRO_ERR_IO; }
+    auto fail = [&](int code, const std::string& m) {
+        fclose(fp);
+        set_error(code, ("castro_sim_read_checkpoint: " + m).c_str());
+        return code;
+    };
+    int ver = 0, ns = 0, nvar = 0, ninst = 0;
+    if (!ck_expect(fp, "castro_b200_checkpoint") || fscanf(fp, "%d", &ver) != 1 || ver != 1 || !ck_expect(fp, "nspec") ||
+        fscanf(fp, "%d", &ns) != 1 || !ck_expect(fp, "nvar") || fscanf(fp, "%d", &nvar) != 1 || !ck_expect(fp, "ninst") ||
+        fscanf(fp, "%d", &ninst) != 1)
+        return fail(CASTRO_ERR_IO, "malformed Header");
+    if (ns != s->ns || nvar != s->nvar || ninst != s->ninst)
+        return fail(CASTRO_ERR_ARG, "species count or instance count differs from this sim's");
+    std::vector<InstState> hs(ninst);
+    std::vector<std::vector<double>> states(ninst);
+    for (int in = 0; in < ninst; ++in) {
+        const castro_instance_desc& D = s->desc[in];
+        int idx = -1, dom[6], nbox = 0;
+        if (!ck_expect(fp, "instance") || fscanf(fp, "%d", &idx) != 1 || idx != in || !ck_expect(fp, "domain") ||
+            fscanf(fp, "%d %d %d %d %d %d", dom, dom + 1, dom + 2, dom + 3, dom + 4, dom + 5) != 6 || !ck_expect(fp, "nbox") ||
+            fscanf(fp, "%d", &nbox) != 1)
+            return fail(CASTRO_ERR_IO, "malformed Header");
+        bool same = nbox == (int)s->inst_boxes[in].size();
+        for (int d = 0; d < 3; ++d) same = same && dom[d] == D.dom_lo[d] && dom[3 + d] == D.dom_hi[d];
+        for (int b = 0; b < nbox; ++b) {
+            int bx[6];
+            if (!ck_expect(fp, "box") || fscanf(fp, "%d %d %d %d %d %d", bx, bx + 1, bx + 2, bx + 3, bx + 4, bx + 5) != 6)
+                return fail(CASTRO_ERR_IO, "malformed Header");
+            if (same) {
+                const BoxDev& B = s->hboxes[s->inst_boxes[in][b]];
+                for (int d = 0; d < 3; ++d) same = same && bx[d] == B.lo[d] && bx[3 + d] == B.hi[d];
+            }
+        }
+        if (!same) return fail(CASTRO_ERR_ARG, "domain or BoxArray differs from this sim's");
+        InstState& st = hs[in];
+        memset(&st, 0, sizeof st);
+        if (!ck_expect(fp, "time") || fscanf(fp, "%la", &st.time) != 1 || !ck_expect(fp, "steps") ||
+            fscanf(fp, "%d", &st.steps) != 1 || !ck_expect(fp, "dt_last") || fscanf(fp, "%la", &st.dt_last) != 1 ||
+            !ck_expect(fp, "stop_time") || fscanf(fp, "%la", &st.stop_time) != 1)
+            return fail(CASTRO_ERR_IO, "malformed Header");
+        st.dt = st.dt_last;   // the last step's dt: computeNewDt's growth limit reads it
+        st.dt_est = 1.79769313486231570e+308;
+        char name[32];
+        snprintf(name, sizeof name, "/State_%05d", in);
+        FILE* fd = fopen((root + name).c_str(), "rb");
+        if (!fd) return fail(CASTRO_ERR_IO, "cannot open " + root + name);
+        size_t n = 0;
+        for (int b : s->inst_boxes[in]) n += (size_t)(npts_reg(s->hboxes[b].lo, s->hboxes[b].hi, R_VALID, 0) * s->nvar);
+        states[in].resize(n);
+        const size_t got = fread(states[in].data(), sizeof(double), n, fd);
+        const bool extra = fgetc(fd) != EOF;
+        fclose(fd);
+        if (got != n || extra) return fail(CASTRO_ERR_IO, std::string(name + 1) + " does not hold the instance's state");
+    }
+    if (!ck_expect(fp, "end")) return fail(CASTRO_ERR_IO, "malformed Header");
+    fclose(fp);
+    // everything read and checked: install it
+    for (int in = 0; in < ninst; ++in) {
+        size_t off = 0;
+        for (int b : s->inst_boxes[in]) {
+            const BoxDev& B = s->hboxes[b];
+            const size_t n = (size_t)(npts_reg(B.lo, B.hi, R_VALID, 0) * s->nvar);
+            if (!cuda_ok(cudaMemcpy(s->U + B.offU, states[in].data() + off, n * sizeof(double), cudaMemcpyHostToDevice),
+                         "restart state"))
+                return castro_last_error();
+            off += n;
+        }
+    }
+    if (!cuda_ok(cudaMemcpy(s->dstate, hs.data(), ninst * sizeof(InstState), cudaMemcpyHostToDevice), "restart dt"))
+        return castro_last_error();
+    if (s->mode == CASTRO_MODE_BATCHED) {
+        bool started = false;
+        for (const InstState& st : hs) started = started || st.steps > 0;
+        if (started) {
+            // the batched step reads the next dt from the state record: form it as
+            // the end of the checkpointed step did (estdt of the state, computeNewDt)
+            if (s->ns == 2) restart_dt_kernels<2>(s);
+            else restart_dt_kernels<13>(s);
+        }
+        s->dt_ready = started;
+        check_launch("castro_sim_read_checkpoint");
+    }
+    cuda_ok(cudaStreamSynchronize(s->st), "restart sync");
+    return castro_last_error();
+}
+
 double castro_sim_blast_radius(castro_sim* s, int inst, double* blast_mass)
 {
     // max density on the host (diagnostic only), then the device reduction
@@ -2170,6 +2428,7 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
                           double* source, const int* sr_lo, const int* sr_hi, double* const* fo, const int* fo_lo,
                           const int* fo_hi, const double* dx, double dt)
 {
+    NvtxRange r("castro_construct_hydro_source_box");
     for (int d = 0; d < 3; ++d)
         if (sb_lo[d] > lo[d] - NG || sb_hi[d] < hi[d] + NG) {
             set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box: Sborder needs 4 ghost zones");
@@ -2315,6 +2574,7 @@ int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const
                            double* source, const int* sr_lo, const int* sr_hi, double* const* fo, const int* fo_lo,
                            const int* fo_hi, const double* dx, double dt)
 {
+    NvtxRange r("castro_construct_hydro_source_box_noalloc");
     for (int d = 0; d < 3; ++d)
         if (sb_lo[d] > lo[d] - NG || sb_hi[d] < hi[d] + NG) {
             set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box_noalloc: Sborder needs 4 ghost zones");
@@ -2529,7 +2789,7 @@ long long castro_sim_eos_failures(castro_sim* s)
     unsigned long long v = 0;
     cudaStreamSynchronize(s->st);
     cuda_ok(cudaMemcpy(&v, p, sizeof v, cudaMemcpyDeviceToHost), "eos failures");
-    return (long long)v;
+    return v >= s->eos_base ? (long long)(v - s->eos_base) : (long long)v;
 }
 
 }  // extern "C"

@@ -29,12 +29,13 @@ inline bool table_read_record(FILE* fp, double* v, int n)
             if (*c == 'D' || *c == 'd') *c = 'E';
         char* s = line;
         while (got < n) {
+            while (*s == ',' || *s == ' ' || *s == '\t') ++s;
+            if (*s == '\n' || *s == '\r' || *s == 0) break;   // the record continues on the next line
             char* e;
             double x = strtod(s, &e);
-            if (e == s) break;
+            if (e == s) return false;                            // not a number: a malformed table
             v[got++] = x;
             s = e;
-            while (*s == ',' || *s == ' ' || *s == '\t') ++s;
         }
     }
     return true;

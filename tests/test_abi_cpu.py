@@ -54,7 +54,7 @@ def test_library_exports_every_symbol(pkg, exact):
     assert L.castro_version() >= 100
 
 
-def test_library_reports_errors_without_gpu(pkg, table):
+def test_library_reports_errors_without_gpu(pkg, table, tmp_path_factory):
     """Entry points report a clean error (no crash) when CUDA is unavailable or
     the table has not been loaded."""
     from conftest import cuda_available
@@ -64,9 +64,20 @@ def test_library_reports_errors_without_gpu(pkg, table):
     L = pkg.castro.load(False)
     L.castro_clear_error()
     L.castro_eos_init_path(table.encode())
-    assert L.castro_last_error() != 0
+    assert L.castro_last_error() == 1     # the table parses; the device upload fails (CASTRO_ERR_CUDA)
     assert L.castro_error_string()
     L.castro_clear_error()
+    # host-side table faults are found before any CUDA call (CASTRO_ERR_TABLE_IO)
+    with open(table) as fp:
+        lines = fp.readlines()
+    d = tmp_path_factory.mktemp("tables")
+    (d / "truncated.dat").write_text("".join(lines[:1000]))
+    lines[7] = "1.0 x2.0\n"
+    (d / "garbled.dat").write_text("".join(lines))
+    del lines
+    for name in ("truncated.dat", "garbled.dat", "absent.dat"):
+        assert L.castro_eos_init_path(str(d / name).encode()) == 3, name
+        L.castro_clear_error()
     lo = (0, 0, 0)
     L.compute_temp(pkg.castro.ivec(lo), pkg.castro.ivec(lo), None, pkg.castro.ivec(lo), pkg.castro.ivec(lo))
     assert L.castro_last_error() == 2   # CASTRO_ERR_NO_TABLE
