@@ -72,6 +72,12 @@ void network_finalize(void);                  /* Castro_F.H:13 */
 /* run-time network (replaces the compile-time parameters of Source/network.F90:7-19) */
 int  castro_network_init(int nspec, const double* aion, const double* zion);
 int  castro_nspec(void);
+/* Keep the packed EOS table (13.9 MB) resident in L2 with a persisting
+ * access-policy window on the streams of sims created afterwards (default on;
+ * 0 switches it off for sims created later).  No reference counterpart: the
+ * reference reads the table through ordinary loads.  The L2 set-aside belongs
+ * to this process's CUDA context and eos_finalize puts the previous value back. */
+void castro_set_table_l2_window(int on);
 void eos_init(void);                          /* Castro_F.H:15: reads ./helm_table.dat (or $CASTRO_HELM_TABLE), eos.F90:580-734 */
 void eos_finalize(void);                      /* Castro_F.H:17 */
 int  castro_eos_init_path(const char* path);  /* eos_init with an explicit table path; returns an error code */

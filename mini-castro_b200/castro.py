@@ -80,7 +80,7 @@ ABI_SYMBOLS = [
     "castro_adj_destroy", "castro_adj_set_problem", "castro_adj_set_shell", "castro_adj_forward",
     "castro_adj_backward", "castro_adj_dt", "castro_adj_final_state", "castro_adj_initial_adjoint",
     "castro_adj_time_ms", "castro_adj_device_bytes", "castro_sim_write_plotfile",
-    "castro_sim_write_checkpoint", "castro_sim_read_checkpoint",
+    "castro_sim_write_checkpoint", "castro_sim_read_checkpoint", "castro_set_table_l2_window",
 ]
 
 
@@ -139,6 +139,7 @@ def load(exact: bool = False) -> C.CDLL:
     L.castro_sim_eos_failures.restype = C.c_longlong
     L.castro_sim_eos_failures.argtypes = [C.c_void_p]
     L.castro_sim_write_plotfile.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
+    L.castro_set_table_l2_window.argtypes = [C.c_int]
     L.castro_sim_write_checkpoint.argtypes = [C.c_void_p, C.c_char_p]
     L.castro_sim_read_checkpoint.argtypes = [C.c_void_p, C.c_char_p]
     L.castro_adj_create.restype = C.c_void_p

@@ -40,6 +40,37 @@ EosTableDev g_eos;
 castro_problem g_prob;
 bool g_prob_set = false;
 
+// The packed node table (the 13 tables the hydro reads, 13.9 MB) is kept in L2
+// by a persisting access-policy window on every sim's streams: between two
+// EOS kernels each step streams gigabytes of face states and fluxes through
+// L2, which would otherwise evict it.  The set-aside is this process's (it ends
+// with the CUDA context) and is put back by eos_finalize.
+bool g_l2_window = true;
+size_t g_table_bytes = 0;
+size_t g_l2_prev_limit = 0;
+bool g_l2_limit_set = false;
+
+void set_l2_limit()
+{
+    int dev = 0;
+    cudaDeviceProp pr;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&pr, dev) != cudaSuccess) return;
+    if (pr.persistingL2CacheMaxSize <= 0 || g_table_bytes == 0) return;
+    if (!g_l2_limit_set && cudaDeviceGetLimit(&g_l2_prev_limit, cudaLimitPersistingL2CacheSize) != cudaSuccess) return;
+    size_t want = g_table_bytes < (size_t)pr.persistingL2CacheMaxSize ? g_table_bytes : (size_t)pr.persistingL2CacheMaxSize;
+    if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) == cudaSuccess) g_l2_limit_set = true;
+    cudaGetLastError();
+}
+
+void restore_l2_limit()
+{
+    if (!g_l2_limit_set) return;
+    cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, g_l2_prev_limit);
+    cudaGetLastError();
+    g_l2_limit_set = false;
+}
+
 void default_network()
 {
     static const double a13[13] = {4., 12., 16., 20., 24., 28., 32., 36., 40., 44., 48., 52., 56.};
@@ -92,6 +123,26 @@ const NetworkDev& network_host()
 }
 unsigned long long* eos_fail_counter() { return d_fail; }
 
+// the table's window on stream st (or no window, when it is switched off)
+void apply_table_l2_window(cudaStream_t st)
+{
+    cudaStreamAttrValue v;
+    memset(&v, 0, sizeof v);
+    if (g_l2_window && g_table && d_node && g_l2_limit_set) {
+        int dev = 0;
+        cudaDeviceProp pr;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&pr, dev) != cudaSuccess) return;
+        size_t n = g_table_bytes < (size_t)pr.accessPolicyMaxWindowSize ? g_table_bytes : (size_t)pr.accessPolicyMaxWindowSize;
+        v.accessPolicyWindow.base_ptr = d_node;
+        v.accessPolicyWindow.num_bytes = n;
+        v.accessPolicyWindow.hitRatio = 1.0f;
+        v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    }
+    cudaStreamSetAttribute(st, cudaStreamAttributeAccessPolicyWindow, &v);
+    cudaGetLastError();
+}
+
 }  // namespace castro
 
 using namespace castro;
@@ -141,6 +192,8 @@ int castro_network_init(int ns, const double* aion, const double* zion)
 
 int castro_nspec(void) { return nspec(); }
 
+void castro_set_table_l2_window(int on) { g_l2_window = on != 0; }
+
 int castro_eos_init_path(const char* path)
 {
     NvtxRange r("eos_init");
@@ -168,6 +221,8 @@ int castro_eos_init_path(const char* path)
         set_error(CASTRO_ERR_CUDA, cudaGetErrorString(e));
         return CASTRO_ERR_CUDA;
     }
+    g_table_bytes = T.node.size() * sizeof(double);
+    set_l2_limit();
     g_eos = T.consts;
     g_eos.node = d_node;
     g_eos.trow = d_trow;
@@ -186,6 +241,7 @@ void eos_init(void)
 
 void eos_finalize(void)
 {
+    restore_l2_limit();
     if (d_node) cudaFree(d_node);
     if (d_trow) cudaFree(d_trow);
     if (d_drow) cudaFree(d_drow);

@@ -51,6 +51,7 @@ void upload_constants_sim(const EosTableDev& e, const NetworkDev& n)
 
 const castro_problem& problem();
 unsigned long long* eos_fail_counter();
+void apply_table_l2_window(cudaStream_t st);
 
 namespace {
 
@@ -1820,6 +1821,9 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
     cuda_ok(cudaStreamCreateWithFlags(&s->st2, cudaStreamNonBlocking), "stream create");
     cuda_ok(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming), "event create");
     cuda_ok(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming), "event create");
+    // the EOS table's L2 window on both streams; stream capture copies it into the step graph's nodes
+    apply_table_l2_window(s->st);
+    apply_table_l2_window(s->st2);
     const int NQS = 6 + ns, NTF = 7 + ns, NQF = 8 + ns, NV = 7 + ns;
 
     long long oU = 0, oUb = 0, oQ = 0, oDiv = 0, oTr = 0, oF1 = 0, oF2 = 0, oFx = 0;

@@ -601,3 +601,49 @@ def test_autograd_function(pkg, table):
     fd = float(Jp - Jm) / (2 * h)
     assert fd == pytest.approx(float(E.grad) * float(E), rel=1e-5)
     run.close()
+
+
+def _fd_steps(run, E0, R0, pert0, a, b, ct, steps=(1e-5, 1e-6, 1e-7)):
+    out = []
+    for h in steps:
+        Jp = run.forward(E0 * (1 + h * a), R0 * (1 + h * b), pert0 + h * ct)
+        Jm = run.forward(E0 * (1 - h * a), R0 * (1 - h * b), pert0 - h * ct)
+        out.append((Jp - Jm) / (2 * h))
+    return out
+
+
+def test_gradient_converged_directions_c4(pkg, table):
+    """The gradient configuration at its own size (64^3, 20 steps, checkpoint 5):
+    along each of 16 seeded directions -- the blast energy alone, the ambient
+    density alone, and 14 random combinations of both with the per-zone
+    perturbation field -- the central finite difference is taken at relative
+    steps 1e-5, 1e-6 and 1e-7.  Where those agree with each other to 1e-7 the
+    finite difference has converged (no limiter or Riemann-sampling branch
+    switch inside its stencil), and there the adjoint must match it to 1e-6;
+    the other directions are reported with their spread."""
+    import torch
+
+    run, inst = _runner(pkg, table, 1, 20, 5)
+    p = inst["problem"]
+    E0, R0 = p["exp_energy"], p["dens_ambient"]
+    pert0 = run.pert.clone()
+    run.forward(E0, R0, pert0)
+    dE, dR, dP = run.backward()
+    n = run.n[0]
+    zero = torch.zeros_like(pert0)
+    dirs = [(1.0, 0.0, zero), (0.0, 1.0, zero)]
+    for a, b, c in _directions(n, 14, 2019):
+        dirs.append((a, b, torch.from_numpy(np.ascontiguousarray(c.transpose(2, 1, 0))).cuda()))
+    converged, other = [], []
+    for a, b, ct in dirs:
+        ad = dE * E0 * a + dR * R0 * b + float((dP * ct).sum())
+        f5, f6, f7 = _fd_steps(run, E0, R0, pert0, a, b, ct)
+        scale = max(abs(f5), abs(f6), abs(f7))
+        spread = max(abs(f5 - f6), abs(f6 - f7), abs(f5 - f7)) / scale
+        err = abs(ad - f6) / max(abs(ad), abs(f6))
+        (converged if spread <= 1e-7 else other).append((err, spread))
+    print("converged directions (rel err, FD spread):", ["%.2e/%.1e" % e for e in converged])
+    print("other directions (rel err, FD spread):", ["%.2e/%.1e" % e for e in other])
+    assert converged, "no direction's finite difference converged"
+    assert max(e for e, _ in converged) <= 1e-6, converged
+    run.close()
