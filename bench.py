@@ -285,10 +285,12 @@ def run_b200(args, pkg, rank, world):
         sim3.close()
         return out
 
-    plain = plain_box = None
+    plain = plain_box = persistent = None
     if rank == 0 and args.plain_steps > 0:
         plain = time_per_box(pkg.castro.MODE_PLAIN)
         plain_box = time_per_box(pkg.castro.MODE_PLAIN_BOX)
+    if rank == 0 and args.persistent_steps > 0:
+        persistent = time_mode(pkg, L, cfg, pkg.castro.MODE_PERSISTENT, args.persistent_steps, zones)
 
     batched_cfg = None
     if args.batched_steps > 0:      # every rank: the instances are split over the ranks
@@ -371,6 +373,7 @@ def run_b200(args, pkg, rank, world):
         "roofline": roof,
         "plain_per_box": plain,
         "plain_box_drop_in": plain_box,
+        "persistent": persistent,
         "batched_config": batched_cfg,
         "adjoint_config": adjoint_cfg,
         "adjoint_forward_ratio": adjoint_cfg["adjoint_forward_ratio"] if adjoint_cfg else None,
@@ -379,6 +382,30 @@ def run_b200(args, pkg, rank, world):
         "clocks": clk.summary(),
     }
     return line
+
+
+def time_mode(pkg, L, cfg, mode, steps, zones):
+    """zone-updates/s of one sim mode on a workload, device-timed on the sim's stream
+    after two untimed steps (the persistent mode: the batched step as one cooperative
+    launch per step over device work queues)."""
+    import torch
+
+    sim = pkg.make_sim(L, cfg, mode)
+    sim.init_data()
+    sim.step(2)
+    sim.sync()
+    st = torch.cuda.ExternalStream(sim.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    sim.step(steps)
+    e1.record(st)
+    e1.synchronize()
+    sim.sync()
+    ms = e0.elapsed_time(e1)
+    out = {"value": zones * steps / (ms * 1e-3), "ms_per_step": ms / steps, "steps": steps,
+           "launches_per_step": sim.launches_per_step()}
+    sim.close()
+    return out
 
 
 def table_window_effect(pkg, L, cfg, reps=3):
@@ -419,6 +446,7 @@ def run_batched_config(pkg, L, args, rank=0, world=1):
                         "rank); no data-path collective" if world > 1 else "one GPU"),
            "scaling": "strong" if world > 1 else "single"}
     for mode, key, steps in ((pkg.castro.MODE_BATCHED, "batched", args.batched_steps),
+                             (pkg.castro.MODE_PERSISTENT, "persistent", args.batched_steps),
                              (pkg.castro.MODE_PLAIN, "plain_per_box", 2)):
         ms = 0.0
         launches = 0
@@ -440,6 +468,7 @@ def run_batched_config(pkg, L, args, rank=0, world=1):
         out[key] = {"value": zones * steps / (ms * 1e-3), "ms_per_step": ms / steps, "steps": steps,
                     "launches_per_step": launches}
     out["speedup_batched_over_plain"] = out["batched"]["value"] / out["plain_per_box"]["value"]
+    out["persistent_over_batched"] = out["persistent"]["value"] / out["batched"]["value"]
     return out
 
 
@@ -620,6 +649,7 @@ def main():
     ap.add_argument("--workload", default="sedov128_pert")
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--batched-steps", type=int, default=18, help="timed steps of the batched configuration (0: skip)")
+    ap.add_argument("--persistent-steps", type=int, default=20, help="timed steps of the one-launch persistent step (0: skip)")
     ap.add_argument("--adjoint-reps", type=int, default=3, help="timed forward+reverse runs of the adjoint configuration (0: skip)")
     ap.add_argument("--adjoint-fd", type=int, default=16, help="finite-difference directions of the gradient check (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

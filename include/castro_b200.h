@@ -51,7 +51,8 @@ enum {
     CASTRO_ERR_NSPEC = 4,       /* network size other than 2 or 13 */
     CASTRO_ERR_ARG = 5,         /* invalid argument */
     CASTRO_ERR_EOS = 6,         /* EOS Newton iteration did not converge */
-    CASTRO_ERR_IO = 7           /* a checkpoint or plotfile could not be read or written */
+    CASTRO_ERR_IO = 7,          /* a checkpoint or plotfile could not be read or written */
+    CASTRO_ERR_TIMEOUT = 8      /* a device-side wait ran out of its iteration limit; the step is void */
 };
 int         castro_last_error(void);          /* sticky: first error since castro_clear_error */
 void        castro_clear_error(void);
@@ -255,9 +256,13 @@ typedef struct castro_sim castro_sim;
 enum { CASTRO_BC_PERIODIC = 0, CASTRO_BC_OUTFLOW = 1 };
 enum { CASTRO_MODE_PLAIN = 0,      /* per-box launches of the per-routine kernels, reference call sequence */
        CASTRO_MODE_BATCHED = 1,    /* fused kernels over every box of every instance, CUDA-graph replay */
-       CASTRO_MODE_PLAIN_BOX = 2 };/* the reference call sequence per box, each box's hydro source from
+       CASTRO_MODE_PLAIN_BOX = 2,  /* the reference call sequence per box, each box's hydro source from
                                     * castro_construct_hydro_source_box (what a Castro host calling the
                                     * coarse entry point from its MFIter loop runs) */
+       CASTRO_MODE_PERSISTENT = 3 };/* the batched step as ONE cooperative launch: resident CTAs pull the
+                                    * work items of every box of every instance from a device queue per
+                                    * stage, grid barriers between stages with bounded waits, the next dt
+                                    * formed in the epilogue */
 
 typedef struct {
     int dom_lo[3], dom_hi[3];
@@ -319,6 +324,13 @@ int    castro_sim_write_plotfile(castro_sim* sim, int inst, const char* dir);
  * run then continues bit for bit as if it had not stopped, in any mode. */
 int    castro_sim_write_checkpoint(castro_sim* sim, const char* dir);
 int    castro_sim_read_checkpoint(castro_sim* sim, const char* dir);
+/* CASTRO_MODE_PERSISTENT: the limit of every grid-barrier wait, in polls of
+ * about 64 ns (default 2^24, ~1 s), after which the step ends with
+ * CASTRO_ERR_TIMEOUT at the next castro_sim_sync.  Fault-injection hook for
+ * tests: when extra > 0 the barrier after stage 'stage' (0 front ... 6 riemann3)
+ * waits for 'extra' more CTAs than exist, so its wait must run out.  No
+ * reference counterpart. */
+int    castro_sim_set_wait_limit(castro_sim* sim, long long polls, int stage, int extra);
 /* the CUDA stream (cudaStream_t) every launch of this sim is issued on */
 void*  castro_sim_stream(castro_sim* sim);
 /* batched mode: one step with a CUDA event around each of the fused kernels

@@ -17,7 +17,7 @@ LIBDIR = os.path.join(HERE, "lib")
 MAX_SPEC = 13
 
 BC_PERIODIC, BC_OUTFLOW = 0, 1
-MODE_PLAIN, MODE_BATCHED, MODE_PLAIN_BOX = 0, 1, 2
+MODE_PLAIN, MODE_BATCHED, MODE_PLAIN_BOX, MODE_PERSISTENT = 0, 1, 2, 3
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -81,6 +81,7 @@ ABI_SYMBOLS = [
     "castro_adj_backward", "castro_adj_dt", "castro_adj_final_state", "castro_adj_initial_adjoint",
     "castro_adj_time_ms", "castro_adj_device_bytes", "castro_sim_write_plotfile",
     "castro_sim_write_checkpoint", "castro_sim_read_checkpoint", "castro_set_table_l2_window",
+    "castro_sim_set_wait_limit",
 ]
 
 
@@ -140,6 +141,7 @@ def load(exact: bool = False) -> C.CDLL:
     L.castro_sim_eos_failures.argtypes = [C.c_void_p]
     L.castro_sim_write_plotfile.argtypes = [C.c_void_p, C.c_int, C.c_char_p]
     L.castro_set_table_l2_window.argtypes = [C.c_int]
+    L.castro_sim_set_wait_limit.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_int]
     L.castro_sim_write_checkpoint.argtypes = [C.c_void_p, C.c_char_p]
     L.castro_sim_read_checkpoint.argtypes = [C.c_void_p, C.c_char_p]
     L.castro_adj_create.restype = C.c_void_p

@@ -215,10 +215,9 @@ struct SimDev {
 // item of a work list -> (box, zone index) of the thread's point in pass rep
 // of the item (an item holds up to BLOCK points per pass); returns false for
 // idle threads
-__device__ __forceinline__ bool work_point_rep(const Work* wl, const SimDev& S, int kind, int subkind_tbx, int rep,
+__device__ __forceinline__ bool work_point_rep(const Work& w, const SimDev& S, int kind, int subkind_tbx, int rep,
                                               int& b, int& sub, Reg& R, int& i, int& j, int& k)
 {
-    const Work w = wl[blockIdx.x];
     const int tp = rep * BLOCK + (int)threadIdx.x;
     if (tp >= w.count) return false;
     b = w.box;
@@ -235,10 +234,10 @@ __device__ __forceinline__ bool work_point_rep(const Work* wl, const SimDev& S, 
     return true;
 }
 
-__device__ __forceinline__ bool work_point(const Work* wl, const SimDev& S, int kind, int subkind_tbx, int& b, int& sub,
+__device__ __forceinline__ bool work_point(const Work& w, const SimDev& S, int kind, int subkind_tbx, int& b, int& sub,
                                           Reg& R, int& i, int& j, int& k)
 {
-    return work_point_rep(wl, S, kind, subkind_tbx, 0, b, sub, R, i, j, k);
+    return work_point_rep(w, S, kind, subkind_tbx, 0, b, sub, R, i, j, k);
 }
 
 // Q lives on grow(domain,4) and Sborder on grow(domain,1) of the box's
@@ -303,11 +302,11 @@ __device__ __forceinline__ double block_min(double m)
 
 // front: clean_state(S_old) -> S_new base; clean_state(Sborder); ctoprim
 template <int NS>
-__global__ void LB_EOS k_front(SimDev S, const Work* wl)
+__device__ __forceinline__ void front_body(const SimDev& S, const Work& w)
 {
     int b, sub, i, j, k;
     Reg R;
-    if (!work_point(wl, S, R_VALID, -1, b, sub, R, i, j, k)) return;
+    if (!work_point(w, S, R_VALID, -1, b, sub, R, i, j, k)) return;
     const BoxDev& B = S.boxes[b];
     constexpr int NVAR = Dims<NS>::NVAR, QVAR = Dims<NS>::QVAR;
     double u[NVAR];
@@ -343,6 +342,12 @@ __global__ void LB_EOS k_front(SimDev S, const Work* wl)
     Q[id4 + R4.np * F::C] = qa[QC];
 }
 
+template <int NS>
+__global__ void LB_EOS k_front(SimDev S, const Work* wl)
+{
+    front_body<NS>(S, wl[blockIdx.x]);
+}
+
 __device__ __forceinline__ int map_bc(int i, int lo, int hi, int bc)
 {
     if (bc == CASTRO_BC_PERIODIC) {
@@ -360,9 +365,8 @@ __device__ __forceinline__ int map_bc(int i, int lo, int hi, int bc)
 // box = any box of the instance (for its arrays), sub = slab of the domain halo.
 // Sources are domain zones, written by k_front, never halo zones.
 template <int NS>
-__global__ void __launch_bounds__(BLOCK) k_ghost(SimDev S, const Work* wl)
+__device__ __forceinline__ void ghost_body(const SimDev& S, const Work& w)
 {
-    const Work w = wl[blockIdx.x];
     if ((int)threadIdx.x >= w.count) return;
     const BoxDev& B = S.boxes[w.box];
     const InstDev& I = S.inst[B.inst];
@@ -390,15 +394,21 @@ __global__ void __launch_bounds__(BLOCK) k_ghost(SimDev S, const Work* wl)
     }
 }
 
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_ghost(SimDev S, const Work* wl)
+{
+    ghost_body<NS>(S, wl[blockIdx.x]);
+}
+
 // prep: divu at the nodes of grow(bx,1) (Castro_hydro_nd.F90:45-63) and the
 // flattening coefficient of every zone of grow(bx,1) (ppm.F90:11-128), which
 // trace_ppm recomputes per direction in the reference and is formed once here
 template <int NS>
-__global__ void __launch_bounds__(BLOCK) k_prep(SimDev S, const Work* wl)
+__device__ __forceinline__ void prep_body(const SimDev& S, const Work& w)
 {
     int b, sub, i, j, k;
     Reg R;
-    if (!work_point(wl, S, R_G1, -1, b, sub, R, i, j, k)) return;
+    if (!work_point(w, S, R_G1, -1, b, sub, R, i, j, k)) return;
     const BoxDev& B = S.boxes[b];
     const InstDev& I = S.inst[B.inst];
     QLoader<NS> ld;
@@ -421,6 +431,12 @@ __global__ void __launch_bounds__(BLOCK) k_prep(SimDev S, const Work* wl)
     long long id = ridx(R, i, j, k);
     S.Div[B.offDiv + id] = ux + vy + wz;
     S.Div[B.offDiv + id + R.np] = uflatten(ld, i, j, k);
+}
+
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_prep(SimDev S, const Work* wl)
+{
+    prep_body<NS>(S, wl[blockIdx.x]);
 }
 
 // trace_ppm (Source/ppm.F90:437-737) along one segment of up to TSEG zones of
@@ -578,11 +594,11 @@ __device__ __forceinline__ void trace_segment(const SimDev& S, const BoxDev& B, 
 }
 
 template <int NS, int PASSES>
-__device__ __forceinline__ void trace_item(const SimDev& S, const Work* wl)
+__device__ __forceinline__ void trace_item(const SimDev& S, const Work& w)
 {
     int b, d, i, j, k;
     Reg R;
-    if (!work_point(wl, S, R_SEG, -1, b, d, R, i, j, k)) return;
+    if (!work_point(w, S, R_SEG, -1, b, d, R, i, j, k)) return;
     const BoxDev& B = S.boxes[b];
     const InstDev& I = S.inst[B.inst];
     const double dt = S.st[B.inst].dt;
@@ -605,13 +621,13 @@ __device__ __forceinline__ void trace_item(const SimDev& S, const Work* wl)
 template <int NS>
 __global__ void LB_TRACE k_trace(SimDev S, const Work* wl)
 {
-    trace_item<NS, CASTRO_TRACE_SPLIT ? 1 : 3>(S, wl);
+    trace_item<NS, CASTRO_TRACE_SPLIT ? 1 : 3>(S, wl[blockIdx.x]);
 }
 
 template <int NS>
 __global__ void LB_TRACE2 k_trace2(SimDev S, const Work* wl)
 {
-    trace_item<NS, 2>(S, wl);
+    trace_item<NS, 2>(S, wl[blockIdx.x]);
 }
 
 // compute_flux on the face (i,j,k) normal to D: left zone i-e_D, right zone i
@@ -651,11 +667,11 @@ __device__ __forceinline__ void load_tf(const double* base, const Reg& R, long l
 
 // riemann1: compute_flux on tbx[d][d] (Castro_hydro.cpp:214-224)
 template <int NS>
-__global__ void LB_RIEMANN k_riemann1(SimDev S, const Work* wl)
+__device__ __forceinline__ void riemann1_body(const SimDev& S, const Work& w)
 {
     int b, d, i, j, k;
     Reg R;
-    if (!work_point(wl, S, R_TBX, 0, b, d, R, i, j, k)) return;
+    if (!work_point(w, S, R_TBX, 0, b, d, R, i, j, k)) return;
     const BoxDev& B = S.boxes[b];
     constexpr int NQS = Dims<NS>::NQS, NVAR = Dims<NS>::NVAR;
     const double* T = S.Tr + B.offTr[d];
@@ -672,6 +688,12 @@ __global__ void LB_RIEMANN k_riemann1(SimDev S, const Work* wl)
     else if (d == 1) g = riemann_at<NS, 1>(ld, i, j, k, ql, qr, flx);
     else g = riemann_at<NS, 2>(ld, i, j, k, ql, qr, flx);
     store_tf<NS>(S.F1 + B.offF1[d], R, f, flx, g.x, g.y);
+}
+
+template <int NS>
+__global__ void LB_RIEMANN k_riemann1(SimDev S, const Work* wl)
+{
+    riemann1_body<NS>(S, wl[blockIdx.x]);
 }
 
 // 8-byte asynchronous global -> shared copies (cp.async, Ampere and later):
@@ -796,12 +818,12 @@ __device__ __forceinline__ void cross_flux_both(const SimDev& S, const BoxDev& B
 
 // riemann2: one thread per face of tbx[a][a] (Castro_hydro.cpp:228-304)
 template <int NS>
-__global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
+__device__ __forceinline__ void riemann2_body(const SimDev& S, const Work& w)
 {
     int bx, a, i, j, k;
     Reg R;
     for (int rp = 0; rp < CASTRO_R2_ROWS; ++rp) {
-        if (!work_point_rep(wl, S, R_TBX, 0, rp, bx, a, R, i, j, k)) return;
+        if (!work_point_rep(w, S, R_TBX, 0, rp, bx, a, R, i, j, k)) return;
         const BoxDev& B = S.boxes[bx];
         const InstDev& I = S.inst[B.inst];
         const double dt = S.st[B.inst].dt;
@@ -812,6 +834,12 @@ __global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
         else if (a == 1) cross_flux_both<NS, 1>(S, B, I, ld, i, j, k, dt);
         else cross_flux_both<NS, 2>(S, B, I, ld, i, j, k, dt);
     }
+}
+
+template <int NS>
+__global__ void LB_RIEMANN k_riemann2(SimDev S, const Work* wl)
+{
+    riemann2_body<NS>(S, wl[blockIdx.x]);
 }
 
 // CASTRO_R3_STAGE: 0 plain loads, 1 the per-face operands of riemann3 that no
@@ -984,12 +1012,12 @@ __device__ __forceinline__ void riemann3_dir(const SimDev& S, const BoxDev& B, c
 
 // riemann3: the final fluxes on ebx[d] from the F2 pool
 template <int NS>
-__global__ void LB_R3 k_riemann3(SimDev S, const Work* wl)
+__device__ __forceinline__ void riemann3_body(const SimDev& S, const Work& w)
 {
     int bx, d, i, j, k;
     Reg R;
     for (int rp = 0; rp < CASTRO_R3_ROWS; ++rp) {
-        if (!work_point_rep(wl, S, R_EBX, -1, rp, bx, d, R, i, j, k)) return;
+        if (!work_point_rep(w, S, R_EBX, -1, rp, bx, d, R, i, j, k)) return;
         const BoxDev& B = S.boxes[bx];
         const InstDev& I = S.inst[B.inst];
         const double dt = S.st[B.inst].dt;
@@ -1002,15 +1030,20 @@ __global__ void LB_R3 k_riemann3(SimDev S, const Work* wl)
     }
 }
 
+template <int NS>
+__global__ void LB_R3 k_riemann3(SimDev S, const Work* wl)
+{
+    riemann3_body<NS>(S, wl[blockIdx.x]);
+}
+
 // update: fill_hydro_source, Saxpy, clean_state (advance), clean_state
 // (post_timestep), estdt of the new state
 template <int NS>
-__global__ void LB_EOS k_update(SimDev S, const Work* wl)
+__device__ __forceinline__ void update_body(const SimDev& S, const Work& w)
 {
     int b, sub, i, j, k;
     Reg R;
-    bool active = work_point(wl, S, R_VALID, -1, b, sub, R, i, j, k);
-    const Work w = wl[blockIdx.x];
+    bool active = work_point(w, S, R_VALID, -1, b, sub, R, i, j, k);
     const BoxDev& B = S.boxes[w.box];
     const InstDev& I = S.inst[B.inst];
     double m = 1.79769313486231570e+308;
@@ -1064,14 +1097,19 @@ __global__ void LB_EOS k_update(SimDev S, const Work* wl)
     if (threadIdx.x == 0) atomic_min_pos(&S.st[B.inst].dt_est, m);
 }
 
+template <int NS>
+__global__ void LB_EOS k_update(SimDev S, const Work* wl)
+{
+    update_body<NS>(S, wl[blockIdx.x]);
+}
+
 // estdt on the current state (computeInitialDt / castro_sim_est_time_step)
 template <int NS>
-__global__ void __launch_bounds__(BLOCK) k_estdt_state(SimDev S, const Work* wl)
+__device__ __forceinline__ void estdt_state_body(const SimDev& S, const Work& w)
 {
     int b, sub, i, j, k;
     Reg R;
-    bool active = work_point(wl, S, R_VALID, -1, b, sub, R, i, j, k);
-    const Work w = wl[blockIdx.x];
+    bool active = work_point(w, S, R_VALID, -1, b, sub, R, i, j, k);
     const BoxDev& B = S.boxes[w.box];
     const InstDev& I = S.inst[B.inst];
     double m = 1.79769313486231570e+308;
@@ -1088,16 +1126,19 @@ __global__ void __launch_bounds__(BLOCK) k_estdt_state(SimDev S, const Work* wl)
     if (threadIdx.x == 0) atomic_min_pos(&S.st[B.inst].dt_est, m);
 }
 
+template <int NS>
+__global__ void __launch_bounds__(BLOCK) k_estdt_state(SimDev S, const Work* wl)
+{
+    estdt_state_body<NS>(S, wl[blockIdx.x]);
+}
+
 // computeInitialDt (DT_FIRST) or, after a step, time/step bookkeeping and
 // computeNewDt (DT_STEP; Source/Castro.cpp:162-341).  DT_RESTART is
 // computeNewDt alone, for a state restored from a checkpoint whose st.dt holds
 // the last step's dt: the same dt the uninterrupted run formed at that step's end.
 enum { DT_STEP = 0, DT_FIRST = 1, DT_RESTART = 2 };
-__global__ void k_dt(SimDev S, int ninst, int first)
+__device__ __forceinline__ void next_dt(InstState& st, int first)
 {
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= ninst) return;
-    InstState& st = S.st[n];
     double est = st.dt_est * cfl;                       // estTimeStep, Castro.cpp:212-213
     double dt_0;
     if (first == DT_FIRST) {
@@ -1117,6 +1158,146 @@ __global__ void k_dt(SimDev S, int ninst, int first)
     }
     st.dt = dt_0;
     st.dt_est = 1.79769313486231570e+308;
+}
+
+__global__ void k_dt(SimDev S, int ninst, int first)
+{
+    int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= ninst) return;
+    next_dt(S.st[n], first);
+}
+
+// ---------------------------------------------------------------------------
+// CASTRO_MODE_PERSISTENT: the whole batched step in ONE cooperative launch.
+// Every CTA stays resident for the step and pulls work items -- (box or
+// domain box, region, chunk) descriptors of every instance -- from one device
+// queue per stage with an atomic counter, so the CTAs that finish early take
+// the remaining items of the ragged BoxArrays and instance sizes.  The stages
+// are those of the ten-kernel graph (front, ghost, prep, trace with both of its
+// passes in one queue, riemann1-3, update); between two stages the CTAs meet
+// at a grid barrier.  Co-residency is guaranteed by the cooperative launch, and
+// every barrier wait is bounded: after PersistArgs::spin_limit polls it
+// records the stage in the control block's error word and the CTA returns,
+// as does every other CTA that sees the word, so a stuck step ends with an
+// error the host reads (castro_sim_sync) instead of a hang.  The update stage
+// folds each box's estdt into its instance's dt_est (warp-shuffle block minimum,
+// one atomic per item: a reduction segmented by instance); the last CTA to
+// finish the step forms every instance's next dt (computeNewDt) in the epilogue.
+// ---------------------------------------------------------------------------
+enum { PS_FRONT = 0, PS_GHOST, PS_PREP, PS_TRACE, PS_R1, PS_R2, PS_R3, PS_UPDATE, PS_COUNT };
+
+struct PersistCtl {
+    unsigned int queue[PS_COUNT];    // next item of each stage's queue
+    unsigned int arrive[PS_COUNT];   // CTAs past each stage
+    unsigned int done;               // CTAs that finished the step
+    int error;                       // 0, or 1 + the stage whose barrier wait ran out
+};
+
+struct PersistArgs {
+    const Work* wl[PS_COUNT];
+    int n[PS_COUNT];                 // items per stage (trace: pass 1 items, then pass 2 items)
+    int trace_items;                 // items of one trace pass
+    PersistCtl* ctl;
+    int ninst;
+    long long spin_limit;            // polls of a barrier wait before it gives up
+    int test_stage;                  // test hook: the barrier after this stage ...
+    int test_extra;                  // ... waits for this many CTAs more than exist (0: none)
+};
+
+#ifndef CASTRO_MINB_PERSIST
+#define CASTRO_MINB_PERSIST 3
+#endif
+#ifndef CASTRO_MINB13_PERSIST
+#define CASTRO_MINB13_PERSIST 2
+#endif
+#define LB_PERSIST CASTRO_LB_NS(CASTRO_MINB_PERSIST, CASTRO_MINB13_PERSIST)
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p)
+{
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ int ld_acquire_s32(const int* p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// grid barrier after stage st; false when a wait ran out (this CTA's or another's)
+__device__ __forceinline__ bool persist_barrier(const PersistArgs& P, int st)
+{
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        __threadfence();                                   // this CTA's stage writes, device-wide
+        atomicAdd(&P.ctl->arrive[st], 1u);
+        const unsigned int target = gridDim.x + (st == P.test_stage ? (unsigned int)P.test_extra : 0u);
+        int ok = 1;
+        long long polls = 0;
+        while (ld_acquire_u32(&P.ctl->arrive[st]) < target) {
+            if (ld_acquire_s32(&P.ctl->error) != 0) { ok = 0; break; }
+            if (++polls > P.spin_limit) {
+                atomicCAS(&P.ctl->error, 0, st + 1);
+                ok = 0;
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <int NS>
+__device__ __forceinline__ void persist_item(const SimDev& S, const SimDev& Sd, const PersistArgs& P, int st, int item)
+{
+    switch (st) {
+    case PS_FRONT: front_body<NS>(S, P.wl[PS_FRONT][item]); break;
+    case PS_GHOST: ghost_body<NS>(S, P.wl[PS_GHOST][item]); break;
+    case PS_PREP: prep_body<NS>(Sd, P.wl[PS_PREP][item]); break;
+    case PS_TRACE:
+        if (!CASTRO_TRACE_SPLIT) trace_item<NS, 3>(Sd, P.wl[PS_TRACE][item]);
+        else if (item < P.trace_items) trace_item<NS, 1>(Sd, P.wl[PS_TRACE][item]);
+        else trace_item<NS, 2>(Sd, P.wl[PS_TRACE][item - P.trace_items]);
+        break;
+    case PS_R1: riemann1_body<NS>(Sd, P.wl[PS_R1][item]); break;
+    case PS_R2: riemann2_body<NS>(Sd, P.wl[PS_R2][item]); break;
+    case PS_R3: riemann3_body<NS>(Sd, P.wl[PS_R3][item]); break;
+    default: update_body<NS>(S, P.wl[PS_UPDATE][item]); break;
+    }
+}
+
+template <int NS>
+__global__ void LB_PERSIST k_step_persistent(SimDev S, PersistArgs P)
+{
+    __shared__ int s_item;
+    SimDev Sd = S;
+    Sd.boxes = S.dom;                                      // the stage kernels' items name domain boxes
+    for (int st = 0; st < PS_COUNT; ++st) {
+        const int n = P.n[st];
+        while (true) {
+            if (threadIdx.x == 0) s_item = (int)atomicAdd(&P.ctl->queue[st], 1u);
+            __syncthreads();
+            const int item = s_item;
+            __syncthreads();                               // every thread has the item before the slot is reused
+            if (item >= n) break;
+            persist_item<NS>(S, Sd, P, st, item);
+        }
+        if (st + 1 < PS_COUNT && !persist_barrier(P, st)) return;
+    }
+    // epilogue: the last CTA to finish forms every instance's next dt from the
+    // dt_est minima its update items folded in
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&P.ctl->done, 1u) == gridDim.x - 1) {
+            __threadfence();
+            for (int n = 0; n < P.ninst; ++n) next_dt(S.st[n], DT_STEP);
+        }
+    }
 }
 
 // FillPatch of Sborder for the plain path: every zone of grow(bx,4) from the
@@ -1151,9 +1332,10 @@ __global__ void __launch_bounds__(BLOCK) k_fill_sborder(SimDev S, int b, double*
 template <int NS>
 __global__ void __launch_bounds__(BLOCK) k_box_prim(SimDev S, const Work* wl, Fab SB)
 {
+    const Work& w = wl[blockIdx.x];
     int b, sub, i, j, k;
     Reg R;
-    if (!work_point(wl, S, R_G4, -1, b, sub, R, i, j, k)) return;
+    if (!work_point(w, S, R_G4, -1, b, sub, R, i, j, k)) return;
     const BoxDev& B = S.boxes[b];
     constexpr int NVAR = Dims<NS>::NVAR, QVAR = Dims<NS>::QVAR;
     double u[NVAR], q[QVAR], qa[NQAUX];
@@ -1188,9 +1370,10 @@ __global__ void __launch_bounds__(BLOCK) k_box_prim(SimDev S, const Work* wl, Fa
 template <int NS>
 __global__ void __launch_bounds__(BLOCK) k_box_source(SimDev S, const Work* wl, Fab SRC)
 {
+    const Work& w = wl[blockIdx.x];
     int b, sub, i, j, k;
     Reg R;
-    if (!work_point(wl, S, R_VALID, -1, b, sub, R, i, j, k)) return;
+    if (!work_point(w, S, R_VALID, -1, b, sub, R, i, j, k)) return;
     const BoxDev& B = S.boxes[b];
     const InstDev& I = S.inst[B.inst];
     constexpr int NVAR = Dims<NS>::NVAR;
@@ -1231,9 +1414,10 @@ __global__ void __launch_bounds__(BLOCK) k_box_source(SimDev S, const Work* wl, 
 template <int NS>
 __global__ void __launch_bounds__(BLOCK) k_box_store_flux(SimDev S, const Work* wl, Fab FO0, Fab FO1, Fab FO2, double dt)
 {
+    const Work& w = wl[blockIdx.x];
     int b, d, i, j, k;
     Reg R;
-    if (!work_point(wl, S, R_EBX, -1, b, d, R, i, j, k)) return;
+    if (!work_point(w, S, R_EBX, -1, b, d, R, i, j, k)) return;
     const BoxDev& B = S.boxes[b];
     const InstDev& I = S.inst[B.inst];
     const Fab& FO = d == 0 ? FO0 : d == 1 ? FO1 : FO2;
@@ -1305,6 +1489,14 @@ struct castro_sim {
     // through castro_last_error when this sim last synchronized
     unsigned long long eos_seen = 0;
     unsigned long long eos_base = 0;   // the counter when this sim was created
+    // CASTRO_MODE_PERSISTENT: control block, arguments and launch shape of the
+    // one cooperative launch per step
+    PersistCtl* pctl = nullptr;
+    PersistArgs pargs;
+    int pgrid = 0;
+    size_t psmem = 0;
+    bool pdirect = false;      // the driver refused to capture the cooperative launch: launch it directly
+    bool failed = false;       // a device wait ran out: the state is void
     // plain-path scratch (largest box)
     double* sb = nullptr;      // Sborder per box (grow 4) for all boxes
     double* src = nullptr;     // hydro_source per box for all boxes
@@ -1716,6 +1908,93 @@ void plain_step(castro_sim* s)
     castro_set_stream(saved);
 }
 
+// CASTRO_MODE_PERSISTENT set-up: the stage queues (the batched path's work
+// lists), the control block, and the launch shape -- one CTA per resident slot
+// of every SM, which the cooperative launch guarantees to be co-resident.
+template <int NS>
+bool persistent_setup(castro_sim* s)
+{
+    if (!dalloc(&s->pctl, 1, "persistent control")) return false;
+    PersistArgs& P = s->pargs;
+    memset(&P, 0, sizeof P);
+    P.wl[PS_FRONT] = s->w_valid;  P.n[PS_FRONT] = s->n_valid;
+    P.wl[PS_GHOST] = s->w_ghost;  P.n[PS_GHOST] = s->n_ghost;
+    P.wl[PS_PREP] = s->w_g1;      P.n[PS_PREP] = s->n_g1;
+    P.wl[PS_TRACE] = s->w_trace;  P.n[PS_TRACE] = s->n_trace * (CASTRO_TRACE_SPLIT ? 2 : 1);
+    P.trace_items = s->n_trace;
+    P.wl[PS_R1] = s->w_tbx;       P.n[PS_R1] = s->n_tbx;
+    P.wl[PS_R2] = s->w_r2;        P.n[PS_R2] = s->n_r2;
+    P.wl[PS_R3] = s->w_r3;        P.n[PS_R3] = s->n_r3;
+    P.wl[PS_UPDATE] = s->w_valid; P.n[PS_UPDATE] = s->n_valid;
+    P.ctl = s->pctl;
+    P.ninst = s->ninst;
+    P.spin_limit = 1LL << 24;
+    P.test_stage = -1;
+    s->psmem = std::max((size_t)R2Slot<NS>::BYTES, (size_t)R3Slot<NS>::BYTES);
+    if (s->psmem > 48 * 1024 &&
+        !cuda_ok(cudaFuncSetAttribute(k_step_persistent<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->psmem),
+                 "persistent step shared memory"))
+        return false;
+    int dev = 0, nsm = 0, coop = 0, per_sm = 0;
+    if (!cuda_ok(cudaGetDevice(&dev), "device") ||
+        !cuda_ok(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "SM count") ||
+        !cuda_ok(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "cooperative launch") ||
+        !cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_persistent<NS>, BLOCK, s->psmem), "occupancy"))
+        return false;
+    if (!coop || per_sm < 1) {
+        set_error(CASTRO_ERR_CUDA, "castro_sim_create: the device cannot run the persistent step (no cooperative launch)");
+        return false;
+    }
+    s->pgrid = nsm * per_sm;
+    return true;
+}
+
+template <int NS>
+void persistent_launch(castro_sim* s)
+{
+    SimDev S = s->dev();
+    PersistArgs P = s->pargs;
+    void* args[] = {&S, &P};
+    cuda_ok(cudaMemsetAsync(s->pctl, 0, sizeof(PersistCtl), s->st), "persistent queue reset");
+    cuda_ok(cudaLaunchCooperativeKernel((const void*)k_step_persistent<NS>, dim3(s->pgrid), dim3(BLOCK), args, s->psmem,
+                                        s->st),
+            "persistent step launch");
+}
+
+template <int NS>
+int persistent_step(castro_sim* s)
+{
+    if (s->failed) {
+        set_error(CASTRO_ERR_TIMEOUT, "castro_sim_step: an earlier step ran out of a device wait; the state is void");
+        return CASTRO_ERR_TIMEOUT;
+    }
+    if (!s->gexec && !s->pdirect) {
+        // one graph per step: the queue reset and the cooperative launch
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ge = nullptr;
+        bool ok = cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            persistent_launch<NS>(s);
+            ok = cudaStreamEndCapture(s->st, &g) == cudaSuccess && g &&
+                 cudaGraphInstantiate(&ge, g, 0) == cudaSuccess && castro_last_error() == 0;
+        }
+        if (ok) {
+            s->graph = g;
+            s->gexec = ge;
+        } else {
+            if (ge) cudaGraphExecDestroy(ge);
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            castro_clear_error();
+            s->pdirect = true;
+        }
+    }
+    if (s->pdirect) persistent_launch<NS>(s);
+    else cuda_ok(cudaGraphLaunch(s->gexec, s->st), "graph launch");
+    s->launches = 1;
+    return castro_last_error();
+}
+
 template <int NS>
 int step_impl(castro_sim* s)
 {
@@ -1732,6 +2011,7 @@ int step_impl(castro_sim* s)
         initial_dt_kernels<NS>(s);
         s->dt_ready = true;
     }
+    if (s->mode == CASTRO_MODE_PERSISTENT) return persistent_step<NS>(s);
     if (!s->gexec) {
         if (!cuda_ok(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal), "begin capture")) return castro_last_error();
         batched_step_kernels<NS>(s);
@@ -1800,7 +2080,8 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
 {
     if (!table_ready()) { set_error(CASTRO_ERR_NO_TABLE, "castro_sim_create: eos_init has not run"); return nullptr; }
     if (ninst < 1 || !desc) { set_error(CASTRO_ERR_ARG, "castro_sim_create: no instances"); return nullptr; }
-    if (mode != CASTRO_MODE_PLAIN && mode != CASTRO_MODE_BATCHED && mode != CASTRO_MODE_PLAIN_BOX) {
+    if (mode != CASTRO_MODE_PLAIN && mode != CASTRO_MODE_BATCHED && mode != CASTRO_MODE_PLAIN_BOX &&
+        mode != CASTRO_MODE_PERSISTENT) {
         set_error(CASTRO_ERR_ARG, "castro_sim_create: unknown mode");
         return nullptr;
     }
@@ -1925,7 +2206,7 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
         }
         cuda_ok(cudaMemcpy(s->dstate, hs.data(), ninst * sizeof(InstState), cudaMemcpyHostToDevice), "state");
     }
-    if (ok && mode == CASTRO_MODE_BATCHED) {
+    if (ok && (mode == CASTRO_MODE_BATCHED || mode == CASTRO_MODE_PERSISTENT)) {
         ok = dalloc(&s->Ub, oUb, "Ub") && dalloc(&s->Q, oQ, "Q") && dalloc(&s->Div, oDiv, "Div") &&
              dalloc(&s->Tr, oTr, "Tr") && dalloc(&s->F1, oF1, "F1") && dalloc(&s->F2, oF2, "F2") && dalloc(&s->Fx, oFx, "Fx");
         build_work(s->hboxes, R_VALID, 1, -1, &s->w_valid, &s->n_valid);
@@ -1938,6 +2219,7 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
         build_work(s->hdom, R_TBX, 3, 0, &s->w_r2, &s->n_r2, CASTRO_R2_ROWS);
         build_work(s->hdom, R_EBX, 3, -1, &s->w_r3, &s->n_r3, CASTRO_R3_ROWS);
         build_ghost_work(s);
+        if (ok && mode == CASTRO_MODE_PERSISTENT) ok = ns == 2 ? persistent_setup<2>(s) : persistent_setup<13>(s);
     }
     if (ok && (mode == CASTRO_MODE_PLAIN || mode == CASTRO_MODE_PLAIN_BOX)) {
         long long nsb = 0, nsrc = 0, mx = 0;
@@ -1970,7 +2252,7 @@ void castro_sim_destroy(castro_sim* s)
     if (s->graph) cudaGraphDestroy(s->graph);
     void* ptrs[] = {s->dboxes, s->ddom, s->dinst, s->dstate, s->downer, s->U, s->Ub, s->Q, s->Div, s->Tr, s->F1, s->F2, s->Fx,
                     s->w_valid, s->w_g4, s->w_g1, s->w_trace, s->w_tbx, s->w_ebx, s->w_r2, s->w_r3, s->w_ghost, s->sb, s->src, s->scratch,
-                    s->d_dtloc, s->d_dtbox};
+                    s->d_dtloc, s->d_dtbox, s->pctl};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s->st) cudaStreamDestroy(s->st);
@@ -2027,8 +2309,9 @@ int castro_sim_download(castro_sim* s, double* host)
 
 int castro_sim_step(castro_sim* s)
 {
-    NvtxRange r(s->mode == CASTRO_MODE_BATCHED ? "castro_sim_step: Castro::advance (batched step graph)"
-                                                : "castro_sim_step: Castro::advance (per-box sequence)");
+    NvtxRange r(s->mode == CASTRO_MODE_BATCHED      ? "castro_sim_step: Castro::advance (batched step graph)"
+                : s->mode == CASTRO_MODE_PERSISTENT ? "castro_sim_step: Castro::advance (one persistent launch)"
+                                                     : "castro_sim_step: Castro::advance (per-box sequence)");
     if (s->ns == 2) return step_impl<2>(s);
     return step_impl<13>(s);
 }
@@ -2054,6 +2337,19 @@ int castro_sim_run_host(castro_sim* s, const double* host_in, int nsteps, double
 int castro_sim_sync(castro_sim* s)
 {
     if (!cuda_ok(cudaStreamSynchronize(s->st), "sync")) return castro_last_error();
+    if (s->pctl && !s->failed) {
+        PersistCtl c;
+        if (cuda_ok(cudaMemcpy(&c, s->pctl, sizeof c, cudaMemcpyDeviceToHost), "persistent control") && c.error != 0) {
+            static const char* stage[PS_COUNT] = {"front", "ghost", "prep", "trace", "riemann1", "riemann2", "riemann3",
+                                                  "update"};
+            char msg[200];
+            snprintf(msg, sizeof msg, "castro_sim: the grid-barrier wait after stage %s ran out of its limit; the step "
+                     "is void", c.error >= 1 && c.error <= PS_COUNT ? stage[c.error - 1] : "?");
+            s->failed = true;
+            set_error(CASTRO_ERR_TIMEOUT, msg);
+            return castro_last_error();
+        }
+    }
     // an EOS Newton iteration that reached its 100-iteration limit (a NaN or
     // otherwise unphysical state) is silent in the reference; here it is an error
     unsigned long long v = 0;
@@ -2354,7 +2650,7 @@ int castro_sim_read_checkpoint(castro_sim* s, const char* dir)
     }
     if (!cuda_ok(cudaMemcpy(s->dstate, hs.data(), ninst * sizeof(InstState), cudaMemcpyHostToDevice), "restart dt"))
         return castro_last_error();
-    if (s->mode == CASTRO_MODE_BATCHED) {
+    if (s->mode == CASTRO_MODE_BATCHED || s->mode == CASTRO_MODE_PERSISTENT) {
         bool started = false;
         for (const InstState& st : hs) started = started || st.steps > 0;
         if (started) {
@@ -2455,9 +2751,9 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
         gb.s = nullptr;
         castro_instance_desc D;
         memset(&D, 0, sizeof D);
-        for (int d = 0; d < 3; ++d) {
+        for (int d = 0; d < 3; ++d) {   // unit zones: every call passes its own dx
             D.dom_lo[d] = lo[d]; D.dom_hi[d] = hi[d];
-            D.problo[d] = 0.0; D.probhi[d] = 1.0;
+            D.problo[d] = 0.0; D.probhi[d] = (double)(hi[d] - lo[d] + 1);
         }
         D.bc = CASTRO_BC_OUTFLOW;
         D.nbox = 1;
@@ -2743,6 +3039,23 @@ int castro_construct_hydro_source_box_noalloc(const int* lo, const int* hi, cons
 }
 
 int castro_sim_launches_per_step(const castro_sim* s) { return s->launches; }
+
+int castro_sim_set_wait_limit(castro_sim* s, long long polls, int stage, int extra)
+{
+    if (!s || s->mode != CASTRO_MODE_PERSISTENT || polls < 1 || extra < 0) {
+        set_error(CASTRO_ERR_ARG, "castro_sim_set_wait_limit: a persistent-mode sim, polls >= 1, extra >= 0");
+        return CASTRO_ERR_ARG;
+    }
+    s->pargs.spin_limit = polls;
+    s->pargs.test_stage = extra > 0 ? stage : -1;
+    s->pargs.test_extra = extra;
+    // the arguments are baked into the captured step: capture again
+    if (s->gexec) cudaGraphExecDestroy(s->gexec);
+    if (s->graph) cudaGraphDestroy(s->graph);
+    s->gexec = nullptr;
+    s->graph = nullptr;
+    return CASTRO_OK;
+}
 
 void* castro_sim_stream(castro_sim* s) { return (void*)s->st; }
 

@@ -38,7 +38,8 @@ def test_enum_constants_agree(pkg):
     assert enums["CASTRO_MODE_PLAIN"] == pkg.castro.MODE_PLAIN
     assert enums["CASTRO_MODE_BATCHED"] == pkg.castro.MODE_BATCHED
     assert enums["CASTRO_MODE_PLAIN_BOX"] == pkg.castro.MODE_PLAIN_BOX
-    assert len({v for k, v in enums.items() if k.startswith("CASTRO_MODE_")}) == 3
+    assert enums["CASTRO_MODE_PERSISTENT"] == pkg.castro.MODE_PERSISTENT
+    assert len({v for k, v in enums.items() if k.startswith("CASTRO_MODE_")}) == 4
 
 
 @pytest.mark.parametrize("exact", [False, True])

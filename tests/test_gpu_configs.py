@@ -6,7 +6,8 @@ level driver on the same inputs:
 * C1  one 64^3 box, outflow, 2 species, 10 steps;
 * C2  128^3 in 64 boxes of 32^3, perturbed density, 50 steps (the full run);
 * C3  256^3 on the uneven BoxArray plus the 32 instances of 32^3..96^3, one step;
-* R   the Source/Prob.F90 problem, 128^3 in 64^3 boxes, 13 species, periodic, 10 steps.
+* R   the Source/Prob.F90 problem, 128^3 in 64^3 boxes, 13 species, periodic, 10 steps;
+* C3 and C2 (10 steps) again with the step as one persistent cooperative launch.
 
 The oracle, the exact build and the production build advance in lockstep.
 Exact build: state and dt bit for bit after every step.  Production build:
@@ -28,11 +29,15 @@ from gpu_harness import RTOL_L1, assert_strict, noise_mask, rel_l1
 
 pytestmark = pytest.mark.gpu
 
+BATCHED, PERSISTENT = 1, 3
 CONFIGS = {
-    "C1_sedov64": (lambda c: c.sedov64(), 10),
-    "C2_sedov128_pert": (lambda c: c.sedov128_pert(), 50),
-    "C3_batched": (lambda c: c.batched(), 1),
-    "R_reference128": (lambda c: c.reference(), 10),
+    "C1_sedov64": (lambda c: c.sedov64(), 10, BATCHED),
+    "C2_sedov128_pert": (lambda c: c.sedov128_pert(), 50, BATCHED),
+    "C3_batched": (lambda c: c.batched(), 1, BATCHED),
+    "R_reference128": (lambda c: c.reference(), 10, BATCHED),
+    # the same step as one cooperative launch over device work queues
+    "C3_batched_persistent": (lambda c: c.batched(), 1, PERSISTENT),
+    "C2_sedov128_pert_persistent": (lambda c: c.sedov128_pert(), 10, PERSISTENT),
 }
 
 
@@ -61,9 +66,9 @@ def _oracle_levels(oracle, pkg, table, cfg, variant):
     return levs
 
 
-def _gpu_sim(pkg, table, cfg, exact):
+def _gpu_sim(pkg, table, cfg, exact, mode):
     L = pkg.castro.init(cfg["network"][0], cfg["network"][1], table, exact=exact)
-    sim = pkg.make_sim(L, cfg, pkg.castro.MODE_BATCHED)
+    sim = pkg.make_sim(L, cfg, mode)
     sim.init_data()
     return sim
 
@@ -75,12 +80,12 @@ def _states(pkg, cfg, sim):
 
 @pytest.mark.parametrize("name", list(CONFIGS))
 def test_config_parity(pkg, table, oracle, name):
-    make, steps = CONFIGS[name]
+    make, steps, mode = CONFIGS[name]
     cfg = make(pkg.configs)
     insts = cfg["instances"]
     levs = _oracle_levels(oracle, pkg, table, cfg, "parity")
-    ex = _gpu_sim(pkg, table, cfg, True)
-    pr = _gpu_sim(pkg, table, cfg, False)
+    ex = _gpu_sim(pkg, table, cfg, True, mode)
+    pr = _gpu_sim(pkg, table, cfg, False, mode)
     periodic = all(i["bc"] == pkg.castro.BC_PERIODIC for i in insts)
     if periodic:
         G0 = _states(pkg, cfg, pr)

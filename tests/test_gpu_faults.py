@@ -3,9 +3,11 @@ hang): a truncated or missing Helmholtz table (eos_init's reader,
 Source/eos.F90:637-670), a NaN-seeded state (EOS Newton solves that reach
 their 100-iteration limit, Source/eos.F90:520-552, reported through
 castro_last_error and the failure counter), and corrupt BoxArrays (rejected
-by castro_sim_create before anything is allocated).  Also: checkpoint /
-restart continues a run bit for bit, and two runs from the same initial state
-are bitwise identical (no races in the batched step).
+by castro_sim_create before anything is allocated), and a grid-barrier wait of
+the persistent step that cannot be satisfied (it gives up after its poll limit
+and the host reads CASTRO_ERR_TIMEOUT).  Also: checkpoint / restart continues
+a run bit for bit, and two runs from the same initial state are bitwise
+identical (no races in the batched step).
 
 NaN inputs are safe on the device by construction: table coordinates pass
 through table_trunc, which maps NaN and infinities to a finite value before
@@ -162,3 +164,32 @@ def test_batched_step_deterministic(pkg, table):
         out.append((sim.download(), sim.dt(0)))
         sim.close()
     assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
+
+
+def test_persistent_wait_limit(pkg, table):
+    """A grid barrier of the persistent step made to wait for one CTA more than
+    exist (a condition set on the host) gives up after its poll limit: the
+    launch ends, castro_sim_sync reports CASTRO_ERR_TIMEOUT, the sim refuses
+    further steps, and the device stays usable -- a fresh sim then matches the
+    ten-kernel graph bit for bit."""
+    L = _lib(pkg, table)
+    K = pkg.castro
+    cfg = pkg.configs.sedov64(scale=4)
+    sim = pkg.make_sim(L, cfg, K.MODE_PERSISTENT)
+    sim.init_data()
+    assert L.castro_sim_set_wait_limit(sim.h, 1 << 12, 2, 1) == 0
+    L.castro_clear_error()
+    sim.step(1)
+    with pytest.raises(K.CastroError, match="castro error 8"):
+        sim.sync()
+    with pytest.raises(K.CastroError, match="castro error 8"):
+        sim.step(1)
+    sim.close()
+    out = []
+    for mode in (K.MODE_PERSISTENT, K.MODE_BATCHED):
+        s2 = pkg.make_sim(L, cfg, mode)
+        s2.init_data()
+        s2.step(3)
+        out.append(s2.download())
+        s2.close()
+    assert np.array_equal(out[0], out[1])

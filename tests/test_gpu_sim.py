@@ -5,7 +5,8 @@ against the oracle's level driver, through the C-ABI castro_sim_* entry points.
 * batched : the fused ten-kernel step over every box of every instance,
             replayed as a CUDA graph;
 * plain_box: the plain host sequence with each box's hydro source from the
-            coarse drop-in castro_construct_hydro_source_box.
+            coarse drop-in castro_construct_hydro_source_box;
+* persistent: the batched step as one cooperative launch over device work queues.
 The exact build must reproduce the oracle bit for bit, dt included; the
 production build within the tolerances of gpu_harness (1e-12 per zone after
 one step, 1e-9 relative L1 after a run, dt within 1e-14).
@@ -72,7 +73,7 @@ WORKLOADS = {
 
 
 @pytest.mark.parametrize("exact", [True, False], ids=["exact", "fast"])
-@pytest.mark.parametrize("mode", [0, 1, 2], ids=["plain", "batched", "plain_box"])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3], ids=["plain", "batched", "plain_box", "persistent"])
 @pytest.mark.parametrize("wl", list(WORKLOADS))
 def test_steps_match_oracle(pkg, table, oracle, wl, mode, exact):
     cfg = WORKLOADS[wl](pkg.configs)
@@ -89,6 +90,8 @@ def test_steps_match_oracle(pkg, table, oracle, wl, mode, exact):
         np.testing.assert_allclose(dts[:, 0], dto, rtol=1e-14)
     if mode == 1:
         assert launches == FUSED_KERNELS_PER_STEP
+    if mode == 3:
+        assert launches == 1          # the whole step in one cooperative launch
 
 
 @pytest.mark.parametrize("exact", [True, False], ids=["exact", "fast"])
