@@ -130,6 +130,12 @@ __device__ __forceinline__ void density_basis(double din, DensityBasis& B)
     int iat = table_trunc((log10(din) - c_eos.dlo) * c_eos.dstpi);   // eos.F90:244-245
     iat = iat > IMAX - 2 ? IMAX - 2 : iat;
     iat = iat < 0 ? 0 : iat;
+    // Within an ulp of a node the last bit of log10 decides the cell, and two
+    // faithful log10s (this device's, a host libm's) can decide differently: the
+    // estimate is settled against the node values, so that the cell is the one
+    // whose nodes bracket the argument, whatever log10 returned.
+    if (iat > 0 && din < __ldg(c_eos.drow + (size_t)iat * ROW_STRIDE)) --iat;
+    else if (iat < IMAX - 2 && din >= __ldg(c_eos.drow + (size_t)(iat + 1) * ROW_STRIDE)) ++iat;
     B.iat = iat;
     const double* dr = c_eos.drow + (size_t)iat * ROW_STRIDE;
     double d0 = __ldg(dr + 0), dd = __ldg(dr + 1), dd2 = __ldg(dr + 2), ddi = __ldg(dr + 3);
@@ -194,6 +200,9 @@ __device__ __forceinline__ void eos_eval_part(double temp, const EosConst& K, co
     int jat = table_trunc((log10(temp) - c_eos.tlo) * c_eos.tstpi);
     jat = jat > JMAX - 2 ? JMAX - 2 : jat;
     jat = jat < 0 ? 0 : jat;
+    // settled against the node temperatures, as the density cell in density_basis
+    if (jat > 0 && temp < __ldg(c_eos.trow + (size_t)jat * ROW_STRIDE)) --jat;
+    else if (jat < JMAX - 2 && temp >= __ldg(c_eos.trow + (size_t)(jat + 1) * ROW_STRIDE)) ++jat;
     const double* tr = c_eos.trow + (size_t)jat * ROW_STRIDE;
     double t0 = __ldg(tr + 0), dt = __ldg(tr + 1), dt2 = __ldg(tr + 2), dti = __ldg(tr + 3), dt2i = __ldg(tr + 4);
     double xt = DMAX((temp - t0) * dti, 0.0);                          // :286

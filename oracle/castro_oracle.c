@@ -376,13 +376,21 @@ void oracle_eos(int input, oracle_eos_t* state)
         dsiondt = (dpiondt * deni + deiondt) * tempi - (pion * deni + eion) * tempi * tempi
                 + 1.5 * kergavo * tempi * ytot1;
 
-        /* hash locate, :242-245 (0-based) */
+        /* hash locate, :242-245 (0-based).  Within an ulp of a node the last
+         * bit of log10 decides the cell, and two faithful log10s (this host's
+         * libm, a GPU's) can decide differently: the estimate is settled against
+         * the node values, so that the cell is the one whose nodes bracket the
+         * argument whatever log10 returned. */
         jat = ftrunc((log10(temp) - tlo) * tstpi);
         if (jat > JMAX - 2) jat = JMAX - 2;
         if (jat < 0) jat = 0;
+        if (jat > 0 && temp < tab_t[jat]) --jat;
+        else if (jat < JMAX - 2 && temp >= tab_t[jat + 1]) ++jat;
         iat = ftrunc((log10(din) - dlo) * dstpi);
         if (iat > IMAX - 2) iat = IMAX - 2;
         if (iat < 0) iat = 0;
+        if (iat > 0 && din < tab_d[iat]) --iat;
+        else if (iat < IMAX - 2 && din >= tab_d[iat + 1]) ++iat;
 
         /* :248-283 */
         fill4(fi + 0, tf, iat, jat);
@@ -438,11 +446,52 @@ void oracle_eos(int input, oracle_eos_t* state)
         ddsi2mt = ddpsi2(mxt);
 
         /* :335-357 */
+#ifndef ORACLE_FACTORED_EOS
         free_e = h5(fi, si0t, si1t, si2t, si0mt, si1mt, si2mt, si0d, si1d, si2d, si0md, si1md, si2md);
         df_d = h5(fi, si0t, si1t, si2t, si0mt, si1mt, si2mt, dsi0d, dsi1d, dsi2d, dsi0md, dsi1md, dsi2md);
         df_t = h5(fi, dsi0t, dsi1t, dsi2t, dsi0mt, dsi1mt, dsi2mt, si0d, si1d, si2d, si0md, si1md, si2md);
         df_tt = h5(fi, ddsi0t, ddsi1t, ddsi2t, ddsi0mt, ddsi1mt, ddsi2mt, si0d, si1d, si2d, si0md, si1md, si2md);
         df_dt = h5(fi, dsi0t, dsi1t, dsi2t, dsi0mt, dsi1mt, dsi2mt, dsi0d, dsi1d, dsi2d, dsi0md, dsi1md, dsi2md);
+#else
+        /* The same 36-term sums factored the way the production GPU build
+         * forms them (temperature direction first for each density order and
+         * density node, then the density direction, in fused multiply-adds):
+         * a reordering of the interpolation's arithmetic, not of its
+         * algorithm.  Only the timing build uses it; the parity build keeps
+         * eos.F90's term order. */
+        {
+            /* fi[4*m + c]: table m in (f, ft, ftt, fd, fdd, fdt, fddt, fdtt, fddtt), corner
+             * c = di + 2*dj; slot of (density order a, temperature order b) */
+            static const int mslot[3][3] = {{0, 1, 2}, {3, 5, 7}, {4, 6, 8}};
+            const double tw[3][3][2] = {{{si0t, si0mt}, {si1t, si1mt}, {si2t, si2mt}},
+                                        {{dsi0t, dsi0mt}, {dsi1t, dsi1mt}, {dsi2t, dsi2mt}},
+                                        {{ddsi0t, ddsi0mt}, {ddsi1t, ddsi1mt}, {ddsi2t, ddsi2mt}}};
+            const double dw[3][2] = {{si0d, si0md}, {si1d, si1md}, {si2d, si2md}};
+            const double ddw[3][2] = {{dsi0d, dsi0md}, {dsi1d, dsi1md}, {dsi2d, dsi2md}};
+            double g[3][3][2];   /* [temperature weight set][density order a][density node di] */
+            for (int a = 0; a < 3; ++a)
+                for (int di = 0; di < 2; ++di) {
+                    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+                    for (int b = 0; b < 3; ++b)
+                        for (int dj = 0; dj < 2; ++dj) {
+                            double v = fi[4 * mslot[a][b] + di + 2 * dj];
+                            s0 = fma(v, tw[0][b][dj], s0);
+                            s1 = fma(v, tw[1][b][dj], s1);
+                            s2 = fma(v, tw[2][b][dj], s2);
+                        }
+                    g[0][a][di] = s0; g[1][a][di] = s1; g[2][a][di] = s2;
+                }
+            free_e = df_d = df_t = df_tt = df_dt = 0.0;
+            for (int a = 0; a < 3; ++a)
+                for (int di = 0; di < 2; ++di) {
+                    free_e = fma(g[0][a][di], dw[a][di], free_e);
+                    df_d = fma(g[0][a][di], ddw[a][di], df_d);
+                    df_t = fma(g[1][a][di], dw[a][di], df_t);
+                    df_tt = fma(g[2][a][di], dw[a][di], df_tt);
+                    df_dt = fma(g[1][a][di], ddw[a][di], df_dt);
+                }
+        }
+#endif
 
         /* :362-385 */
         si0t = xpsi0(xt);

@@ -3,11 +3,12 @@ comparison criteria.
 
 Tolerances (FP64):
 * exact build (-DCASTRO_EXACT --fmad=false): bit-for-bit equality with the oracle;
-* production build: per component, max |gpu - oracle| / max(|oracle|, FLOOR * scale_c)
-  <= RTOL_STEP after one step, where scale_c is the component's largest
-  magnitude in the array (this keeps zones whose value is round-off noise around
-  zero -- e.g. momentum far from the blast -- from dominating), and relative L1
-  per component <= RTOL_L1 after a full run.
+* production build, small cases: per component, max |gpu - oracle| /
+  max(|oracle|, FLOOR * scale_c) <= RTOL_STEP after one step, where scale_c is
+  the component's largest magnitude in the array, and relative L1 per component
+  <= RTOL_L1 after a run;
+* production build at the configurations' own sizes: the strict per-zone
+  criterion below (no magnitude floor; round-off noise zones reported apart).
 """
 from __future__ import annotations
 
@@ -71,9 +72,10 @@ def scaled_err(a: np.ndarray, b: np.ndarray) -> np.ndarray:
 # is round-off noise -- the result of a cancellation, so that any other correct
 # rounding of the same algorithm moves it far more than 1e-12 -- cannot meet a
 # per-zone relative bar in a contracting build.  Such zones are identified
-# without the GPU: the oracle's contracting build (liboracle_fast.so, FMA) is
-# run on the same inputs, and a zone it moves by more than NOISE_RTOL relative
-# is noise.  Noise zones are reported apart and must agree to NOISE_ABS of their
+# without the GPU: the oracle's timing build (liboracle_fast.so: FMA contraction
+# and the table interpolation summed in the production build's order) is run on
+# the same inputs, and a zone it moves by more than NOISE_RTOL relative is noise.
+# Noise zones are reported apart and must agree to NOISE_ABS of their
 # component's largest magnitude; every other zone must meet RTOL_STEP.
 TINY = float(np.finfo(np.float64).tiny)
 NOISE_RTOL = 1e-14
@@ -94,9 +96,11 @@ def strict_zone_report(gpu: np.ndarray, ref: np.ndarray, noise: np.ndarray) -> l
     for c in range(nc):
         a, b, n = A[:, c], B[:, c], N[:, c]
         d = np.abs(a - b)
-        rel = d / np.maximum(np.abs(b), TINY)
+        with np.errstate(over="ignore"):
+            rel = d / np.maximum(np.abs(b), TINY)
         scale = float(np.abs(b).max()) or 1.0
         out.append({"zones": int(b.size), "noise_zones": int(n.sum()),
+                    "zones_above_rtol": int((rel > RTOL_STEP).sum()),
                     "max_rel": float(rel[~n].max()) if (~n).any() else 0.0,
                     "noise_max_abs_over_scale": float(d[n].max() / scale) if n.any() else 0.0})
     return out

@@ -118,6 +118,7 @@ def test_config_parity(pkg, table, oracle, name):
                 "max_rel_non_noise": max(r["max_rel"] for p in per for r in p),
                 "noise_zones_per_component": [sum(p[c]["noise_zones"] for p in per) for c in range(len(per[0]))],
                 "noise_max_abs_over_scale": max(r["noise_max_abs_over_scale"] for p in per for r in p),
+                "zones_above_1e-12_per_component": [sum(p[c]["zones_above_rtol"] for p in per) for c in range(len(per[0]))],
             }
         if s == steps - 1:
             Gp = _states(pkg, cfg, pr)
