@@ -7,13 +7,14 @@ The product is the CUDA library ``lib/libcastro_b200.so`` (C-ABI in
 * ``configs``    -- the Sedov workloads (BoxArrays, networks, problem constants)
 * ``helm_table`` -- writer of the Helmholtz table file read by ``eos_init``
 * ``replicas``   -- the multi-GPU (one replica per rank) reductions
+* ``shard``      -- one level's boxes sharded over ranks: halo exchange, dt min-reduction
 * ``adjoint``    -- gradients of a Sedov run (reverse sweep) and its torch.autograd wrapper
 * ``plotfile``   -- reader of the AMReX plotfiles the library writes
 * ``build``      -- nvcc recipe for the sm_100a libraries
 """
-from . import adjoint, castro, configs, helm_table, plotfile, replicas  # noqa: F401
+from . import adjoint, castro, configs, helm_table, plotfile, replicas, shard  # noqa: F401
 
-__all__ = ["adjoint", "castro", "configs", "helm_table", "plotfile", "replicas", "make_sim"]
+__all__ = ["adjoint", "castro", "configs", "helm_table", "plotfile", "replicas", "shard", "make_sim"]
 
 
 def make_sim(L, cfg, mode=castro.MODE_BATCHED):
