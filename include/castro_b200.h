@@ -102,6 +102,10 @@ void compute_temp(const int* lo, const int* hi, double* state, const int* s_lo, 
 /* Castro_F.H:41-45 -> timestep.F90:12; dt is a device/managed double lowered atomically */
 void estdt(const int* lo, const int* hi, const double* state, const int* s_lo, const int* s_hi,
            const double* dx, double* dt);
+/* MultiFab::Saxpy(S_new, dt, hydro_source) of Source/Castro_advance.cpp:74 (an
+ * AMReX call, not a Castro_F.H routine): u[m] = u[m] + dt * src[m] over n
+ * doubles of device memory, on the library stream */
+void castro_saxpy(double* u, const double* src, long long n, double dt);
 /* Castro_F.H:47-53 -> Castro_hydro_nd.F90:301 */
 void store_flux(const int* lo, const int* hi,
                 double* flux_out, const int* fo_lo, const int* fo_hi,

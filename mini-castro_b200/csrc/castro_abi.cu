@@ -533,6 +533,21 @@ void estdt(const int* lo, const int* hi, const double* s, const int* s_lo, const
     CASTRO_DISPATCH_NS(estdt_impl, lo, hi, make_fab(s, s_lo, s_hi), dx, dt);
 }
 
+// MultiFab::Saxpy of Source/Castro_advance.cpp:74 (U_new = U_old + dt * source)
+// on n contiguous doubles of one FAB
+__global__ void k_saxpy_host_dt(double* u, const double* src, long long n, double dt)
+{
+    const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < n) u[m] = u[m] + dt * src[m];
+}
+
+void castro_saxpy(double* u, const double* src, long long n, double dt)
+{
+    if (n <= 0) return;
+    k_saxpy_host_dt<<<(unsigned)((n + 255) / 256), 256, 0, stream()>>>(u, src, n, dt);
+    check_launch("castro_saxpy");
+}
+
 void store_flux(const int* lo, const int* hi, double* fo, const int* fo_lo, const int* fo_hi,
                 double* fi, const int* fi_lo, const int* fi_hi, double* a, const int* a_lo, const int* a_hi,
                 const double dt)

@@ -158,7 +158,10 @@ class GpuKernels:
         return src
 
     def saxpy(self, u, dt, src):
-        u.add_(src * dt)          # u + (dt * src), Source/Castro_advance.cpp:74
+        import ctypes as C
+
+        self.L.castro_saxpy(C.c_void_p(u.data_ptr()), C.c_void_p(src.data_ptr()), u.numel(), C.c_double(dt))
+        castro.check(self.L, "castro_saxpy")
 
     def gather(self, a, idx):
         return a.view(self.nvar, -1)[:, self.torch.as_tensor(idx, device=a.device)]
