@@ -74,9 +74,11 @@ def scaled_err(a: np.ndarray, b: np.ndarray) -> np.ndarray:
 # per-zone relative bar in a contracting build.  Such zones are identified
 # without the GPU: the oracle's timing build (liboracle_fast.so: FMA contraction
 # and the table interpolation summed in the production build's order) is run on
-# the same inputs, and a zone it moves by more than NOISE_RTOL relative is noise.
-# Noise zones are reported apart and must agree to NOISE_ABS of their
-# component's largest magnitude; every other zone must meet RTOL_STEP.
+# the same inputs, and a zone it moves by more than NOISE_RTOL relative is noise;
+# so is a zone whose one-step value is a cancellation (cancellation_mask: below
+# CANCEL of the magnitude of the state and flux terms that formed it).  Noise
+# zones are reported apart and must agree to NOISE_ABS of their component's
+# largest magnitude; every other zone must meet RTOL_STEP.
 TINY = float(np.finfo(np.float64).tiny)
 NOISE_RTOL = 1e-14
 NOISE_ABS = 1e-13
@@ -85,6 +87,48 @@ NOISE_ABS = 1e-13
 def noise_mask(ref: np.ndarray, contracted: np.ndarray) -> np.ndarray:
     """Zones (per component) whose value the contracting CPU build moves by more than NOISE_RTOL."""
     return np.abs(contracted - ref) > NOISE_RTOL * np.maximum(np.abs(ref), TINY)
+
+
+CANCEL = 1e-3
+
+
+def cancellation_mask(u_old: np.ndarray, u_new: np.ndarray, dt: float, dx: float) -> np.ndarray:
+    """Zones (per component) whose value after one step is below CANCEL of the
+    magnitude of the terms that formed it: U_new = U_old + dt * (flux difference)
+    / dx, each face flux bounded by the old state of the zone and its six face
+    neighbours -- rho|u| (density), rho u^2 + p (momenta), (E + p)|u|
+    (total energy), (rho e + p)|u| + p|u| (internal energy, with p div u) --
+    with p bounded by rho e (gamma - 1 <= 1).  Such a value is a cancellation:
+    its relative rounding error is amplified by more than 1/CANCEL, so a
+    per-zone relative bar of 1e-12 does not apply to it.  Only density, momenta
+    and energies are flux balances: the temperature is an EOS output, and the
+    species slots hold X after normalize_species (the reference divides rho X
+    by its sum, Source/Castro_nd.F90:152-154), so neither is flagged here."""
+    rho = u_old[..., 0]
+    u = [u_old[..., 1 + d] / rho for d in range(3)]
+    speed = np.abs(u[0]) + np.abs(u[1]) + np.abs(u[2])
+    rhoe = np.abs(u_old[..., 5])
+    p = rhoe
+    scale = {0: rho * speed, 1: rho * speed * speed + p, 4: (np.abs(u_old[..., 4]) + p) * speed,
+             5: (rhoe + p) * speed + p * speed}
+    scale[2] = scale[3] = scale[1]
+
+    def nbr_max(a):
+        g = np.pad(a, 1, mode="edge")
+        out = a.copy()
+        for d in range(3):
+            lo = [slice(1, -1)] * 3
+            hi = [slice(1, -1)] * 3
+            lo[d], hi[d] = slice(0, -2), slice(2, None)
+            out = np.maximum(out, np.maximum(g[tuple(lo)], g[tuple(hi)]))
+        return out
+
+    mask = np.zeros(u_new.shape, dtype=bool)
+    for c in range(6):
+        f = scale[c]
+        terms = np.abs(u_old[..., c]) + 6.0 * dt / dx * nbr_max(f)
+        mask[..., c] = np.abs(u_new[..., c]) < CANCEL * terms
+    return mask
 
 
 def strict_zone_report(gpu: np.ndarray, ref: np.ndarray, noise: np.ndarray) -> list[dict]:

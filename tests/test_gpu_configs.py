@@ -13,9 +13,10 @@ The oracle, the exact build and the production build advance in lockstep.
 Exact build: state and dt bit for bit after every step.  Production build:
 dt within 1e-14 every step; after the first step every zone within 1e-12
 relative (no floor beyond the smallest normal double) except the round-off
-noise zones, which are identified by the oracle's own contracting build and
-reported apart (gpu_harness); relative L1 per component <= 1e-9 after the full
-run.  R (periodic) also conserves mass and total energy to 1e-13.
+noise zones -- those the oracle's own timing build (another rounding of the same
+algorithm) moves by more than 1e-14, and those whose value is a cancellation,
+below 1e-3 of the state and flux terms that formed it -- which are reported
+apart (gpu_harness); relative L1 per component <= 1e-9 after the full run.  R (periodic) also conserves mass and total energy to 1e-13.
 """
 from __future__ import annotations
 
@@ -25,7 +26,7 @@ import os
 import numpy as np
 import pytest
 
-from gpu_harness import RTOL_L1, assert_strict, noise_mask, rel_l1
+from gpu_harness import RTOL_L1, assert_strict, cancellation_mask, noise_mask, rel_l1
 
 pytestmark = pytest.mark.gpu
 
@@ -91,6 +92,7 @@ def test_config_parity(pkg, table, oracle, name):
         G0 = _states(pkg, cfg, pr)
         tot0 = [(g[..., 0].sum(), g[..., 4].sum()) for g in G0]
     report = {"steps": steps, "instances": len(insts), "zones": pkg.configs.zones(cfg)}
+    Gstart = [oracle.assemble(lev, i) for (lev, _), i in zip(levs, insts)]
     for s in range(steps):
         dto = [lev.coarse_step(i.get("stop_time", -1.0)) for (lev, _), i in zip(levs, insts)]
         ex.step(1)
@@ -111,9 +113,10 @@ def test_config_parity(pkg, table, oracle, name):
             Gp = _states(pkg, cfg, pr)
             per = []
             for n, ((lev, _), i) in enumerate(zip(fast, insts)):
-                noise = noise_mask(Go[n], oracle.assemble(lev, i))
+                dx = (i["probhi"][0] - i["problo"][0]) / (i["dom_hi"][0] - i["dom_lo"][0] + 1)
+                noise = noise_mask(Go[n], oracle.assemble(lev, i)) | cancellation_mask(Gstart[n], Go[n], dto[n], dx)
                 per.append(assert_strict(Gp[n], Go[n], noise, what=f"{name} step 1 instance {n}"))
-            del fast, Gp
+            del fast, Gp, Gstart
             report["one_step"] = {
                 "max_rel_non_noise": max(r["max_rel"] for p in per for r in p),
                 "noise_zones_per_component": [sum(p[c]["noise_zones"] for p in per) for c in range(len(per[0]))],
