@@ -120,11 +120,15 @@ CASTRO_HD void eos_eval_t(const EosTableDev& tb, const S& temp, const S& den, co
     int iat = table_trunc((log10(val(din)) - tb.dlo) * tb.dstpi);
     iat = iat > IMAX - 2 ? IMAX - 2 : iat;
     iat = iat < 0 ? 0 : iat;
-    // the cells settled against the node values, as the forward EOS does
-    if (jat > 0 && val(temp) < tld(tb.trow + (size_t)jat * ROW_STRIDE)) --jat;
-    else if (jat < JMAX - 2 && val(temp) >= tld(tb.trow + (size_t)(jat + 1) * ROW_STRIDE)) ++jat;
-    if (iat > 0 && val(din) < tld(tb.drow + (size_t)iat * ROW_STRIDE)) --iat;
-    else if (iat < IMAX - 2 && val(din) >= tld(tb.drow + (size_t)(iat + 1) * ROW_STRIDE)) ++iat;
+    // the cells settled against the node values (a row's lower and upper node), as the forward EOS does
+    {
+        const double* r = tb.trow + (size_t)jat * ROW_STRIDE;
+        if ((jat > 0 && val(temp) < tld(r)) || (jat < JMAX - 2 && val(temp) >= tld(r + ROW_NEXT)))
+            jat += val(temp) < tld(r) ? -1 : 1;
+        r = tb.drow + (size_t)iat * ROW_STRIDE;
+        if ((iat > 0 && val(din) < tld(r)) || (iat < IMAX - 2 && val(din) >= tld(r + ROW_NEXT)))
+            iat += val(din) < tld(r) ? -1 : 1;
+    }
     const double* tr = tb.trow + (size_t)jat * ROW_STRIDE;
     const double t0 = tld(tr + 0), dt = tld(tr + 1), dt2 = tld(tr + 2), dti = tld(tr + 3), dt2i = tld(tr + 4);
     const double* dr = tb.drow + (size_t)iat * ROW_STRIDE;

@@ -59,6 +59,9 @@ enum { N_F = 0, N_FT, N_FTT, N_FD, N_FDD, N_FDT, N_FDDT, N_FDTT, N_FDDTT,
        N_DPDF, N_DPDFT, N_DPDFD, N_DPDFDT };
 // per-row records: t/d, dt/dd, dt2/dd2, dti/ddi, dt2i/dd2i
 constexpr int ROW_STRIDE = 8;
+// slot of a temperature / density row record holding the next node's value
+// (the cell's upper bound); the record is one 64-byte line
+constexpr int ROW_NEXT = 5;
 
 struct EosTableDev {
     const double* node;   // [JMAX][IMAX][NODE_STRIDE]
@@ -134,11 +137,15 @@ __device__ __forceinline__ void density_basis(double din, DensityBasis& B)
     // faithful log10s (this device's, a host libm's) can decide differently: the
     // estimate is settled against the node values, so that the cell is the one
     // whose nodes bracket the argument, whatever log10 returned.
-    if (iat > 0 && din < __ldg(c_eos.drow + (size_t)iat * ROW_STRIDE)) --iat;
-    else if (iat < IMAX - 2 && din >= __ldg(c_eos.drow + (size_t)(iat + 1) * ROW_STRIDE)) ++iat;
-    B.iat = iat;
     const double* dr = c_eos.drow + (size_t)iat * ROW_STRIDE;
     double d0 = __ldg(dr + 0), dd = __ldg(dr + 1), dd2 = __ldg(dr + 2), ddi = __ldg(dr + 3);
+    const double d1 = __ldg(dr + ROW_NEXT);
+    if ((iat > 0 && din < d0) || (iat < IMAX - 2 && din >= d1)) {
+        iat += din < d0 ? -1 : 1;
+        dr = c_eos.drow + (size_t)iat * ROW_STRIDE;
+        d0 = __ldg(dr + 0); dd = __ldg(dr + 1); dd2 = __ldg(dr + 2); ddi = __ldg(dr + 3);
+    }
+    B.iat = iat;
     double xd = DMAX((din - d0) * ddi, 0.0);                         // eos.F90:287
     double mxd = 1.0 - xd;
     B.si.w[0][0] = psi0(xd);
@@ -200,11 +207,16 @@ __device__ __forceinline__ void eos_eval_part(double temp, const EosConst& K, co
     int jat = table_trunc((log10(temp) - c_eos.tlo) * c_eos.tstpi);
     jat = jat > JMAX - 2 ? JMAX - 2 : jat;
     jat = jat < 0 ? 0 : jat;
-    // settled against the node temperatures, as the density cell in density_basis
-    if (jat > 0 && temp < __ldg(c_eos.trow + (size_t)jat * ROW_STRIDE)) --jat;
-    else if (jat < JMAX - 2 && temp >= __ldg(c_eos.trow + (size_t)(jat + 1) * ROW_STRIDE)) ++jat;
+    // settled against the node temperatures, as the density cell in
+    // density_basis: a row record holds its cell's lower and upper nodes
     const double* tr = c_eos.trow + (size_t)jat * ROW_STRIDE;
     double t0 = __ldg(tr + 0), dt = __ldg(tr + 1), dt2 = __ldg(tr + 2), dti = __ldg(tr + 3), dt2i = __ldg(tr + 4);
+    const double t1 = __ldg(tr + ROW_NEXT);
+    if ((jat > 0 && temp < t0) || (jat < JMAX - 2 && temp >= t1)) {
+        jat += temp < t0 ? -1 : 1;
+        tr = c_eos.trow + (size_t)jat * ROW_STRIDE;
+        t0 = __ldg(tr + 0); dt = __ldg(tr + 1); dt2 = __ldg(tr + 2); dti = __ldg(tr + 3); dt2i = __ldg(tr + 4);
+    }
     double xt = DMAX((temp - t0) * dti, 0.0);                          // :286
     double mxt = 1.0 - xt;
 

@@ -92,6 +92,7 @@ inline int read_helm_table(const char* path, HostTable& T)
         T.trow[(size_t)j * ROW_STRIDE + 2] = dt2;
         T.trow[(size_t)j * ROW_STRIDE + 3] = (j < JM - 1) ? 1.0 / dt : 0.0;
         T.trow[(size_t)j * ROW_STRIDE + 4] = (j < JM - 1) ? 1.0 / dt2 : 0.0;
+        T.trow[(size_t)j * ROW_STRIDE + ROW_NEXT] = (j < JM - 1) ? t[j + 1] : HUGE_VAL;
     }
     for (int i = 0; i < IM; ++i) {
         double dd = (i < IM - 1) ? d[i + 1] - d[i] : 0.0;
@@ -101,6 +102,7 @@ inline int read_helm_table(const char* path, HostTable& T)
         T.drow[(size_t)i * ROW_STRIDE + 2] = dd2;
         T.drow[(size_t)i * ROW_STRIDE + 3] = (i < IM - 1) ? 1.0 / dd : 0.0;
         T.drow[(size_t)i * ROW_STRIDE + 4] = (i < IM - 1) ? 1.0 / dd2 : 0.0;
+        T.drow[(size_t)i * ROW_STRIDE + ROW_NEXT] = (i < IM - 1) ? d[i + 1] : HUGE_VAL;
     }
     // physical constants, Source/eos.F90:129-137
     const double h = 6.6260689633e-27, avo_eos = 6.0221417930e23, clight = 2.99792458e10;
