@@ -295,6 +295,14 @@ def run_b200(args, pkg, rank, world):
     batched_cfg = None
     if args.batched_steps > 0:      # every rank: the instances are split over the ranks
         batched_cfg = run_batched_config(pkg, L, args, rank, world)
+    large_cfg = None
+    if rank == 0 and args.large_steps > 0:
+        big = pkg.configs.large()
+        large_cfg = {"workload": "large: 384^3 Sedov in an uneven BoxArray of 32^3..64^3 boxes, perturbed density, "
+                                 "2 species (the 100-step run timed over its first steps)",
+                     "zones": pkg.configs.zones(big), "boxes": len(big["instances"][0]["boxes"]),
+                     "batched": time_mode(pkg, L, big, pkg.castro.MODE_BATCHED, args.large_steps,
+                                          pkg.configs.zones(big))}
     adjoint_cfg = None
     if rank == 0 and args.adjoint_reps > 0:
         adjoint_cfg = run_adjoint_config(pkg, args)
@@ -375,6 +383,7 @@ def run_b200(args, pkg, rank, world):
         "plain_box_drop_in": plain_box,
         "persistent": persistent,
         "batched_config": batched_cfg,
+        "large_config": large_cfg,
         "adjoint_config": adjoint_cfg,
         "adjoint_forward_ratio": adjoint_cfg["adjoint_forward_ratio"] if adjoint_cfg else None,
         "eos_newton_failures": failures,
@@ -650,6 +659,7 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--batched-steps", type=int, default=18, help="timed steps of the batched configuration (0: skip)")
     ap.add_argument("--persistent-steps", type=int, default=20, help="timed steps of the one-launch persistent step (0: skip)")
+    ap.add_argument("--large-steps", type=int, default=5, help="timed steps of the 384^3 configuration (0: skip)")
     ap.add_argument("--adjoint-reps", type=int, default=3, help="timed forward+reverse runs of the adjoint configuration (0: skip)")
     ap.add_argument("--adjoint-fd", type=int, default=16, help="finite-difference directions of the gradient check (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
