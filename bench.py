@@ -306,6 +306,8 @@ def run_b200(args, pkg, rank, world):
     adjoint_cfg = None
     if rank == 0 and args.adjoint_reps > 0:
         adjoint_cfg = run_adjoint_config(pkg, args)
+    if rank == 0 and args.large_adjoint > 0:
+        large_cfg = dict(large_cfg or {}, adjoint=run_large_adjoint(pkg))
 
     value = pkg.replicas.whole_job_rate(zones, args.steps, ms, world)
     hbm, peak_kind = peaks()
@@ -616,6 +618,40 @@ def time_oracle(pkg, workload, steps, warmup, variant):
     return pkg.configs.zones(cfg) * steps / t, t, cores
 
 
+def run_large_adjoint(pkg, slab_nz=32, first_step=50, nsteps=100, ckpt=5):
+    """The large configuration's gradient: 384^3 Sedov with the seeded density
+    perturbation, 100 steps of which the last 50 are differentiated (objective:
+    the shell kinetic energy), checkpoint every 5 steps, each step reversed
+    slab by slab (z-slabs of 32 zones) so that one slab's arrays are held.  Times
+    the forward (all 100 steps) and the reverse sweep (the last 50)."""
+    import torch
+
+    cfg = pkg.configs.large()
+    inst = cfg["instances"][0]
+    table = pkg.helm_table.ensure_table()
+    L = pkg.castro.init(*cfg["network"], table)
+    torch.cuda.empty_cache()
+    out = {"workload": "large: 384^3 Sedov, perturbed density, 100 steps, adjoint of the last 50, checkpoint 5, "
+                       "shell 0.3-0.4", "slab_nz": slab_nz, "first_step": first_step}
+    try:
+        run = pkg.adjoint.SedovAdjoint(L, inst, nsteps, ckpt, (0.3, 0.4), slab_nz=slab_nz, first_step=first_step)
+    except pkg.castro.CastroError as e:
+        out["skipped"] = str(e)
+        return out
+    p = inst["problem"]
+    J = run.forward(p["exp_energy"], p["dens_ambient"])
+    run.backward()
+    Vb = run.state_adjoint()
+    f_ms, b_ms = run.time_ms()
+    out.update({"J": J, "dJ_dV_norm": float(Vb.norm()), "forward_ms": f_ms, "backward_ms": b_ms,
+                "backward_over_forward_of_the_window": b_ms / (f_ms * (nsteps - first_step) / nsteps),
+                "device_bytes": run.device_bytes()})
+    run.close()
+    del Vb
+    torch.cuda.empty_cache()
+    return out
+
+
 def cpu_baseline(pkg, args, steps=5):
     """Both oracle builds on the full workload: the timing build is the baseline's value."""
     out = {}
@@ -660,6 +696,7 @@ def main():
     ap.add_argument("--batched-steps", type=int, default=18, help="timed steps of the batched configuration (0: skip)")
     ap.add_argument("--persistent-steps", type=int, default=20, help="timed steps of the one-launch persistent step (0: skip)")
     ap.add_argument("--large-steps", type=int, default=5, help="timed steps of the 384^3 configuration (0: skip)")
+    ap.add_argument("--large-adjoint", type=int, default=1, help="the 384^3 configuration's 50-step adjoint (0: skip)")
     ap.add_argument("--adjoint-reps", type=int, default=3, help="timed forward+reverse runs of the adjoint configuration (0: skip)")
     ap.add_argument("--adjoint-fd", type=int, default=16, help="finite-difference directions of the gradient check (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

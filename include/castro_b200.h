@@ -217,10 +217,10 @@ int  castro_set_problem(const castro_problem* p);
  * fused: Sborder (grow(box,4), NVAR comps, already cleaned) -> source on the box
  * (accumulated into 'source', which the caller zeroes like hydro_source.setVal(0)).
  * fluxes_out[d] (optional, may be NULL): dt*F*A on the faces of the box
- * (store_flux).  Uses library-managed scratch: one set per device, allocated on
- * the first call and again when the box shape changes (so do not capture such a
- * call in a CUDA graph); the box position, geometry and dt travel as kernel
- * arguments, so calls for boxes of one shape allocate nothing. */
+ * (store_flux).  Uses library-managed scratch: per device, one set per box shape
+ * for the 8 shapes used last, allocated on a shape's first call (so do not capture
+ * such a call in a CUDA graph); the box position, geometry and dt travel as kernel
+ * arguments, so calls for the cached shapes allocate nothing. */
 int castro_construct_hydro_source_box(const int* lo, const int* hi,
                                       const double* sborder, const int* sb_lo, const int* sb_hi,
                                       double* source, const int* sr_lo, const int* sr_hi,
@@ -448,6 +448,20 @@ void fill_hydro_source_adj(const int* lo, const int* hi, const double* sourceb, 
  * desc->prob.pert (optional) must stay valid until the object is destroyed. */
 typedef struct castro_adj castro_adj;
 castro_adj* castro_adj_create(const castro_instance_desc* desc, int nsteps, int checkpoint_interval);
+/* The same with two more choices, for domains whose per-step arrays do not fit
+ * the device whole: slab_nz > 0 reverses every step slab by slab (z-slabs of
+ * slab_nz zones, which must divide the domain's z extent): each slab recomputes
+ * its forward from the domain's state with its true ghost zones, reverses it
+ * seeded by the slab's part of the state adjoint, and adds its Sborder adjoint
+ * into the domain's, so only one slab's intermediates and adjoints are held
+ * (the states, checkpoints and state adjoints stay domain-sized).  first_step
+ * > 0 differentiates only steps first_step .. nsteps-1: the forward runs the
+ * earlier steps without recording, castro_adj_backward returns zero for the
+ * problem parameters, and castro_adj_initial_adjoint gives dJ/dV at first_step.
+ * castro_adj_create(desc, n, k) is castro_adj_create_window(desc, n, k, 0, 0).
+ * No reference counterpart. */
+castro_adj* castro_adj_create_window(const castro_instance_desc* desc, int nsteps, int checkpoint_interval,
+                                     int slab_nz, int first_step);
 void   castro_adj_destroy(castro_adj* adj);
 /* new problem constants (energy, ambient density, perturbation ...) for the next forward */
 int    castro_adj_set_problem(castro_adj* adj, const castro_problem* prob);
@@ -459,7 +473,8 @@ int    castro_adj_forward(castro_adj* adj, double* J);
  * accumulated into it */
 int    castro_adj_backward(castro_adj* adj, double* dJ_dE, double* dJ_drho, double* dJ_dpert);
 double castro_adj_dt(const castro_adj* adj, int step);
-/* device copies (domain box, NVAR comps): final state / adjoint of the initial state */
+/* device copies (domain box, NVAR comps): final state / adjoint of the state at
+ * the window's first step (the initial state when first_step is 0) */
 int    castro_adj_final_state(const castro_adj* adj, double* dst);
 int    castro_adj_initial_adjoint(const castro_adj* adj, double* dst);
 /* device time of the last forward (which=0) or backward (which=1) call, ms */

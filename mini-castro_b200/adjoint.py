@@ -21,7 +21,12 @@ from . import castro
 
 
 class SedovAdjoint:
-    def __init__(self, L: C.CDLL, inst: dict, nsteps: int, checkpoint: int = 5, shell=(0.3, 0.4)):
+    """slab_nz > 0 reverses each step slab by slab (z-slabs of slab_nz zones);
+    first_step > 0 differentiates only steps first_step..nsteps-1, with respect
+    to the state at first_step (``state_adjoint``)."""
+
+    def __init__(self, L: C.CDLL, inst: dict, nsteps: int, checkpoint: int = 5, shell=(0.3, 0.4),
+                 slab_nz: int = 0, first_step: int = 0):
         import torch
 
         self.L = L
@@ -52,7 +57,7 @@ class SedovAdjoint:
         desc.box_hi = one_hi.ctypes.data_as(castro._ip)
         desc.prob = self._problem(p["exp_energy"], p["dens_ambient"])
         desc.stop_time = inst.get("stop_time", -1.0)
-        self.h = L.castro_adj_create(C.byref(desc), nsteps, checkpoint)
+        self.h = L.castro_adj_create_window(C.byref(desc), nsteps, checkpoint, slab_nz, first_step)
         castro.check(L, "castro_adj_create")
         if not self.h:
             raise castro.CastroError("castro_adj_create returned NULL")
@@ -104,6 +109,17 @@ class SedovAdjoint:
         castro.check(self.L, "castro_adj_backward")
         torch.cuda.synchronize()
         return dE.value, dr.value, gp
+
+    def state_adjoint(self):
+        """dJ/dV at the window's first step as a C-order (NVAR, nz, ny, nx) CUDA tensor
+        (after backward)."""
+        import torch
+
+        nv = 7 + castro_nspec(self.L)
+        t = torch.empty((nv,) + self.n[::-1], dtype=torch.float64, device="cuda")
+        self.L.castro_adj_initial_adjoint(self.h, C.c_void_p(t.data_ptr()))
+        castro.check(self.L, "castro_adj_initial_adjoint")
+        return t
 
     def dts(self) -> list[float]:
         return [self.L.castro_adj_dt(self.h, n) for n in range(self.nsteps)]

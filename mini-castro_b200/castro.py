@@ -81,7 +81,7 @@ ABI_SYMBOLS = [
     "castro_adj_backward", "castro_adj_dt", "castro_adj_final_state", "castro_adj_initial_adjoint",
     "castro_adj_time_ms", "castro_adj_device_bytes", "castro_sim_write_plotfile",
     "castro_sim_write_checkpoint", "castro_sim_read_checkpoint", "castro_set_table_l2_window",
-    "castro_sim_set_wait_limit", "castro_saxpy",
+    "castro_sim_set_wait_limit", "castro_saxpy", "castro_adj_create_window",
 ]
 
 
@@ -147,6 +147,8 @@ def load(exact: bool = False) -> C.CDLL:
     L.castro_sim_read_checkpoint.argtypes = [C.c_void_p, C.c_char_p]
     L.castro_adj_create.restype = C.c_void_p
     L.castro_adj_create.argtypes = [C.POINTER(InstanceDesc), C.c_int, C.c_int]
+    L.castro_adj_create_window.restype = C.c_void_p
+    L.castro_adj_create_window.argtypes = [C.POINTER(InstanceDesc), C.c_int, C.c_int, C.c_int, C.c_int]
     L.castro_adj_destroy.argtypes = [C.c_void_p]
     L.castro_adj_set_problem.argtypes = [C.c_void_p, C.POINTER(Problem)]
     L.castro_adj_set_shell.argtypes = [C.c_void_p, C.c_double, C.c_double]

@@ -882,6 +882,14 @@ struct Prim {
 
 struct castro_adj {
     int ns = 2, nv = 9, qv = 10;
+    // dom: the instance's domain, held as one box.  bx and its grown boxes are
+    // the working box: the domain itself, or one z-slab of it when the step is
+    // reversed slab by slab (the per-step arrays are then slab-sized and move
+    // from slab to slab; the states and their adjoints stay domain-sized)
+    IBx dom{};
+    std::vector<IBx> slabs;
+    std::vector<Arr*> slab_arrs;
+    int n_start = 0;   // first step of the differentiated window (0: from initdata)
     IBx bx{}, obx{}, qbx{}, ebx[3], gebx[3], tbx[3][3];
     int bc = CASTRO_BC_OUTFLOW;
     double dx[3] = {0, 0, 0}, problo[3] = {0, 0, 0}, probhi[3] = {0, 0, 0};
@@ -929,6 +937,35 @@ struct StreamScope {
     ~StreamScope() { castro_set_stream(saved); }
 };
 
+// the working box and its grown boxes (Source/Castro_hydro.cpp:81-101)
+void set_geometry(castro_adj* a, const IBx& b)
+{
+    a->bx = b;
+    a->obx = growb(b, 1, 1, 1);
+    a->qbx = growb(b, NG, NG, NG);
+    for (int d = 0; d < 3; ++d) {
+        a->ebx[d] = b;
+        a->ebx[d].hi[d] += 1;
+        a->gebx[d] = growb(a->ebx[d], 1, 1, 1);
+    }
+    a->tbx[0][0] = growb(a->ebx[0], 0, 1, 1); a->tbx[0][1] = growb(a->ebx[0], 0, 0, 1); a->tbx[0][2] = growb(a->ebx[0], 0, 1, 0);
+    a->tbx[1][0] = growb(a->ebx[1], 0, 0, 1); a->tbx[1][1] = growb(a->ebx[1], 1, 0, 1); a->tbx[1][2] = growb(a->ebx[1], 1, 0, 0);
+    a->tbx[2][0] = growb(a->ebx[2], 0, 1, 0); a->tbx[2][1] = growb(a->ebx[2], 1, 0, 0); a->tbx[2][2] = growb(a->ebx[2], 1, 1, 0);
+}
+
+// make slab s the working box: the slab-sized arrays (every slab has the same
+// shape) are re-labelled with the slab's z position
+void use_slab(castro_adj* a, int s)
+{
+    const int shift = a->slabs[s].lo[2] - a->bx.lo[2];
+    if (shift == 0) return;
+    set_geometry(a, a->slabs[s]);
+    for (Arr* r : a->slab_arrs) {
+        r->b.lo[2] += shift;
+        r->b.hi[2] += shift;
+    }
+}
+
 bool alloc_arr(castro_adj* a, Arr& r, const IBx& b, int nc)
 {
     r.b = b;
@@ -972,9 +1009,9 @@ void clean(const IBx& b, const Arr& u)
 template <int NS>
 void fill_sborder(castro_adj* a)
 {
-    Fab S = a->P->Sb.fab(), A = a->P->A.fab();
+    Fab S = a->P->Sb.fab(), A = a->P->A.fab();     // A: the domain's cleaned S_old
     const int bc = a->bc;
-    const IBx bx = a->bx;
+    const IBx bx = a->dom;
     launch_box("adj fill", a->qbx.lo, a->qbx.hi, [=] __device__(int i, int j, int k) {
         int ii = map_bc_adj(i, bx.lo[0], bx.hi[0], bc);
         int jj = map_bc_adj(j, bx.lo[1], bx.hi[1], bc);
@@ -988,9 +1025,9 @@ void fill_sborder(castro_adj* a)
 template <int NS>
 void fill_clean_adj(castro_adj* a)
 {
-    Fab SB = a->Sbb.fab(), A = a->P->A.fab(), AB = a->Ab.fab();
+    Fab SB = a->Sbb.fab(), A = a->P->A.fab(), AB = a->Ab.fab();   // A, AB: domain-sized
     const int bc = a->bc;
-    const IBx bx = a->bx;
+    const IBx bx = a->dom;
     launch_box("adj fill_clean", a->qbx.lo, a->qbx.hi, [=] __device__(int i, int j, int k) {
         constexpr int NV = Dims<NS>::NVAR;
         int ii = map_bc_adj(i, bx.lo[0], bx.hi[0], bc);
@@ -1135,19 +1172,31 @@ void adj_prof_report()
 }
 
 // B = A + dt*src (valid box); Saxpy of Source/Castro_advance.cpp:74
-__global__ void k_saxpy_adj(const double* a, const double* src, double* b, long long n, double dt)
+// clean_state(S_old) of the whole domain, Castro_advance.cpp:51: the step's
+// every working box (the domain, or each slab in turn) fills its Sborder from it
+void begin_step(castro_adj* a, const Arr& Vin)
 {
-    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n) b[t] = a[t] + dt * src[t];
+    copy(a->P->A, Vin, a->st);
+    clean(a->dom, a->P->A);
 }
 
-// the forward of one step from V (valid) with every intermediate kept
+__global__ void k_saxpy_box(BoxRange r, Fab A, Fab S, Fab B, int nv, double dt)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= r.n) return;
+    const int i = r.lx + (int)(t % r.nx);
+    const long long t2 = t / r.nx;
+    const int j = r.ly + (int)(t2 % r.ny);
+    const int k = r.lz + (int)(t2 / r.ny);
+    for (int n = 0; n < nv; ++n) B(i, j, k, n) = A(i, j, k, n) + dt * S(i, j, k, n);
+}
+
+// the forward of one step on the working box from the domain's cleaned S_old
+// (begin_step), with every intermediate kept
 template <int NS>
-void forward_step(castro_adj* a, const Arr& Vin, double dt)
+void forward_step(castro_adj* a, double dt)
 {
     cudaStream_t st = a->st;
-    copy(a->P->A, Vin, st);
-    clean(a->bx, a->P->A);                                        // clean_state(S_old)
     fill_sborder<NS>(a);
     clean(a->qbx, a->P->Sb);                                      // clean_state(Sborder)
     const IBx &bx = a->bx, &obx = a->obx, &qbx = a->qbx;
@@ -1203,16 +1252,31 @@ void forward_step(castro_adj* a, const Arr& Vin, double dt)
                       a->P->qe[1].p, a->gebx[1].lo, a->gebx[1].hi, a->P->qe[2].p, a->gebx[2].lo, a->gebx[2].hi,
                       a->area[0].p, a->gebx[0].lo, a->gebx[0].hi, a->area[1].p, a->gebx[1].lo, a->gebx[1].hi,
                       a->area[2].p, a->gebx[2].lo, a->gebx[2].hi, a->vol.p, bx.lo, bx.hi, a->dx, dt);
-    long long n = a->P->A.n();
-    k_saxpy_adj<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a->P->A.p, a->P->src.p, a->P->Bs.p, n, dt);
+    {
+        BoxRange r = make_range(bx.lo, bx.hi);                      // B = A + dt * src on the working box
+        k_saxpy_box<<<(unsigned)((r.n + 255) / 256), 256, 0, st>>>(r, a->P->A.fab(), a->P->src.fab(), a->P->Bs.fab(),
+                                                                     Dims<NS>::NVAR, dt);
+    }
     copy(a->P->Cs, a->P->Bs, st);
     clean(bx, a->P->Cs);                                          // clean_state(S_new), Castro_advance.cpp
 }
 
-// V_{n+1} = clean(C)
+__global__ void k_copy_box(BoxRange r, Fab D, Fab S, int nv)
+{
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= r.n) return;
+    const int i = r.lx + (int)(t % r.nx);
+    const long long t2 = t / r.nx;
+    const int j = r.ly + (int)(t2 % r.ny);
+    const int k = r.lz + (int)(t2 / r.ny);
+    for (int n = 0; n < nv; ++n) D(i, j, k, n) = S(i, j, k, n);
+}
+
+// V_{n+1} = clean(C) on the working box of the domain-sized Vout
 void finish_step(castro_adj* a, const Arr& Vout)
 {
-    copy(Vout, a->P->Cs, a->st);
+    BoxRange r = make_range(a->bx.lo, a->bx.hi);
+    k_copy_box<<<(unsigned)((r.n + 255) / 256), 256, 0, a->st>>>(r, Vout.fab(), a->P->Cs.fab(), a->nv);
     clean(a->bx, Vout);                                        // post_timestep clean_state, Castro.cpp:369
 }
 
@@ -1221,7 +1285,7 @@ double est_min(castro_adj* a, const Arr& V)
 {
     double big = 1.79769313486231570e+308;
     cudaMemcpyAsync(a->d_est, &big, sizeof big, cudaMemcpyHostToDevice, a->st);
-    estdt(a->bx.lo, a->bx.hi, V.p, V.b.lo, V.b.hi, a->dx, a->d_est);
+    estdt(a->dom.lo, a->dom.hi, V.p, V.b.lo, V.b.hi, a->dx, a->d_est);
     double v;
     cudaMemcpyAsync(&v, a->d_est, sizeof v, cudaMemcpyDeviceToHost, a->st);
     cudaStreamSynchronize(a->st);
@@ -1240,7 +1304,7 @@ double objective(castro_adj* a, const Arr& V, bool grad, const Arr& Vb)
                  c2 = 0.5 * (a->problo[2] + a->probhi[2]);
     const double L = a->probhi[0] - a->problo[0];
     const double r0 = a->shell_r0 * L, r1 = a->shell_r1 * L, dV = dx0 * dx1 * dx2;
-    launch_sum("adj objective", a->bx.lo, a->bx.hi, [=] __device__(int i, int j, int k) -> double {
+    launch_sum("adj objective", a->dom.lo, a->dom.hi, [=] __device__(int i, int j, int k) -> double {
         const double x = pl0 + (i + 0.5) * dx0 - c0, y = pl1 + (j + 0.5) * dx1 - c1, z = pl2 + (k + 0.5) * dx2 - c2;
         const double r = sqrt(x * x + y * y + z * z);
         if (r < r0 || r > r1) return 0.0;
@@ -1267,7 +1331,7 @@ void estdt_adj(castro_adj* a, const Arr& V, double minval, const double* scale, 
     int big = 0x7fffffff;
     cudaMemcpyAsync(a->d_idx, &big, sizeof big, cudaMemcpyHostToDevice, a->st);
     Fab U = V.fab();
-    const IBx bx = a->bx;
+    const IBx bx = a->dom;
     const double dx0 = a->dx[0], dx1 = a->dx[1], dx2 = a->dx[2];
     int* idx = a->d_idx;
     const int nx = bx.hi[0] - bx.lo[0] + 1, ny = bx.hi[1] - bx.lo[1] + 1;
@@ -1453,8 +1517,18 @@ void gather_records(const IBx& fb, int n, const IBx& zb0, Fab L0, Fab R0, bool t
 // reverse of one step: a->Vb holds the adjoint of V_{n+1} on entry and of V_n
 // on exit; slots 0..9 of a->d_scal receive the adjoint of dt_n from this
 // step's uses of it
+// the reverse of one step begins: the domain's S_old adjoint and the scalar
+// accumulators (every working box adds to them)
+void reverse_begin(castro_adj* a)
+{
+    zero(a->Ab, a->st);
+    cudaMemsetAsync(a->d_scal, 0, 32 * sizeof(double), a->st);
+}
+
+// the reverse of one step on the working box, seeded by the adjoint of
+// V_{n+1} on that box (Vb), with the forward intermediates of the same box
 template <int NS>
-void reverse_step(castro_adj* a, const Arr& Vn, double dt)
+void reverse_step(castro_adj* a, double dt)
 {
     cudaStream_t st = a->st;
     const IBx &bx = a->bx, &obx = a->obx, &qbx = a->qbx;
@@ -1469,14 +1543,14 @@ void reverse_step(castro_adj* a, const Arr& Vn, double dt)
         zero(a->qmb[d][d], st);
         zero(a->qpb[d][d], st);
     }
-    cudaMemsetAsync(a->d_scal, 0, 32 * sizeof(double), st);
     double* sc = a->d_scal;
     adj_mark(a, "zero adjoint arrays");
     // V_{n+1} = clean(C), C = clean(B)
     clean_state_adj_impl<NS>(bx.lo, bx.hi, a->P->Cs.fab(), a->Vb.fab(), true);
     clean_state_adj_impl<NS>(bx.lo, bx.hi, a->P->Bs.fab(), a->Vb.fab(), true);
     adj_stage(a, "end cleans");
-    // B = A + dt*src: Ab = Bb, srcb = dt*Bb, dtb += sum(src*Bb)
+    // B = A + dt*src: Ab += Bb (other working boxes' Sborder adjoints may be
+    // there already), srcb = dt*Bb, dtb += sum(src*Bb)
     {
         Fab BB = a->Vb.fab(), AB = a->Ab.fab(), SB = a->srcb.fab(), S = a->P->src.fab();
         launch_sum("adj saxpy", bx.lo, bx.hi, [=] __device__(int i, int j, int k) -> double {
@@ -1484,7 +1558,7 @@ void reverse_step(castro_adj* a, const Arr& Vn, double dt)
 #pragma unroll
             for (int n = 0; n < Dims<NS>::NVAR; ++n) {
                 double b = BB(i, j, k, n);
-                AB(i, j, k, n) = b;
+                AB(i, j, k, n) += b;
                 SB(i, j, k, n) = dt * b;
                 s += S(i, j, k, n) * b;
             }
@@ -1554,9 +1628,16 @@ void reverse_step(castro_adj* a, const Arr& Vn, double dt)
     adj_stage(a, "ctoprim");
     fill_clean_adj<NS>(a);
     adj_stage(a, "sborder fill+clean");
-    clean_state_adj_impl<NS>(bx.lo, bx.hi, Vn.fab(), a->Ab.fab(), true);
+}
+
+// the reverse of one step ends: clean_state(S_old) of the domain reversed, and
+// the adjoint of V_n replaces that of V_{n+1}
+template <int NS>
+void reverse_end(castro_adj* a, const Arr& Vn)
+{
+    clean_state_adj_impl<NS>(a->dom.lo, a->dom.hi, Vn.fab(), a->Ab.fab(), true);
     adj_stage(a, "start clean");
-    copy(a->Vb, a->Ab, st);
+    copy(a->Vb, a->Ab, a->st);
 }
 
 // adjoint of dt_n: its uses in step n (slots 0..9 of sc), the growth-limit
@@ -1587,19 +1668,20 @@ int adj_forward(castro_adj* a)
     a->P = &a->sets[0];
     castro_problem saved = castro::problem();
     castro_set_problem(&a->prob);
-    initdata(a->bx.lo, a->bx.hi, a->V.p, a->bx.lo, a->bx.hi, a->dx, a->problo, a->probhi);
+    initdata(a->dom.lo, a->dom.hi, a->V.p, a->dom.lo, a->dom.hi, a->dx, a->problo, a->probhi);
     castro_set_problem(&saved);
     const int N = a->nsteps;
     a->dts.assign(N, 0.0); a->times.assign(N + 1, 0.0); a->ests.assign(N, 0.0); a->estmin.assign(N, 0.0);
     a->limited.assign(N, 0); a->clamped.assign(N, 0);
     double time = 0.0, dt_prev = 0.0;
-    // the last checkpoint segment keeps its states and intermediates, so the
-    // reverse sweep starts without recomputing it
-    const int K = a->ckpt;
-    const int n0_last = ((N - 1) / K) * K;
+    // checkpoints from the window's first step on; the last checkpoint segment
+    // keeps its states and intermediates, so the reverse sweep starts without
+    // recomputing it
+    const int K = a->ckpt, S0 = a->n_start;
+    const int n0_last = S0 + ((N - 1 - S0) / K) * K;
     const bool keep_last = (int)a->sets.size() >= K;
     for (int n = 0; n < N; ++n) {
-        if (n % a->ckpt == 0) copy(a->ckpts[n / a->ckpt], a->V, a->st);
+        if (n >= S0 && (n - S0) % K == 0) copy(a->ckpts[(n - S0) / K], a->V, a->st);
         if (keep_last && n >= n0_last) {
             a->P = &a->sets[n - n0_last];
             copy(a->seg[n - n0_last], a->V, a->st);
@@ -1623,8 +1705,12 @@ int adj_forward(castro_adj* a)
         a->ests[n] = est;
         a->dts[n] = dt;
         a->times[n] = time;
-        forward_step<NS>(a, a->V, dt);
-        finish_step(a, a->V);
+        begin_step(a, a->V);
+        for (int sl = 0; sl < (int)a->slabs.size(); ++sl) {   // V is rewritten box by box; the boxes read P->A
+            use_slab(a, sl);
+            forward_step<NS>(a, dt);
+            finish_step(a, a->V);
+        }
         time += dt;
         dt_prev = dt;
     }
@@ -1698,7 +1784,7 @@ void initdata_adj(castro_adj* a, double* dE, double* drho, double* pertb)
     }
     const bool want_pb = has_pert && pertb;
     Fab UB = a->Vb.fab();
-    launch_box("initdata_adj", a->bx.lo, a->bx.hi, [=] __device__(int i, int j, int k) {
+    launch_box("initdata_adj", a->dom.lo, a->dom.hi, [=] __device__(int i, int j, int k) {
         const double e_ambient = sc[20];
         double xmin = pl0 + dx0 * (double)i, ymin = pl1 + dx1 * (double)j, zmin = pl2 + dx2 * (double)k;
         int npert = 0, nambient = 0;
@@ -1743,34 +1829,49 @@ int adj_backward(castro_adj* a, double* dE, double* drho, double* pertb)
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, a->st);
-    const int N = a->nsteps, K = a->ckpt;
+    const int N = a->nsteps, K = a->ckpt, S0 = a->n_start;
+    const int nsl = (int)a->slabs.size();
     zero(a->Vb, a->st);
     objective<NS>(a, a->Vfinal, true, a->Vb);
     // chain[0..N-1]: adjoint of dt_n from the growth limit of later steps;
     // chain[N]: adjoint of the running time (stop-time clamp); chain[N+1]: scale
     cudaMemsetAsync(a->d_chain, 0, (N + 2) * sizeof(double), a->st);
-    const int nseg = (N + K - 1) / K;
+    const int nseg = (N - S0 + K - 1) / K;
     for (int sgi = nseg - 1; sgi >= 0; --sgi) {
-        const int n0 = sgi * K, n1 = std::min(N, n0 + K);
+        const int n0 = S0 + sgi * K, n1 = std::min(N, n0 + K);
         adj_mark(a, "(segment start)");
         const bool keep = (int)a->sets.size() >= K;
         const bool ready = keep && a->last_seg_ready && sgi == nseg - 1;
         if (!ready) copy(a->seg[0], a->ckpts[sgi], a->st);
         for (int n = n0; n < (ready ? n0 : n1 - (keep ? 0 : 1)); ++n) {
             a->P = &a->sets[keep ? n - n0 : 0];
-            forward_step<NS>(a, a->seg[n - n0], a->dts[n]);
-            if (n < n1 - 1) finish_step(a, a->seg[n - n0 + 1]);
+            begin_step(a, a->seg[n - n0]);
+            for (int sl = 0; sl < nsl; ++sl) {
+                use_slab(a, sl);
+                forward_step<NS>(a, a->dts[n]);
+                if (n < n1 - 1) finish_step(a, a->seg[n - n0 + 1]);
+            }
         }
         adj_mark(a, "segment recompute");
         for (int n = n1 - 1; n >= n0; --n) {
             if (keep) {
+                // the whole domain is the working box and the set holds its intermediates
                 a->P = &a->sets[n - n0];
+                reverse_begin(a);
+                reverse_step<NS>(a, a->dts[n]);
             } else {
+                // every working box: its intermediates recomputed, then reversed
                 a->P = &a->sets[0];
-                forward_step<NS>(a, a->seg[n - n0], a->dts[n]);
+                begin_step(a, a->seg[n - n0]);
+                reverse_begin(a);
+                for (int sl = 0; sl < nsl; ++sl) {
+                    use_slab(a, sl);
+                    forward_step<NS>(a, a->dts[n]);
+                    adj_mark(a, "step recompute");
+                    reverse_step<NS>(a, a->dts[n]);
+                }
             }
-            adj_mark(a, "step recompute");
-            reverse_step<NS>(a, a->seg[n - n0], a->dts[n]);
+            reverse_end<NS>(a, a->seg[n - n0]);
             // dt_n = rule(V_n, dt_{n-1}, time_n), reversed on the device
             const int branch = a->clamped[n] ? 1 : (n > 0 && a->limited[n]) ? 2 : 0;
             k_dt_chain<<<1, 1, 0, a->st>>>(a->d_scal, a->dx[0], a->dx[1], a->dx[2], a->d_chain, n, N, branch,
@@ -1782,9 +1883,16 @@ int adj_backward(castro_adj* a, double* dE, double* drho, double* pertb)
     }
     // earlier segments reused the sets: a second reverse sweep recomputes
     a->last_seg_ready = a->last_seg_ready && nseg == 1;
-    adj_mark(a, "(init start)");
-    initdata_adj<NS>(a, dE, drho, pertb);
-    adj_mark(a, "initdata adjoint");
+    if (S0 == 0) {
+        adj_mark(a, "(init start)");
+        initdata_adj<NS>(a, dE, drho, pertb);
+        adj_mark(a, "initdata adjoint");
+    } else {
+        // the window starts at a state, not at initdata: its adjoint is Vb
+        // (castro_adj_initial_adjoint); the problem parameters get none
+        *dE = 0.0;
+        *drho = 0.0;
+    }
     adj_prof_report();
     cudaEventRecord(e1, a->st);
     cudaEventSynchronize(e1);
@@ -1798,17 +1906,26 @@ int adj_backward(castro_adj* a, double* dE, double* drho, double* pertb)
 
 extern "C" {
 
-castro_adj* castro_adj_create(const castro_instance_desc* desc, int nsteps, int checkpoint_interval)
+castro_adj* castro_adj_create_window(const castro_instance_desc* desc, int nsteps, int checkpoint_interval,
+                                     int slab_nz, int first_step)
 {
-    if (!desc || nsteps < 1 || checkpoint_interval < 1) { set_error(CASTRO_ERR_ARG, "castro_adj_create: arguments"); return nullptr; }
+    if (!desc || nsteps < 1 || checkpoint_interval < 1 || first_step < 0 || first_step >= nsteps || slab_nz < 0) {
+        set_error(CASTRO_ERR_ARG, "castro_adj_create: arguments");
+        return nullptr;
+    }
     if (!table_ready()) { set_error(CASTRO_ERR_NO_TABLE, "castro_adj_create: eos_init has not run"); return nullptr; }
+    const int nz = desc->dom_hi[2] - desc->dom_lo[2] + 1;
+    if (slab_nz > 0 && slab_nz < nz && nz % slab_nz != 0) {
+        set_error(CASTRO_ERR_ARG, "castro_adj_create: the slab thickness must divide the domain's z extent");
+        return nullptr;
+    }
     castro_adj* a = new castro_adj();
     a->ns = nspec();
     a->nv = 7 + a->ns;
     a->qv = 8 + a->ns;
     for (int d = 0; d < 3; ++d) {
-        a->bx.lo[d] = desc->dom_lo[d];
-        a->bx.hi[d] = desc->dom_hi[d];
+        a->dom.lo[d] = desc->dom_lo[d];
+        a->dom.hi[d] = desc->dom_hi[d];
         a->problo[d] = desc->problo[d];
         a->probhi[d] = desc->probhi[d];
         a->dx[d] = (desc->probhi[d] - desc->problo[d]) / (double)(desc->dom_hi[d] - desc->dom_lo[d] + 1);
@@ -1818,16 +1935,15 @@ castro_adj* castro_adj_create(const castro_instance_desc* desc, int nsteps, int 
     a->stop_time = desc->stop_time;
     a->nsteps = nsteps;
     a->ckpt = checkpoint_interval;
-    a->obx = growb(a->bx, 1, 1, 1);
-    a->qbx = growb(a->bx, NG, NG, NG);
-    for (int d = 0; d < 3; ++d) {
-        a->ebx[d] = a->bx;
-        a->ebx[d].hi[d] += 1;
-        a->gebx[d] = growb(a->ebx[d], 1, 1, 1);
+    a->n_start = first_step;
+    const int tz = (slab_nz > 0 && slab_nz < nz) ? slab_nz : nz;
+    for (int z0 = a->dom.lo[2]; z0 <= a->dom.hi[2]; z0 += tz) {
+        IBx b = a->dom;
+        b.lo[2] = z0;
+        b.hi[2] = z0 + tz - 1;
+        a->slabs.push_back(b);
     }
-    a->tbx[0][0] = growb(a->ebx[0], 0, 1, 1); a->tbx[0][1] = growb(a->ebx[0], 0, 0, 1); a->tbx[0][2] = growb(a->ebx[0], 0, 1, 0);
-    a->tbx[1][0] = growb(a->ebx[1], 0, 0, 1); a->tbx[1][1] = growb(a->ebx[1], 1, 0, 1); a->tbx[1][2] = growb(a->ebx[1], 1, 0, 0);
-    a->tbx[2][0] = growb(a->ebx[2], 0, 1, 0); a->tbx[2][1] = growb(a->ebx[2], 1, 0, 0); a->tbx[2][2] = growb(a->ebx[2], 1, 1, 0);
+    set_geometry(a, a->slabs[0]);
     if (cudaStreamCreateWithFlags(&a->st, cudaStreamNonBlocking) != cudaSuccess) {
         set_error(CASTRO_ERR_CUDA, "castro_adj_create: stream");
         delete a;
@@ -1835,31 +1951,40 @@ castro_adj* castro_adj_create(const castro_instance_desc* desc, int nsteps, int 
     }
     const int NV = a->nv, QV = a->qv;
     bool ok = true;
-    const int nck = (nsteps + checkpoint_interval - 1) / checkpoint_interval;
+    // slab-sized arrays move with the working box (use_slab)
+    auto sa = [&](Arr& r, const IBx& b, int nc) {
+        if (!ok) return false;
+        ok = alloc_arr(a, r, b, nc);
+        if (ok) a->slab_arrs.push_back(&r);
+        return ok;
+    };
+    const int nck = (nsteps - first_step + checkpoint_interval - 1) / checkpoint_interval;
     a->ckpts.resize(nck);
     a->seg.resize(checkpoint_interval);
-    for (auto& r : a->ckpts) ok = ok && alloc_arr(a, r, a->bx, NV);
-    for (auto& r : a->seg) ok = ok && alloc_arr(a, r, a->bx, NV);
-    for (Arr* r : {&a->V, &a->Vfinal, &a->Vb, &a->Ab, &a->srcb}) ok = ok && alloc_arr(a, *r, a->bx, NV);
-    ok = ok && alloc_arr(a, a->vol, a->bx, 1);
-    ok = ok && alloc_arr(a, a->Sbb, a->qbx, NV) && alloc_arr(a, a->qb, a->qbx, QV) && alloc_arr(a, a->qab, a->qbx, NQAUX);
-    ok = ok && alloc_arr(a, a->divb, a->obx, 1) && alloc_arr(a, a->flb, a->obx, 1);
+    for (auto& r : a->ckpts) ok = ok && alloc_arr(a, r, a->dom, NV);
+    for (auto& r : a->seg) ok = ok && alloc_arr(a, r, a->dom, NV);
+    for (Arr* r : {&a->V, &a->Vfinal, &a->Vb, &a->Ab}) ok = ok && alloc_arr(a, *r, a->dom, NV);
+    sa(a->srcb, a->bx, NV);
+    sa(a->vol, a->bx, 1);
+    sa(a->Sbb, a->qbx, NV) && sa(a->qb, a->qbx, QV) && sa(a->qab, a->qbx, NQAUX);
+    sa(a->divb, a->obx, 1) && sa(a->flb, a->obx, 1);
     for (int d = 0; d < 3 && ok; ++d) {
         for (int e = 0; e < 3 && ok; ++e) {
-            ok = ok && alloc_arr(a, a->qmb[d][e], a->obx, QV) && alloc_arr(a, a->qpb[d][e], a->obx, QV);
-            if (d != e) ok = ok && alloc_arr(a, a->F2b[d][e], a->obx, NV) && alloc_arr(a, a->G2b[d][e], a->obx, NGDNV);
+            sa(a->qmb[d][e], a->obx, QV) && sa(a->qpb[d][e], a->obx, QV);
+            if (d != e) sa(a->F2b[d][e], a->obx, NV) && sa(a->G2b[d][e], a->obx, NGDNV);
         }
-        ok = ok && alloc_arr(a, a->F1b[d], a->obx, NV) && alloc_arr(a, a->G1b[d], a->obx, NGDNV);
-        ok = ok && alloc_arr(a, a->qlb[d], a->obx, QV) && alloc_arr(a, a->qrb[d], a->obx, QV);
-        ok = ok && alloc_arr(a, a->fluxb[d], a->gebx[d], NV) && alloc_arr(a, a->qeb[d], a->gebx[d], NGDNV);
-        ok = ok && alloc_arr(a, a->area[d], a->gebx[d], 1);
+        sa(a->F1b[d], a->obx, NV) && sa(a->G1b[d], a->obx, NGDNV);
+        sa(a->qlb[d], a->obx, QV) && sa(a->qrb[d], a->obx, QV);
+        sa(a->fluxb[d], a->gebx[d], NV) && sa(a->qeb[d], a->gebx[d], NGDNV);
+        sa(a->area[d], a->gebx[d], 1);
         for (int e = 0; e < 3 && ok; ++e)
-            if (e != d) ok = ok && alloc_arr(a, a->T1L[d][e], a->obx, a->nv) && alloc_arr(a, a->T1R[d][e], a->obx, a->nv);
+            if (e != d) sa(a->T1L[d][e], a->obx, a->nv) && sa(a->T1R[d][e], a->obx, a->nv);
         for (int e = 0; e < 2 && ok; ++e)
-            ok = ok && alloc_arr(a, a->T2L[d][e], a->obx, a->nv) && alloc_arr(a, a->T2R[d][e], a->obx, a->nv);
+            sa(a->T2L[d][e], a->obx, a->nv) && sa(a->T2R[d][e], a->obx, a->nv);
     }
     // per-step forward intermediates: a set per segment step when they fit in
-    // 70% of the free device memory, else one set recomputed per step
+    // 70% of the free device memory (the whole domain as one working box only),
+    // else one set recomputed per step
     auto set_bytes = [&]() {
         long long n = 4 * nptsb(a->bx) * NV + nptsb(a->qbx) * (NV + QV + NQAUX) + nptsb(a->obx) * (1 + QV);
         n += nptsb(a->obx) * (18LL * QV + 3LL * (NV + NGDNV) + 6LL * (NV + NGDNV) + 6LL * QV);
@@ -1868,21 +1993,23 @@ castro_adj* castro_adj_create(const castro_instance_desc* desc, int nsteps, int 
     };
     size_t fr = 0, tot = 0;
     cudaMemGetInfo(&fr, &tot);
-    int nsets = (ok && (size_t)checkpoint_interval * set_bytes() < (size_t)(0.7 * (double)fr)) ? checkpoint_interval : 1;
+    int nsets = (ok && a->slabs.size() == 1 && (size_t)checkpoint_interval * set_bytes() < (size_t)(0.7 * (double)fr))
+                    ? checkpoint_interval : 1;
     a->sets.resize(nsets);
     for (Prim& P : a->sets) {
-        for (Arr* r : {&P.A, &P.Bs, &P.Cs, &P.src}) ok = ok && alloc_arr(a, *r, a->bx, NV);
-        ok = ok && alloc_arr(a, P.Sb, a->qbx, NV) && alloc_arr(a, P.q, a->qbx, QV) && alloc_arr(a, P.qaux, a->qbx, NQAUX);
-        ok = ok && alloc_arr(a, P.div, a->obx, 1) && alloc_arr(a, P.qint, a->obx, QV);
+        ok = ok && alloc_arr(a, P.A, a->dom, NV);     // the domain's cleaned S_old
+        for (Arr* r : {&P.Bs, &P.Cs, &P.src}) sa(*r, a->bx, NV);
+        sa(P.Sb, a->qbx, NV) && sa(P.q, a->qbx, QV) && sa(P.qaux, a->qbx, NQAUX);
+        sa(P.div, a->obx, 1) && sa(P.qint, a->obx, QV);
         for (int d = 0; d < 3 && ok; ++d) {
             for (int e = 0; e < 3 && ok; ++e) {
-                ok = ok && alloc_arr(a, P.qm[d][e], a->obx, QV) && alloc_arr(a, P.qp[d][e], a->obx, QV);
-                if (d != e) ok = ok && alloc_arr(a, P.F2[d][e], a->obx, NV) && alloc_arr(a, P.G2[d][e], a->obx, NGDNV);
+                sa(P.qm[d][e], a->obx, QV) && sa(P.qp[d][e], a->obx, QV);
+                if (d != e) sa(P.F2[d][e], a->obx, NV) && sa(P.G2[d][e], a->obx, NGDNV);
             }
-            ok = ok && alloc_arr(a, P.F1[d], a->obx, NV) && alloc_arr(a, P.G1[d], a->obx, NGDNV);
-            ok = ok && alloc_arr(a, P.ql[d], a->obx, QV) && alloc_arr(a, P.qr[d], a->obx, QV);
-            ok = ok && alloc_arr(a, P.Fav[d], a->gebx[d], NV) && alloc_arr(a, P.flux[d], a->gebx[d], NV);
-            ok = ok && alloc_arr(a, P.qe[d], a->gebx[d], NGDNV);
+            sa(P.F1[d], a->obx, NV) && sa(P.G1[d], a->obx, NGDNV);
+            sa(P.ql[d], a->obx, QV) && sa(P.qr[d], a->obx, QV);
+            sa(P.Fav[d], a->gebx[d], NV) && sa(P.flux[d], a->gebx[d], NV);
+            sa(P.qe[d], a->gebx[d], NGDNV);
         }
     }
     a->P = &a->sets[0];
@@ -1923,6 +2050,11 @@ castro_adj* castro_adj_create(const castro_instance_desc* desc, int nsteps, int 
         return nullptr;
     }
     return a;
+}
+
+castro_adj* castro_adj_create(const castro_instance_desc* desc, int nsteps, int checkpoint_interval)
+{
+    return castro_adj_create_window(desc, nsteps, checkpoint_interval, 0, 0);
 }
 
 void castro_adj_destroy(castro_adj* a)

@@ -2700,15 +2700,20 @@ double castro_sim_blast_radius(castro_sim* s, int inst, double* blast_mass)
 
 }  // extern "C"
 
-// Library-managed scratch of castro_construct_hydro_source_box, one per
-// device, reused while the box shape does not change.
+// Library-managed scratch of castro_construct_hydro_source_box: per device, a
+// set of cached sims keyed by box shape and species count (a BoxArray of a few
+// shapes, like the configs' uneven ones, allocates each shape once), the least
+// recently used one destroyed when the set is full.
 struct BoxScratch {
-    int lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
+    int n[3] = {0, 0, 0};
     int ns = 0;
     castro_sim* s = nullptr;
+    unsigned long long used = 0;
 };
 constexpr int BOX_MAX_DEVICES = 64;
-static BoxScratch g_box[BOX_MAX_DEVICES];
+constexpr int BOX_CACHE_SHAPES = 8;
+static BoxScratch g_box[BOX_MAX_DEVICES][BOX_CACHE_SHAPES];
+static unsigned long long g_box_clock[BOX_MAX_DEVICES] = {};
 
 // Position, geometry and dt of one castro_construct_hydro_source_box call,
 // passed by value (kernel arguments are copied at launch, also into a graph
@@ -2740,13 +2745,20 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
         set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box: device index beyond 63");
         return CASTRO_ERR_ARG;
     }
-    BoxScratch& gb = g_box[dev];
     // the cached arrays and work lists depend on the box's shape only; its
     // position is passed with every call, so that a host walking the boxes of
     // a BoxArray reuses them
-    bool same = gb.s && gb.ns == NS;
-    for (int d = 0; d < 3 && same; ++d) same = gb.hi[d] - gb.lo[d] == hi[d] - lo[d];
-    if (!same) {
+    int shape[3];
+    for (int d = 0; d < 3; ++d) shape[d] = hi[d] - lo[d] + 1;
+    BoxScratch* hit = nullptr;
+    BoxScratch* victim = &g_box[dev][0];
+    for (int c = 0; c < BOX_CACHE_SHAPES; ++c) {
+        BoxScratch& e = g_box[dev][c];
+        if (e.s && e.ns == NS && e.n[0] == shape[0] && e.n[1] == shape[1] && e.n[2] == shape[2]) { hit = &e; break; }
+        if (!e.s ? victim->s != nullptr : (victim->s && e.used < victim->used)) victim = &e;
+    }
+    if (!hit) {
+        BoxScratch& gb = *victim;
         if (gb.s) castro_sim_destroy(gb.s);
         gb.s = nullptr;
         castro_instance_desc D;
@@ -2763,10 +2775,12 @@ static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const 
         D.stop_time = -1.0;
         gb.s = castro_sim_create(1, &D, CASTRO_MODE_BATCHED);
         if (!gb.s) return castro_last_error();
-        for (int d = 0; d < 3; ++d) { gb.lo[d] = lo[d]; gb.hi[d] = hi[d]; }
+        for (int d = 0; d < 3; ++d) gb.n[d] = shape[d];
         gb.ns = NS;
+        hit = &gb;
     }
-    castro_sim* s = gb.s;
+    hit->used = ++g_box_clock[dev];
+    castro_sim* s = hit->s;
     // position, geometry and dt of this call (the box is its own instance domain)
     BoxDev B = s->hboxes[0];
     InstDev I = s->hinst[0];
