@@ -5,16 +5,17 @@ The product is the CUDA library ``lib/libcastro_b200.so`` (C-ABI in
 
 * ``castro``     -- ctypes binding of the C-ABI (simulation objects, per-routine calls)
 * ``configs``    -- the Sedov workloads (BoxArrays, networks, problem constants)
-* ``helm_table`` -- writer of the Helmholtz table file read by ``eos_init``
+* ``helm_table`` -- writer of the Helmholtz table file read by ``eos_init`` (analytic non-degenerate gas)
+* ``helm_fd``    -- the same file computed from Fermi-Dirac integrals (electron-positron gas in pair equilibrium)
 * ``replicas``   -- the multi-GPU (one replica per rank) reductions
 * ``shard``      -- one level's boxes sharded over ranks: halo exchange, dt min-reduction
 * ``adjoint``    -- gradients of a Sedov run (reverse sweep) and its torch.autograd wrapper
 * ``plotfile``   -- reader of the AMReX plotfiles the library writes
 * ``build``      -- nvcc recipe for the sm_100a libraries
 """
-from . import adjoint, castro, configs, helm_table, plotfile, replicas, shard  # noqa: F401
+from . import adjoint, castro, configs, helm_fd, helm_table, plotfile, replicas, shard  # noqa: F401
 
-__all__ = ["adjoint", "castro", "configs", "helm_table", "plotfile", "replicas", "shard", "make_sim"]
+__all__ = ["adjoint", "castro", "configs", "helm_fd", "helm_table", "plotfile", "replicas", "shard", "make_sim"]
 
 
 def make_sim(L, cfg, mode=castro.MODE_BATCHED):
