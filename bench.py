@@ -303,6 +303,17 @@ def run_b200(args, pkg, rank, world):
                      "zones": pkg.configs.zones(big), "boxes": len(big["instances"][0]["boxes"]),
                      "batched": time_mode(pkg, L, big, pkg.castro.MODE_BATCHED, args.large_steps,
                                           pkg.configs.zones(big))}
+    fd_leg = None
+    if rank == 0 and args.fd_table_steps > 0:
+        # the same workload and step on the Fermi-Dirac electron-positron table
+        fd_path = pkg.helm_fd.ensure_table()
+        L.castro_eos_init_path(fd_path.encode())
+        pkg.castro.check(L, "eos_init (Fermi-Dirac table)")
+        fd_leg = time_mode(pkg, L, cfg, pkg.castro.MODE_BATCHED, args.fd_table_steps, zones)
+        fd_leg["table"] = "Fermi-Dirac electron-positron gas in pair equilibrium (helm_fd.py)"
+        fd_leg["helm_table_sha256"] = pkg.helm_table.sha256(fd_path)
+        L.castro_eos_init_path(table.encode())
+        pkg.castro.check(L, "eos_init")
     adjoint_cfg = None
     if rank == 0 and args.adjoint_reps > 0:
         adjoint_cfg = run_adjoint_config(pkg, args)
@@ -385,6 +396,7 @@ def run_b200(args, pkg, rank, world):
         "plain_box_drop_in": plain_box,
         "persistent": persistent,
         "batched_config": batched_cfg,
+        "fd_table": fd_leg,
         "large_config": large_cfg,
         "adjoint_config": adjoint_cfg,
         "adjoint_forward_ratio": adjoint_cfg["adjoint_forward_ratio"] if adjoint_cfg else None,
@@ -699,6 +711,8 @@ def main():
     ap.add_argument("--large-adjoint", type=int, default=1, help="the 384^3 configuration's 50-step adjoint (0: skip)")
     ap.add_argument("--adjoint-reps", type=int, default=3, help="timed forward+reverse runs of the adjoint configuration (0: skip)")
     ap.add_argument("--adjoint-fd", type=int, default=16, help="finite-difference directions of the gradient check (0: skip)")
+    ap.add_argument("--fd-table-steps", type=int, default=10,
+                    help="timed steps of the workload on the Fermi-Dirac table (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scale", type=int, default=1, help="divide the workload's zone counts (profiling runs only)")
     args = ap.parse_args()

@@ -217,10 +217,12 @@ int  castro_set_problem(const castro_problem* p);
  * fused: Sborder (grow(box,4), NVAR comps, already cleaned) -> source on the box
  * (accumulated into 'source', which the caller zeroes like hydro_source.setVal(0)).
  * fluxes_out[d] (optional, may be NULL): dt*F*A on the faces of the box
- * (store_flux).  Uses library-managed scratch: per device, one set per box shape
- * for the 8 shapes used last, allocated on a shape's first call (so do not capture
- * such a call in a CUDA graph); the box position, geometry and dt travel as kernel
- * arguments, so calls for the cached shapes allocate nothing. */
+ * (store_flux).  Uses library-managed scratch: one device array per device,
+ * grown to the largest box seen so far; a call for a box larger than every
+ * earlier one synchronizes the device and allocates (so do not capture such a
+ * call in a CUDA graph), and every other call allocates nothing, whatever the
+ * mix of box shapes. Calls share the array: calls that overlap on the GPU
+ * (streams without ordering between them) race. */
 int castro_construct_hydro_source_box(const int* lo, const int* hi,
                                       const double* sborder, const int* sb_lo, const int* sb_hi,
                                       double* source, const int* sr_lo, const int* sr_hi,

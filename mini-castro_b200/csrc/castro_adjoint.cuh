@@ -114,10 +114,10 @@ CASTRO_HD void eos_eval_t(const EosTableDev& tb, const S& temp, const S& den, co
     S deiondd = (1.5 * dpiondd - eion) * deni;
     S deiondt = 1.5 * dpiondt * deni;
 
-    int jat = table_trunc((log10(val(temp)) - tb.tlo) * tb.tstpi);
+    int jat = table_trunc((table_log10(val(temp)) - tb.tlo) * tb.tstpi);
     jat = jat > JMAX - 2 ? JMAX - 2 : jat;
     jat = jat < 0 ? 0 : jat;
-    int iat = table_trunc((log10(val(din)) - tb.dlo) * tb.dstpi);
+    int iat = table_trunc((table_log10(val(din)) - tb.dlo) * tb.dstpi);
     iat = iat > IMAX - 2 ? IMAX - 2 : iat;
     iat = iat < 0 ? 0 : iat;
     // the cells settled against the node values (a row's lower and upper node), as the forward EOS does

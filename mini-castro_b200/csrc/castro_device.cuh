@@ -128,15 +128,29 @@ struct DensityBasis {
     Basis4 xsi;
 };
 
+// log10 of a table coordinate, good to ~1e-5 of a cell (single-precision
+// hardware log2; every argument here is a positive temperature or density far
+// inside float range, and NaN stays NaN): the cell it selects is settled
+// against the node values right after, so the cell -- and every result -- is
+// the one a double-precision log10 leads to.
+CASTRO_HD double table_log10(double x)
+{
+#ifdef __CUDA_ARCH__
+    return (double)__log2f((float)x) * 0.30102999566398119521;
+#else
+    return log10(x);   // host builds of the stages (the adjoint self-test)
+#endif
+}
+
 __device__ __forceinline__ void density_basis(double din, DensityBasis& B)
 {
-    int iat = table_trunc((log10(din) - c_eos.dlo) * c_eos.dstpi);   // eos.F90:244-245
+    int iat = table_trunc((table_log10(din) - c_eos.dlo) * c_eos.dstpi);   // eos.F90:244-245
     iat = iat > IMAX - 2 ? IMAX - 2 : iat;
     iat = iat < 0 ? 0 : iat;
-    // Within an ulp of a node the last bit of log10 decides the cell, and two
-    // faithful log10s (this device's, a host libm's) can decide differently: the
-    // estimate is settled against the node values, so that the cell is the one
-    // whose nodes bracket the argument, whatever log10 returned.
+    // Near a node the rounding of the logarithm decides the cell (the last bit
+    // of a double log10, or the ~1e-5 cell of table_log10): the estimate is
+    // settled against the node values, so that the cell is the one whose nodes
+    // bracket the argument, whatever the logarithm returned.
     const double* dr = c_eos.drow + (size_t)iat * ROW_STRIDE;
     double d0 = __ldg(dr + 0), dd = __ldg(dr + 1), dd2 = __ldg(dr + 2), ddi = __ldg(dr + 3);
     const double d1 = __ldg(dr + ROW_NEXT);
@@ -187,11 +201,16 @@ __device__ __forceinline__ void eos_eval_part(double temp, const EosConst& K, co
 {
     constexpr bool FULL = WHAT == EVAL_FULL;
     const double den = K.den, deni = K.deni, ytot1 = K.ytot1, ye = K.ye, din = K.din;
-    double tempi = 1.0 / temp;
     // radiation, :207-213
     double prad = c_eos.asoli3 * temp * temp * temp * temp;
     double dpraddd = 0.0;
+#ifdef CASTRO_EXACT
+    double tempi = 1.0 / temp;
     double dpraddt = 4.0 * prad * tempi;
+#else
+    // 4 a T^3 / 3 without the division by T (the production build's rounding)
+    double dpraddt = 4.0 * (c_eos.asoli3 * temp * temp * temp);
+#endif
     double erad = 3.0 * prad * deni;
     double deraddd = FULL ? -erad * deni : 0.0;
     double deraddt = 3.0 * dpraddt * deni;
@@ -204,7 +223,7 @@ __device__ __forceinline__ void eos_eval_part(double temp, const EosConst& K, co
     double deiondt = 1.5 * dpiondt * deni;
 
     // temperature cell, :242-243
-    int jat = table_trunc((log10(temp) - c_eos.tlo) * c_eos.tstpi);
+    int jat = table_trunc((table_log10(temp) - c_eos.tlo) * c_eos.tstpi);
     jat = jat > JMAX - 2 ? JMAX - 2 : jat;
     jat = jat < 0 ? 0 : jat;
     // settled against the node temperatures, as the density cell in
@@ -442,8 +461,13 @@ __device__ __forceinline__ EosResult eos_solve(double rho, double T, double v_wa
         temp = DMAX(0.5 * temp_old, DMIN(temp, 2.0 * temp_old));
         temp = DMAX(c_eos.mintemp, temp);
         T = temp;
+#ifdef CASTRO_EXACT
         double error = fabs((temp - temp_old) / temp_old);
         if (error < 1.e-8) converged = true;
+#else
+        // |dT / T_old| < 1e-8 without the division
+        if (fabs(temp - temp_old) < 1.e-8 * fabs(temp_old)) converged = true;
+#endif
     }
     // ended by the iteration limit: the reference's outputs are those of the
     // last iteration's evaluation, here a light one

@@ -2700,122 +2700,6 @@ double castro_sim_blast_radius(castro_sim* s, int inst, double* blast_mass)
 
 }  // extern "C"
 
-// Library-managed scratch of castro_construct_hydro_source_box: per device, a
-// set of cached sims keyed by box shape and species count (a BoxArray of a few
-// shapes, like the configs' uneven ones, allocates each shape once), the least
-// recently used one destroyed when the set is full.
-struct BoxScratch {
-    int n[3] = {0, 0, 0};
-    int ns = 0;
-    castro_sim* s = nullptr;
-    unsigned long long used = 0;
-};
-constexpr int BOX_MAX_DEVICES = 64;
-constexpr int BOX_CACHE_SHAPES = 8;
-static BoxScratch g_box[BOX_MAX_DEVICES][BOX_CACHE_SHAPES];
-static unsigned long long g_box_clock[BOX_MAX_DEVICES] = {};
-
-// Position, geometry and dt of one castro_construct_hydro_source_box call,
-// passed by value (kernel arguments are copied at launch, also into a graph
-// node under stream capture) into the cached sim's records.
-__global__ void k_box_setup(BoxDev B, InstDev I, InstState st, BoxDev* dB, BoxDev* dDom, InstDev* dI, InstState* dS)
-{
-    if (threadIdx.x == 0) {
-        *dB = B;
-        *dDom = B;
-        *dI = I;
-        *dS = st;
-    }
-}
-
-template <int NS>
-static int box_hydro_impl(const int* lo, const int* hi, const double* sb, const int* sb_lo, const int* sb_hi,
-                          double* source, const int* sr_lo, const int* sr_hi, double* const* fo, const int* fo_lo,
-                          const int* fo_hi, const double* dx, double dt)
-{
-    NvtxRange r("castro_construct_hydro_source_box");
-    for (int d = 0; d < 3; ++d)
-        if (sb_lo[d] > lo[d] - NG || sb_hi[d] < hi[d] + NG) {
-            set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box: Sborder needs 4 ghost zones");
-            return CASTRO_ERR_ARG;
-        }
-    int dev = 0;
-    if (!cuda_ok(cudaGetDevice(&dev), "castro_construct_hydro_source_box: cudaGetDevice")) return CASTRO_ERR_CUDA;
-    if (dev < 0 || dev >= BOX_MAX_DEVICES) {
-        set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box: device index beyond 63");
-        return CASTRO_ERR_ARG;
-    }
-    // the cached arrays and work lists depend on the box's shape only; its
-    // position is passed with every call, so that a host walking the boxes of
-    // a BoxArray reuses them
-    int shape[3];
-    for (int d = 0; d < 3; ++d) shape[d] = hi[d] - lo[d] + 1;
-    BoxScratch* hit = nullptr;
-    BoxScratch* victim = &g_box[dev][0];
-    for (int c = 0; c < BOX_CACHE_SHAPES; ++c) {
-        BoxScratch& e = g_box[dev][c];
-        if (e.s && e.ns == NS && e.n[0] == shape[0] && e.n[1] == shape[1] && e.n[2] == shape[2]) { hit = &e; break; }
-        if (!e.s ? victim->s != nullptr : (victim->s && e.used < victim->used)) victim = &e;
-    }
-    if (!hit) {
-        BoxScratch& gb = *victim;
-        if (gb.s) castro_sim_destroy(gb.s);
-        gb.s = nullptr;
-        castro_instance_desc D;
-        memset(&D, 0, sizeof D);
-        for (int d = 0; d < 3; ++d) {   // unit zones: every call passes its own dx
-            D.dom_lo[d] = lo[d]; D.dom_hi[d] = hi[d];
-            D.problo[d] = 0.0; D.probhi[d] = (double)(hi[d] - lo[d] + 1);
-        }
-        D.bc = CASTRO_BC_OUTFLOW;
-        D.nbox = 1;
-        D.box_lo = lo;
-        D.box_hi = hi;
-        castro_problem_defaults(&D.prob);
-        D.stop_time = -1.0;
-        gb.s = castro_sim_create(1, &D, CASTRO_MODE_BATCHED);
-        if (!gb.s) return castro_last_error();
-        for (int d = 0; d < 3; ++d) gb.n[d] = shape[d];
-        gb.ns = NS;
-        hit = &gb;
-    }
-    hit->used = ++g_box_clock[dev];
-    castro_sim* s = hit->s;
-    // position, geometry and dt of this call (the box is its own instance domain)
-    BoxDev B = s->hboxes[0];
-    InstDev I = s->hinst[0];
-    for (int d = 0; d < 3; ++d) {
-        B.lo[d] = lo[d]; B.hi[d] = hi[d];
-        I.dom_lo[d] = lo[d]; I.dom_hi[d] = hi[d];
-        I.dx[d] = dx[d];
-    }
-    InstState st;
-    memset(&st, 0, sizeof st);
-    st.dt = dt;
-    st.stop_time = -1.0;
-    cudaStream_t cs = castro::stream();
-    k_box_setup<<<1, 32, 0, cs>>>(B, I, st, s->dboxes, s->ddom, s->dinst, s->dstate);
-    SimDev S = s->dev(), Sd = s->dev_dom();   // one box, which is the instance domain
-    k_box_prim<NS><<<s->n_g4, BLOCK, 0, cs>>>(S, s->w_g4, make_fab(sb, sb_lo, sb_hi));
-    k_prep<NS><<<s->n_g1, BLOCK, 0, cs>>>(Sd, s->w_g1);
-    k_trace<NS><<<s->n_trace, BLOCK, 0, cs>>>(Sd, s->w_trace);
-    if (CASTRO_TRACE_SPLIT) k_trace2<NS><<<s->n_trace, BLOCK, 0, cs>>>(Sd, s->w_trace);
-    k_riemann1<NS><<<s->n_tbx, BLOCK, 0, cs>>>(Sd, s->w_tbx);
-    k_riemann2<NS><<<s->n_tbx, BLOCK, R2Slot<NS>::BYTES, cs>>>(Sd, s->w_tbx);
-    k_riemann3<NS><<<s->n_ebx, BLOCK, R3Slot<NS>::BYTES, cs>>>(Sd, s->w_ebx);
-    k_box_source<NS><<<s->n_valid, BLOCK, 0, cs>>>(S, s->w_valid, make_fab(source, sr_lo, sr_hi));
-    if (fo) {
-        Fab F[3];
-        for (int d = 0; d < 3; ++d) {
-            F[d] = fo[d] ? make_fab(fo[d], fo_lo + 3 * d, fo_hi + 3 * d) : Fab{};
-            if (!fo[d]) F[d].p = nullptr;
-        }
-        k_box_store_flux<NS><<<s->n_ebx, BLOCK, 0, cs>>>(S, s->w_ebx, F[0], F[1], F[2], dt);
-    }
-    check_launch("castro_construct_hydro_source_box");
-    return castro_last_error();
-}
-
 // ---------------------------------------------------------------------------
 // castro_construct_hydro_source_box_noalloc: the same fused per-box hydro
 // source, with every scratch array carved out of one file-scope device array
@@ -2883,6 +2767,117 @@ __global__ void k_noalloc_setup(BoxDev B, InstDev I, InstState st, NoallocLists 
     }
 }
 
+// Layout of one box's stage arrays and work lists, shared by both box entry
+// points: records and work lists at the head of the scratch (meta), then the
+// stage arrays (pools) at the offsets BoxDev carries.
+struct BoxPlan {
+    BoxDev B;
+    NoallocLists NLs;
+    int nblocks[NL_COUNT];
+    long long meta_bytes;     // BoxDev, InstDev, InstState records and the work list
+    long long pool_doubles;   // the stage arrays
+};
+
+template <int NS>
+BoxPlan box_plan(const int* lo, const int* hi)
+{
+    BoxPlan P;
+    memset(&P, 0, sizeof P);
+    const int NV = Dims<NS>::NVAR, NQF = QF<NS>::N, NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF;
+    BoxDev& B = P.B;
+    for (int d = 0; d < 3; ++d) { B.lo[d] = lo[d]; B.hi[d] = hi[d]; }
+    B.inst = 0;
+    long long o = 0;
+    auto take = [&](long long n) { long long r = o; o += (n + 31) / 32 * 32; return r; };   // 256-byte aligned
+    B.offU = 0;
+    B.offUb = take(npts_reg(B.lo, B.hi, R_G1, 0) * NV);
+    B.offQ = take(npts_reg(B.lo, B.hi, R_G4, 0) * NQF);
+    B.offDiv = take(npts_reg(B.lo, B.hi, R_G1, 0) * 2);
+    for (int d = 0; d < 3; ++d) {
+        B.offTr[d] = take(npts_reg(B.lo, B.hi, R_TBX, 4 * d) * 2 * NQS);
+        B.offF1[d] = take(npts_reg(B.lo, B.hi, R_TBX, 4 * d) * NTF);
+        B.offFx[d] = take(npts_reg(B.lo, B.hi, R_EBX, d) * (NV + 1));
+    }
+    for (int a = 0; a < 3; ++a)
+        for (int bb = 0; bb < 3; ++bb)
+            if (a != bb) B.offF2[pair_index(a, bb)] = take(npts_reg(B.lo, B.hi, R_TBX, 3 * a + bb) * NTF);
+    P.pool_doubles = o;
+
+    const int kinds[NL_COUNT] = {R_VALID, R_G4, R_G1, R_SEG, R_TBX, R_EBX};
+    const int nsubs[NL_COUNT] = {1, 1, 1, 3, 3, 3};
+    int total = 0;
+    for (int l = 0; l < NL_COUNT; ++l) {
+        P.NLs.nsub[l] = nsubs[l];
+        P.NLs.first[l] = total;
+        int nb = 0;
+        for (int sub = 0; sub < nsubs[l]; ++sub) {
+            int rs = sub;
+            if (l == NL_TBX) rs = 4 * sub;
+            P.NLs.np[l][sub] = npts_reg(B.lo, B.hi, kinds[l], rs);
+            nb += (int)((P.NLs.np[l][sub] + BLOCK - 1) / BLOCK);
+        }
+        P.nblocks[l] = nb;
+        total += nb;
+    }
+    P.NLs.total = total;
+    P.meta_bytes = 1024 + (long long)total * (long long)sizeof(Work);
+    return P;
+}
+
+// The per-box hydro source over a scratch whose first meta_doubles hold the
+// records and work lists and the rest the stage arrays of plan P.
+template <int NS>
+int box_hydro_launch(const BoxPlan& P, double* base, long long meta_doubles, const double* sb, const int* sb_lo,
+                     const int* sb_hi, double* source, const int* sr_lo, const int* sr_hi, double* const* fo,
+                     const int* fo_lo, const int* fo_hi, const double* dx, double dt, const char* who)
+{
+    char* mb = reinterpret_cast<char*>(base);
+    BoxDev* dB = reinterpret_cast<BoxDev*>(mb);
+    InstDev* dI = reinterpret_cast<InstDev*>(mb + 256);
+    InstState* dS = reinterpret_cast<InstState*>(mb + 512);
+    Work* work = reinterpret_cast<Work*>(mb + 1024);
+    double* pools = base + meta_doubles;
+
+    InstDev I;
+    memset(&I, 0, sizeof I);
+    for (int d = 0; d < 3; ++d) { I.dom_lo[d] = P.B.lo[d]; I.dom_hi[d] = P.B.hi[d]; I.dx[d] = dx[d]; }
+    I.bc = CASTRO_BC_OUTFLOW;
+    I.g = 1;
+    InstState st;
+    memset(&st, 0, sizeof st);
+    st.dt = dt;
+    st.stop_time = -1.0;
+
+    const int total = P.NLs.total;
+    const int* nblocks = P.nblocks;
+    const NoallocLists& NLs = P.NLs;
+    cudaStream_t cs = castro::stream();
+    k_noalloc_setup<<<(total + 127) / 128, 128, 0, cs>>>(P.B, I, st, NLs, dB, dI, dS, work);
+    SimDev S;
+    memset(&S, 0, sizeof S);
+    S.boxes = dB; S.dom = dB; S.inst = dI; S.st = dS;   // the box is the instance domain
+    S.Ub = pools; S.Q = pools; S.Div = pools; S.Tr = pools; S.F1 = pools; S.F2 = pools; S.Fx = pools;
+    const Work* W = work;
+    k_box_prim<NS><<<nblocks[NL_G4], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G4], make_fab(sb, sb_lo, sb_hi));
+    k_prep<NS><<<nblocks[NL_G1], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G1]);
+    k_trace<NS><<<nblocks[NL_TRACE], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TRACE]);
+    if (CASTRO_TRACE_SPLIT) k_trace2<NS><<<nblocks[NL_TRACE], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TRACE]);
+    k_riemann1<NS><<<nblocks[NL_TBX], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TBX]);
+    k_riemann2<NS><<<nblocks[NL_TBX], BLOCK, R2Slot<NS>::BYTES, cs>>>(S, W + NLs.first[NL_TBX]);
+    k_riemann3<NS><<<nblocks[NL_EBX], BLOCK, R3Slot<NS>::BYTES, cs>>>(S, W + NLs.first[NL_EBX]);
+    k_box_source<NS><<<nblocks[NL_VALID], BLOCK, 0, cs>>>(S, W + NLs.first[NL_VALID], make_fab(source, sr_lo, sr_hi));
+    if (fo) {
+        Fab F[3];
+        for (int d = 0; d < 3; ++d) {
+            F[d] = fo[d] ? make_fab(fo[d], fo_lo + 3 * d, fo_hi + 3 * d) : Fab{};
+            if (!fo[d]) F[d].p = nullptr;
+        }
+        k_box_store_flux<NS><<<nblocks[NL_EBX], BLOCK, 0, cs>>>(S, W + NLs.first[NL_EBX], F[0], F[1], F[2], dt);
+    }
+    check_launch(who);
+    return castro_last_error();
+}
+
 template <int NS>
 int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const int* sb_lo, const int* sb_hi,
                            double* source, const int* sr_lo, const int* sr_hi, double* const* fo, const int* fo_lo,
@@ -2917,101 +2912,81 @@ int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const
         set_error(CASTRO_ERR_CUDA, "castro_construct_hydro_source_box_noalloc: device set-up failed on this device");
         return CASTRO_ERR_CUDA;
     }
-    double* base = g_noalloc_addr[dev];
-
-    // layout: records and work lists in the first NOALLOC_META_BYTES, then the pools
-    const int NV = Dims<NS>::NVAR, NQF = QF<NS>::N, NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF;
-    BoxDev B;
-    memset(&B, 0, sizeof B);
-    for (int d = 0; d < 3; ++d) { B.lo[d] = lo[d]; B.hi[d] = hi[d]; }
-    B.inst = 0;
-    long long o = 0;
-    auto take = [&](long long n) { long long r = o; o += (n + 31) / 32 * 32; return r; };   // 256-byte aligned
-    B.offU = 0;
-    B.offUb = take(npts_reg(B.lo, B.hi, R_G1, 0) * NV);
-    B.offQ = take(npts_reg(B.lo, B.hi, R_G4, 0) * NQF);
-    B.offDiv = take(npts_reg(B.lo, B.hi, R_G1, 0) * 2);
-    for (int d = 0; d < 3; ++d) {
-        B.offTr[d] = take(npts_reg(B.lo, B.hi, R_TBX, 4 * d) * 2 * NQS);
-        B.offF1[d] = take(npts_reg(B.lo, B.hi, R_TBX, 4 * d) * NTF);
-        B.offFx[d] = take(npts_reg(B.lo, B.hi, R_EBX, d) * (NV + 1));
-    }
-    for (int a = 0; a < 3; ++a)
-        for (int bb = 0; bb < 3; ++bb)
-            if (a != bb) B.offF2[pair_index(a, bb)] = take(npts_reg(B.lo, B.hi, R_TBX, 3 * a + bb) * NTF);
-
-    NoallocLists NLs;
-    memset(&NLs, 0, sizeof NLs);
-    const int kinds[NL_COUNT] = {R_VALID, R_G4, R_G1, R_SEG, R_TBX, R_EBX};
-    const int nsubs[NL_COUNT] = {1, 1, 1, 3, 3, 3};
-    int total = 0;
-    int nblocks[NL_COUNT];
-    for (int l = 0; l < NL_COUNT; ++l) {
-        NLs.nsub[l] = nsubs[l];
-        NLs.first[l] = total;
-        int nb = 0;
-        for (int sub = 0; sub < nsubs[l]; ++sub) {
-            int rs = sub;
-            if (l == NL_TBX) rs = 4 * sub;
-            NLs.np[l][sub] = npts_reg(B.lo, B.hi, kinds[l], rs);
-            nb += (int)((NLs.np[l][sub] + BLOCK - 1) / BLOCK);
-        }
-        nblocks[l] = nb;
-        total += nb;
-    }
-    NLs.total = total;
-    const long long meta = 1024 + (long long)total * (long long)sizeof(Work);
+    const BoxPlan P = box_plan<NS>(lo, hi);
     const long long meta_doubles = NOALLOC_META_BYTES / 8;
-    if (meta > NOALLOC_META_BYTES || meta_doubles + o > NOALLOC_DOUBLES) {
+    if (P.meta_bytes > NOALLOC_META_BYTES || meta_doubles + P.pool_doubles > NOALLOC_DOUBLES) {
         char msg[200];
         snprintf(msg, sizeof msg,
                  "castro_construct_hydro_source_box_noalloc: box needs %lld doubles of scratch, the static array holds %lld "
-                 "(at most 16^3 zones with 13 species, 21^3 with 2)", meta_doubles + o, NOALLOC_DOUBLES);
+                 "(at most 16^3 zones with 13 species, 21^3 with 2)", meta_doubles + P.pool_doubles, NOALLOC_DOUBLES);
         set_error(CASTRO_ERR_ARG, msg);
         return CASTRO_ERR_ARG;
     }
-    char* mb = reinterpret_cast<char*>(base);
-    BoxDev* dB = reinterpret_cast<BoxDev*>(mb);
-    InstDev* dI = reinterpret_cast<InstDev*>(mb + 256);
-    InstState* dS = reinterpret_cast<InstState*>(mb + 512);
-    Work* work = reinterpret_cast<Work*>(mb + 1024);
-    double* pools = base + meta_doubles;
+    return box_hydro_launch<NS>(P, g_noalloc_addr[dev], meta_doubles, sb, sb_lo, sb_hi, source, sr_lo, sr_hi, fo, fo_lo,
+                                fo_hi, dx, dt, "castro_construct_hydro_source_box_noalloc");
+}
 
-    InstDev I;
-    memset(&I, 0, sizeof I);
-    for (int d = 0; d < 3; ++d) { I.dom_lo[d] = lo[d]; I.dom_hi[d] = hi[d]; I.dx[d] = dx[d]; }
-    I.bc = CASTRO_BC_OUTFLOW;
-    I.g = 1;
-    InstState st;
-    memset(&st, 0, sizeof st);
-    st.dt = dt;
-    st.stop_time = -1.0;
+// Library-managed scratch of castro_construct_hydro_source_box: one device
+// array per device, grown to the largest box seen so far (the stage arrays and
+// work lists of any box fit a scratch sized for a larger one, and every call
+// lays its box out afresh), so that a BoxArray of any mix of shapes allocates
+// once per new largest box, not once per shape.
+struct BoxArena {
+    double* p = nullptr;
+    long long cap = 0;   // doubles
+};
+constexpr int BOX_MAX_DEVICES = 64;
+BoxArena g_box_arena[BOX_MAX_DEVICES];
+std::mutex g_box_mu[BOX_MAX_DEVICES];
+std::once_flag g_box_once[BOX_MAX_DEVICES][2];
+int g_box_setup_rc[BOX_MAX_DEVICES][2] = {};
 
-    cudaStream_t cs = castro::stream();
-    k_noalloc_setup<<<(total + 127) / 128, 128, 0, cs>>>(B, I, st, NLs, dB, dI, dS, work);
-    SimDev S;
-    memset(&S, 0, sizeof S);
-    S.boxes = dB; S.dom = dB; S.inst = dI; S.st = dS;   // the box is the instance domain
-    S.Ub = pools; S.Q = pools; S.Div = pools; S.Tr = pools; S.F1 = pools; S.F2 = pools; S.Fx = pools;
-    const Work* W = work;
-    k_box_prim<NS><<<nblocks[NL_G4], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G4], make_fab(sb, sb_lo, sb_hi));
-    k_prep<NS><<<nblocks[NL_G1], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G1]);
-    k_trace<NS><<<nblocks[NL_TRACE], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TRACE]);
-    if (CASTRO_TRACE_SPLIT) k_trace2<NS><<<nblocks[NL_TRACE], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TRACE]);
-    k_riemann1<NS><<<nblocks[NL_TBX], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TBX]);
-    k_riemann2<NS><<<nblocks[NL_TBX], BLOCK, R2Slot<NS>::BYTES, cs>>>(S, W + NLs.first[NL_TBX]);
-    k_riemann3<NS><<<nblocks[NL_EBX], BLOCK, R3Slot<NS>::BYTES, cs>>>(S, W + NLs.first[NL_EBX]);
-    k_box_source<NS><<<nblocks[NL_VALID], BLOCK, 0, cs>>>(S, W + NLs.first[NL_VALID], make_fab(source, sr_lo, sr_hi));
-    if (fo) {
-        Fab F[3];
-        for (int d = 0; d < 3; ++d) {
-            F[d] = fo[d] ? make_fab(fo[d], fo_lo + 3 * d, fo_hi + 3 * d) : Fab{};
-            if (!fo[d]) F[d].p = nullptr;
+template <int NS>
+int box_hydro_impl(const int* lo, const int* hi, const double* sb, const int* sb_lo, const int* sb_hi,
+                   double* source, const int* sr_lo, const int* sr_hi, double* const* fo, const int* fo_lo,
+                   const int* fo_hi, const double* dx, double dt)
+{
+    NvtxRange r("castro_construct_hydro_source_box");
+    for (int d = 0; d < 3; ++d)
+        if (sb_lo[d] > lo[d] - NG || sb_hi[d] < hi[d] + NG) {
+            set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box: Sborder needs 4 ghost zones");
+            return CASTRO_ERR_ARG;
         }
-        k_box_store_flux<NS><<<nblocks[NL_EBX], BLOCK, 0, cs>>>(S, W + NLs.first[NL_EBX], F[0], F[1], F[2], dt);
+    int dev = 0;
+    if (!cuda_ok(cudaGetDevice(&dev), "castro_construct_hydro_source_box: cudaGetDevice")) return CASTRO_ERR_CUDA;
+    if (dev < 0 || dev >= BOX_MAX_DEVICES) {
+        set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box: device index beyond 63");
+        return CASTRO_ERR_ARG;
     }
-    check_launch("castro_construct_hydro_source_box_noalloc");
-    return castro_last_error();
+    const int nsi = NS == 2 ? 0 : 1;
+    std::call_once(g_box_once[dev][nsi], [dev, nsi]() {
+        if (!set_kernel_attributes<NS>()) g_box_setup_rc[dev][nsi] = CASTRO_ERR_CUDA;
+    });
+    if (g_box_setup_rc[dev][nsi] != 0) {
+        set_error(CASTRO_ERR_CUDA, "castro_construct_hydro_source_box: device set-up failed on this device");
+        return CASTRO_ERR_CUDA;
+    }
+    const BoxPlan P = box_plan<NS>(lo, hi);
+    const long long meta_doubles = (P.meta_bytes + 255) / 256 * 32;
+    const long long need = meta_doubles + P.pool_doubles;
+    double* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_box_mu[dev]);
+        BoxArena& A = g_box_arena[dev];
+        if (A.cap < need) {
+            // kernels of earlier calls may still read the old array
+            if (A.p && !cuda_ok(cudaDeviceSynchronize(), "castro_construct_hydro_source_box: synchronize before growing"))
+                return CASTRO_ERR_CUDA;
+            if (A.p) cudaFree(A.p);
+            A.p = nullptr;
+            A.cap = 0;
+            if (!dalloc(&A.p, (size_t)need, "castro_construct_hydro_source_box: scratch")) return CASTRO_ERR_CUDA;
+            A.cap = need;
+        }
+        base = A.p;
+    }
+    return box_hydro_launch<NS>(P, base, meta_doubles, sb, sb_lo, sb_hi, source, sr_lo, sr_hi, fo, fo_lo, fo_hi, dx, dt,
+                                "castro_construct_hydro_source_box");
 }
 
 }  // namespace
