@@ -321,11 +321,6 @@ def _jet_fun(x: Jet, derivs):
     return out
 
 
-def _jet_pow(x: Jet, e):
-    x0 = x.c[0]
-    return _jet_fun(x, [x0 ** e, e * x0 ** (e - 1), e * (e - 1) * x0 ** (e - 2), e * (e - 1) * (e - 2) * x0 ** (e - 3)])
-
-
 def _jet_vars(shape):
     """Jets of the two expansion variables themselves."""
     a = Jet(np.zeros((len(_IDX),) + shape))
@@ -519,3 +514,10 @@ def ensure_table(path: str = DEFAULT_PATH) -> str:
     if not os.path.exists(path):
         write_table(path)
     return path
+
+
+if __name__ == "__main__":
+    import sys
+
+    p = write_table(sys.argv[1] if len(sys.argv) > 1 else DEFAULT_PATH)
+    print(p, _ht.sha256(p))

@@ -7,19 +7,29 @@ reaches), against the oracle on the same file:
 
 * compute_temp (the EOS_RE Newton inversion) on zones spread log-uniformly over
   1e-4..1e6 g/cc and 1e4..1e10 K;
-* 16^3 Sedov runs of 5 steps: the 2-species outflow problem and the reference
-  problem's constants (13 species, periodic).
+* 16^3 runs of 5 steps that stay inside the table: a Sedov blast of 1e24 erg
+  in rho = 1 (a pair plasma at ~5e9 K in the blast, 1e6 K outside) and the
+  reference problem's constants (13 species, rho = 1e4, periodic).
 
-The exact build must match the oracle bit for bit, the production build to the
-tolerances of the other kernel and step tests.  The table is generated on
-first use (data/helm_table_fd.dat) when it is not already there.
+The exact build must match the oracle bit for bit.  On this table the
+reference algorithm is sensitive to rounding where the configurations' table
+is not: the EOS_RE Newton loop stops at |dT/T| < 1e-8, and in degenerate and
+pair-dominated zones (T fixed by e only to ~1e-16 x eta, e(T) steep) a
+last-bit difference can move a zone across that threshold.  The oracle's own
+contracting build (liboracle_fast.so, FMA and the production build's table
+contraction) already departs from its parity build by up to ~4e-11 of a
+component's largest magnitude after five steps, and dt by ~1e-13.  The
+production build must stay within four times that departure, plus 1e-12
+(1e-14 for dt): no further from the reference than another correct rounding
+of the same algorithm.  The table is generated on first use
+(data/helm_table_fd.dat) when it is not already there.
 """
 from __future__ import annotations
 
 import numpy as np
 import pytest
 
-from gpu_harness import RTOL_KERNEL, RTOL_STEP, assert_match, from_dev, to_dev
+from gpu_harness import from_dev, scaled_err, to_dev
 
 pytestmark = pytest.mark.gpu
 
@@ -54,6 +64,15 @@ def _random_state(oracle, A, Z, n=8, seed=7):
     return U, T
 
 
+def _within_rounding_spread(gpu, par, fast, what):
+    """gpu (production build) no further from par (oracle parity build) than
+    four times the oracle's contracting build is, per component, plus 1e-12."""
+    e_gpu = scaled_err(gpu, par)
+    e_cpu = scaled_err(fast, par)
+    bound = 4.0 * e_cpu + 1e-12
+    assert (e_gpu <= bound).all(), f"{what}: production {e_gpu} against the contracting oracle build {e_cpu}"
+
+
 @pytest.mark.parametrize("exact", [True, False], ids=["exact", "fast"])
 def test_compute_temp_on_fd_table(pkg, fd_table, oracle, exact):
     A, Z = pkg.configs.NET2
@@ -61,20 +80,44 @@ def test_compute_temp_on_fd_table(pkg, fd_table, oracle, exact):
     oracle.eos_init(fd_table)
     U, T = _random_state(oracle, A, Z)
     lo, hi = (0, 0, 0), (7, 7, 7)
-    ref = np.asfortranarray(U.copy())
-    oracle.call("compute_temp", lo, hi, ref, lo, hi)
-    assert np.abs(ref[..., 6] / T - 1).max() < 1e-7           # the inversion recovers T
+    ref = {}
+    for variant in ("parity", "fast"):
+        oracle.network_init(A, Z, variant)
+        oracle.eos_init(fd_table, variant)
+        r = np.asfortranarray(U.copy())
+        oracle.lib(variant).oracle_compute_temp(oracle.ivec(lo), oracle.ivec(hi), oracle.ptr(r), oracle.ivec(lo),
+                                                oracle.ivec(hi))
+        ref[variant] = r
+    assert np.abs(ref["parity"][..., 6] / T - 1).max() < 1e-7        # the inversion recovers T
     L = pkg.castro.init(A, Z, fd_table, exact=exact)
     d = to_dev(U)
     pkg.castro.call(L, "compute_temp", lo, hi, d, lo, hi)
     got = from_dev(d)
-    assert_match(got, ref, exact, rtol=RTOL_KERNEL, what="compute_temp on the Fermi-Dirac table")
+    if exact:
+        np.testing.assert_array_equal(got, ref["parity"])
+    else:
+        _within_rounding_spread(got, ref["parity"], ref["fast"], "compute_temp on the Fermi-Dirac table")
+
+
+def _sedov_pairs(c):
+    inst = c.instance(16, c.uniform_boxes(16, 16), bc=1, prob=c.problem(exp_energy=1e24))
+    return dict(name="sedov16_pairs", network=c.NET2, steps=5, instances=[inst])
 
 
 WORKLOADS = {
-    "sedov16_outflow": lambda c: c.sedov64(scale=4),                 # 16^3, 2 species, rho 1, T 1e6
+    "sedov16_pairs": _sedov_pairs,                                      # 2 species, rho 1, blast ~5e9 K
     "reference16_periodic": lambda c: c.reference(scale=8, max_box=64),  # 13 species, rho 1e4, p 1e21
 }
+
+
+def _oracle_run(pkg, oracle, table, cfg, steps, variant):
+    A, Z = cfg["network"]
+    oracle.network_init(A, Z, variant)
+    oracle.eos_init(table, variant)
+    inst = cfg["instances"][0]
+    lev, _ = oracle.level_from_instance(inst, pkg.configs.nvar(cfg), variant=variant)
+    dts = [lev.coarse_step(-1.0) for _ in range(steps)]
+    return oracle.assemble(lev, inst), np.array(dts)
 
 
 @pytest.mark.parametrize("exact", [True, False], ids=["exact", "fast"])
@@ -83,12 +126,8 @@ def test_sedov_on_fd_table(pkg, fd_table, oracle, wl, exact):
     cfg = WORKLOADS[wl](pkg.configs)
     A, Z = cfg["network"]
     steps = 5
-    oracle.network_init(A, Z)
-    oracle.eos_init(fd_table)
     inst = cfg["instances"][0]
-    lev, _ = oracle.level_from_instance(inst, pkg.configs.nvar(cfg))
-    dto = [lev.coarse_step(-1.0) for _ in range(steps)]
-    Go = oracle.assemble(lev, inst)
+    Go, dto = _oracle_run(pkg, oracle, fd_table, cfg, steps, "parity")
     L = pkg.castro.init(A, Z, fd_table, exact=exact)
     sim = pkg.make_sim(L, cfg, pkg.castro.MODE_BATCHED)
     sim.init_data()
@@ -99,9 +138,12 @@ def test_sedov_on_fd_table(pkg, fd_table, oracle, wl, exact):
     G = pkg.castro.assemble(inst, sim.box_states()[0])
     assert sim.eos_failures() == 0
     sim.close()
+    dts = np.array(dts)
     if exact:
         np.testing.assert_array_equal(G, Go)
-        assert dts == dto
+        assert list(dts) == list(dto)
     else:
-        assert_match(G, Go, False, rtol=RTOL_STEP * 10, what=f"{wl} on the Fermi-Dirac table")
-        np.testing.assert_allclose(dts, dto, rtol=1e-14)
+        Gf, dtf = _oracle_run(pkg, oracle, fd_table, cfg, steps, "fast")
+        _within_rounding_spread(G, Go, Gf, f"{wl} on the Fermi-Dirac table")
+        spread = np.abs(dtf / dto - 1).max()
+        assert np.abs(dts / dto - 1).max() <= 4.0 * spread + 1e-14, (dts / dto - 1, spread)
