@@ -217,12 +217,14 @@ int  castro_set_problem(const castro_problem* p);
  * fused: Sborder (grow(box,4), NVAR comps, already cleaned) -> source on the box
  * (accumulated into 'source', which the caller zeroes like hydro_source.setVal(0)).
  * fluxes_out[d] (optional, may be NULL): dt*F*A on the faces of the box
- * (store_flux).  Uses library-managed scratch: one device array per device,
- * grown to the largest box seen so far; a call for a box larger than every
- * earlier one synchronizes the device and allocates (so do not capture such a
+ * (store_flux).  Runs on the stream of castro_set_stream.  Uses library-
+ * managed scratch: one device array per (device, stream), up to 16 streams per
+ * device, grown to the largest box seen on that stream so far; a call for a
+ * box larger than every earlier one on its stream (or the first call of a
+ * 17th stream) synchronizes the device and allocates (so do not capture such a
  * call in a CUDA graph), and every other call allocates nothing, whatever the
- * mix of box shapes. Calls share the array: calls that overlap on the GPU
- * (streams without ordering between them) race. */
+ * mix of box shapes.  Calls on one stream are ordered by it; calls on
+ * different streams may overlap, as an AMReX MFIter loop's do. */
 int castro_construct_hydro_source_box(const int* lo, const int* hi,
                                       const double* sborder, const int* sb_lo, const int* sb_hi,
                                       double* source, const int* sr_lo, const int* sr_hi,

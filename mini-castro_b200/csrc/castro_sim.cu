@@ -1501,8 +1501,18 @@ struct castro_sim {
     double* sb = nullptr;      // Sborder per box (grow 4) for all boxes
     double* src = nullptr;     // hydro_source per box for all boxes
     std::vector<long long> offSb, offSrc;
-    double* scratch = nullptr;
     long long scratch_n = 0;
+    // The per-box host sequence deals its boxes round-robin to PLAIN_STREAMS
+    // streams, as AMReX's MFIter does with its GPU streams (4 by default,
+    // amrex.max_gpu_streams), each with its own construct_hydro_source
+    // scratch; every loop over the boxes starts after the step's stream
+    // (fork) and ends before its next work (join), as an MFIter loop ends with
+    // a synchronisation of its streams.
+    static constexpr int PLAIN_STREAMS = 4;
+    cudaStream_t pst[PLAIN_STREAMS] = {};
+    cudaEvent_t pev[PLAIN_STREAMS] = {};
+    cudaEvent_t pfork = nullptr;
+    double* scratch[PLAIN_STREAMS] = {};
     double* d_dtloc = nullptr; // managed-style reduction target of estdt
     double* d_dtbox = nullptr; // dt per instance for the plain saxpy
     SimDev dev() const
@@ -1705,14 +1715,14 @@ void plain_clean(const int* lo, const int* hi, double* u, const int* ulo, const 
 
 // Castro::construct_hydro_source for one box through the per-routine entry
 // points, Source/Castro_hydro.cpp:31-397
-void plain_hydro_box(castro_sim* s, const IBox& bx, double* sbp, double* srcp, const int* domlo, const int* domhi,
-                     const double* dx, double dt)
+void plain_hydro_box(castro_sim* s, double* scratch, const IBox& bx, double* sbp, double* srcp, const int* domlo,
+                     const int* domhi, const double* dx, double dt)
 {
     const int NV = s->nvar, QV = s->nvar + 1;
     IBox obx = grow(bx, 1, 1, 1), qbx = grow(bx, NG, NG, NG);
     IBox sbx = qbx;
     IBox ebx[3], gebx[3], tbx[3][3];
-    double* cur = s->scratch;
+    double* cur = scratch;
     auto take = [&](const IBox& b, int nc) { double* p = cur; cur += npts(b) * nc; return p; };
     PlainScratch P;
     P.q = take(qbx, QV);
@@ -1740,7 +1750,7 @@ void plain_hydro_box(castro_sim* s, const IBox& bx, double* sbp, double* srcp, c
     P.ql = take(obx, QV);
     P.qr = take(obx, QV);
     P.vol = take(bx, 1);
-    if (cur - s->scratch > s->scratch_n) { set_error(CASTRO_ERR_ARG, "plain path scratch overflow"); return; }
+    if (cur - scratch > s->scratch_n) { set_error(CASTRO_ERR_ARG, "plain path scratch overflow"); return; }
 
     double hdtdx[3], cdtdx[3];
     for (int d = 0; d < 3; ++d) { hdtdx[d] = 0.5 * dt / dx[d]; cdtdx[d] = dt / dx[d] / 3.0; }
@@ -1786,11 +1796,11 @@ void plain_hydro_box(castro_sim* s, const IBox& bx, double* sbp, double* srcp, c
     double area[3] = {dx[1] * dx[2], dx[0] * dx[2], dx[0] * dx[1]};
     for (int d = 0; d < 3; ++d) {
         long long n = npts(gebx[d]);
-        k_fill<<<(unsigned)((n + 255) / 256), 256, 0, s->st>>>(P.area[d], n, area[d]);
+        k_fill<<<(unsigned)((n + 255) / 256), 256, 0, castro::stream()>>>(P.area[d], n, area[d]);
     }
     {
         long long n = npts(bx);
-        k_fill<<<(unsigned)((n + 255) / 256), 256, 0, s->st>>>(P.vol, n, dx[0] * dx[1] * dx[2]);
+        k_fill<<<(unsigned)((n + 255) / 256), 256, 0, castro::stream()>>>(P.vol, n, dx[0] * dx[1] * dx[2]);
     }
     fill_hydro_source(bx.lo, bx.hi, sbp, sbx.lo, sbx.hi, P.q, qbx.lo, qbx.hi, srcp, bx.lo, bx.hi,
                       P.flux[0], gebx[0].lo, gebx[0].hi, P.flux[1], gebx[1].lo, gebx[1].hi,
@@ -1821,6 +1831,24 @@ void plain_step(castro_sim* s)
 {
     SimDev S = s->dev();
     cudaStream_t saved = castro::stream();
+    constexpr int NPS = castro_sim::PLAIN_STREAMS;
+    // an MFIter loop: its boxes dealt round-robin to the pool's streams, which
+    // start after the work issued so far on s->st and end before its next work
+    auto fork = [&]() {
+        cudaEventRecord(s->pfork, s->st);
+        for (int k = 0; k < NPS; ++k) cudaStreamWaitEvent(s->pst[k], s->pfork, 0);
+    };
+    auto join = [&]() {
+        for (int k = 0; k < NPS; ++k) {
+            cudaEventRecord(s->pev[k], s->pst[k]);
+            cudaStreamWaitEvent(s->st, s->pev[k], 0);
+        }
+        castro_set_stream(s->st);
+    };
+    auto box_stream = [&](int i) {
+        castro_set_stream(s->pst[i % NPS]);
+        return s->pst[i % NPS];
+    };
     castro_set_stream(s->st);
     for (int in = 0; in < s->ninst; ++in) {
         InstState hs;
@@ -1828,15 +1856,20 @@ void plain_step(castro_sim* s)
         cudaStreamSynchronize(s->st);
         const castro_instance_desc& D = s->desc[in];
         const double* dx = &s->hdx[3 * in];
+        const std::vector<int>& boxes = s->inst_boxes[in];
+        const int nb = (int)boxes.size();
         // computeInitialDt / computeNewDt, Source/Castro.cpp:175-341
         {
             NvtxRange r("computeNewDt: estTimeStep");
             double big = 1.79769313486231570e+308;
             cudaMemcpyAsync(s->d_dtloc, &big, sizeof big, cudaMemcpyHostToDevice, s->st);
-            for (int b : s->inst_boxes[in]) {
-                const BoxDev& B = s->hboxes[b];
+            fork();
+            for (int i = 0; i < nb; ++i) {      // each box lowers the one minimum (atomically)
+                box_stream(i);
+                const BoxDev& B = s->hboxes[boxes[i]];
                 estdt(B.lo, B.hi, s->U + B.offU, B.lo, B.hi, dx, s->d_dtloc);
             }
+            join();
             double dtl;
             cudaMemcpyAsync(&dtl, s->d_dtloc, sizeof dtl, cudaMemcpyDeviceToHost, s->st);
             cudaStreamSynchronize(s->st);
@@ -1849,55 +1882,62 @@ void plain_step(castro_sim* s)
             hs.dt = dt_0;
         }
         const double dt = hs.dt;
+        cudaMemcpyAsync(s->d_dtbox, &hs.dt, sizeof(double), cudaMemcpyHostToDevice, s->st);
         // Castro::advance, Source/Castro_advance.cpp:32-97
         NvtxRange adv("Castro::advance");
         {
             NvtxRange r("clean_state(S_old)");
-            for (int b : s->inst_boxes[in]) {
-                const BoxDev& B = s->hboxes[b];
+            fork();
+            for (int i = 0; i < nb; ++i) {
+                box_stream(i);
+                const BoxDev& B = s->hboxes[boxes[i]];
                 plain_clean(B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
             }
+            join();
         }
-        NvtxRange fp("FillPatch(Sborder) + clean_state(Sborder)");
-        for (int b : s->inst_boxes[in]) {
-            const BoxDev& B = s->hboxes[b];
-            long long n = npts_reg(B.lo, B.hi, R_G4, 0);
-            k_fill_sborder<NS><<<(unsigned)((n + BLOCK - 1) / BLOCK), BLOCK, 0, s->st>>>(S, b, s->sb + s->offSb[b]);
-        }
-        for (int b : s->inst_boxes[in]) {
-            const BoxDev& B = s->hboxes[b];
-            IBox bx{{B.lo[0], B.lo[1], B.lo[2]}, {B.hi[0], B.hi[1], B.hi[2]}};
-            IBox g = grow(bx, NG, NG, NG);
-            plain_clean(g.lo, g.hi, s->sb + s->offSb[b], g.lo, g.hi);
-        }
-        NvtxRange hs_r("construct_hydro_source");
-        for (int b : s->inst_boxes[in]) {
-            const BoxDev& B = s->hboxes[b];
-            IBox bx{{B.lo[0], B.lo[1], B.lo[2]}, {B.hi[0], B.hi[1], B.hi[2]}};
-            long long n = npts(bx) * s->nvar;
-            cudaMemsetAsync(s->src + s->offSrc[b], 0, n * sizeof(double), s->st);   // hydro_source.setVal(0)
-            if (s->mode == CASTRO_MODE_PLAIN_BOX) {
+        {
+            // every box's ghost zones come from its neighbours' cleaned S_old
+            NvtxRange r("FillPatch(Sborder) + clean_state(Sborder)");
+            fork();
+            for (int i = 0; i < nb; ++i) {
+                const int b = boxes[i];
+                cudaStream_t st = box_stream(i);
+                const BoxDev& B = s->hboxes[b];
+                long long n = npts_reg(B.lo, B.hi, R_G4, 0);
+                k_fill_sborder<NS><<<(unsigned)((n + BLOCK - 1) / BLOCK), BLOCK, 0, st>>>(S, b, s->sb + s->offSb[b]);
+                IBox bx{{B.lo[0], B.lo[1], B.lo[2]}, {B.hi[0], B.hi[1], B.hi[2]}};
                 IBox g = grow(bx, NG, NG, NG);
-                castro_construct_hydro_source_box(bx.lo, bx.hi, s->sb + s->offSb[b], g.lo, g.hi, s->src + s->offSrc[b],
-                                                  bx.lo, bx.hi, nullptr, nullptr, nullptr, D.dom_lo, D.dom_hi, dx, dt);
-            } else {
-                plain_hydro_box(s, bx, s->sb + s->offSb[b], s->src + s->offSrc[b], D.dom_lo, D.dom_hi, dx, dt);
+                plain_clean(g.lo, g.hi, s->sb + s->offSb[b], g.lo, g.hi);
             }
+            join();
         }
-        cudaMemcpyAsync(s->d_dtbox, &hs.dt, sizeof(double), cudaMemcpyHostToDevice, s->st);
-        for (int b : s->inst_boxes[in]) {
-            const BoxDev& B = s->hboxes[b];
-            long long n = npts_reg(B.lo, B.hi, R_VALID, 0) * s->nvar;
-            k_saxpy<<<(unsigned)((n + 255) / 256), 256, 0, s->st>>>(s->U + B.offU, s->src + s->offSrc[b], n, s->d_dtbox);
-        }
-        for (int b : s->inst_boxes[in]) {
-            const BoxDev& B = s->hboxes[b];
-            plain_clean(B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
-        }
-        // post_timestep: clean_state(S_new), Source/Castro.cpp:369
-        for (int b : s->inst_boxes[in]) {
-            const BoxDev& B = s->hboxes[b];
-            plain_clean(B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
+        {
+            // construct_hydro_source, the update (Saxpy) and clean_state(S_new) of
+            // post_timestep (Source/Castro.cpp:369) touch the box's own arrays only
+            NvtxRange r("construct_hydro_source + Saxpy + clean_state(S_new)");
+            fork();
+            for (int i = 0; i < nb; ++i) {
+                const int b = boxes[i];
+                cudaStream_t st = box_stream(i);
+                const BoxDev& B = s->hboxes[b];
+                IBox bx{{B.lo[0], B.lo[1], B.lo[2]}, {B.hi[0], B.hi[1], B.hi[2]}};
+                long long n = npts(bx) * s->nvar;
+                cudaMemsetAsync(s->src + s->offSrc[b], 0, n * sizeof(double), st);   // hydro_source.setVal(0)
+                if (s->mode == CASTRO_MODE_PLAIN_BOX) {
+                    IBox g = grow(bx, NG, NG, NG);
+                    castro_construct_hydro_source_box(bx.lo, bx.hi, s->sb + s->offSb[b], g.lo, g.hi,
+                                                      s->src + s->offSrc[b], bx.lo, bx.hi, nullptr, nullptr, nullptr,
+                                                      D.dom_lo, D.dom_hi, dx, dt);
+                } else {
+                    plain_hydro_box(s, s->scratch[i % NPS], bx, s->sb + s->offSb[b], s->src + s->offSrc[b], D.dom_lo,
+                                    D.dom_hi, dx, dt);
+                }
+                long long nv = npts_reg(B.lo, B.hi, R_VALID, 0) * s->nvar;
+                k_saxpy<<<(unsigned)((nv + 255) / 256), 256, 0, st>>>(s->U + B.offU, s->src + s->offSrc[b], nv, s->d_dtbox);
+                plain_clean(B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
+                plain_clean(B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
+            }
+            join();
         }
         hs.time = hs.time + hs.dt;
         hs.steps += 1;
@@ -2232,7 +2272,13 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
             mx = std::max(mx, plain_scratch_size(bx, NV));
         }
         s->scratch_n = mx;
-        ok = dalloc(&s->sb, nsb, "Sborder") && dalloc(&s->src, nsrc, "hydro_source") && dalloc(&s->scratch, mx, "scratch");
+        ok = dalloc(&s->sb, nsb, "Sborder") && dalloc(&s->src, nsrc, "hydro_source");
+        for (int k = 0; ok && k < castro_sim::PLAIN_STREAMS; ++k) {
+            ok = cuda_ok(cudaStreamCreateWithFlags(&s->pst[k], cudaStreamNonBlocking), "stream create") &&
+                 cuda_ok(cudaEventCreateWithFlags(&s->pev[k], cudaEventDisableTiming), "event create") &&
+                 (mode == CASTRO_MODE_PLAIN_BOX || dalloc(&s->scratch[k], mx, "scratch"));
+        }
+        ok = ok && cuda_ok(cudaEventCreateWithFlags(&s->pfork, cudaEventDisableTiming), "event create");
         // the work list of the valid region is still used by estdt of the sim API
         build_work(s->hboxes, R_VALID, 1, -1, &s->w_valid, &s->n_valid);
     }
@@ -2251,10 +2297,16 @@ void castro_sim_destroy(castro_sim* s)
     if (s->gexec) cudaGraphExecDestroy(s->gexec);
     if (s->graph) cudaGraphDestroy(s->graph);
     void* ptrs[] = {s->dboxes, s->ddom, s->dinst, s->dstate, s->downer, s->U, s->Ub, s->Q, s->Div, s->Tr, s->F1, s->F2, s->Fx,
-                    s->w_valid, s->w_g4, s->w_g1, s->w_trace, s->w_tbx, s->w_ebx, s->w_r2, s->w_r3, s->w_ghost, s->sb, s->src, s->scratch,
+                    s->w_valid, s->w_g4, s->w_g1, s->w_trace, s->w_tbx, s->w_ebx, s->w_r2, s->w_r3, s->w_ghost, s->sb, s->src,
                     s->d_dtloc, s->d_dtbox, s->pctl};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    for (int k = 0; k < castro_sim::PLAIN_STREAMS; ++k) {
+        if (s->scratch[k]) cudaFree(s->scratch[k]);
+        if (s->pst[k]) cudaStreamDestroy(s->pst[k]);
+        if (s->pev[k]) cudaEventDestroy(s->pev[k]);
+    }
+    if (s->pfork) cudaEventDestroy(s->pfork);
     if (s->st) cudaStreamDestroy(s->st);
     if (s->st2) cudaStreamDestroy(s->st2);
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
@@ -2927,16 +2979,24 @@ int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const
 }
 
 // Library-managed scratch of castro_construct_hydro_source_box: one device
-// array per device, grown to the largest box seen so far (the stage arrays and
-// work lists of any box fit a scratch sized for a larger one, and every call
-// lays its box out afresh), so that a BoxArray of any mix of shapes allocates
-// once per new largest box, not once per shape.
+// array per (device, stream) -- calls on different streams may overlap on the
+// GPU, as an AMReX host's MFIter loop does over its GPU streams -- grown to the
+// largest box seen on that stream so far (the stage arrays and work lists of
+// any box fit a scratch sized for a larger one, and every call lays its box out
+// afresh), so that a BoxArray of any mix of shapes allocates once per new
+// largest box, not once per shape.  Up to BOX_ARENAS streams per device; the
+// least recently used one's array is released (after a device synchronisation)
+// for a stream beyond that.
 struct BoxArena {
+    cudaStream_t st = nullptr;
     double* p = nullptr;
     long long cap = 0;   // doubles
+    unsigned long long used = 0;
 };
 constexpr int BOX_MAX_DEVICES = 64;
-BoxArena g_box_arena[BOX_MAX_DEVICES];
+constexpr int BOX_ARENAS = 16;
+BoxArena g_box_arena[BOX_MAX_DEVICES][BOX_ARENAS];
+unsigned long long g_box_clock[BOX_MAX_DEVICES] = {};
 std::mutex g_box_mu[BOX_MAX_DEVICES];
 std::once_flag g_box_once[BOX_MAX_DEVICES][2];
 int g_box_setup_rc[BOX_MAX_DEVICES][2] = {};
@@ -2970,20 +3030,34 @@ int box_hydro_impl(const int* lo, const int* hi, const double* sb, const int* sb
     const long long meta_doubles = (P.meta_bytes + 255) / 256 * 32;
     const long long need = meta_doubles + P.pool_doubles;
     double* base = nullptr;
+    const cudaStream_t cs = castro::stream();
     {
         std::lock_guard<std::mutex> lock(g_box_mu[dev]);
-        BoxArena& A = g_box_arena[dev];
-        if (A.cap < need) {
-            // kernels of earlier calls may still read the old array
-            if (A.p && !cuda_ok(cudaDeviceSynchronize(), "castro_construct_hydro_source_box: synchronize before growing"))
-                return CASTRO_ERR_CUDA;
-            if (A.p) cudaFree(A.p);
-            A.p = nullptr;
-            A.cap = 0;
-            if (!dalloc(&A.p, (size_t)need, "castro_construct_hydro_source_box: scratch")) return CASTRO_ERR_CUDA;
-            A.cap = need;
+        BoxArena* A = nullptr;
+        BoxArena* victim = &g_box_arena[dev][0];
+        for (int c = 0; c < BOX_ARENAS && !A; ++c) {
+            BoxArena& e = g_box_arena[dev][c];
+            if (e.p && e.st == cs) A = &e;
+            else if (!e.p ? victim->p != nullptr : (victim->p && e.used < victim->used)) victim = &e;
         }
-        base = A.p;
+        if (!A) {   // a stream new to this device: a free slot, or the least recently used stream's array
+            A = victim;
+            if (A->p && !cuda_ok(cudaDeviceSynchronize(), "castro_construct_hydro_source_box: synchronize before reuse"))
+                return CASTRO_ERR_CUDA;   // kernels of that stream's calls may still read it
+            A->st = cs;
+        }
+        if (A->cap < need) {
+            // kernels of earlier calls may still read the old array
+            if (A->p && !cuda_ok(cudaDeviceSynchronize(), "castro_construct_hydro_source_box: synchronize before growing"))
+                return CASTRO_ERR_CUDA;
+            if (A->p) cudaFree(A->p);
+            A->p = nullptr;
+            A->cap = 0;
+            if (!dalloc(&A->p, (size_t)need, "castro_construct_hydro_source_box: scratch")) return CASTRO_ERR_CUDA;
+            A->cap = need;
+        }
+        A->used = ++g_box_clock[dev];
+        base = A->p;
     }
     return box_hydro_launch<NS>(P, base, meta_doubles, sb, sb_lo, sb_hi, source, sr_lo, sr_hi, fo, fo_lo, fo_hi, dx, dt,
                                 "castro_construct_hydro_source_box");
