@@ -12,13 +12,13 @@ reaches), against the oracle on the same file:
   reference problem's constants (13 species, rho = 1e4, periodic).
 
 The exact build must match the oracle bit for bit.  On this table the
-reference algorithm is sensitive to rounding where the configurations' table
-is not: the EOS_RE Newton loop stops at |dT/T| < 1e-8, and in degenerate and
-pair-dominated zones (T fixed by e only to ~1e-16 x eta, e(T) steep) a
-last-bit difference can move a zone across that threshold.  The oracle's own
-contracting build (liboracle_fast.so, FMA and the production build's table
-contraction) already departs from its parity build by up to ~4e-11 of a
-component's largest magnitude after five steps, and dt by ~1e-13.  The
+reference algorithm is far more sensitive to rounding than on the
+configurations' table (degenerate zones fix T by e only to ~1e-16 x eta,
+pair-dominated zones have a steep e(T), and the EOS_RE Newton loop stops at
+|dT/T| < 1e-8): the oracle's own contracting build (liboracle_fast.so, FMA and
+the production build's table contraction) already departs from its parity
+build by up to ~4e-11 of a component's largest magnitude after five steps, and
+dt by ~1e-13, where on the analytic table the two agree to ~1e-13.  The
 production build must stay within four times that departure, plus 1e-12
 (1e-14 for dt): no further from the reference than another correct rounding
 of the same algorithm.  The table is generated on first use
