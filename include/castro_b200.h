@@ -79,6 +79,19 @@ int  castro_nspec(void);
  * reference reads the table through ordinary loads.  The L2 set-aside belongs
  * to this process's CUDA context and eos_finalize puts the previous value back. */
 void castro_set_table_l2_window(int on);
+
+/* Option, off by default (no counterpart in the reference): the interface
+ * pressure in the normal momentum flux of compute_flux, flx(im1) = rho u u + p,
+ * as full Castro has it in Cartesian geometry.  The reference's compute_flux
+ * (Source/riemann.F90:306-308) and consup (Source/Castro_hydro_nd.F90:344-441)
+ * put no pressure gradient in the momentum equation, so its blasts expand far
+ * slower than a Sedov-Taylor blast; with the option the same kernels follow the
+ * Sedov-Taylor solution.  Library-wide (every kernel, the adjoint included),
+ * read when a kernel runs; the oracle's oracle_set_momentum_flux_pressure is
+ * its counterpart. */
+void castro_set_momentum_flux_pressure(int on);
+int  castro_momentum_flux_pressure(void);
+
 void eos_init(void);                          /* Castro_F.H:15: reads ./helm_table.dat (or $CASTRO_HELM_TABLE), eos.F90:580-734 */
 void eos_finalize(void);                      /* Castro_F.H:17 */
 int  castro_eos_init_path(const char* path);  /* eos_init with an explicit table path; returns an error code */

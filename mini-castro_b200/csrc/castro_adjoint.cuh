@@ -1197,6 +1197,9 @@ CASTRO_HD void riemann_cgf_adj(const double* ql, const double* qr, double gamcl,
     F_rhob += flxb[im3] * qv2; qv2b += flxb[im3] * F_rho;
     F_rhob += flxb[im2] * qv1; qv1b += flxb[im2] * F_rho;
     F_rhob += flxb[im1] * qu; qub += flxb[im1] * F_rho;
+#ifdef __CUDA_ARCH__
+    if (c_net.mom_flux_p) qpb += flxb[im1];      // flx[im1] = F_rho qu + qp
+#endif
     F_rhob += flxb[URHO];
     qrhob += F_rhob * qu;
     qub += F_rhob * qrho;

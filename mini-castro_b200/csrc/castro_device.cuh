@@ -77,6 +77,11 @@ struct EosTableDev {
 struct NetworkDev {
     int nspec;
     double aion[MAX_SPEC], zion[MAX_SPEC], aion_inv[MAX_SPEC];
+    // 1: the interface pressure in the normal momentum flux, as full Castro has
+    // it in Cartesian geometry (castro_set_momentum_flux_pressure); 0, the
+    // default: the reference's compute_flux, whose momentum flux is rho u u
+    // alone (Source/riemann.F90:306-308)
+    int mom_flux_p;
 };
 
 // Each translation unit holds its own copy; castro_upload_constants_<tu>()
@@ -995,6 +1000,9 @@ CASTRO_HD void riemann_cgf(const double* ql, const double* qr, double gamcl, dou
     double rhoeint = regdnv;
     flx[URHO] = qrho * u_adv;
     flx[im1] = flx[URHO] * qu;
+#ifdef __CUDA_ARCH__
+    if (c_net.mom_flux_p) flx[im1] = flx[im1] + qp;
+#endif
     flx[im2] = flx[URHO] * qv1;
     flx[im3] = flx[URHO] * qv2;
     double rhoetot = rhoeint + 0.5 * qrho * (qu * qu + qv1 * qv1 + qv2 * qv2);

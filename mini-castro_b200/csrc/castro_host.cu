@@ -75,7 +75,9 @@ void default_network()
 {
     static const double a13[13] = {4., 12., 16., 20., 24., 28., 32., 36., 40., 44., 48., 52., 56.};
     static const double z13[13] = {2., 6., 8., 10., 12., 14., 16., 18., 20., 22., 24., 26., 28.};
+    const int mfp = g_net.mom_flux_p;   // an option, not part of the network
     memset(&g_net, 0, sizeof g_net);
+    g_net.mom_flux_p = mfp;
     g_net.nspec = 13;
     for (int n = 0; n < 13; ++n) {
         g_net.aion[n] = a13[n];
@@ -178,7 +180,9 @@ int castro_network_init(int ns, const double* aion, const double* zion)
         set_error(CASTRO_ERR_NSPEC, "castro_network_init: nspec must be 2 or 13");
         return CASTRO_ERR_NSPEC;
     }
+    const int mfp = g_net.mom_flux_p;   // an option, not part of the network
     memset(&g_net, 0, sizeof g_net);
+    g_net.mom_flux_p = mfp;
     g_net.nspec = ns;
     for (int n = 0; n < ns; ++n) {
         g_net.aion[n] = aion[n];
@@ -193,6 +197,14 @@ int castro_network_init(int ns, const double* aion, const double* zion)
 int castro_nspec(void) { return nspec(); }
 
 void castro_set_table_l2_window(int on) { g_l2_window = on != 0; }
+
+void castro_set_momentum_flux_pressure(int on)
+{
+    g_net.mom_flux_p = on != 0;
+    if (g_table) upload_all();
+}
+
+int castro_momentum_flux_pressure(void) { return g_net.mom_flux_p; }
 
 int castro_eos_init_path(const char* path)
 {

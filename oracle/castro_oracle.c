@@ -21,6 +21,10 @@
 #include <float.h>
 #ifdef _OPENMP
 #include <omp.h>
+
+/* the interface pressure in the normal momentum flux: off, as in the reference
+ * (see oracle_set_momentum_flux_pressure) */
+static int g_mom_flux_p = 0;   /* see oracle_set_momentum_flux_pressure */
 #endif
 
 /* ------------------------------------------------------------------------ */
@@ -1334,6 +1338,7 @@ void oracle_compute_flux(const int* lo, const int* hi,
                 double rhoeint = AT(qint, i, j, k, QREINT);
                 AT(flx, i, j, k, URHO) = AT(qint, i, j, k, QRHO) * u_adv;
                 AT(flx, i, j, k, im1) = AT(flx, i, j, k, URHO) * AT(qint, i, j, k, iu);
+                if (g_mom_flux_p) AT(flx, i, j, k, im1) = AT(flx, i, j, k, im1) + AT(qint, i, j, k, QPRES);
                 AT(flx, i, j, k, im2) = AT(flx, i, j, k, URHO) * AT(qint, i, j, k, iv1);
                 AT(flx, i, j, k, im3) = AT(flx, i, j, k, URHO) * AT(qint, i, j, k, iv2);
                 double qu = AT(qint, i, j, k, iu), q1 = AT(qint, i, j, k, iv1), q2 = AT(qint, i, j, k, iv2);
@@ -1561,6 +1566,13 @@ static oracle_prob_t prob = {
 };
 
 void oracle_set_problem(const oracle_prob_t* p) { prob = *p; }
+
+/* Option (off by default, as in the reference): the interface pressure in the
+ * normal momentum flux, as full Castro has it for Cartesian geometry.  The
+ * reference's compute_flux omits it (Source/riemann.F90:306-308), and nothing
+ * else adds a pressure gradient to the momentum (consup adds only p div u to
+ * rho e, Source/Castro_hydro_nd.F90:425-434). */
+void oracle_set_momentum_flux_pressure(int on) { g_mom_flux_p = on; }
 
 void oracle_initdata(const int* lo, const int* hi, double* up, const int* u_lo, const int* u_hi,
                      const double* dx, const double* problo, const double* probhi)

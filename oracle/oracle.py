@@ -83,6 +83,7 @@ def _bind(L):
     L.oracle_eos_init.argtypes = [C.c_char_p]
     L.oracle_eos.argtypes = [C.c_int, C.POINTER(EosT)]
     L.oracle_set_problem.argtypes = [C.POINTER(ProbT)]
+    L.oracle_set_momentum_flux_pressure.argtypes = [C.c_int]
     L.oracle_level_create.restype = C.c_void_p
     L.oracle_level_create.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _dp, _dp, C.c_int]
     L.oracle_level_destroy.argtypes = [C.c_void_p]
@@ -124,6 +125,11 @@ def network_init(aion, zion, variant: str = "parity"):
     a = np.ascontiguousarray(aion, dtype=np.float64)
     z = np.ascontiguousarray(zion, dtype=np.float64)
     assert lib(variant).oracle_network_init(len(a), ptr(a), ptr(z)) == 0
+
+
+def set_momentum_flux_pressure(on: bool, variant: str = "parity"):
+    """The interface pressure in the normal momentum flux (off, as in the reference)."""
+    lib(variant).oracle_set_momentum_flux_pressure(1 if on else 0)
 
 
 def eos_init(path: str, variant: str = "parity"):

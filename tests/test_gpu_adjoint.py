@@ -298,6 +298,18 @@ def test_compute_flux_adj(env, d):
                   {"f": shape(OBX, NV), "g": shape(OBX, NGDNV)}, masks={"f": [UTEMP]}, seed=10 + d)
 
 
+@pytest.mark.parametrize("d", [0, 2])
+def test_compute_flux_adj_momentum_pressure(env, d):
+    """The same probe with the interface pressure in the normal momentum flux
+    (castro_set_momentum_flux_pressure; the reference has none)."""
+    L = env["L"]
+    L.castro_set_momentum_flux_pressure(1)
+    try:
+        test_compute_flux_adj(env, d)
+    finally:
+        L.castro_set_momentum_flux_pressure(0)
+
+
 def _riemann1(env, d):
     K, L = env["K"], env["L"]
     b = TBX[(d, d)]
