@@ -104,3 +104,59 @@ def test_sedov_taylor_gpu(pkg, table):
     assert sel.any() and np.all(np.abs(ratios[sel] - 1.0) < 0.03), list(zip(radii, ratios))
     ref = _blast(pkg, table, 64, False, max_steps=300)
     assert ref[-1][1] / ref[-1][2] < 0.6, ref
+
+
+def _sod_gpu(pkg, table, exact, on):
+    import test_sod_known_answer as S
+
+    C = pkg.configs
+    inst = dict(S.sod_domain(), problem=C.problem(r_init=0.1), n=S.NX, stop_time=S.T_END)
+    cfg = dict(name="sod", network=C.NET2, steps=0, instances=[inst])
+    L = pkg.castro.init(*C.NET2, table, exact=exact)
+    L.castro_set_momentum_flux_pressure(1 if on else 0)
+    try:
+        sim = pkg.make_sim(L, cfg, pkg.castro.MODE_BATCHED)
+        sim.upload(S.sod_state(9).ravel(order="F"))
+        dts = []
+        for _ in range(2000):
+            if sim.time(0) >= S.T_END * (1 - 1e-12):
+                break
+            sim.step(1)
+            dts.append(sim.dt(0))
+        G = pkg.castro.assemble(inst, sim.box_states()[0])
+        t = sim.time(0)
+        sim.close()
+    finally:
+        L.castro_set_momentum_flux_pressure(0)
+    return t, G, dts
+
+
+def test_sod_gpu(pkg, table, oracle):
+    """The Sod shock tube of test_sod_known_answer.py on the GPU, uploaded as the
+    initial state: the production build with the option to 2% of the exact
+    solution in relative L1, and the exact build with the option bit for bit
+    against the oracle (parity build) with its option."""
+    import test_sod_known_answer as S
+
+    t, G, _ = _sod_gpu(pkg, table, False, True)
+    assert abs(t / S.T_END - 1) < 1e-12
+    err = S.l1_error(G[:, :, :, 0].mean(axis=(1, 2)), t)
+    print("GPU Sod L1(rho):", err)
+    assert err < 0.02
+    # exact build against the parity oracle, both with the option
+    t, G, dts = _sod_gpu(pkg, table, True, True)
+    A, Z = pkg.configs.NET2
+    oracle.network_init(A, Z)
+    oracle.eos_init(table)
+    oracle.set_momentum_flux_pressure(True)
+    try:
+        D = S.sod_domain()
+        lev = oracle.Level(D["boxes"], D["dom_lo"], D["dom_hi"], D["problo"], D["probhi"], D["bc"], 9)
+        lev.state(0)[...] = S.sod_state(9)
+        dto = []
+        while lev.time < S.T_END * (1 - 1e-12):
+            dto.append(lev.coarse_step(S.T_END))
+        np.testing.assert_array_equal(G, lev.state(0))
+        assert dts == dto
+    finally:
+        oracle.set_momentum_flux_pressure(False)
