@@ -9,6 +9,9 @@
 //                              configuration: rho, T, E, r = 4 zones, X = 0.5/0.5)
 //   nspec=13|2, bc=periodic|outflow, mode=batched|plain, table=<helm_table.dat>
 //   rho, T, E (sedov problem constants)
+//   momentum_flux_pressure=0|1 (1: the interface pressure in the normal
+//                              momentum flux, as full Castro has it; the
+//                              reference, and the default, have none)
 // and prints the reference's progress lines and figure of merit.
 #include <stdio.h>
 #include <stdlib.h>
@@ -45,7 +48,8 @@ void usage()
     printf("stop_time (0.01): The stopping time of the simulation, in seconds.\n");
     printf("max_step (10000000): The maximum number of timesteps to take.\n\n");
     printf("B200 additions: problem=reference|sedov nspec=13|2 bc=periodic|outflow mode=batched|plain table=<path>\n"
-           "               plot_file=<dir> (AMReX plotfile of the final state)\n\n");
+           "               plot_file=<dir> (AMReX plotfile of the final state)\n"
+           "               momentum_flux_pressure=0|1 (1: pressure in the momentum flux, as full Castro)\n\n");
 }
 
 }  // namespace
@@ -87,6 +91,7 @@ extern "C" int castro_main(int argc, char** argv)
         const double a[2] = {4.0, 16.0}, z[2] = {2.0, 8.0};
         castro_network_init(2, a, z);
     }
+    castro_set_momentum_flux_pressure((int)geti("momentum_flux_pressure", 0));
     std::string table = gets("table", getenv("CASTRO_HELM_TABLE") ? getenv("CASTRO_HELM_TABLE") : "helm_table.dat");
     if (castro_eos_init_path(table.c_str()) != CASTRO_OK) {
         fprintf(stderr, "eos_init: %s\n", castro_error_string());
