@@ -112,6 +112,11 @@ void normalize_species(const int* lo, const int* hi, double* state, const int* s
 void reset_internal_e(const int* lo, const int* hi, double* state, const int* s_lo, const int* s_hi);
 /* Castro_F.H:37-39 -> Castro_nd.F90:253 */
 void compute_temp(const int* lo, const int* hi, double* state, const int* s_lo, const int* s_hi);
+/* Coarse entry point for Castro::clean_state on one box (Source/Castro.cpp:563-591):
+ * enforce_minimum_density, normalize_species, reset_internal_e and compute_temp
+ * in one launch instead of four.  Each of the four is pointwise, so applying
+ * them zone by zone gives the four calls' results bit for bit. */
+void castro_clean_state(const int* lo, const int* hi, double* state, const int* s_lo, const int* s_hi);
 /* Castro_F.H:41-45 -> timestep.F90:12; dt is a device/managed double lowered atomically */
 void estdt(const int* lo, const int* hi, const double* state, const int* s_lo, const int* s_hi,
            const double* dx, double* dt);

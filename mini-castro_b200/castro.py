@@ -65,7 +65,7 @@ ABI_SYMBOLS = [
     "castro_last_error", "castro_clear_error", "castro_error_string", "castro_version", "castro_set_stream",
     "castro_get_stream", "castro_exact_build", "network_init", "network_finalize", "castro_network_init",
     "castro_nspec", "eos_init", "eos_finalize", "castro_eos_init_path", "ctoprim", "enforce_minimum_density",
-    "normalize_species", "reset_internal_e", "compute_temp", "estdt", "store_flux", "fill_hydro_source",
+    "normalize_species", "reset_internal_e", "compute_temp", "castro_clean_state", "estdt", "store_flux", "fill_hydro_source",
     "normalize_species_fluxes", "apply_av", "trans1", "trans2", "compute_flux", "divu", "trace_ppm", "initdata",
     "denerror", "calculate_blast_radius", "castro_problem_defaults", "castro_set_problem",
     "castro_construct_hydro_source_box", "castro_sim_create", "castro_sim_destroy", "castro_sim_nbox",

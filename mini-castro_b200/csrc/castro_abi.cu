@@ -88,7 +88,8 @@ void clean_impl(const char* what, const int* lo, const int* hi, Fab U)
         if (WHICH == 0) enforce_minimum_density_pt<NS>(u);
         else if (WHICH == 1) normalize_species_pt<NS>(u);
         else if (WHICH == 2) reset_internal_e_pt<NS>(u);
-        else compute_temp_pt<NS>(u);
+        else if (WHICH == 3) compute_temp_pt<NS>(u);
+        else clean_state_pt<NS>(u);      // the four in a row: each is pointwise
 #pragma unroll
         for (int n = 0; n < NVAR; ++n) U(i, j, k, n) = u[n];
     });
@@ -459,6 +460,7 @@ template <int NS> void emd_impl(const int* lo, const int* hi, Fab U) { clean_imp
 template <int NS> void nsp_impl(const int* lo, const int* hi, Fab U) { clean_impl<NS, 1>("normalize_species", lo, hi, U); }
 template <int NS> void rie_impl(const int* lo, const int* hi, Fab U) { clean_impl<NS, 2>("reset_internal_e", lo, hi, U); }
 template <int NS> void ctp_impl(const int* lo, const int* hi, Fab U) { clean_impl<NS, 3>("compute_temp", lo, hi, U); }
+template <int NS> void cls_impl(const int* lo, const int* hi, Fab U) { clean_impl<NS, 4>("castro_clean_state", lo, hi, U); }
 
 template <int NS>
 void blast_impl(const int* lo, const int* hi, Fab U, const double* dx, const double* problo, const double* probhi,
@@ -526,6 +528,11 @@ void reset_internal_e(const int* lo, const int* hi, double* s, const int* s_lo, 
 void compute_temp(const int* lo, const int* hi, double* s, const int* s_lo, const int* s_hi)
 {
     CASTRO_DISPATCH_NS(ctp_impl, lo, hi, make_fab(s, s_lo, s_hi));
+}
+
+void castro_clean_state(const int* lo, const int* hi, double* s, const int* s_lo, const int* s_hi)
+{
+    CASTRO_DISPATCH_NS(cls_impl, lo, hi, make_fab(s, s_lo, s_hi));
 }
 
 void estdt(const int* lo, const int* hi, const double* s, const int* s_lo, const int* s_hi, const double* dx, double* dt)

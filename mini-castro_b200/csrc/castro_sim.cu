@@ -1704,9 +1704,14 @@ IBox grow(IBox b, int gx, int gy, int gz)
 }
 long long npts(const IBox& b) { return (long long)(b.hi[0] - b.lo[0] + 1) * (b.hi[1] - b.lo[1] + 1) * (b.hi[2] - b.lo[2] + 1); }
 
-void plain_clean(const int* lo, const int* hi, double* u, const int* ulo, const int* uhi)
+// Castro::clean_state, Source/Castro.cpp:563-591: the reference's four calls
+// (the per-routine path), or the coarse castro_clean_state (the drop-in path)
+void plain_clean(const castro_sim* s, const int* lo, const int* hi, double* u, const int* ulo, const int* uhi)
 {
-    // Castro::clean_state, Source/Castro.cpp:563-591
+    if (s->mode == CASTRO_MODE_PLAIN_BOX) {
+        castro_clean_state(lo, hi, u, ulo, uhi);
+        return;
+    }
     enforce_minimum_density(lo, hi, u, ulo, uhi);
     normalize_species(lo, hi, u, ulo, uhi);
     reset_internal_e(lo, hi, u, ulo, uhi);
@@ -1891,7 +1896,7 @@ void plain_step(castro_sim* s)
             for (int i = 0; i < nb; ++i) {
                 box_stream(i);
                 const BoxDev& B = s->hboxes[boxes[i]];
-                plain_clean(B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
+                plain_clean(s, B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
             }
             join();
         }
@@ -1907,7 +1912,7 @@ void plain_step(castro_sim* s)
                 k_fill_sborder<NS><<<(unsigned)((n + BLOCK - 1) / BLOCK), BLOCK, 0, st>>>(S, b, s->sb + s->offSb[b]);
                 IBox bx{{B.lo[0], B.lo[1], B.lo[2]}, {B.hi[0], B.hi[1], B.hi[2]}};
                 IBox g = grow(bx, NG, NG, NG);
-                plain_clean(g.lo, g.hi, s->sb + s->offSb[b], g.lo, g.hi);
+                plain_clean(s, g.lo, g.hi, s->sb + s->offSb[b], g.lo, g.hi);
             }
             join();
         }
@@ -1934,8 +1939,8 @@ void plain_step(castro_sim* s)
                 }
                 long long nv = npts_reg(B.lo, B.hi, R_VALID, 0) * s->nvar;
                 k_saxpy<<<(unsigned)((nv + 255) / 256), 256, 0, st>>>(s->U + B.offU, s->src + s->offSrc[b], nv, s->d_dtbox);
-                plain_clean(B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
-                plain_clean(B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
+                plain_clean(s, B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
+                plain_clean(s, B.lo, B.hi, s->U + B.offU, B.lo, B.hi);
             }
             join();
         }

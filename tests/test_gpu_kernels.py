@@ -202,6 +202,15 @@ def test_clean_state_routines(env):
         assert_match(from_dev(t), C.rec[name + "_out"], exact, what=name)
 
 
+def test_castro_clean_state(env):
+    """The coarse castro_clean_state (the four routines in one launch) against the
+    oracle's four routines applied in turn, from the raw Sborder."""
+    C, L, exact, K = env
+    t = to_dev(C.rec["enforce_minimum_density_in"])
+    K.call(L, "castro_clean_state", C.sb_lo, C.sb_hi, t, C.sb_lo, C.sb_hi)
+    assert_match(from_dev(t), C.rec["compute_temp_out"], exact, what="castro_clean_state")
+
+
 def test_ctoprim(env):
     C, L, exact, K = env
     q, qa = nan_dev(C.qlo, C.qhi, C.qv), nan_dev(C.qlo, C.qhi, 4)
