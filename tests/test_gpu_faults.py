@@ -151,14 +151,17 @@ def test_checkpoint_restart_bitwise(pkg, table, tmp_path, exact):
     c.close()
 
 
-def test_batched_step_deterministic(pkg, table):
+@pytest.mark.parametrize("mode", [1, 2, 0, 3], ids=["batched", "plain_box", "plain", "persistent"])
+def test_step_deterministic(pkg, table, mode):
     """Two runs from the same initial state agree bit for bit (production build):
-    no race or order-dependent reduction in the step."""
+    no race or order-dependent reduction in the step -- in the batched graph, in
+    the per-box host sequences whose boxes run concurrently on four streams
+    (per-stream scratch), and in the one-launch step's work queues."""
     L = _lib(pkg, table)
     cfg = pkg.configs.sedov128_pert(scale=4, max_box=8)   # 32^3 in 64 boxes
     out = []
     for _ in range(2):
-        sim = pkg.make_sim(L, cfg, pkg.castro.MODE_BATCHED)
+        sim = pkg.make_sim(L, cfg, mode)
         sim.init_data()
         sim.step(5)
         out.append((sim.download(), sim.dt(0)))
