@@ -86,9 +86,10 @@ void castro_set_table_l2_window(int on);
  * (Source/riemann.F90:306-308) and consup (Source/Castro_hydro_nd.F90:344-441)
  * put no pressure gradient in the momentum equation, so its blasts expand far
  * slower than a Sedov-Taylor blast; with the option the same kernels follow the
- * Sedov-Taylor solution.  Library-wide (every kernel, the adjoint included),
- * read when a kernel runs; the oracle's oracle_set_momentum_flux_pressure is
- * its counterpart. */
+ * Sedov-Taylor solution.  Library-wide (every kernel, the adjoint included);
+ * the call waits for the kernels already queued on the device, which run with
+ * the old setting.  The oracle's oracle_set_momentum_flux_pressure is its
+ * counterpart. */
 void castro_set_momentum_flux_pressure(int on);
 int  castro_momentum_flux_pressure(void);
 

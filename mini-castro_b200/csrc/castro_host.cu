@@ -201,7 +201,11 @@ void castro_set_table_l2_window(int on) { g_l2_window = on != 0; }
 void castro_set_momentum_flux_pressure(int on)
 {
     g_net.mom_flux_p = on != 0;
-    if (g_table) upload_all();
+    if (!g_table) return;   // uploaded with the table
+    // kernels already queued on any stream read the constants when they run:
+    // let them finish under the old value first
+    cudaDeviceSynchronize();
+    upload_all();
 }
 
 int castro_momentum_flux_pressure(void) { return g_net.mom_flux_p; }
