@@ -7,7 +7,8 @@
 // plus keys for what the reference hard-codes:
 //   problem=reference|sedov   (Source/Prob.F90 constants, or the unit-cube
 //                              configuration: rho, T, E, r = 4 zones, X = 0.5/0.5)
-//   nspec=13|2, bc=periodic|outflow, mode=batched|plain, table=<helm_table.dat>
+//   nspec=13|2, bc=periodic|outflow, mode=batched|persistent|plain|plain_box,
+//   table=<helm_table.dat>
 //   rho, T, E (sedov problem constants)
 //   momentum_flux_pressure=0|1 (1: the interface pressure in the normal
 //                              momentum flux, as full Castro has it; the
@@ -47,7 +48,8 @@ void usage()
     printf("max_level (0): The maximum adaptive mesh refinement level (zero-indexed).\n");
     printf("stop_time (0.01): The stopping time of the simulation, in seconds.\n");
     printf("max_step (10000000): The maximum number of timesteps to take.\n\n");
-    printf("B200 additions: problem=reference|sedov nspec=13|2 bc=periodic|outflow mode=batched|plain table=<path>\n"
+    printf("B200 additions: problem=reference|sedov nspec=13|2 bc=periodic|outflow\n"
+           "               mode=batched|persistent|plain|plain_box table=<path>\n"
            "               plot_file=<dir> (AMReX plotfile of the final state)\n"
            "               momentum_flux_pressure=0|1 (1: pressure in the momentum flux, as full Castro)\n\n");
 }
@@ -79,7 +81,15 @@ extern "C" int castro_main(int argc, char** argv)
     std::string problem = gets("problem", "reference");
     int nspec = (int)geti("nspec", problem == "reference" ? 13 : 2);
     int bc = gets("bc", problem == "reference" ? "periodic" : "outflow") == "periodic" ? CASTRO_BC_PERIODIC : CASTRO_BC_OUTFLOW;
-    int mode = gets("mode", "batched") == "plain" ? CASTRO_MODE_PLAIN : CASTRO_MODE_BATCHED;
+    const std::string mode_s = gets("mode", "batched");
+    int mode = CASTRO_MODE_BATCHED;
+    if (mode_s == "plain") mode = CASTRO_MODE_PLAIN;
+    else if (mode_s == "plain_box") mode = CASTRO_MODE_PLAIN_BOX;
+    else if (mode_s == "persistent") mode = CASTRO_MODE_PERSISTENT;
+    else if (mode_s != "batched") {
+        fprintf(stderr, "mode must be batched, persistent, plain or plain_box\n");
+        return 1;
+    }
     if (max_level != 0) { fprintf(stderr, "max_level > 0 is not supported (single-level advance only)\n"); return 1; }
 
     printf("Initializing AMR driver using the following runtime parameters:\n\n");

@@ -13,11 +13,12 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def test_miniapp_report_and_blast_radius(pkg, table, oracle):
+@pytest.mark.parametrize("mode", ["batched", "persistent", "plain", "plain_box"])
+def test_miniapp_report_and_blast_radius(pkg, table, oracle, mode):
     exe = os.path.join(os.path.dirname(pkg.castro.lib_path(False)), "castro_b200.ex")
     assert os.path.exists(exe), exe
     out = subprocess.run([exe, "n_cell=16", "max_box_size=8", "max_step=4", "diagnostic_interval=2",
-                          f"table={table}"], capture_output=True, text=True, timeout=300)
+                          f"table={table}", f"mode={mode}"], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stderr
     txt = out.stdout
     assert "Starting mini-Castro..." in txt
