@@ -136,8 +136,8 @@ class GpuKernels:
         return self.torch.zeros(npts(lo, hi) * self.nvar, dtype=self.torch.float64, device="cuda")
 
     def clean(self, a, alo, ahi, lo, hi):
-        for name in self.CLEAN:
-            castro.call(self.L, name, list(lo), list(hi), a, list(alo), list(ahi))
+        # Castro::clean_state: the four routines of CLEAN in one launch (castro_clean_state)
+        castro.call(self.L, "castro_clean_state", list(lo), list(hi), a, list(alo), list(ahi))
 
     def estdt(self, u, lo, hi, dx) -> float:
         self.dtbuf.fill_(1.79769313486231570e308)
