@@ -125,6 +125,28 @@ void estdt(const int* lo, const int* hi, const double* state, const int* s_lo, c
  * AMReX call, not a Castro_F.H routine): u[m] = u[m] + dt * src[m] over n
  * doubles of device memory, on the library stream */
 void castro_saxpy(double* u, const double* src, long long n, double dt);
+
+/* The AMR pieces (no counterpart in the reference's own code, which hands them to
+ * AMReX): Castro::reflux's flux register (Source/Castro.cpp:451-483) and
+ * Castro::avgDown (:486-504).  Fluxes are store_flux's dt * F * A on face boxes.
+ * For the coarse faces [flo, fhi] (coarse indices, normal direction dir) on one
+ * side of a fine patch refined by `ratio`:
+ *   crse_init: reg = -crse_flux;
+ *   fine_add:  reg += the sum of the ratio^2 fine face fluxes over each coarse face
+ *              (call once per fine substep);
+ *   reflux:    the coarse zone on `side` of each face (0: below, the patch above;
+ *              1: above) gets -reg / volume (side 0) or +reg / volume (side 1).
+ * average_down: each coarse zone of [clo, chi] = the mean of its ratio^3 fine zones. */
+void castro_flux_register_crse_init(const int* flo, const int* fhi, double* reg, const int* r_lo, const int* r_hi,
+                                    const double* crse_flux, const int* c_lo, const int* c_hi, int ncomp);
+void castro_flux_register_fine_add(const int* flo, const int* fhi, int dir, double* reg, const int* r_lo,
+                                   const int* r_hi, const double* fine_flux, const int* f_lo, const int* f_hi,
+                                   int ncomp, int ratio);
+void castro_flux_register_reflux(const int* flo, const int* fhi, int dir, int side, double* state, const int* s_lo,
+                                 const int* s_hi, const double* reg, const int* r_lo, const int* r_hi, int ncomp,
+                                 double volume);
+void castro_average_down(const int* clo, const int* chi, double* crse, const int* c_lo, const int* c_hi,
+                         const double* fine, const int* f_lo, const int* f_hi, int ncomp, int ratio);
 /* Castro_F.H:47-53 -> Castro_hydro_nd.F90:301 */
 void store_flux(const int* lo, const int* hi,
                 double* flux_out, const int* fo_lo, const int* fo_hi,

@@ -82,6 +82,8 @@ ABI_SYMBOLS = [
     "castro_adj_time_ms", "castro_adj_device_bytes", "castro_sim_write_plotfile",
     "castro_sim_write_checkpoint", "castro_sim_read_checkpoint", "castro_set_table_l2_window",
     "castro_set_momentum_flux_pressure", "castro_momentum_flux_pressure",
+    "castro_flux_register_crse_init", "castro_flux_register_fine_add", "castro_flux_register_reflux",
+    "castro_average_down",
     "castro_sim_set_wait_limit", "castro_saxpy", "castro_adj_create_window",
 ]
 

@@ -548,6 +548,83 @@ __global__ void k_saxpy_host_dt(double* u, const double* src, long long n, doubl
     if (m < n) u[m] = u[m] + dt * src[m];
 }
 
+// ---------------------------------------------------------------------------
+// The AMR pieces of Castro.cpp (Castro::reflux, Source/Castro.cpp:451-483;
+// Castro::avgDown, :486-504), which the reference delegates to AMReX's
+// FluxRegister and amrex::average_down: the register of one side of a fine
+// patch on the coarse faces it covers, and the conservative average of fine
+// zones onto the coarse zones beneath them.  Fluxes are in store_flux's form,
+// dt * F * A, on face boxes (node-centred in the normal direction).
+// ---------------------------------------------------------------------------
+void castro_flux_register_crse_init(const int* flo, const int* fhi, double* reg, const int* r_lo, const int* r_hi,
+                                    const double* crse_flux, const int* c_lo, const int* c_hi, int ncomp)
+{
+    Fab R = make_fab(reg, r_lo, r_hi), F = make_fab(crse_flux, c_lo, c_hi);
+    launch_box("castro_flux_register_crse_init", flo, fhi, [=] __device__(int i, int j, int k) {
+        for (int n = 0; n < ncomp; ++n) R(i, j, k, n) = -F(i, j, k, n);
+    });
+}
+
+void castro_flux_register_fine_add(const int* flo, const int* fhi, int dir, double* reg, const int* r_lo,
+                                   const int* r_hi, const double* fine_flux, const int* f_lo, const int* f_hi,
+                                   int ncomp, int ratio)
+{
+    if (dir < 0 || dir > 2 || ratio < 1) {
+        set_error(CASTRO_ERR_ARG, "castro_flux_register_fine_add: dir 0..2, ratio >= 1");
+        return;
+    }
+    Fab R = make_fab(reg, r_lo, r_hi), F = make_fab(fine_flux, f_lo, f_hi);
+    launch_box("castro_flux_register_fine_add", flo, fhi, [=] __device__(int i, int j, int k) {
+        // the ratio^2 fine faces on coarse face (i,j,k): the same plane, ratio x ratio across it
+        const int fi = i * ratio, fj = j * ratio, fk = k * ratio;
+        const int na = dir == 0 ? 1 : ratio, nb = dir == 1 ? 1 : ratio, nc = dir == 2 ? 1 : ratio;
+        for (int n = 0; n < ncomp; ++n) {
+            double s = 0.0;
+            for (int c = 0; c < nc; ++c)
+                for (int b = 0; b < nb; ++b)
+                    for (int a = 0; a < na; ++a) s = s + F(fi + a, fj + b, fk + c, n);
+            R(i, j, k, n) = R(i, j, k, n) + s;
+        }
+    });
+}
+
+void castro_flux_register_reflux(const int* flo, const int* fhi, int dir, int side, double* state, const int* s_lo,
+                                 const int* s_hi, const double* reg, const int* r_lo, const int* r_hi, int ncomp,
+                                 double volume)
+{
+    if (dir < 0 || dir > 2 || (side != 0 && side != 1) || !(volume > 0.0)) {
+        set_error(CASTRO_ERR_ARG, "castro_flux_register_reflux: dir 0..2, side 0/1, volume > 0");
+        return;
+    }
+    Fab S = make_fab(state, s_lo, s_hi), R = make_fab(reg, r_lo, r_hi);
+    const double scale = (side == 0 ? -1.0 : 1.0) / volume;
+    launch_box("castro_flux_register_reflux", flo, fhi, [=] __device__(int i, int j, int k) {
+        // side 0: the coarse zone is below the face (the fine patch above), side 1: above it
+        const int zi = i - (side == 0 && dir == 0), zj = j - (side == 0 && dir == 1), zk = k - (side == 0 && dir == 2);
+        for (int n = 0; n < ncomp; ++n) S(zi, zj, zk, n) = S(zi, zj, zk, n) + scale * R(i, j, k, n);
+    });
+}
+
+void castro_average_down(const int* clo, const int* chi, double* crse, const int* c_lo, const int* c_hi,
+                         const double* fine, const int* f_lo, const int* f_hi, int ncomp, int ratio)
+{
+    if (ratio < 1) {
+        set_error(CASTRO_ERR_ARG, "castro_average_down: ratio >= 1");
+        return;
+    }
+    Fab C = make_fab(crse, c_lo, c_hi), F = make_fab(fine, f_lo, f_hi);
+    const double inv = 1.0 / ((double)ratio * ratio * ratio);
+    launch_box("castro_average_down", clo, chi, [=] __device__(int i, int j, int k) {
+        for (int n = 0; n < ncomp; ++n) {
+            double s = 0.0;
+            for (int c = 0; c < ratio; ++c)
+                for (int b = 0; b < ratio; ++b)
+                    for (int a = 0; a < ratio; ++a) s = s + F(i * ratio + a, j * ratio + b, k * ratio + c, n);
+            C(i, j, k, n) = s * inv;
+        }
+    });
+}
+
 void castro_saxpy(double* u, const double* src, long long n, double dt)
 {
     if (n <= 0) return;
