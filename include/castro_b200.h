@@ -136,7 +136,9 @@ void castro_saxpy(double* u, const double* src, long long n, double dt);
  *              (call once per fine substep);
  *   reflux:    the coarse zone on `side` of each face (0: below, the patch above;
  *              1: above) gets -reg / volume (side 0) or +reg / volume (side 1).
- * average_down: each coarse zone of [clo, chi] = the mean of its ratio^3 fine zones. */
+ * average_down: each coarse zone of [clo, chi] = the mean of its ratio^3 fine zones.
+ * A zone or face the call would read or write outside its array's box: nothing
+ * is launched and castro_last_error() is CASTRO_ERR_ARG. */
 void castro_flux_register_crse_init(const int* flo, const int* fhi, double* reg, const int* r_lo, const int* r_hi,
                                     const double* crse_flux, const int* c_lo, const int* c_hi, int ncomp);
 void castro_flux_register_fine_add(const int* flo, const int* fhi, int dir, double* reg, const int* r_lo,

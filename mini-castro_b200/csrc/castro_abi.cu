@@ -556,9 +556,43 @@ __global__ void k_saxpy_host_dt(double* u, const double* src, long long n, doubl
 // zones onto the coarse zones beneath them.  Fluxes are in store_flux's form,
 // dt * F * A, on face boxes (node-centred in the normal direction).
 // ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+// [lo, hi] inside [alo, ahi] (an empty box is inside anything)
+bool box_inside(const int* lo, const int* hi, const int* alo, const int* ahi)
+{
+    for (int d = 0; d < 3; ++d)
+        if (lo[d] <= hi[d] && (lo[d] < alo[d] || hi[d] > ahi[d])) return false;
+    return true;
+}
+// the fine cells or faces under coarse [lo, hi] refined by r (faces: not refined along dir, dir < 0 for cells)
+void refine_box(const int* lo, const int* hi, int r, int dir, int* flo, int* fhi)
+{
+    for (int d = 0; d < 3; ++d) {
+        flo[d] = lo[d] * r;
+        fhi[d] = d == dir ? hi[d] * r : hi[d] * r + r - 1;
+    }
+}
+bool amr_args_ok(const char* who, bool ok)
+{
+    if (!ok) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "%s: a box the call reads or writes lies outside its array", who);
+        set_error(CASTRO_ERR_ARG, msg);
+    }
+    return ok;
+}
+}  // namespace
+
+extern "C" {
+
 void castro_flux_register_crse_init(const int* flo, const int* fhi, double* reg, const int* r_lo, const int* r_hi,
                                     const double* crse_flux, const int* c_lo, const int* c_hi, int ncomp)
 {
+    if (!amr_args_ok("castro_flux_register_crse_init",
+                     ncomp > 0 && box_inside(flo, fhi, r_lo, r_hi) && box_inside(flo, fhi, c_lo, c_hi)))
+        return;
     Fab R = make_fab(reg, r_lo, r_hi), F = make_fab(crse_flux, c_lo, c_hi);
     launch_box("castro_flux_register_crse_init", flo, fhi, [=] __device__(int i, int j, int k) {
         for (int n = 0; n < ncomp; ++n) R(i, j, k, n) = -F(i, j, k, n);
@@ -573,6 +607,11 @@ void castro_flux_register_fine_add(const int* flo, const int* fhi, int dir, doub
         set_error(CASTRO_ERR_ARG, "castro_flux_register_fine_add: dir 0..2, ratio >= 1");
         return;
     }
+    int ffl[3], ffh[3];
+    refine_box(flo, fhi, ratio, dir, ffl, ffh);
+    if (!amr_args_ok("castro_flux_register_fine_add",
+                     ncomp > 0 && box_inside(flo, fhi, r_lo, r_hi) && box_inside(ffl, ffh, f_lo, f_hi)))
+        return;
     Fab R = make_fab(reg, r_lo, r_hi), F = make_fab(fine_flux, f_lo, f_hi);
     launch_box("castro_flux_register_fine_add", flo, fhi, [=] __device__(int i, int j, int k) {
         // the ratio^2 fine faces on coarse face (i,j,k): the same plane, ratio x ratio across it
@@ -596,6 +635,11 @@ void castro_flux_register_reflux(const int* flo, const int* fhi, int dir, int si
         set_error(CASTRO_ERR_ARG, "castro_flux_register_reflux: dir 0..2, side 0/1, volume > 0");
         return;
     }
+    int zlo[3] = {flo[0], flo[1], flo[2]}, zhi[3] = {fhi[0], fhi[1], fhi[2]};
+    if (side == 0) { zlo[dir] -= 1; zhi[dir] -= 1; }
+    if (!amr_args_ok("castro_flux_register_reflux",
+                     ncomp > 0 && box_inside(flo, fhi, r_lo, r_hi) && box_inside(zlo, zhi, s_lo, s_hi)))
+        return;
     Fab S = make_fab(state, s_lo, s_hi), R = make_fab(reg, r_lo, r_hi);
     const double scale = (side == 0 ? -1.0 : 1.0) / volume;
     launch_box("castro_flux_register_reflux", flo, fhi, [=] __device__(int i, int j, int k) {
@@ -612,6 +656,11 @@ void castro_average_down(const int* clo, const int* chi, double* crse, const int
         set_error(CASTRO_ERR_ARG, "castro_average_down: ratio >= 1");
         return;
     }
+    int fl[3], fh[3];
+    refine_box(clo, chi, ratio, -1, fl, fh);
+    if (!amr_args_ok("castro_average_down",
+                     ncomp > 0 && box_inside(clo, chi, c_lo, c_hi) && box_inside(fl, fh, f_lo, f_hi)))
+        return;
     Fab C = make_fab(crse, c_lo, c_hi), F = make_fab(fine, f_lo, f_hi);
     const double inv = 1.0 / ((double)ratio * ratio * ratio);
     launch_box("castro_average_down", clo, chi, [=] __device__(int i, int j, int k) {

@@ -53,6 +53,29 @@ def test_average_down_matches_numpy(pkg, table):
     np.testing.assert_allclose(from_dev(crse), ref, rtol=1e-15, atol=1e-15)
 
 
+def test_amr_calls_reject_boxes_outside_their_arrays(pkg, table):
+    import torch
+
+    L = _lib(pkg, table)
+    K = pkg.castro
+    clo, chi = (0, 0, 0), (3, 3, 3)
+    crse = torch.zeros((2, 4, 4, 4), dtype=torch.float64, device="cuda")
+    fine = torch.ones((2, 7, 8, 8), dtype=torch.float64, device="cuda")   # one fine zone short along x
+    L.castro_clear_error()
+    L.castro_average_down(_v(K, clo), _v(K, chi), C.c_void_p(crse.data_ptr()), _v(K, clo), _v(K, chi),
+                          C.c_void_p(fine.data_ptr()), _v(K, (0, 0, 0)), _v(K, (6, 7, 7)), 2, 2)
+    assert L.castro_last_error() == 5 and b"outside" in L.castro_error_string()
+    L.castro_clear_error()
+    reg = torch.zeros((2, 4, 4, 1), dtype=torch.float64, device="cuda")
+    L.castro_flux_register_reflux(_v(K, (0, 0, 0)), _v(K, (0, 3, 3)), 0, 0, C.c_void_p(crse.data_ptr()), _v(K, clo),
+                                  _v(K, chi), C.c_void_p(reg.data_ptr()), _v(K, (0, 0, 0)), _v(K, (0, 3, 3)), 2,
+                                  C.c_double(1.0))   # side 0 of face plane 0: the zones at x = -1
+    assert L.castro_last_error() == 5
+    L.castro_clear_error()
+    torch.cuda.synchronize()
+    assert float(crse.abs().max()) == 0.0      # nothing was launched
+
+
 @pytest.mark.parametrize("d", [0, 1, 2])
 def test_flux_register_matches_numpy(pkg, table, d):
     import torch
