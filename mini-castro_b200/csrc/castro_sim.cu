@@ -2935,17 +2935,48 @@ int box_hydro_launch(const BoxPlan& P, double* base, long long meta_doubles, con
     return castro_last_error();
 }
 
+// The arrays a box call touches cover what it touches: Sborder grow(box, 4), the
+// source the box, each requested flux array its face box.  Checked on the host
+// before anything is launched.
+bool box_call_args_ok(const char* who, const int* lo, const int* hi, const int* sb_lo, const int* sb_hi,
+                      const int* sr_lo, const int* sr_hi, double* const* fo, const int* fo_lo, const int* fo_hi)
+{
+    char msg[200];
+    for (int d = 0; d < 3; ++d) {
+        if (lo[d] > hi[d]) { snprintf(msg, sizeof msg, "%s: empty box", who); set_error(CASTRO_ERR_ARG, msg); return false; }
+        if (sb_lo[d] > lo[d] - NG || sb_hi[d] < hi[d] + NG) {
+            snprintf(msg, sizeof msg, "%s: Sborder needs 4 ghost zones", who);
+            set_error(CASTRO_ERR_ARG, msg);
+            return false;
+        }
+        if (sr_lo[d] > lo[d] || sr_hi[d] < hi[d]) {
+            snprintf(msg, sizeof msg, "%s: the source array does not cover the box", who);
+            set_error(CASTRO_ERR_ARG, msg);
+            return false;
+        }
+    }
+    if (fo)
+        for (int f = 0; f < 3; ++f) {
+            if (!fo[f]) continue;
+            for (int d = 0; d < 3; ++d)
+                if (fo_lo[3 * f + d] > lo[d] || fo_hi[3 * f + d] < hi[d] + (d == f)) {
+                    snprintf(msg, sizeof msg, "%s: flux array %d does not cover the box's faces", who, f);
+                    set_error(CASTRO_ERR_ARG, msg);
+                    return false;
+                }
+        }
+    return true;
+}
+
 template <int NS>
 int box_hydro_noalloc_impl(const int* lo, const int* hi, const double* sb, const int* sb_lo, const int* sb_hi,
                            double* source, const int* sr_lo, const int* sr_hi, double* const* fo, const int* fo_lo,
                            const int* fo_hi, const double* dx, double dt)
 {
     NvtxRange r("castro_construct_hydro_source_box_noalloc");
-    for (int d = 0; d < 3; ++d)
-        if (sb_lo[d] > lo[d] - NG || sb_hi[d] < hi[d] + NG) {
-            set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box_noalloc: Sborder needs 4 ghost zones");
-            return CASTRO_ERR_ARG;
-        }
+    if (!box_call_args_ok("castro_construct_hydro_source_box_noalloc", lo, hi, sb_lo, sb_hi, sr_lo, sr_hi, fo, fo_lo,
+                          fo_hi))
+        return CASTRO_ERR_ARG;
     int dev = 0;
     if (!cuda_ok(cudaGetDevice(&dev), "castro_construct_hydro_source_box_noalloc: cudaGetDevice")) return CASTRO_ERR_CUDA;
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
@@ -3012,11 +3043,8 @@ int box_hydro_impl(const int* lo, const int* hi, const double* sb, const int* sb
                    const int* fo_hi, const double* dx, double dt)
 {
     NvtxRange r("castro_construct_hydro_source_box");
-    for (int d = 0; d < 3; ++d)
-        if (sb_lo[d] > lo[d] - NG || sb_hi[d] < hi[d] + NG) {
-            set_error(CASTRO_ERR_ARG, "castro_construct_hydro_source_box: Sborder needs 4 ghost zones");
-            return CASTRO_ERR_ARG;
-        }
+    if (!box_call_args_ok("castro_construct_hydro_source_box", lo, hi, sb_lo, sb_hi, sr_lo, sr_hi, fo, fo_lo, fo_hi))
+        return CASTRO_ERR_ARG;
     int dev = 0;
     if (!cuda_ok(cudaGetDevice(&dev), "castro_construct_hydro_source_box: cudaGetDevice")) return CASTRO_ERR_CUDA;
     if (dev < 0 || dev >= BOX_MAX_DEVICES) {

@@ -107,6 +107,44 @@ def test_corrupt_boxarray_rejected(pkg, table, case):
     L.castro_clear_error()
 
 
+
+
+@pytest.mark.parametrize("entry", ["castro_construct_hydro_source_box", "castro_construct_hydro_source_box_noalloc"])
+@pytest.mark.parametrize("bad", ["sborder", "source", "flux"])
+def test_box_entry_point_rejects_short_arrays(pkg, table, entry, bad):
+    """An array that does not cover what the per-box call would touch (Sborder
+    without 4 ghost zones, a source smaller than the box, a flux array smaller
+    than the box's faces): CASTRO_ERR_ARG before anything is launched."""
+    import ctypes as C
+
+    import torch
+
+    L = _lib(pkg, table)
+    K = pkg.castro
+    lo, hi = (0, 0, 0), (7, 7, 7)
+    sblo, sbhi = [-4, -4, -4], [11, 11, 11]
+    srlo, srhi = [0, 0, 0], [7, 7, 7]
+    fo = [torch.zeros(9 * 9 * 8 * 8, dtype=torch.float64, device="cuda") for _ in range(3)]
+    folo, fohi = [0] * 9, [8, 7, 7, 7, 8, 7, 7, 7, 8]
+    if bad == "sborder":
+        sbhi[2] = 10
+    elif bad == "source":
+        srhi[0] = 6
+    else:
+        fohi[4] = 7                       # the y-face array stops one face short
+    sb = torch.ones(9 * 16 ** 3, dtype=torch.float64, device="cuda")
+    src = torch.zeros(9 * 8 ** 3, dtype=torch.float64, device="cuda")
+    ptrs = (C.c_void_p * 3)(*[f.data_ptr() for f in fo])
+    L.castro_clear_error()
+    rc = getattr(L, entry)(K.ivec(lo), K.ivec(hi), C.c_void_p(sb.data_ptr()), K.ivec(sblo), K.ivec(sbhi),
+                           C.c_void_p(src.data_ptr()), K.ivec(srlo), K.ivec(srhi), ptrs, (C.c_int * 9)(*folo),
+                           (C.c_int * 9)(*fohi), K.ivec(lo), K.ivec(hi), K.dvec([1.0, 1.0, 1.0]), C.c_double(1e-6))
+    assert rc == ERR_ARG, L.castro_error_string()
+    L.castro_clear_error()
+    torch.cuda.synchronize()
+    assert float(src.abs().max()) == 0.0 and all(float(f.abs().max()) == 0.0 for f in fo)
+
+
 @pytest.mark.parametrize("exact", [True, False], ids=["exact", "fast"])
 def test_checkpoint_restart_bitwise(pkg, table, tmp_path, exact):
     """3 steps, checkpoint, 2 more steps; a fresh sim restarted from the
