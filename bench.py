@@ -199,16 +199,30 @@ def fp64_block(flops: float, ms: float, peak: float) -> dict:
     return {"achieved": ach, "frac": ach / peak if peak else None}
 
 
-def path_roofline(zones, ms_per_step, bpz, hbm, flops_per_zone, fp64_peak) -> dict:
+def path_roofline(zones, ms_per_step, bpz, hbm, flops_per_zone, fp64_peak, ref_flops=None) -> dict:
     """Step-level roofline of a whole path: algorithmic bytes and the counted
-    FP64 work of the batched step per zone-update, over the path's step time."""
+    FP64 work of the batched step per zone-update, over the path's step time
+    (and, when given, the reference algorithm's counted operations)."""
     gbs = zones * bpz / (ms_per_step * 1e-3) / 1e9
     out = {"hbm": {"achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
                    "algorithmic_bytes_per_zone_update": bpz}}
     if flops_per_zone:
         out["fp64"] = dict(fp64_block(zones * flops_per_zone, ms_per_step, fp64_peak), peak=fp64_peak,
                            unit="TFLOP/s", flops_per_zone_update=flops_per_zone)
+    if ref_flops:
+        out["fp64_reference_algorithm"] = dict(fp64_block(zones * ref_flops, ms_per_step, fp64_peak),
+                                               peak=fp64_peak, unit="TFLOP/s", flops_per_zone_update=ref_flops)
     return out
+
+
+def reference_algorithm_ops(workload: str):
+    """The reference algorithm's floating-point operations per zone-update of a
+    workload, as the oracle's counting build measured them (oracle/count_ops.py)."""
+    path = os.path.join(ROOT, "profiles", "fp64_ops_reference_algorithm.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as fp:
+        return json.load(fp).get(workload)
 
 
 def run_b200(args, pkg, rank, world):
@@ -354,6 +368,17 @@ def run_b200(args, pkg, rank, world):
         if per_kernel.get(dom):
             roof_fp64.update(fp64_block(zones * per_kernel[dom], prof[dom], fp64_peak))
             roof_fp64["kernel_flops_per_zone_update"] = per_kernel[dom]
+    ref_ops = reference_algorithm_ops(args.workload)
+    ref_flops = ref_ops["flops_per_zone_update"] if ref_ops else None
+    if roof_fp64 is not None and ref_ops:
+        # the survey's FP64 fraction: zone-updates/s x the reference algorithm's counted operations
+        # (add, mul, div, sqrt, transcendental as one each) / the measured FP64 peak.  This build
+        # executes fewer (flops_per_zone_update, counted by ncu with an FMA as two): no per-box
+        # ghost-zone recompute, energy-only Newton evaluations, the table cell by a settled log2.
+        roof_fp64["reference_algorithm"] = dict(
+            fp64_block(zones * ref_flops, step_ms, fp64_peak), flops_per_zone_update=ref_flops,
+            ops_per_zone_update=ref_ops["per_zone_update"],
+            source="oracle/count_ops.py: the oracle's parity algorithm with every floating-point operation counted")
     alg = zones * alg_bpz
     roof = {"bound": "hbm", "kernel": dom, "unit": "GB/s", "peak": hbm, "peak_kind": peak_kind,
             "algorithmic_bytes_per_zone_update": alg_bpz, "algorithmic_bytes_per_launch": alg,
@@ -369,7 +394,8 @@ def run_b200(args, pkg, rank, world):
                         "intermediates included): how well it streams what the design keeps in HBM"}}
     for leg in (plain, plain_box):
         if leg:
-            leg["roofline"] = path_roofline(zones, leg["ms_per_step"], alg_bpz, hbm, flops_per_zone, fp64_peak)
+            leg["roofline"] = path_roofline(zones, leg["ms_per_step"], alg_bpz, hbm, flops_per_zone, fp64_peak,
+                                            ref_flops)
     line = {
         "metric": METRIC,
         "value": value,

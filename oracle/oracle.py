@@ -17,7 +17,10 @@ LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 # the two builds of oracle/Makefile: "parity" (non-contracting, the checker) and
 # "fast" (-O3 -march=native with FMA contraction: the timed CPU baseline, and an
 # independent rounding of the same algorithm for the noise classification)
-LIB_PATHS = {"parity": LIB_PATH, "fast": os.path.join(HERE, "_build", "liboracle_fast.so")}
+# and "count" (the parity build with every floating-point operation counted, op_count.cpp)
+LIB_PATHS = {"parity": LIB_PATH, "fast": os.path.join(HERE, "_build", "liboracle_fast.so"),
+             "count": os.path.join(HERE, "_build", "liboracle_count.so")}
+OP_CLASSES = ("add", "mul", "div", "sqrt", "transcendental", "compare", "sign")
 
 MAX_SPEC = 13
 EOS_INPUT_RT, EOS_INPUT_RE, EOS_INPUT_RP = 1, 2, 3
@@ -51,9 +54,9 @@ class ProbT(C.Structure):
 
 
 def build(force: bool = False) -> str:
-    src = os.path.join(HERE, "castro_oracle.c")
-    stale = [p for p in LIB_PATHS.values()
-             if not os.path.exists(p) or os.path.getmtime(p) < os.path.getmtime(src)]
+    srcs = [os.path.join(HERE, f) for f in ("castro_oracle.c", "castro_oracle.h", "op_count.cpp")]
+    newest = max(os.path.getmtime(f) for f in srcs)
+    stale = [p for p in LIB_PATHS.values() if not os.path.exists(p) or os.path.getmtime(p) < newest]
     if force or stale:
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
@@ -105,7 +108,25 @@ def _bind(L):
     L.oracle_level_steps.argtypes = [C.c_void_p]
     L.oracle_level_blast_radius.restype = C.c_double
     L.oracle_level_blast_radius.argtypes = [C.c_void_p, _dp]
+    if hasattr(L, "oracle_op_counts"):
+        L.oracle_op_counts.restype = None
+        L.oracle_op_counts.argtypes = [C.POINTER(C.c_ulonglong)]
+        L.oracle_op_counts_reset.restype = None
+        L.oracle_op_counts_reset.argtypes = []
     return L
+
+
+def op_counts_reset():
+    """Zero the counting build's operation counters."""
+    lib("count").oracle_op_counts_reset()
+
+
+def op_counts() -> dict:
+    """Floating-point operations the counting build has executed since the last
+    reset, summed over threads, by class (OP_CLASSES)."""
+    out = (C.c_ulonglong * len(OP_CLASSES))()
+    lib("count").oracle_op_counts(out)
+    return dict(zip(OP_CLASSES, (int(v) for v in out)))
 
 
 def ptr(a: np.ndarray):

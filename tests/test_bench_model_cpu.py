@@ -62,3 +62,21 @@ def test_autotune_labels_distinct():
     n = 1 + sum(len([v for v in vals if v != A.DEFAULTS[k]]) for k, vals in A.KNOBS)
     assert len(labels) == n
     assert set(A.DEFAULTS) == {k for k, _ in A.KNOBS}
+
+
+def test_reference_algorithm_fp64_fraction():
+    """The FP64 fraction on the reference algorithm's counted operations
+    (profiles/fp64_ops_reference_algorithm.json, oracle/count_ops.py):
+    zone-updates/s x counted flops / peak, beside the executed-work figure."""
+    b = _bench()
+    ops = b.reference_algorithm_ops("sedov128_pert")
+    assert ops and ops["zones"] == 128 ** 3 and ops["boxes"] == 64
+    per = ops["per_zone_update"]
+    assert abs(per["add"] + per["mul"] + per["div"] + per["sqrt"] + per["transcendental"]
+               - ops["flops_per_zone_update"]) < 1.0
+    zones, ms, peak = 128 ** 3, 3.4, 33.8
+    r = b.path_roofline(zones, ms, 144, 6500.0, 13000.0, peak, ops["flops_per_zone_update"])
+    want = zones * ops["flops_per_zone_update"] / (ms * 1e-3) / 1e12
+    assert abs(r["fp64_reference_algorithm"]["achieved"] - want) < 1e-9 * want
+    assert abs(r["fp64_reference_algorithm"]["frac"] - want / peak) < 1e-12
+    assert r["fp64"]["flops_per_zone_update"] == 13000.0
