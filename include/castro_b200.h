@@ -93,6 +93,20 @@ void castro_set_table_l2_window(int on);
 void castro_set_momentum_flux_pressure(int on);
 int  castro_momentum_flux_pressure(void);
 
+/* Option, off by default: Coulomb corrections in the EOS.  The reference's
+ * eos.F90 has none; its 2017 runs used them ("Initializing Helmholtz EOS and
+ * using Coulomb corrections", scaling/summitdev_20171020/1.out:14).  The ion
+ * plasma's excess energy and pressure in a uniform electron background from
+ * the fits of Yakovlev & Shalybkov (1989), as the Helmholtz EOS applies them
+ * (Timmes & Swesty 2000): added to p, e and their density and temperature
+ * derivatives wherever the EOS is evaluated, unless the totals would turn
+ * non-positive there.  The forward paths only: the adjoint (castro_adj_*, the
+ * *_adj routines that call the EOS) refuses to run with it (CASTRO_ERR_ARG).
+ * The call waits for the kernels already queued on the device.  The oracle's
+ * oracle_set_coulomb_corrections is its counterpart. */
+void castro_set_coulomb_corrections(int on);
+int  castro_coulomb_corrections(void);
+
 void eos_init(void);                          /* Castro_F.H:15: reads ./helm_table.dat (or $CASTRO_HELM_TABLE), eos.F90:580-734 */
 void eos_finalize(void);                      /* Castro_F.H:17 */
 int  castro_eos_init_path(const char* path);  /* eos_init with an explicit table path; returns an error code */

@@ -61,15 +61,17 @@ __device__ __forceinline__ void load_tflux(const Fab& f, const Fab& qg, int i, i
     r[R::UG] = qg(i, j, k, GDU + normal);
 }
 
-template <int NS>
-void ctoprim_impl(const int* lo, const int* hi, Fab U, Fab Q, Fab QA)
+// Routines that call the EOS run the instantiation with or without the Coulomb
+// corrections (COUL), as the library is set.
+template <int NS, bool COUL>
+void ctoprim_run(const int* lo, const int* hi, Fab U, Fab Q, Fab QA)
 {
     launch_box("ctoprim", lo, hi, [=] __device__(int i, int j, int k) {
         constexpr int NVAR = Dims<NS>::NVAR, QVAR = Dims<NS>::QVAR;
         double u[NVAR], q[QVAR], qa[NQAUX];
 #pragma unroll
         for (int n = 0; n < NVAR; ++n) u[n] = U(i, j, k, n);
-        ctoprim_pt<NS>(u, q, qa);
+        ctoprim_pt<NS, COUL>(u, q, qa);
 #pragma unroll
         for (int n = 0; n < QVAR; ++n) Q(i, j, k, n) = q[n];
 #pragma unroll
@@ -77,22 +79,36 @@ void ctoprim_impl(const int* lo, const int* hi, Fab U, Fab Q, Fab QA)
     });
 }
 
-template <int NS, int WHICH>
-void clean_impl(const char* what, const int* lo, const int* hi, Fab U)
+template <int NS>
+void ctoprim_impl(const int* lo, const int* hi, Fab U, Fab Q, Fab QA)
+{
+    if (coulomb_on()) ctoprim_run<NS, true>(lo, hi, U, Q, QA);
+    else ctoprim_run<NS, false>(lo, hi, U, Q, QA);
+}
+
+template <int NS, int WHICH, bool COUL>
+void clean_run(const char* what, const int* lo, const int* hi, Fab U)
 {
     launch_box(what, lo, hi, [=] __device__(int i, int j, int k) {
         constexpr int NVAR = Dims<NS>::NVAR;
         double u[NVAR];
 #pragma unroll
         for (int n = 0; n < NVAR; ++n) u[n] = U(i, j, k, n);
-        if (WHICH == 0) enforce_minimum_density_pt<NS>(u);
+        if (WHICH == 0) enforce_minimum_density_pt<NS, COUL>(u);
         else if (WHICH == 1) normalize_species_pt<NS>(u);
-        else if (WHICH == 2) reset_internal_e_pt<NS>(u);
-        else if (WHICH == 3) compute_temp_pt<NS>(u);
-        else clean_state_pt<NS>(u);      // the four in a row: each is pointwise
+        else if (WHICH == 2) reset_internal_e_pt<NS, COUL>(u);
+        else if (WHICH == 3) compute_temp_pt<NS, COUL>(u);
+        else clean_state_pt<NS, COUL>(u);   // the four in a row: each is pointwise
 #pragma unroll
         for (int n = 0; n < NVAR; ++n) U(i, j, k, n) = u[n];
     });
+}
+
+template <int NS, int WHICH>
+void clean_impl(const char* what, const int* lo, const int* hi, Fab U)
+{
+    if (WHICH != 1 && coulomb_on()) clean_run<NS, WHICH, true>(what, lo, hi, U);
+    else clean_run<NS, WHICH, false>(what, lo, hi, U);
 }
 
 __device__ __forceinline__ void atomic_min_double(double* addr, double v)
@@ -108,7 +124,7 @@ __device__ __forceinline__ void atomic_min_double(double* addr, double v)
     }
 }
 
-template <int NS>
+template <int NS, bool COUL>
 __global__ void k_estdt(BoxRange r, Fab U, double dx0, double dx1, double dx2, double* dt)
 {
     __shared__ double red[32];
@@ -122,7 +138,7 @@ __global__ void k_estdt(BoxRange r, Fab U, double dx0, double dx1, double dx2, d
         double u[Dims<NS>::NVAR];
 #pragma unroll
         for (int n = 0; n < Dims<NS>::NVAR; ++n) u[n] = U(i, j, k, n);
-        m = estdt_pt<NS>(u, dx0, dx1, dx2);
+        m = estdt_pt<NS, COUL>(u, dx0, dx1, dx2);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = DMIN(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -142,7 +158,9 @@ void estdt_impl(const int* lo, const int* hi, Fab U, const double* dx, double* d
     BoxRange r = make_range(lo, hi);
     if (r.n == 0) return;
     const int B = 128;
-    k_estdt<NS><<<(unsigned)((r.n + B - 1) / B), B, 0, stream()>>>(r, U, dx[0], dx[1], dx[2], dt);
+    const unsigned g = (unsigned)((r.n + B - 1) / B);
+    if (coulomb_on()) k_estdt<NS, true><<<g, B, 0, stream()>>>(r, U, dx[0], dx[1], dx[2], dt);
+    else k_estdt<NS, false><<<g, B, 0, stream()>>>(r, U, dx[0], dx[1], dx[2], dt);
     check_launch("estdt");
 }
 
@@ -347,18 +365,11 @@ namespace {
 
 struct SpeciesX { double x[MAX_SPEC]; };
 
-template <int NS>
-void initdata_impl(const int* lo, const int* hi, Fab U, const double* dx, const double* problo, const double* probhi)
+// the ambient internal energy of initdata, Prob.F90:51-59, into *d_e (one
+// EOS call; a single-thread kernel keeps it on the device EOS)
+template <int NS, bool COUL>
+void ambient_energy(double* d_e, SpeciesX xs, int from_T, double rho_a, double T_a, double p_a)
 {
-    const castro_problem P = castro::problem();
-    // ambient internal energy, Prob.F90:51-59: one EOS call on the host side
-    // of the launch (a single-thread kernel keeps it on the device EOS)
-    double* d_e = nullptr;
-    if (cudaMallocAsync(&d_e, sizeof(double), stream()) != cudaSuccess) { set_error(1, "initdata: alloc"); return; }
-    SpeciesX xs;
-    for (int n = 0; n < MAX_SPEC; ++n) xs.x[n] = P.X[n];
-    const int from_T = P.ambient_from_T;
-    const double rho_a = P.dens_ambient, p_a = P.p_ambient, T_a = P.T_ambient;
     const int one[3] = {0, 0, 0};
     launch_box<32>("initdata(ambient)", one, one, [=] __device__(int, int, int) {
         double s1 = 0.0, s2 = 0.0;
@@ -367,12 +378,26 @@ void initdata_impl(const int* lo, const int* hi, Fab U, const double* dx, const 
         EosResult r;
         if (from_T) {
             double abar = 1.0 / s1;
-            r = eos_solve<EOS_RT>(rho_a, T_a, 0.0, abar, abar * s2);
+            r = eos_solve<EOS_RT, COUL>(rho_a, T_a, 0.0, abar, abar * s2);
         } else {
-            r = eos_solve<EOS_RP>(rho_a, 1.e4, p_a, c_net.aion[0], c_net.zion[0]);
+            r = eos_solve<EOS_RP, COUL>(rho_a, 1.e4, p_a, c_net.aion[0], c_net.zion[0]);
         }
         *d_e = r.e;
     });
+}
+
+template <int NS>
+void initdata_impl(const int* lo, const int* hi, Fab U, const double* dx, const double* problo, const double* probhi)
+{
+    const castro_problem P = castro::problem();
+    double* d_e = nullptr;
+    if (cudaMallocAsync(&d_e, sizeof(double), stream()) != cudaSuccess) { set_error(1, "initdata: alloc"); return; }
+    SpeciesX xs;
+    for (int n = 0; n < MAX_SPEC; ++n) xs.x[n] = P.X[n];
+    const int from_T = P.ambient_from_T;
+    const double rho_a = P.dens_ambient, p_a = P.p_ambient, T_a = P.T_ambient;
+    if (coulomb_on()) ambient_energy<NS, true>(d_e, xs, from_T, rho_a, T_a, p_a);
+    else ambient_energy<NS, false>(d_e, xs, from_T, rho_a, T_a, p_a);
     const double r_init = P.r_init;
     const double vctr = (4.0 / 3.0) * 3.14159265358979323846 * (r_init * r_init * r_init);
     const double e_exp = P.exp_energy / vctr / P.dens_ambient;

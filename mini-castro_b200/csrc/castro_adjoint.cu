@@ -692,6 +692,15 @@ void fill_hydro_source_adj_impl(const int* lo, const int* hi, Fab SRCB, Fab Q0, 
     });
 }
 
+// The reverse EOS has no Coulomb corrections: with them switched on, every
+// entry point that would differentiate an EOS call refuses (CASTRO_ERR_ARG).
+bool coulomb_refused(const char* who)
+{
+    if (!network_host().coulomb) return false;
+    set_error(CASTRO_ERR_ARG, (std::string(who) + ": the adjoint EOS has no Coulomb corrections").c_str());
+    return true;
+}
+
 }  // namespace
 
 // ============================================================================
@@ -703,6 +712,7 @@ void ctoprim_adj(const int* lo, const int* hi, const double* u, const int* u_lo,
                  const double* qb, const int* qb_lo, const int* qb_hi, const double* qab, const int* qab_lo,
                  const int* qab_hi, double* ub, const int* ub_lo, const int* ub_hi)
 {
+    if (coulomb_refused("ctoprim_adj")) return;
     CASTRO_DISPATCH_NS(ctoprim_adj_impl, lo, hi, make_fab(u, u_lo, u_hi), make_fab(qb, qb_lo, qb_hi),
                        make_fab(qab, qab_lo, qab_hi), make_fab(ub, ub_lo, ub_hi));
 }
@@ -710,6 +720,7 @@ void ctoprim_adj(const int* lo, const int* hi, const double* u, const int* u_lo,
 void clean_state_adj(const int* lo, const int* hi, const double* u, const int* u_lo, const int* u_hi, double* ub,
                      const int* ub_lo, const int* ub_hi)
 {
+    if (coulomb_refused("clean_state_adj")) return;
     CASTRO_DISPATCH_NS(clean_state_adj_impl, lo, hi, make_fab(u, u_lo, u_hi), make_fab(ub, ub_lo, ub_hi));
 }
 
@@ -1339,7 +1350,7 @@ void estdt_adj(castro_adj* a, const Arr& V, double minval, const double* scale, 
         double u[Dims<NS>::NVAR];
 #pragma unroll
         for (int n = 0; n < Dims<NS>::NVAR; ++n) u[n] = U(i, j, k, n);
-        if (estdt_pt<NS>(u, dx0, dx1, dx2) == minval)
+        if (estdt_pt<NS, false>(u, dx0, dx1, dx2) == minval)   // (the adjoint runs without Coulomb corrections)
             atomicMin(idx, (i - bx.lo[0]) + nx * ((j - bx.lo[1]) + ny * (k - bx.lo[2])));
     });
     Fab UB = Vb.fab();
@@ -1914,6 +1925,7 @@ castro_adj* castro_adj_create_window(const castro_instance_desc* desc, int nstep
         return nullptr;
     }
     if (!table_ready()) { set_error(CASTRO_ERR_NO_TABLE, "castro_adj_create: eos_init has not run"); return nullptr; }
+    if (coulomb_refused("castro_adj_create")) return nullptr;
     const int nz = desc->dom_hi[2] - desc->dom_lo[2] + 1;
     if (slab_nz > 0 && slab_nz < nz && nz % slab_nz != 0) {
         set_error(CASTRO_ERR_ARG, "castro_adj_create: the slab thickness must divide the domain's z extent");
@@ -2090,6 +2102,7 @@ int castro_adj_forward(castro_adj* a, double* J)
 {
     NvtxRange r("castro_adj_forward");
     if (!a) { set_error(CASTRO_ERR_ARG, "castro_adj_forward: null"); return CASTRO_ERR_ARG; }
+    if (coulomb_refused("castro_adj_forward")) return CASTRO_ERR_ARG;
     int rc = CASTRO_ERR_NSPEC;
     if (a->ns == 2) rc = adj_forward<2>(a);
     else if (a->ns == 13) rc = adj_forward<13>(a);
@@ -2101,6 +2114,7 @@ int castro_adj_backward(castro_adj* a, double* dJ_dE, double* dJ_drho, double* d
 {
     NvtxRange r("castro_adj_backward");
     if (!a || !dJ_dE || !dJ_drho) { set_error(CASTRO_ERR_ARG, "castro_adj_backward: arguments"); return CASTRO_ERR_ARG; }
+    if (coulomb_refused("castro_adj_backward")) return CASTRO_ERR_ARG;
     if (a->ns == 2) return adj_backward<2>(a, dJ_dE, dJ_drho, dJ_dpert);
     if (a->ns == 13) return adj_backward<13>(a, dJ_dE, dJ_drho, dJ_dpert);
     return CASTRO_ERR_NSPEC;

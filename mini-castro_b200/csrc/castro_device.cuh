@@ -68,7 +68,7 @@ struct EosTableDev {
     const double* trow;   // [JMAX][ROW_STRIDE]
     const double* drow;   // [IMAX][ROW_STRIDE]
     double tlo, dlo, tstpi, dstpi, mintemp;
-    double asoli3, kergavo, avo_eos, sioncon;
+    double asoli3, kergavo, avo_eos, sioncon, kerg;
     // incremented when a Newton inversion ends unconverged after 100
     // iterations (the reference continues silently, eos.F90:193-554)
     unsigned long long* fail_count;
@@ -82,12 +82,19 @@ struct NetworkDev {
     // default: the reference's compute_flux, whose momentum flux is rho u u
     // alone (Source/riemann.F90:306-308)
     int mom_flux_p;
+    // 1: the EOS with Coulomb corrections (castro_set_coulomb_corrections); 0,
+    // the default: the reference's eos.F90, which has none
+    int coulomb;
 };
 
 // Each translation unit holds its own copy; castro_upload_constants_<tu>()
 // fills it (see castro_host.cu).
 static __constant__ EosTableDev c_eos;
 static __constant__ NetworkDev c_net;
+
+// the library's Coulomb setting (castro_set_coulomb_corrections), read by the
+// host code that launches the EOS kernels to pick their instantiation
+bool coulomb_on();
 
 CASTRO_HD double fmaxf_(double a, double b) { return (a > b) ? a : b; }
 CASTRO_HD double fminf_(double a, double b) { return (a < b) ? a : b; }
@@ -191,8 +198,64 @@ struct EosEval {
 };
 
 struct EosConst {   // per-call constants of the Newton loop
-    double den, deni, ytot1, ye, din;
+    double den, deni, ytot1, ye, din, zbar;
 };
+
+// Coulomb corrections of an ion plasma in a uniform electron background (off
+// by default: the reference's eos.F90 has none; its 2017 runs had them on,
+// scaling/summitdev_20171020/1.out:14).  The fits of Yakovlev & Shalybkov
+// (1989) as the Helmholtz EOS applies them (Timmes & Swesty 2000): with n_i =
+// N_A rho / abar, the ion-sphere radius a = (3 / (4 pi n_i))^(1/3) and the
+// coupling Gamma = zbar^2 q_e^2 / (a k T), the excess energy per ion in kT is
+// a1 Gamma + b1 Gamma^(1/4) + c1 Gamma^(-1/4) + d1 for Gamma >= 1 and
+// -3 c2 Gamma^(3/2) + a2 Gamma^b2 below (c2 = 1 / (2 sqrt 3), Debye-Hueckel),
+// the excess pressure a third of the excess energy density; Gamma goes as
+// rho^(1/3) / T.  Operation for operation the oracle's coulomb(), whose cube
+// root and power are the host libm's: the two agree to an ulp, not bit for bit.
+namespace coul {
+constexpr double QE = 4.80320427e-10;   // electron charge, esu
+constexpr double A1 = -0.898004, B1 = 0.96786, C1 = 0.220703, D1 = -0.86097;
+constexpr double A2 = 0.29561, B2 = 1.9885, C2 = 0.288675;
+constexpr double FOUR_PI = 4.0 * 3.14159265358979323846;
+}  // namespace coul
+
+struct CoulombTerms {
+    double p, e, dedt, dpdd, dpdt, dedd;
+};
+
+__device__ __forceinline__ void coulomb_terms(double den, double temp, double ytot1, double zbar, double pion,
+                                              double dpiondd, double dpiondt, CoulombTerms& c)
+{
+    double xni = c_eos.avo_eos * ytot1 * den;
+    double a_ion = cbrt(3.0 / (coul::FOUR_PI * xni));
+    double gam = zbar * zbar * coul::QE * coul::QE / (a_ion * c_eos.kerg * temp);
+    double gdd = gam / (3.0 * den);
+    double gdt = -gam / temp;
+    double y = c_eos.kergavo * ytot1;
+    if (gam >= 1.0) {
+        double x = sqrt(sqrt(gam));
+        double u = coul::A1 * gam + coul::B1 * x + coul::C1 / x + coul::D1;
+        double du = coul::A1 + 0.25 * (coul::B1 * x - coul::C1 / x) / gam;
+        c.e = y * temp * u;
+        c.dedd = y * temp * du * gdd;
+        c.dedt = y * u + y * temp * du * gdt;
+        c.p = den * c.e / 3.0;
+        c.dpdd = (c.e + den * c.dedd) / 3.0;
+        c.dpdt = den * c.dedt / 3.0;
+    } else {
+        double sg = sqrt(gam);
+        double g32 = gam * sg;
+        double gb = pow(gam, coul::B2);
+        double z = coul::C2 * g32 - coul::A2 * gb / 3.0;
+        double dz = 1.5 * coul::C2 * sg - coul::A2 * coul::B2 * gb / (3.0 * gam);
+        c.p = -pion * z;
+        c.dpdd = -(dpiondd * z + pion * dz * gdd);
+        c.dpdt = -(dpiondt * z + pion * dz * gdt);
+        c.e = 3.0 * c.p / den;
+        c.dedd = 3.0 * c.dpdd / den - 3.0 * c.p / (den * den);
+        c.dedt = 3.0 * c.dpdt / den;
+    }
+}
 
 // The electron-positron part plus radiation and ions at temperature temp,
 // eos.F90:195-518 (entropy, eta and xne are not formed: no hydro consumer).
@@ -200,8 +263,9 @@ struct EosConst {   // per-call constants of the Newton loop
 // (EOS_RE) reads -- skipping the density derivatives, the pressure-derivative
 // table and gamma_1; every quantity it does form is the full evaluation's,
 // operation for operation.
+// COUL adds the Coulomb corrections (full evaluations only).
 enum { EVAL_FULL = 0, EVAL_ENERGY_ONLY = 1 };
-template <int WHAT>
+template <int WHAT, bool COUL = false>
 __device__ __forceinline__ void eos_eval_part(double temp, const EosConst& K, const DensityBasis& B, EosEval& r)
 {
     constexpr bool FULL = WHAT == EVAL_FULL;
@@ -395,6 +459,19 @@ __device__ __forceinline__ void eos_eval_part(double temp, const EosConst& K, co
     double dpresdt = dpraddt + dpiondt + dpepdt;
     double denerdd = deraddd + deiondd + deepdd;
     double denerdt = deraddt + deiondt + deepdt;
+    if constexpr (COUL) {
+        static_assert(FULL, "the Coulomb corrections enter full evaluations");
+        CoulombTerms c;
+        coulomb_terms(den, temp, ytot1, K.zbar, pion, dpiondd, dpiondt, c);
+        if (pres + c.p > 0.0 && ener + c.e > 0.0) {   // kept only while the totals stay positive
+            pres = pres + c.p;
+            ener = ener + c.e;
+            dpresdd = dpresdd + c.dpdd;
+            dpresdt = dpresdt + c.dpdt;
+            denerdd = denerdd + c.dedd;
+            denerdt = denerdt + c.dedt;
+        }
+    }
 
     // :491-507
     double zz = pres * deni;
@@ -411,9 +488,10 @@ __device__ __forceinline__ void eos_eval_part(double temp, const EosConst& K, co
     r.dedr = denerdd;
 }
 
+template <bool COUL = false>
 __device__ __forceinline__ void eos_eval(double temp, const EosConst& K, const DensityBasis& B, EosEval& r)
 {
-    eos_eval_part<EVAL_FULL>(temp, K, B, r);
+    eos_eval_part<EVAL_FULL, COUL>(temp, K, B, r);
 }
 
 struct EosResult {
@@ -425,8 +503,12 @@ enum { EOS_RT = 1, EOS_RE = 2, EOS_RP = 3 };   // eos.F90:11-13
 // eos(input, state): the Newton inversion of eos.F90:181-574.  v_want is e for
 // EOS_RE and p for EOS_RP (ignored for EOS_RT).  OUTPUTS = false when the
 // caller reads only T (and the input e or p back): the evaluation after
-// convergence, which only forms the other outputs, is then not made.
-template <int MODE, bool OUTPUTS = true>
+// convergence, which only forms the other outputs, is then not made.  COUL:
+// with the Coulomb corrections -- a compile-time choice, so that the kernels
+// instantiated without them (the default) carry none of their code; every
+// kernel that calls the EOS is instantiated both ways and its launch picks
+// the instantiation from the library's setting (coulomb_on()).
+template <int MODE, bool COUL, bool OUTPUTS = true>
 __device__ __forceinline__ EosResult eos_solve(double rho, double T, double v_want, double abar, double zbar)
 {
     EosConst K;
@@ -435,6 +517,7 @@ __device__ __forceinline__ EosResult eos_solve(double rho, double T, double v_wa
     K.ye = zbar / abar;
     K.din = K.ye * rho;
     K.deni = 1.0 / rho;
+    K.zbar = zbar;
     DensityBasis B;
     density_basis(K.din, B);
 
@@ -451,14 +534,16 @@ __device__ __forceinline__ EosResult eos_solve(double rho, double T, double v_wa
         double temp = T;
         if (converged) {
             if (OUTPUTS) {
-                eos_eval(temp, K, B, r);
+                eos_eval<COUL>(temp, K, B, r);
                 full = true;
             }
             break;
         }
         temp_last = temp;
-        if (MODE == EOS_RE) eos_eval_part<EVAL_ENERGY_ONLY>(temp, K, B, r);
-        else eos_eval(temp, K, B, r);
+        // (with the Coulomb corrections, every iteration's evaluation is the
+        // full one: its e and de/dT are the light one's plus the corrections)
+        if (MODE == EOS_RE && !COUL) eos_eval_part<EVAL_ENERGY_ONLY>(temp, K, B, r);
+        else eos_eval<COUL>(temp, K, B, r);
         double temp_old = temp;
         double v = (MODE == EOS_RE) ? r.e : r.p;
         double dvdx = (MODE == EOS_RE) ? r.dedT : r.dpdT;
@@ -476,7 +561,7 @@ __device__ __forceinline__ EosResult eos_solve(double rho, double T, double v_wa
     }
     // ended by the iteration limit: the reference's outputs are those of the
     // last iteration's evaluation, here a light one
-    if (OUTPUTS && MODE == EOS_RE && !full) eos_eval(temp_last, K, B, r);
+    if (OUTPUTS && MODE == EOS_RE && !full) eos_eval<COUL>(temp_last, K, B, r);
     if (!converged && c_eos.fail_count) atomicAdd(c_eos.fail_count, 1ULL);
     EosResult o;
     o.T = T;
@@ -512,7 +597,7 @@ __device__ __forceinline__ void abar_zbar_cons(const double* u, double rhoInv, d
 // ---------------------------------------------------------------------------
 // State cleaning on one zone, Source/Castro_nd.F90:69-297
 // ---------------------------------------------------------------------------
-template <int NS>
+template <int NS, bool COUL>
 __device__ __forceinline__ void enforce_minimum_density_pt(double* u)
 {
     if (u[URHO] < small_dens) {                                        // :95-119
@@ -525,7 +610,7 @@ __device__ __forceinline__ void enforce_minimum_density_pt(double* u)
         for (int n = 0; n < NS; ++n) s2 = s2 + u[UFS + n] * c_net.zion[n] * c_net.aion_inv[n];
         double abar = 1.0 / (s1 / small_dens);
         double zbar = abar * (s2 / small_dens);
-        EosResult r = eos_solve<EOS_RT>(small_dens, small_temp, 0.0, abar, zbar);
+        EosResult r = eos_solve<EOS_RT, COUL>(small_dens, small_temp, 0.0, abar, zbar);
         u[URHO] = small_dens;
         u[UTEMP] = r.T;
         u[UMX] = 0.0;
@@ -549,7 +634,7 @@ __device__ __forceinline__ void normalize_species_pt(double* u)
     for (int n = 0; n < NS; ++n) u[UFS + n] = u[UFS + n] / sum;
 }
 
-template <int NS>
+template <int NS, bool COUL>
 __device__ __forceinline__ void reset_internal_e_pt(double* u)
 {
     double rhoInv = 1.0 / u[URHO];                                     // :196-244
@@ -561,7 +646,7 @@ __device__ __forceinline__ void reset_internal_e_pt(double* u)
         if (u[UEINT] < 0.0) {
             double abar, zbar;
             abar_zbar_cons<NS>(u, rhoInv, abar, zbar);
-            EosResult r = eos_solve<EOS_RT>(u[URHO], small_temp, 0.0, abar, zbar);
+            EosResult r = eos_solve<EOS_RT, COUL>(u[URHO], small_temp, 0.0, abar, zbar);
             u[UEINT] = u[URHO] * r.e;
         }
         u[UEDEN] = u[UEINT] + u[URHO] * ke;
@@ -572,41 +657,41 @@ __device__ __forceinline__ void reset_internal_e_pt(double* u)
         } else if (u[UEINT] <= 0.0) {
             double abar, zbar;
             abar_zbar_cons<NS>(u, rhoInv, abar, zbar);
-            EosResult r = eos_solve<EOS_RT>(u[URHO], small_temp, 0.0, abar, zbar);
+            EosResult r = eos_solve<EOS_RT, COUL>(u[URHO], small_temp, 0.0, abar, zbar);
             u[UEINT] = u[URHO] * r.e;
         }
     }
 }
 
-template <int NS>
+template <int NS, bool COUL>
 __device__ __forceinline__ void compute_temp_pt(double* u)
 {
     double rhoInv = 1.0 / u[URHO];                                     // :280-291
     double abar, zbar;
     abar_zbar_cons<NS>(u, rhoInv, abar, zbar);
-    EosResult r = eos_solve<EOS_RE, false>(u[URHO], u[UTEMP], u[UEINT] * rhoInv, abar, zbar);   // reads T only
+    EosResult r = eos_solve<EOS_RE, COUL, false>(u[URHO], u[UTEMP], u[UEINT] * rhoInv, abar, zbar);   // reads T only
     u[UTEMP] = r.T;
     u[UEINT] = u[URHO] * r.e;
 }
 
 // Castro::clean_state on one zone (Source/Castro.cpp:563-591)
-template <int NS>
+template <int NS, bool COUL>
 __device__ __forceinline__ void clean_state_pt(double* u)
 {
-    enforce_minimum_density_pt<NS>(u);
+    enforce_minimum_density_pt<NS, COUL>(u);
     normalize_species_pt<NS>(u);
-    reset_internal_e_pt<NS>(u);
-    compute_temp_pt<NS>(u);
+    reset_internal_e_pt<NS, COUL>(u);
+    compute_temp_pt<NS, COUL>(u);
 }
 
 // estdt on one zone, Source/timestep.F90:446-468: min over directions of dx/(c+|u|)
-template <int NS>
+template <int NS, bool COUL>
 __device__ __forceinline__ double estdt_pt(const double* u, double dx0, double dx1, double dx2)
 {
     double rhoInv = 1.0 / u[URHO];
     double abar, zbar;
     abar_zbar_cons<NS>(u, rhoInv, abar, zbar);
-    EosResult r = eos_solve<EOS_RE>(u[URHO], u[UTEMP], u[UEINT] * rhoInv, abar, zbar);
+    EosResult r = eos_solve<EOS_RE, COUL>(u[URHO], u[UTEMP], u[UEINT] * rhoInv, abar, zbar);
     double ux = u[UMX] * rhoInv;
     double uy = u[UMY] * rhoInv;
     double uz = u[UMZ] * rhoInv;
@@ -619,7 +704,7 @@ __device__ __forceinline__ double estdt_pt(const double* u, double dx0, double d
 
 // ctoprim on one zone, Source/Castro_hydro_nd.F90:115-164.  q is the full
 // QVAR record, qaux the NQAUX record.
-template <int NS>
+template <int NS, bool COUL>
 __device__ __forceinline__ void ctoprim_pt(const double* u, double* q, double* qaux)
 {
     q[QRHO] = u[URHO];
@@ -642,7 +727,7 @@ __device__ __forceinline__ void ctoprim_pt(const double* u, double* q, double* q
     for (int n = 0; n < NS; ++n) s2 = s2 + q[QFS + n] * c_net.zion[n] * c_net.aion_inv[n];
     double abar = 1.0 / s1;
     double zbar = abar * s2;
-    EosResult r = eos_solve<EOS_RE>(q[QRHO], q[QTEMP], q[QREINT], abar, zbar);
+    EosResult r = eos_solve<EOS_RE, COUL>(q[QRHO], q[QTEMP], q[QREINT], abar, zbar);
     q[QTEMP] = r.T;
     q[QREINT] = r.e * q[QRHO];
     q[QPRES] = r.p;

@@ -75,9 +75,10 @@ void default_network()
 {
     static const double a13[13] = {4., 12., 16., 20., 24., 28., 32., 36., 40., 44., 48., 52., 56.};
     static const double z13[13] = {2., 6., 8., 10., 12., 14., 16., 18., 20., 22., 24., 26., 28.};
-    const int mfp = g_net.mom_flux_p;   // an option, not part of the network
+    const int mfp = g_net.mom_flux_p, coul = g_net.coulomb;   // options, not part of the network
     memset(&g_net, 0, sizeof g_net);
     g_net.mom_flux_p = mfp;
+    g_net.coulomb = coul;
     g_net.nspec = 13;
     for (int n = 0; n < 13; ++n) {
         g_net.aion[n] = a13[n];
@@ -124,6 +125,7 @@ const NetworkDev& network_host()
     return g_net;
 }
 unsigned long long* eos_fail_counter() { return d_fail; }
+bool coulomb_on() { return g_net.coulomb != 0; }
 
 // the table's window on stream st (or no window, when it is switched off)
 void apply_table_l2_window(cudaStream_t st)
@@ -180,9 +182,10 @@ int castro_network_init(int ns, const double* aion, const double* zion)
         set_error(CASTRO_ERR_NSPEC, "castro_network_init: nspec must be 2 or 13");
         return CASTRO_ERR_NSPEC;
     }
-    const int mfp = g_net.mom_flux_p;   // an option, not part of the network
+    const int mfp = g_net.mom_flux_p, coul = g_net.coulomb;   // options, not part of the network
     memset(&g_net, 0, sizeof g_net);
     g_net.mom_flux_p = mfp;
+    g_net.coulomb = coul;
     g_net.nspec = ns;
     for (int n = 0; n < ns; ++n) {
         g_net.aion[n] = aion[n];
@@ -209,6 +212,16 @@ void castro_set_momentum_flux_pressure(int on)
 }
 
 int castro_momentum_flux_pressure(void) { return g_net.mom_flux_p; }
+
+void castro_set_coulomb_corrections(int on)
+{
+    g_net.coulomb = on != 0;
+    if (!g_table) return;   // uploaded with the table
+    cudaDeviceSynchronize();   // queued kernels finish under the old value
+    upload_all();
+}
+
+int castro_coulomb_corrections(void) { return g_net.coulomb; }
 
 int castro_eos_init_path(const char* path)
 {

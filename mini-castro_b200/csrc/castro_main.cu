@@ -13,6 +13,9 @@
 //   momentum_flux_pressure=0|1 (1: the interface pressure in the normal
 //                              momentum flux, as full Castro has it; the
 //                              reference, and the default, have none)
+//   use_eos_coulomb=0|1        (1: Coulomb corrections in the EOS, as the
+//                              reference's 2017 runs had them; its eos.F90,
+//                              and the default, have none)
 // and prints the reference's progress lines and figure of merit.
 #include <stdio.h>
 #include <stdlib.h>
@@ -51,7 +54,8 @@ void usage()
     printf("B200 additions: problem=reference|sedov nspec=13|2 bc=periodic|outflow\n"
            "               mode=batched|persistent|plain|plain_box table=<path>\n"
            "               plot_file=<dir> (AMReX plotfile of the final state)\n"
-           "               momentum_flux_pressure=0|1 (1: pressure in the momentum flux, as full Castro)\n\n");
+           "               momentum_flux_pressure=0|1 (1: pressure in the momentum flux, as full Castro)\n"
+           "               use_eos_coulomb=0|1 (1: Coulomb corrections in the EOS)\n\n");
 }
 
 }  // namespace
@@ -102,6 +106,7 @@ extern "C" int castro_main(int argc, char** argv)
         castro_network_init(2, a, z);
     }
     castro_set_momentum_flux_pressure((int)geti("momentum_flux_pressure", 0));
+    castro_set_coulomb_corrections((int)geti("use_eos_coulomb", 0));
     std::string table = gets("table", getenv("CASTRO_HELM_TABLE") ? getenv("CASTRO_HELM_TABLE") : "helm_table.dat");
     if (castro_eos_init_path(table.c_str()) != CASTRO_OK) {
         fprintf(stderr, "eos_init: %s\n", castro_error_string());

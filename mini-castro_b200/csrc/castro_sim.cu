@@ -301,7 +301,7 @@ __device__ __forceinline__ double block_min(double m)
 // ---------------------------------------------------------------------------
 
 // front: clean_state(S_old) -> S_new base; clean_state(Sborder); ctoprim
-template <int NS>
+template <int NS, bool COUL>
 __device__ __forceinline__ void front_body(const SimDev& S, const Work& w)
 {
     int b, sub, i, j, k;
@@ -314,10 +314,10 @@ __device__ __forceinline__ void front_body(const SimDev& S, const Work& w)
     long long id = ridx(R, i, j, k);
 #pragma unroll
     for (int n = 0; n < NVAR; ++n) u[n] = U[id + R.np * n];
-    clean_state_pt<NS>(u);                          // Castro_advance.cpp:51
+    clean_state_pt<NS, COUL>(u);                    // Castro_advance.cpp:51
 #pragma unroll
     for (int n = 0; n < NVAR; ++n) U[id + R.np * n] = u[n];
-    clean_state_pt<NS>(u);                          // Castro_advance.cpp:66 (valid part of Sborder)
+    clean_state_pt<NS, COUL>(u);                    // Castro_advance.cpp:66 (valid part of Sborder)
     const InstDev& I = S.inst[B.inst];
     const Reg R1 = u_region(I);
     double* Ub = S.Ub + B.offUb;
@@ -325,7 +325,7 @@ __device__ __forceinline__ void front_body(const SimDev& S, const Work& w)
 #pragma unroll
     for (int n = 0; n < NVAR; ++n) Ub[id1 + R1.np * n] = u[n];
     double q[QVAR], qa[NQAUX];
-    ctoprim_pt<NS>(u, q, qa);                       // Castro_hydro.cpp:64-70
+    ctoprim_pt<NS, COUL>(u, q, qa);                 // Castro_hydro.cpp:64-70
     const Reg R4 = q_region(I);
     double* Q = S.Q + B.offQ;
     long long id4 = ridx(R4, i, j, k);
@@ -342,10 +342,10 @@ __device__ __forceinline__ void front_body(const SimDev& S, const Work& w)
     Q[id4 + R4.np * F::C] = qa[QC];
 }
 
-template <int NS>
+template <int NS, bool COUL>
 __global__ void LB_EOS k_front(SimDev S, const Work* wl)
 {
-    front_body<NS>(S, wl[blockIdx.x]);
+    front_body<NS, COUL>(S, wl[blockIdx.x]);
 }
 
 __device__ __forceinline__ int map_bc(int i, int lo, int hi, int bc)
@@ -1038,7 +1038,7 @@ __global__ void LB_R3 k_riemann3(SimDev S, const Work* wl)
 
 // update: fill_hydro_source, Saxpy, clean_state (advance), clean_state
 // (post_timestep), estdt of the new state
-template <int NS>
+template <int NS, bool COUL>
 __device__ __forceinline__ void update_body(const SimDev& S, const Work& w)
 {
     int b, sub, i, j, k;
@@ -1086,25 +1086,25 @@ __device__ __forceinline__ void update_body(const SimDev& S, const Work& w)
             }
             u[n] = un + dt * src;                        // MultiFab::Saxpy, Castro_advance.cpp:74
         }
-        clean_state_pt<NS>(u);                           // Castro_advance.cpp:78
-        clean_state_pt<NS>(u);                           // Castro.cpp:369
+        clean_state_pt<NS, COUL>(u);                     // Castro_advance.cpp:78
+        clean_state_pt<NS, COUL>(u);                     // Castro.cpp:369
 #pragma unroll
         for (int n = 0; n < NVAR; ++n) U[id + R.np * n] = u[n];
-        m = estdt_pt<NS>(u, I.dx[0], I.dx[1], I.dx[2]);  // Castro.cpp:191-203 of the next coarse step
+        m = estdt_pt<NS, COUL>(u, I.dx[0], I.dx[1], I.dx[2]);   // Castro.cpp:191-203 of the next coarse step
     }
     // one box per block: the block reduction has a single instance target
     m = block_min(m);
     if (threadIdx.x == 0) atomic_min_pos(&S.st[B.inst].dt_est, m);
 }
 
-template <int NS>
+template <int NS, bool COUL>
 __global__ void LB_EOS k_update(SimDev S, const Work* wl)
 {
-    update_body<NS>(S, wl[blockIdx.x]);
+    update_body<NS, COUL>(S, wl[blockIdx.x]);
 }
 
 // estdt on the current state (computeInitialDt / castro_sim_est_time_step)
-template <int NS>
+template <int NS, bool COUL>
 __device__ __forceinline__ void estdt_state_body(const SimDev& S, const Work& w)
 {
     int b, sub, i, j, k;
@@ -1120,16 +1120,16 @@ __device__ __forceinline__ void estdt_state_body(const SimDev& S, const Work& w)
         double u[NVAR];
 #pragma unroll
         for (int n = 0; n < NVAR; ++n) u[n] = U[id + R.np * n];
-        m = estdt_pt<NS>(u, I.dx[0], I.dx[1], I.dx[2]);
+        m = estdt_pt<NS, COUL>(u, I.dx[0], I.dx[1], I.dx[2]);
     }
     m = block_min(m);
     if (threadIdx.x == 0) atomic_min_pos(&S.st[B.inst].dt_est, m);
 }
 
-template <int NS>
+template <int NS, bool COUL>
 __global__ void __launch_bounds__(BLOCK) k_estdt_state(SimDev S, const Work* wl)
 {
-    estdt_state_body<NS>(S, wl[blockIdx.x]);
+    estdt_state_body<NS, COUL>(S, wl[blockIdx.x]);
 }
 
 // computeInitialDt (DT_FIRST) or, after a step, time/step bookkeeping and
@@ -1252,11 +1252,11 @@ __device__ __forceinline__ bool persist_barrier(const PersistArgs& P, int st)
     return s_ok != 0;
 }
 
-template <int NS>
+template <int NS, bool COUL>
 __device__ __forceinline__ void persist_item(const SimDev& S, const SimDev& Sd, const PersistArgs& P, int st, int item)
 {
     switch (st) {
-    case PS_FRONT: front_body<NS>(S, P.wl[PS_FRONT][item]); break;
+    case PS_FRONT: front_body<NS, COUL>(S, P.wl[PS_FRONT][item]); break;
     case PS_GHOST: ghost_body<NS>(S, P.wl[PS_GHOST][item]); break;
     case PS_PREP: prep_body<NS>(Sd, P.wl[PS_PREP][item]); break;
     case PS_TRACE:
@@ -1267,11 +1267,11 @@ __device__ __forceinline__ void persist_item(const SimDev& S, const SimDev& Sd, 
     case PS_R1: riemann1_body<NS>(Sd, P.wl[PS_R1][item]); break;
     case PS_R2: riemann2_body<NS>(Sd, P.wl[PS_R2][item]); break;
     case PS_R3: riemann3_body<NS>(Sd, P.wl[PS_R3][item]); break;
-    default: update_body<NS>(S, P.wl[PS_UPDATE][item]); break;
+    default: update_body<NS, COUL>(S, P.wl[PS_UPDATE][item]); break;
     }
 }
 
-template <int NS>
+template <int NS, bool COUL>
 __global__ void LB_PERSIST k_step_persistent(SimDev S, PersistArgs P)
 {
     __shared__ int s_item;
@@ -1285,7 +1285,7 @@ __global__ void LB_PERSIST k_step_persistent(SimDev S, PersistArgs P)
             const int item = s_item;
             __syncthreads();                               // every thread has the item before the slot is reused
             if (item >= n) break;
-            persist_item<NS>(S, Sd, P, st, item);
+            persist_item<NS, COUL>(S, Sd, P, st, item);
         }
         if (st + 1 < PS_COUNT && !persist_barrier(P, st)) return;
     }
@@ -1329,7 +1329,7 @@ __global__ void __launch_bounds__(BLOCK) k_fill_sborder(SimDev S, int b, double*
 
 // primitive variables straight from a caller's Sborder over grow(bx,4)
 // (construct_hydro_source's ctoprim, Source/Castro_hydro.cpp:64-70)
-template <int NS>
+template <int NS, bool COUL>
 __global__ void __launch_bounds__(BLOCK) k_box_prim(SimDev S, const Work* wl, Fab SB)
 {
     const Work& w = wl[blockIdx.x];
@@ -1341,7 +1341,7 @@ __global__ void __launch_bounds__(BLOCK) k_box_prim(SimDev S, const Work* wl, Fa
     double u[NVAR], q[QVAR], qa[NQAUX];
 #pragma unroll
     for (int n = 0; n < NVAR; ++n) u[n] = SB(i, j, k, n);
-    ctoprim_pt<NS>(u, q, qa);
+    ctoprim_pt<NS, COUL>(u, q, qa);
     const InstDev& I = S.inst[B.inst];
     const Reg RQ = q_region(I);   // grow(bx,4): the instance domain is the box here
     double* Q = S.Q + B.offQ;
@@ -1484,6 +1484,7 @@ struct castro_sim {
     bool dt_ready = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
+    bool graph_coul = false;   // the Coulomb setting the captured step's EOS kernels were instantiated for
     int launches = 0;
     // EOS Newton non-convergences (library-wide counter) already reported
     // through castro_last_error when this sim last synchronized
@@ -1630,12 +1631,20 @@ void build_ghost_work(castro_sim* s)
         cuda_ok(cudaMemcpy(s->w_ghost, w.data(), w.size() * sizeof(Work), cudaMemcpyHostToDevice), "ghost work list copy");
 }
 
+// Launch of a kernel that calls the EOS: the instantiation with or without the
+// Coulomb corrections, as the library is set (castro_set_coulomb_corrections).
+#define CASTRO_EOS_LAUNCH(K, NS, GRID, BLK, SMEM, ST, ...)                         \
+    do {                                                                           \
+        if (coulomb_on()) K<NS, true><<<GRID, BLK, SMEM, ST>>>(__VA_ARGS__);        \
+        else K<NS, false><<<GRID, BLK, SMEM, ST>>>(__VA_ARGS__);                     \
+    } while (0)
+
 template <int NS>
 void batched_step_kernels(castro_sim* s)
 {
     SimDev S = s->dev(), Sd = s->dev_dom();
     cudaStream_t st = s->st;
-    k_front<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid);
+    CASTRO_EOS_LAUNCH(k_front, NS, s->n_valid, BLOCK, 0, st, S, s->w_valid);
     k_ghost<NS><<<s->n_ghost, BLOCK, 0, st>>>(S, s->w_ghost);
     k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(Sd, s->w_g1);
     if (CASTRO_TRACE_SPLIT) {
@@ -1652,7 +1661,7 @@ void batched_step_kernels(castro_sim* s)
     k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(Sd, s->w_tbx);
     k_riemann2<NS><<<s->n_r2, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_r2);
     k_riemann3<NS><<<s->n_r3, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_r3);
-    k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid);
+    CASTRO_EOS_LAUNCH(k_update, NS, s->n_valid, BLOCK, 0, st, S, s->w_valid);
     k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0);
 }
 
@@ -1666,7 +1675,7 @@ void profile_kernel(castro_sim* s, const SimDev& S, int k)
     SimDev Sd = S;
     Sd.boxes = S.dom;
     switch (k) {
-    case 0: k_front<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid); break;
+    case 0: CASTRO_EOS_LAUNCH(k_front, NS, s->n_valid, BLOCK, 0, st, S, s->w_valid); break;
     case 1: k_ghost<NS><<<s->n_ghost, BLOCK, 0, st>>>(S, s->w_ghost); break;
     case 2: k_prep<NS><<<s->n_g1, BLOCK, 0, st>>>(Sd, s->w_g1); break;
     case 3: k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace); break;
@@ -1674,7 +1683,7 @@ void profile_kernel(castro_sim* s, const SimDev& S, int k)
     case 4: k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(Sd, s->w_tbx); break;
     case 5: k_riemann2<NS><<<s->n_r2, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_r2); break;
     case 6: k_riemann3<NS><<<s->n_r3, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_r3); break;
-    case 7: k_update<NS><<<s->n_valid, BLOCK, 0, st>>>(S, s->w_valid); break;
+    case 7: CASTRO_EOS_LAUNCH(k_update, NS, s->n_valid, BLOCK, 0, st, S, s->w_valid); break;
     default: k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0); break;
     }
 }
@@ -1683,7 +1692,7 @@ template <int NS>
 void initial_dt_kernels(castro_sim* s)
 {
     SimDev S = s->dev();
-    k_estdt_state<NS><<<s->n_valid, BLOCK, 0, s->st>>>(S, s->w_valid);
+    CASTRO_EOS_LAUNCH(k_estdt_state, NS, s->n_valid, BLOCK, 0, s->st, S, s->w_valid);
     k_dt<<<(s->ninst + 63) / 64, 64, 0, s->st>>>(S, s->ninst, 1);
 }
 
@@ -1977,15 +1986,23 @@ bool persistent_setup(castro_sim* s)
     P.test_stage = -1;
     s->psmem = std::max((size_t)R2Slot<NS>::BYTES, (size_t)R3Slot<NS>::BYTES);
     if (s->psmem > 48 * 1024 &&
-        !cuda_ok(cudaFuncSetAttribute(k_step_persistent<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->psmem),
-                 "persistent step shared memory"))
+        (!cuda_ok(cudaFuncSetAttribute(k_step_persistent<NS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)s->psmem), "persistent step shared memory") ||
+         !cuda_ok(cudaFuncSetAttribute(k_step_persistent<NS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)s->psmem), "persistent step shared memory")))
         return false;
-    int dev = 0, nsm = 0, coop = 0, per_sm = 0;
+    // the grid is co-resident for both instantiations (with and without the
+    // Coulomb corrections): the smaller of their occupancies
+    int dev = 0, nsm = 0, coop = 0, per_sm = 0, per_sm_c = 0;
     if (!cuda_ok(cudaGetDevice(&dev), "device") ||
         !cuda_ok(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev), "SM count") ||
         !cuda_ok(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "cooperative launch") ||
-        !cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_persistent<NS>, BLOCK, s->psmem), "occupancy"))
+        !cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_persistent<NS, false>, BLOCK, s->psmem),
+                 "occupancy") ||
+        !cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_c, k_step_persistent<NS, true>, BLOCK, s->psmem),
+                 "occupancy"))
         return false;
+    per_sm = std::min(per_sm, per_sm_c);
     if (!coop || per_sm < 1) {
         set_error(CASTRO_ERR_CUDA, "castro_sim_create: the device cannot run the persistent step (no cooperative launch)");
         return false;
@@ -2001,8 +2018,8 @@ void persistent_launch(castro_sim* s)
     PersistArgs P = s->pargs;
     void* args[] = {&S, &P};
     cuda_ok(cudaMemsetAsync(s->pctl, 0, sizeof(PersistCtl), s->st), "persistent queue reset");
-    cuda_ok(cudaLaunchCooperativeKernel((const void*)k_step_persistent<NS>, dim3(s->pgrid), dim3(BLOCK), args, s->psmem,
-                                        s->st),
+    const void* kern = coulomb_on() ? (const void*)k_step_persistent<NS, true> : (const void*)k_step_persistent<NS, false>;
+    cuda_ok(cudaLaunchCooperativeKernel(kern, dim3(s->pgrid), dim3(BLOCK), args, s->psmem, s->st),
             "persistent step launch");
 }
 
@@ -2026,6 +2043,7 @@ int persistent_step(castro_sim* s)
         if (ok) {
             s->graph = g;
             s->gexec = ge;
+            s->graph_coul = coulomb_on();
         } else {
             if (ge) cudaGraphExecDestroy(ge);
             if (g) cudaGraphDestroy(g);
@@ -2056,12 +2074,20 @@ int step_impl(castro_sim* s)
         initial_dt_kernels<NS>(s);
         s->dt_ready = true;
     }
+    if (s->gexec && s->graph_coul != coulomb_on()) {
+        // the Coulomb setting changed since the step was captured: capture again
+        cudaGraphExecDestroy(s->gexec);
+        cudaGraphDestroy(s->graph);
+        s->gexec = nullptr;
+        s->graph = nullptr;
+    }
     if (s->mode == CASTRO_MODE_PERSISTENT) return persistent_step<NS>(s);
     if (!s->gexec) {
         if (!cuda_ok(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal), "begin capture")) return castro_last_error();
         batched_step_kernels<NS>(s);
         if (!cuda_ok(cudaStreamEndCapture(s->st, &s->graph), "end capture")) return castro_last_error();
         if (!cuda_ok(cudaGraphInstantiate(&s->gexec, s->graph, 0), "graph instantiate")) return castro_last_error();
+        s->graph_coul = coulomb_on();
     }
     cuda_ok(cudaGraphLaunch(s->gexec, s->st), "graph launch");
     s->launches = 9 + (CASTRO_TRACE_SPLIT ? 1 : 0);
@@ -2623,7 +2649,7 @@ template <int NS>
 void restart_dt_kernels(castro_sim* s)
 {
     SimDev S = s->dev();
-    k_estdt_state<NS><<<s->n_valid, BLOCK, 0, s->st>>>(S, s->w_valid);
+    CASTRO_EOS_LAUNCH(k_estdt_state, NS, s->n_valid, BLOCK, 0, s->st, S, s->w_valid);
     k_dt<<<(s->ninst + 63) / 64, 64, 0, s->st>>>(S, s->ninst, DT_RESTART);
 }
 
@@ -2915,7 +2941,7 @@ int box_hydro_launch(const BoxPlan& P, double* base, long long meta_doubles, con
     S.boxes = dB; S.dom = dB; S.inst = dI; S.st = dS;   // the box is the instance domain
     S.Ub = pools; S.Q = pools; S.Div = pools; S.Tr = pools; S.F1 = pools; S.F2 = pools; S.Fx = pools;
     const Work* W = work;
-    k_box_prim<NS><<<nblocks[NL_G4], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G4], make_fab(sb, sb_lo, sb_hi));
+    CASTRO_EOS_LAUNCH(k_box_prim, NS, nblocks[NL_G4], BLOCK, 0, cs, S, W + NLs.first[NL_G4], make_fab(sb, sb_lo, sb_hi));
     k_prep<NS><<<nblocks[NL_G1], BLOCK, 0, cs>>>(S, W + NLs.first[NL_G1]);
     k_trace<NS><<<nblocks[NL_TRACE], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TRACE]);
     if (CASTRO_TRACE_SPLIT) k_trace2<NS><<<nblocks[NL_TRACE], BLOCK, 0, cs>>>(S, W + NLs.first[NL_TRACE]);

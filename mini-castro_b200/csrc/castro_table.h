@@ -118,6 +118,7 @@ inline int read_helm_table(const char* path, HostTable& T)
     c.asoli3 = asol / 3.0;
     c.kergavo = kerg * avo_eos;
     c.avo_eos = avo_eos;
+    c.kerg = kerg;
     c.sioncon = (2.0 * M_PI * amu * kerg) / (h * h);
     c.fail_count = nullptr;
     return 0;

@@ -21,11 +21,14 @@
 #include <float.h>
 #ifdef _OPENMP
 #include <omp.h>
+#endif
 
 /* the interface pressure in the normal momentum flux: off, as in the reference
  * (see oracle_set_momentum_flux_pressure) */
-static int g_mom_flux_p = 0;   /* see oracle_set_momentum_flux_pressure */
-#endif
+static int g_mom_flux_p = 0;
+/* Coulomb corrections in the EOS: off, as in the reference (see
+ * oracle_set_coulomb_corrections) */
+static int g_coulomb = 0;
 
 /* ------------------------------------------------------------------------ */
 /* Index maps, Source/Castro_nd.F90:14-57 (0-based)                          */
@@ -317,6 +320,68 @@ static inline void fill4(double* fi, const double* a, int iat, int jat)
     fi[3] = TB(a, iat + 1, jat + 1);
 }
 
+/* Coulomb corrections of an ion plasma in a uniform electron background
+ * (absent from the reference's eos.F90; the 2017 runs of the reference had
+ * them on): the fits of Yakovlev & Shalybkov (1989, Sov. Sci. Rev. E Astrophys.
+ * Space Phys. 7, 311), as the Helmholtz EOS (Timmes & Swesty 2000, ApJS 126,
+ * 501) applies them.  With n_i = N_A rho / abar the ion density, a =
+ * (3 / (4 pi n_i))^(1/3) the ion-sphere radius and Gamma = zbar^2 q_e^2 / (a k T)
+ * the coupling parameter, the excess internal energy per ion in kT is
+ *   Gamma >= 1:  u = a1 Gamma + b1 Gamma^(1/4) + c1 Gamma^(-1/4) + d1
+ *   Gamma <  1:  u = -3 c2 Gamma^(3/2) + a2 Gamma^b2   (c2 = 1/(2 sqrt 3): Debye-Hueckel)
+ * and, the excess pressure of a Coulomb system being a third of its energy
+ * density, p = rho e / 3.  The entropy is u - f with f the excess free energy
+ * (f' = u / Gamma), the strong branch's integration constant -e1.  Gamma goes
+ * as rho^(1/3) / T, which gives the derivatives. */
+static const double COUL_QE = 4.80320427e-10;                      /* electron charge, esu */
+static const double COUL_A1 = -0.898004, COUL_B1 = 0.96786, COUL_C1 = 0.220703, COUL_D1 = -0.86097,
+                    COUL_E1 = 2.5269, COUL_A2 = 0.29561, COUL_B2 = 1.9885, COUL_C2 = 0.288675;
+
+typedef struct { double p, dpdd, dpdt, e, dedd, dedt, s, dsdd, dsdt; } coulomb_t;
+
+static void coulomb(double den, double temp, double ytot1, double zbar, double pion, double dpiondd,
+                    double dpiondt, coulomb_t* c)
+{
+    double xni = avo_eos * ytot1 * den;
+    double a_ion = cbrt(3.0 / (4.0 * M_PI * xni));
+    double gam = zbar * zbar * COUL_QE * COUL_QE / (a_ion * kerg * temp);
+    double gdd = gam / (3.0 * den);                 /* dGamma/drho */
+    double gdt = -gam / temp;                       /* dGamma/dT */
+    double y = kergavo * ytot1;                     /* k N_A / abar */
+    if (gam >= 1.0) {
+        double x = sqrt(sqrt(gam));
+        double u = COUL_A1 * gam + COUL_B1 * x + COUL_C1 / x + COUL_D1;
+        double du = COUL_A1 + 0.25 * (COUL_B1 * x - COUL_C1 / x) / gam;
+        c->e = y * temp * u;
+        c->dedd = y * temp * du * gdd;
+        c->dedt = y * u + y * temp * du * gdt;
+        c->p = den * c->e / 3.0;
+        c->dpdd = (c->e + den * c->dedd) / 3.0;
+        c->dpdt = den * c->dedt / 3.0;
+        double sv = 3.0 * COUL_B1 * x - 5.0 * COUL_C1 / x + COUL_D1 * (log(gam) - 1.0) - COUL_E1;
+        double dsv = (0.75 * COUL_B1 * x + 1.25 * COUL_C1 / x + COUL_D1) / gam;
+        c->s = -y * sv;
+        c->dsdd = -y * dsv * gdd;
+        c->dsdt = -y * dsv * gdt;
+    } else {
+        double g32 = gam * sqrt(gam);
+        double gb = pow(gam, COUL_B2);
+        double z = COUL_C2 * g32 - COUL_A2 * gb / 3.0;
+        double dz = 1.5 * COUL_C2 * sqrt(gam) - COUL_A2 * COUL_B2 * gb / (3.0 * gam);
+        c->p = -pion * z;
+        c->dpdd = -(dpiondd * z + pion * dz * gdd);
+        c->dpdt = -(dpiondt * z + pion * dz * gdt);
+        c->e = 3.0 * c->p / den;
+        c->dedd = 3.0 * c->dpdd / den - 3.0 * c->p / (den * den);
+        c->dedt = 3.0 * c->dpdt / den;
+        double sv = COUL_C2 * g32 - COUL_A2 * (COUL_B2 - 1.0) / COUL_B2 * gb;
+        double dsv = 1.5 * COUL_C2 * sqrt(gam) - COUL_A2 * (COUL_B2 - 1.0) * gb / gam;
+        c->s = -y * sv;
+        c->dsdd = -y * dsv * gdd;
+        c->dsdt = -y * dsv * gdt;
+    }
+}
+
 /* eos, Source/eos.F90:141-576 */
 void oracle_eos(int input, oracle_eos_t* state)
 {
@@ -562,6 +627,23 @@ void oracle_eos(int input, oracle_eos_t* state)
         denerdt = deraddt + deiondt + deepdt;
         dentrdd = dsraddd + dsiondd + dsepdd;
         dentrdt = dsraddt + dsiondt + dsepdt;
+
+        if (g_coulomb) {
+            coulomb_t c;
+            coulomb(den, temp, ytot1, state->zbar, pion, dpiondd, dpiondt, &c);
+            /* kept only while the totals stay positive */
+            if (pres + c.p > 0.0 && ener + c.e > 0.0) {
+                pres = pres + c.p;
+                ener = ener + c.e;
+                entr = entr + c.s;
+                dpresdd = dpresdd + c.dpdd;
+                dpresdt = dpresdt + c.dpdt;
+                denerdd = denerdd + c.dedd;
+                denerdt = denerdt + c.dedt;
+                dentrdd = dentrdd + c.dsdd;
+                dentrdt = dentrdt + c.dsdt;
+            }
+        }
 
         /* :491-518 */
         zz = pres * deni;
@@ -1573,6 +1655,11 @@ void oracle_set_problem(const oracle_prob_t* p) { prob = *p; }
  * else adds a pressure gradient to the momentum (consup adds only p div u to
  * rho e, Source/Castro_hydro_nd.F90:425-434). */
 void oracle_set_momentum_flux_pressure(int on) { g_mom_flux_p = on; }
+
+/* Option (off by default, as in the reference): the EOS with the Coulomb
+ * corrections above, as the reference's 2017 runs used them
+ * (scaling/summitdev_20171020/1.out:14). */
+void oracle_set_coulomb_corrections(int on) { g_coulomb = on; }
 
 void oracle_initdata(const int* lo, const int* hi, double* up, const int* u_lo, const int* u_hi,
                      const double* dx, const double* problo, const double* probhi)

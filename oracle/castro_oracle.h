@@ -65,6 +65,8 @@ void oracle_eos(int input, oracle_eos_t* state);
 void oracle_set_problem(const oracle_prob_t* prob);
 /* the interface pressure in the normal momentum flux (off by default, as in the reference) */
 void oracle_set_momentum_flux_pressure(int on);
+/* Coulomb corrections in the EOS (off by default, as in the reference's eos.F90) */
+void oracle_set_coulomb_corrections(int on);
 
 /* Source/Castro_F.H entry points, same argument order and meaning. */
 void oracle_ctoprim(const int* lo, const int* hi,

@@ -6,7 +6,7 @@
  * unchanged as C++ with `double` replaced by CountedDouble, a one-member
  * struct whose operators do the same IEEE double operation and bump a
  * per-thread counter by class: add (and subtract), mul, div, sqrt,
- * transcendental (log, log10, exp, pow), compare (<, >, ==, ... and so every
+ * transcendental (log, log10, exp, pow, cbrt), compare (<, >, ==, ... and so every
  * max/min), and sign operations (fabs, copysign).  Built with
  * -ffp-contract=off like the parity build, so a*b+c stays a multiply and an
  * add and the results are bit for bit the parity build's (the operators only
@@ -100,6 +100,8 @@ inline CD log10(CD x) { opcount::bump(opcount::TRANSC); return CD(std::log10(x.v
 inline CD exp(CD x) { opcount::bump(opcount::TRANSC); return CD(std::exp(x.v)); }
 inline CD pow(CD x, CD y) { opcount::bump(opcount::TRANSC); return CD(std::pow(x.v, y.v)); }
 inline CD pow(double x, CD y) { return pow(CD(x), y); }
+inline CD pow(CD x, double y) { return pow(x, CD(y)); }
+inline CD cbrt(CD x) { opcount::bump(opcount::TRANSC); return CD(std::cbrt(x.v)); }
 inline CD fabs(CD x) { opcount::bump(opcount::SIGN); return CD(std::fabs(x.v)); }
 inline CD copysign(CD x, CD y) { opcount::bump(opcount::SIGN); return CD(std::copysign(x.v, y.v)); }
 inline CD copysign(double x, CD y) { return copysign(CD(x), y); }

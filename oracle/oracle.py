@@ -87,6 +87,8 @@ def _bind(L):
     L.oracle_eos.argtypes = [C.c_int, C.POINTER(EosT)]
     L.oracle_set_problem.argtypes = [C.POINTER(ProbT)]
     L.oracle_set_momentum_flux_pressure.argtypes = [C.c_int]
+    L.oracle_set_coulomb_corrections.restype = None
+    L.oracle_set_coulomb_corrections.argtypes = [C.c_int]
     L.oracle_level_create.restype = C.c_void_p
     L.oracle_level_create.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _dp, _dp, C.c_int]
     L.oracle_level_destroy.argtypes = [C.c_void_p]
@@ -153,17 +155,22 @@ def set_momentum_flux_pressure(on: bool, variant: str = "parity"):
     lib(variant).oracle_set_momentum_flux_pressure(1 if on else 0)
 
 
+def set_coulomb_corrections(on: bool, variant: str = "parity"):
+    """Coulomb corrections in the EOS (off, as in the reference's eos.F90)."""
+    lib(variant).oracle_set_coulomb_corrections(1 if on else 0)
+
+
 def eos_init(path: str, variant: str = "parity"):
     rc = lib(variant).oracle_eos_init(path.encode())
     if rc != 0:
         raise RuntimeError(f"oracle_eos_init({path}) failed: {rc}")
 
 
-def eos(mode: int, **fields) -> EosT:
+def eos(mode: int, variant: str = "parity", **fields) -> EosT:
     st = EosT()
     for k, v in fields.items():
         setattr(st, k, float(v))
-    lib().oracle_eos(mode, C.byref(st))
+    lib(variant).oracle_eos(mode, C.byref(st))
     return st
 
 
