@@ -102,8 +102,11 @@ int  castro_momentum_flux_pressure(void);
  * derivatives wherever the EOS is evaluated, unless the totals would turn
  * non-positive there.  The forward paths only: the adjoint (castro_adj_*, the
  * *_adj routines that call the EOS) refuses to run with it (CASTRO_ERR_ARG).
- * The call waits for the kernels already queued on the device.  The oracle's
- * oracle_set_coulomb_corrections is its counterpart. */
+ * The call waits for the kernels already queued on the device.  Each launch
+ * reads the setting (a sim captures its step again when it changed); a CUDA
+ * graph a caller captured around the per-box entry points keeps the setting it
+ * was captured with.  The oracle's oracle_set_coulomb_corrections is its
+ * counterpart. */
 void castro_set_coulomb_corrections(int on);
 int  castro_coulomb_corrections(void);
 
