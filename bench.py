@@ -143,7 +143,7 @@ def kernel_bytes(cfg, nspec):
     the BoxArray; ghost fills each instance's domain halo; prep, trace and the
     three Riemann kernels walk each instance's domain as one region."""
     NV, NQF, NQS, NTF = 7 + nspec, 8 + nspec, 6 + nspec, 7 + nspec
-    tot = dict(front=0, ghost=0, trace=0, trace2=0, riemann1=0, riemann2=0, riemann3=0, update=0)
+    tot = dict(front=0, ghost=0, trace=0, trace2=0, riemann1=0, riemann2=0, riemann3=0, riemann23=0, update=0)
 
     def regions(n):
         v = n[0] * n[1] * n[2]
@@ -180,6 +180,8 @@ def kernel_bytes(cfg, nspec):
         # one thread per face of tbx[a][a] reads its two trace states once for both cross fluxes
         tot["riemann2"] += 8 * (tdd * 2 * NQS + tdd * NTF + g4d * 2 + tab * NTF)
         tot["riemann3"] += 8 * (eb * 2 * NQS + tab * NTF + g1d * NV + g1d + g4d * 2 + eb * (NV + 1))
+        # riemann2 + riemann3 per column tile: the cross-flux records stay in shared memory
+        tot["riemann23"] += 8 * (tdd * 2 * NQS + tdd * NTF + g4d * 2 + g1d * NV + g1d + eb * (NV + 1))
         tot["update"] += 8 * eb * (NV + 1)   # every final-flux record of the domain read once
         for lo, hi in inst["boxes"]:
             v = regions([h - l + 1 for l, h in zip(lo, hi)])[0]
@@ -305,6 +307,19 @@ def run_b200(args, pkg, rank, world):
         plain_box = time_per_box(pkg.castro.MODE_PLAIN_BOX)
     if rank == 0 and args.persistent_steps > 0:
         persistent = time_mode(pkg, L, cfg, pkg.castro.MODE_PERSISTENT, args.persistent_steps, zones)
+    column_tiles = None
+    if rank == 0 and args.column_tile_steps > 0 and nspec == 2:
+        # riemann2 + riemann3 as one column-tile kernel with the cross fluxes in shared memory (opt-in)
+        L.castro_set_column_tiles(1)
+        try:
+            column_tiles = time_mode(pkg, L, cfg, pkg.castro.MODE_BATCHED, args.column_tile_steps, zones)
+            sim_ct = pkg.make_sim(L, cfg, pkg.castro.MODE_BATCHED)
+            sim_ct.init_data()
+            sim_ct.step(2)
+            column_tiles["kernel_ms"] = sim_ct.profile_step()
+            sim_ct.close()
+        finally:
+            L.castro_set_column_tiles(0)
 
     batched_cfg = None
     if args.batched_steps > 0:      # every rank: the instances are split over the ranks
@@ -426,6 +441,7 @@ def run_b200(args, pkg, rank, world):
         "plain_per_box": plain,
         "plain_box_drop_in": plain_box,
         "persistent": persistent,
+        "column_tiles": column_tiles,
         "batched_config": batched_cfg,
         "fd_table": fd_leg,
         "large_config": large_cfg,
@@ -749,6 +765,8 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--batched-steps", type=int, default=18, help="timed steps of the batched configuration (0: skip)")
     ap.add_argument("--persistent-steps", type=int, default=20, help="timed steps of the one-launch persistent step (0: skip)")
+    ap.add_argument("--column-tile-steps", type=int, default=10,
+                    help="timed steps with riemann2 + riemann3 as one column-tile kernel (0: skip)")
     ap.add_argument("--large-steps", type=int, default=5, help="timed steps of the 384^3 configuration (0: skip)")
     ap.add_argument("--large-adjoint", type=int, default=1, help="the 384^3 configuration's 50-step adjoint (0: skip)")
     ap.add_argument("--adjoint-reps", type=int, default=3, help="timed forward+reverse runs of the adjoint configuration (0: skip)")

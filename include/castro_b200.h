@@ -79,6 +79,15 @@ int  castro_nspec(void);
  * reference reads the table through ordinary loads.  The L2 set-aside belongs
  * to this process's CUDA context and eos_finalize puts the previous value back. */
 void castro_set_table_l2_window(int on);
+/* Batched sims (2 species) created afterwards form the cross fluxes and the
+ * final fluxes of the CTU step (Source/Castro_hydro.cpp:228-359) in one kernel
+ * per column tile, marching in z with the cross-flux records in shared memory,
+ * instead of two kernels passing them through HBM; results are the same bit for
+ * bit.  Off by default: on B200 the fused kernel, at lower occupancy than the
+ * two kernels and with a block-wide barrier per phase and plane, is slower.  No
+ * reference counterpart. */
+void castro_set_column_tiles(int on);
+int  castro_column_tiles(void);
 
 /* Option, off by default (no counterpart in the reference): the interface
  * pressure in the normal momentum flux of compute_flux, flx(im1) = rho u u + p,

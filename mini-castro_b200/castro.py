@@ -83,6 +83,7 @@ ABI_SYMBOLS = [
     "castro_sim_write_checkpoint", "castro_sim_read_checkpoint", "castro_set_table_l2_window",
     "castro_set_momentum_flux_pressure", "castro_momentum_flux_pressure",
     "castro_set_coulomb_corrections", "castro_coulomb_corrections",
+    "castro_set_column_tiles", "castro_column_tiles",
     "castro_flux_register_crse_init", "castro_flux_register_fine_add", "castro_flux_register_reflux",
     "castro_average_down",
     "castro_sim_set_wait_limit", "castro_saxpy", "castro_adj_create_window",
@@ -148,6 +149,8 @@ def load(exact: bool = False) -> C.CDLL:
     L.castro_set_momentum_flux_pressure.argtypes = [C.c_int]
     L.castro_momentum_flux_pressure.restype = C.c_int
     L.castro_set_coulomb_corrections.argtypes = [C.c_int]
+    L.castro_set_column_tiles.argtypes = [C.c_int]
+    L.castro_column_tiles.restype = C.c_int
     L.castro_coulomb_corrections.restype = C.c_int
     L.castro_saxpy.argtypes = [C.c_void_p, C.c_void_p, C.c_longlong, C.c_double]
     L.castro_sim_set_wait_limit.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_int]

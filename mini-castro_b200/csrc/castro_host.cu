@@ -46,6 +46,8 @@ bool g_prob_set = false;
 // L2, which would otherwise evict it.  The set-aside is this process's (it ends
 // with the CUDA context) and is put back by eos_finalize.
 bool g_l2_window = true;
+// batched sims created afterwards run riemann2 + riemann3 as one column-tile kernel (2 species)
+bool g_column_tiles = false;
 size_t g_table_bytes = 0;
 size_t g_l2_prev_limit = 0;
 bool g_l2_limit_set = false;
@@ -126,6 +128,7 @@ const NetworkDev& network_host()
 }
 unsigned long long* eos_fail_counter() { return d_fail; }
 bool coulomb_on() { return g_net.coulomb != 0; }
+bool column_tiles_on() { return g_column_tiles; }
 
 // the table's window on stream st (or no window, when it is switched off)
 void apply_table_l2_window(cudaStream_t st)
@@ -200,6 +203,8 @@ int castro_network_init(int ns, const double* aion, const double* zion)
 int castro_nspec(void) { return nspec(); }
 
 void castro_set_table_l2_window(int on) { g_l2_window = on != 0; }
+void castro_set_column_tiles(int on) { g_column_tiles = on != 0; }
+int castro_column_tiles(void) { return g_column_tiles ? 1 : 0; }
 
 void castro_set_momentum_flux_pressure(int on)
 {

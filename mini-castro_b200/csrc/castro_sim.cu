@@ -51,6 +51,7 @@ void upload_constants_sim(const EosTableDev& e, const NetworkDev& n)
 
 const castro_problem& problem();
 unsigned long long* eos_fail_counter();
+bool column_tiles_on();
 void apply_table_l2_window(cudaStream_t st);
 
 namespace {
@@ -1036,6 +1037,225 @@ __global__ void LB_R3 k_riemann3(SimDev S, const Work* wl)
     riemann3_body<NS>(S, wl[blockIdx.x]);
 }
 
+// ---------------------------------------------------------------------------
+// riemann23 (castro_set_column_tiles; off by default, measured slower on B200
+// than riemann2 + riemann3): riemann2 and riemann3 fused per column tile.  One block owns the
+// zone columns [xa, xb] x [ya, yb] of an instance domain over a chunk of
+// planes [za, zb] and marches up through it; the six cross fluxes
+// (Castro_hydro.cpp:228-304) are formed into shared memory, two planes of
+// each at most, and the final fluxes (Castro_hydro.cpp:307-359) read them
+// there: the cross-flux records never go through HBM.  Every flux is formed by
+// the same per-face stages as riemann2 / riemann3 on the same inputs, so the
+// results are those of the two kernels, bit for bit.
+//
+// Iteration m (m = za-1 .. zb', zb' = zb + 1 at the domain's top, else zb):
+//   A: XY(m), YX(m)                    planes za-1 .. zb'  (F^z of the faces m-1/2, m+1/2)
+//      XZ(m), YZ(m)                    planes za .. zb     (F^y(m), F^x(m))
+//      ZY(m+1), ZX(m+1)                z-faces m+1/2, for m+1 in za .. zb+1
+//   B: F^x(m), F^y(m)                  planes za .. zb
+//      F^z(m) (the face m-1/2)         za .. zb'
+// XY is the F^{x|y} record of an x-face, ZY the F^{z|y} record of a z-face, and
+// so on; z-face index k is the face k-1/2.  The block's x-faces are [xa, xb]
+// (and xb+1 at the domain's high x end), likewise in y and z; the cross
+// fluxes its final fluxes need reach one zone column beyond the tile.
+// ---------------------------------------------------------------------------
+#ifndef CASTRO_R23_TX
+#define CASTRO_R23_TX 8
+#endif
+#ifndef CASTRO_R23_TY
+#define CASTRO_R23_TY 8
+#endif
+#ifndef CASTRO_R23_ZC
+#define CASTRO_R23_ZC 16      // planes per block
+#endif
+#ifndef CASTRO_R23_NT
+#define CASTRO_R23_NT 128     // threads per block
+#endif
+#ifndef CASTRO_R23_MINB
+#define CASTRO_R23_MINB 3
+#endif
+
+struct TileItem { int inst, x0, y0, z0; };
+
+// A cross-flux record buffer in shared memory: planes of nx x ny records whose
+// slot (0,0) is zone column (x0, y0); component c of slot s at base[c * slots + s]
+struct SmemTF {
+    double* base;
+    int slots, x0, y0, nx, ny, two;
+    __device__ __forceinline__ int slot(int i, int j, int k) const
+    {
+        return (i - x0) + nx * ((j - y0) + ny * (two ? (k & 1) : 0));
+    }
+    template <int NS>
+    __device__ __forceinline__ void load(int i, int j, int k, double* r) const
+    {
+        const double* p = base + slot(i, j, k);
+#pragma unroll
+        for (int c = 0; c < TF<NS>::N; ++c) r[c] = p[c * slots];
+    }
+};
+
+template <int NS>
+struct SmemTFLoader {
+    SmemTF b;
+    __device__ __forceinline__ void operator()(int i, int j, int k, double* r) const { b.template load<NS>(i, j, k, r); }
+};
+
+template <int NS>
+struct R23Layout {
+    static constexpr int TX = CASTRO_R23_TX, TY = CASTRO_R23_TY, NTF = TF<NS>::N;
+    // records per buffer (all planes): XY, YX, XZ, YZ, ZY, ZX
+    static constexpr int S_XY = (TX + 1) * TY * 2, S_YX = TX * (TY + 1) * 2;
+    static constexpr int S_XZ = (TX + 1) * (TY + 2), S_YZ = (TX + 2) * (TY + 1);
+    static constexpr int S_ZY = (TX + 2) * TY * 2, S_ZX = TX * (TY + 2) * 2;
+    static constexpr int O_XY = 0, O_YX = O_XY + NTF * S_XY, O_XZ = O_YX + NTF * S_YX, O_YZ = O_XZ + NTF * S_XZ,
+                         O_ZY = O_YZ + NTF * S_YZ, O_ZX = O_ZY + NTF * S_ZY, DOUBLES = O_ZX + NTF * S_ZX;
+    static constexpr int BYTES = DOUBLES * 8;
+};
+
+// F^{A|Bd} of the A-normal face (i,j,k) into the record slot out[c * stride]:
+// cross_flux_store's arithmetic (trans1 of both trace states, compute_flux)
+template <int NS, int A, int Bd>
+__device__ __forceinline__ void cross_flux_rec(const SimDev& S, const BoxDev& B, int i, int j, int k, double cdtdx,
+                                               const double* lq, double gl, double gr, double cl, double cr,
+                                               double* out, int stride)
+{
+    constexpr int NQS = Dims<NS>::NQS, NTF = Dims<NS>::NTF, NVAR = Dims<NS>::NVAR;
+    constexpr int eax = A == 0, eay = A == 1, eaz = A == 2;
+    constexpr int ebx_ = Bd == 0, eby = Bd == 1, ebz = Bd == 2;
+    const Reg RF = make_reg(B.lo, B.hi, R_TBX, 4 * Bd);
+    const double* F = S.F1 + B.offF1[Bd];
+    double st2[2][NQS];
+#pragma unroll
+    for (int D = -1; D <= 0; ++D) {
+        double fr[NTF], fl[NTF];
+        const int il = i + D * eax, jl = j + D * eay, kl = k + D * eaz;
+        load_tf<NS>(F, RF, ridx(RF, il + ebx_, jl + eby, kl + ebz), fr);
+        load_tf<NS>(F, RF, ridx(RF, il, jl, kl), fl);
+        trans1_state<NS>(lq + (D + 1) * NQS, fr, fl, D == -1 ? gl : gr, cdtdx, st2[D + 1]);
+    }
+    double flx[NVAR], qg[NGDNV];
+    riemann_cgf<NS, A>(st2[0], st2[1], gl, gr, cl, cr, flx, qg, nullptr);
+    using T_ = TF<NS>;
+    out[stride * T_::RHO] = flx[URHO];
+    out[stride * T_::MX] = flx[UMX];
+    out[stride * T_::MY] = flx[UMY];
+    out[stride * T_::MZ] = flx[UMZ];
+    out[stride * T_::ED] = flx[UEDEN];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) out[stride * (T_::X + n)] = flx[UFS + n];
+    out[stride * T_::PG] = qg[GDPRES];
+    out[stride * T_::UG] = qg[GDU + A];
+}
+
+// the cross fluxes of the A-normal face (i,j,k) that the tile needs: F^{A|B1}
+// into o1 (null: not needed), F^{A|B2} into o2; the face's trace states,
+// gamma_1 and sound speeds are read once for both
+template <int NS, int A>
+__device__ __forceinline__ void cross_pair(const SimDev& S, const BoxDev& B, const InstDev& I, const QLoader<NS>& ld,
+                                           int i, int j, int k, double dt, double* o1, int s1, double* o2, int s2)
+{
+    constexpr int NQS = Dims<NS>::NQS;
+    constexpr int B1 = A == 0 ? 1 : 0, B2 = A == 2 ? 1 : 2;
+    constexpr int eax = A == 0, eay = A == 1, eaz = A == 2;
+    const Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * A);
+    const double* T = S.Tr + B.offTr[A];
+    const long long ft = ridx(RT, i, j, k);
+    double lq[2 * NQS];
+#pragma unroll
+    for (int c = 0; c < 2 * NQS; ++c) lq[c] = T[ft + RT.np * c];
+    const long long zl = ridx(ld.R, i - eax, j - eay, k - eaz), zr = ridx(ld.R, i, j, k);
+    const double gl = ld.base[zl + ld.R.np * QF<NS>::GAMC], gr = ld.base[zr + ld.R.np * QF<NS>::GAMC];
+    const double cl = ld.base[zl + ld.R.np * QF<NS>::C], cr = ld.base[zr + ld.R.np * QF<NS>::C];
+    if (o1) cross_flux_rec<NS, A, B1>(S, B, i, j, k, dt / I.dx[B1] / 3.0, lq, gl, gr, cl, cr, o1, s1);
+    if (o2) cross_flux_rec<NS, A, B2>(S, B, i, j, k, dt / I.dx[B2] / 3.0, lq, gl, gr, cl, cr, o2, s2);
+}
+
+template <int NS>
+__global__ void __launch_bounds__(CASTRO_R23_NT, CASTRO_R23_MINB) k_riemann23(SimDev S, const TileItem* items)
+{
+    using L = R23Layout<NS>;
+    extern __shared__ double r23_smem[];
+    const TileItem it = items[blockIdx.x];
+    const BoxDev& B = S.boxes[it.inst];                 // the instance domain (the stage arrays' box)
+    const InstDev& I = S.inst[B.inst];
+    const double dt = S.st[B.inst].dt;
+    QLoader<NS> ld;
+    ld.base = S.Q + B.offQ;
+    ld.R = q_region(I);
+    const int xa = it.x0, xb = min(it.x0 + L::TX - 1, B.hi[0]);
+    const int ya = it.y0, yb = min(it.y0 + L::TY - 1, B.hi[1]);
+    const int za = it.z0, zb = min(it.z0 + CASTRO_R23_ZC - 1, B.hi[2]);
+    const int fxb = xb + (xb == B.hi[0]), fyb = yb + (yb == B.hi[1]), fzb = zb + (zb == B.hi[2]);
+    SmemTF XY{r23_smem + L::O_XY, L::S_XY, xa, ya, L::TX + 1, L::TY, 1};
+    SmemTF YX{r23_smem + L::O_YX, L::S_YX, xa, ya, L::TX, L::TY + 1, 1};
+    SmemTF XZ{r23_smem + L::O_XZ, L::S_XZ, xa, ya - 1, L::TX + 1, L::TY + 2, 0};
+    SmemTF YZ{r23_smem + L::O_YZ, L::S_YZ, xa - 1, ya, L::TX + 2, L::TY + 1, 0};
+    SmemTF ZY{r23_smem + L::O_ZY, L::S_ZY, xa - 1, ya, L::TX + 2, L::TY, 1};
+    SmemTF ZX{r23_smem + L::O_ZX, L::S_ZX, xa, ya - 1, L::TX, L::TY + 2, 1};
+    // phase A tasks: x-faces [xa, xb+1] x [ya-1, fyb], y-faces [xa-1, fxb] x
+    // [ya, yb+1], z-faces [xa-1, fxb] x [ya-1, fyb]
+    const int nxA = xb + 2 - xa, nyA = fyb - ya + 2;
+    const int nxB = fxb - xa + 2, nyB = yb + 2 - ya;
+    const int nxC = fxb - xa + 2, nyC = fyb - ya + 2;
+    const int cA = nxA * nyA, cB = nxB * nyB, cC = nxC * nyC;
+    // phase B: x-faces [xa, fxb] x [ya, yb], y-faces [xa, xb] x [ya, fyb], z-faces [xa, xb] x [ya, yb]
+    const int fx_n = (fxb - xa + 1) * (yb - ya + 1), fy_n = (xb - xa + 1) * (fyb - ya + 1);
+    const int fz_n = (xb - xa + 1) * (yb - ya + 1);
+    for (int m = za - 1; m <= fzb; ++m) {
+        const bool pXZ = m >= za && m <= zb;               // XZ, YZ of plane m
+        const bool pZ = m <= zb;                           // z-face m+1 in [za, zb+1]
+        const int ntask = cA + cB + (pZ ? cC : 0);
+        for (int t = threadIdx.x; t < ntask; t += CASTRO_R23_NT) {
+            if (t < cA) {                                  // x-face (i, j, m): XY and XZ
+                const int i = xa + t % nxA, j = ya - 1 + t / nxA;
+                const bool xy = j >= ya && j <= yb;
+                if (!xy && !pXZ) continue;
+                cross_pair<NS, 0>(S, B, I, ld, i, j, m, dt, xy ? XY.base + XY.slot(i, j, m) : nullptr, XY.slots,
+                                  pXZ ? XZ.base + XZ.slot(i, j, m) : nullptr, XZ.slots);
+            } else if (t < cA + cB) {                      // y-face (i, j, m): YX and YZ
+                const int u = t - cA;
+                const int i = xa - 1 + u % nxB, j = ya + u / nxB;
+                const bool yx = i >= xa && i <= xb;
+                if (!yx && !pXZ) continue;
+                cross_pair<NS, 1>(S, B, I, ld, i, j, m, dt, yx ? YX.base + YX.slot(i, j, m) : nullptr, YX.slots,
+                                  pXZ ? YZ.base + YZ.slot(i, j, m) : nullptr, YZ.slots);
+            } else {                                       // z-face (i, j, m+1): ZX and ZY
+                const int u = t - cA - cB;
+                const int i = xa - 1 + u % nxC, j = ya - 1 + u / nxC;
+                const bool zy = j >= ya && j <= yb;
+                const bool zx = i >= xa && i <= xb;
+                if (!zy && !zx) continue;
+                cross_pair<NS, 2>(S, B, I, ld, i, j, m + 1, dt, zx ? ZX.base + ZX.slot(i, j, m + 1) : nullptr,
+                                  ZX.slots, zy ? ZY.base + ZY.slot(i, j, m + 1) : nullptr, ZY.slots);
+            }
+        }
+        __syncthreads();
+        const bool fxy = m >= za && m <= zb;               // F^x(m), F^y(m)
+        const bool fz = m >= za;                           // F^z of the face m-1/2 (m <= fzb)
+        const int nB = (fxy ? fx_n + fy_n : 0) + (fz ? fz_n : 0);
+        for (int t = threadIdx.x; t < nB; t += CASTRO_R23_NT) {
+            int u = fxy ? t : t + fx_n + fy_n;
+            if (u < fx_n) {
+                const int w = fxb - xa + 1;
+                const int i = xa + u % w, j = ya + u / w;
+                final_flux<NS, 0, false>(S, B, I, ld, i, j, m, dt, SmemTFLoader<NS>{YZ}, SmemTFLoader<NS>{ZY}, nullptr);
+            } else if (u < fx_n + fy_n) {
+                u -= fx_n;
+                const int w = xb - xa + 1;
+                const int i = xa + u % w, j = ya + u / w;
+                final_flux<NS, 1, false>(S, B, I, ld, i, j, m, dt, SmemTFLoader<NS>{XZ}, SmemTFLoader<NS>{ZX}, nullptr);
+            } else {
+                u -= fx_n + fy_n;
+                const int w = xb - xa + 1;
+                const int i = xa + u % w, j = ya + u / w;
+                final_flux<NS, 2, false>(S, B, I, ld, i, j, m, dt, SmemTFLoader<NS>{XY}, SmemTFLoader<NS>{YX}, nullptr);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // update: fill_hydro_source, Saxpy, clean_state (advance), clean_state
 // (post_timestep), estdt of the new state
 template <int NS, bool COUL>
@@ -1481,6 +1701,10 @@ struct castro_sim {
     Work *w_valid = nullptr, *w_g4 = nullptr, *w_g1 = nullptr, *w_trace = nullptr, *w_tbx = nullptr,
          *w_ebx = nullptr, *w_r2 = nullptr, *w_r3 = nullptr, *w_ghost = nullptr;
     int n_valid = 0, n_g4 = 0, n_g1 = 0, n_trace = 0, n_tbx = 0, n_ebx = 0, n_r2 = 0, n_r3 = 0, n_ghost = 0;
+    // column tiles of riemann23 (2 species, batched mode): the step runs it in place of riemann2 + riemann3
+    TileItem* w_r23 = nullptr;
+    int n_r23 = 0;
+    bool r23 = false;
     bool dt_ready = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -1639,6 +1863,33 @@ void build_ghost_work(castro_sim* s)
         else K<NS, false><<<GRID, BLK, SMEM, ST>>>(__VA_ARGS__);                     \
     } while (0)
 
+// riemann23's column tiles over every instance domain; its shared memory
+bool build_r23_work(castro_sim* s)
+{
+    std::vector<TileItem> w;
+    for (size_t in = 0; in < s->hdom.size(); ++in) {
+        const BoxDev& D = s->hdom[in];
+        for (int z = D.lo[2]; z <= D.hi[2]; z += CASTRO_R23_ZC)
+            for (int y = D.lo[1]; y <= D.hi[1]; y += CASTRO_R23_TY)
+                for (int x = D.lo[0]; x <= D.hi[0]; x += CASTRO_R23_TX) w.push_back(TileItem{(int)in, x, y, z});
+    }
+    if (!cuda_ok(cudaFuncSetAttribute(k_riemann23<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, R23Layout<2>::BYTES),
+                 "riemann23 shared memory") ||
+        !dalloc(&s->w_r23, w.size(), "riemann23 tiles") ||
+        !cuda_ok(cudaMemcpy(s->w_r23, w.data(), w.size() * sizeof(TileItem), cudaMemcpyHostToDevice), "riemann23 tiles"))
+        return false;
+    s->n_r23 = (int)w.size();
+    s->r23 = true;
+    return true;
+}
+
+template <int NS>
+void launch_riemann23(castro_sim* s, const SimDev& Sd, cudaStream_t st)
+{
+    if constexpr (NS == 2)
+        k_riemann23<2><<<s->n_r23, CASTRO_R23_NT, R23Layout<2>::BYTES, st>>>(Sd, s->w_r23);
+}
+
 template <int NS>
 void batched_step_kernels(castro_sim* s)
 {
@@ -1659,8 +1910,12 @@ void batched_step_kernels(castro_sim* s)
         k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace);
     }
     k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(Sd, s->w_tbx);
-    k_riemann2<NS><<<s->n_r2, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_r2);
-    k_riemann3<NS><<<s->n_r3, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_r3);
+    if (s->r23) {
+        launch_riemann23<NS>(s, Sd, st);
+    } else {
+        k_riemann2<NS><<<s->n_r2, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_r2);
+        k_riemann3<NS><<<s->n_r3, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_r3);
+    }
     CASTRO_EOS_LAUNCH(k_update, NS, s->n_valid, BLOCK, 0, st, S, s->w_valid);
     k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0);
 }
@@ -1681,8 +1936,13 @@ void profile_kernel(castro_sim* s, const SimDev& S, int k)
     case 3: k_trace<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace); break;
     case 9: k_trace2<NS><<<s->n_trace, BLOCK, 0, st>>>(Sd, s->w_trace); break;
     case 4: k_riemann1<NS><<<s->n_tbx, BLOCK, 0, st>>>(Sd, s->w_tbx); break;
-    case 5: k_riemann2<NS><<<s->n_r2, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_r2); break;
-    case 6: k_riemann3<NS><<<s->n_r3, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_r3); break;
+    case 5:
+        if (s->r23) launch_riemann23<NS>(s, Sd, st);   // riemann2 and riemann3 in one kernel
+        else k_riemann2<NS><<<s->n_r2, BLOCK, R2Slot<NS>::BYTES, st>>>(Sd, s->w_r2);
+        break;
+    case 6:
+        if (!s->r23) k_riemann3<NS><<<s->n_r3, BLOCK, R3Slot<NS>::BYTES, st>>>(Sd, s->w_r3);
+        break;
     case 7: CASTRO_EOS_LAUNCH(k_update, NS, s->n_valid, BLOCK, 0, st, S, s->w_valid); break;
     default: k_dt<<<(s->ninst + 63) / 64, 64, 0, st>>>(S, s->ninst, 0); break;
     }
@@ -2090,7 +2350,7 @@ int step_impl(castro_sim* s)
         s->graph_coul = coulomb_on();
     }
     cuda_ok(cudaGraphLaunch(s->gexec, s->st), "graph launch");
-    s->launches = 9 + (CASTRO_TRACE_SPLIT ? 1 : 0);
+    s->launches = 9 + (CASTRO_TRACE_SPLIT ? 1 : 0) - (s->r23 ? 1 : 0);
     return castro_last_error();
 }
 
@@ -2290,6 +2550,7 @@ castro_sim* castro_sim_create(int ninst, const castro_instance_desc* desc, int m
         build_work(s->hdom, R_TBX, 3, 0, &s->w_r2, &s->n_r2, CASTRO_R2_ROWS);
         build_work(s->hdom, R_EBX, 3, -1, &s->w_r3, &s->n_r3, CASTRO_R3_ROWS);
         build_ghost_work(s);
+        if (ok && ns == 2 && column_tiles_on() && mode == CASTRO_MODE_BATCHED) ok = build_r23_work(s);
         if (ok && mode == CASTRO_MODE_PERSISTENT) ok = ns == 2 ? persistent_setup<2>(s) : persistent_setup<13>(s);
     }
     if (ok && (mode == CASTRO_MODE_PLAIN || mode == CASTRO_MODE_PLAIN_BOX)) {
@@ -2329,7 +2590,7 @@ void castro_sim_destroy(castro_sim* s)
     if (s->graph) cudaGraphDestroy(s->graph);
     void* ptrs[] = {s->dboxes, s->ddom, s->dinst, s->dstate, s->downer, s->U, s->Ub, s->Q, s->Div, s->Tr, s->F1, s->F2, s->Fx,
                     s->w_valid, s->w_g4, s->w_g1, s->w_trace, s->w_tbx, s->w_ebx, s->w_r2, s->w_r3, s->w_ghost, s->sb, s->src,
-                    s->d_dtloc, s->d_dtbox, s->pctl};
+                    s->d_dtloc, s->d_dtbox, s->pctl, s->w_r23};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int k = 0; k < castro_sim::PLAIN_STREAMS; ++k) {
@@ -3188,14 +3449,15 @@ int castro_sim_profile_step(castro_sim* s, double* ms, const char** names)
     static const int ids[10] = {0, 1, 2, 3, 9, 4, 5, 6, 7, 8};
     static const char* kn[10] = {"front", "ghost", "prep", "trace", "trace2", "riemann1", "riemann2", "riemann3", "update",
                                  "dt"};
-    const int NK = CASTRO_TRACE_SPLIT ? 10 : 9;
     int order[10], m = 0;
     const char* nm[10];
     for (int q = 0; q < 10; ++q) {
         if (ids[q] == 9 && !CASTRO_TRACE_SPLIT) continue;
+        if (ids[q] == 6 && s->r23) continue;          // riemann23 runs as id 5
         order[m] = ids[q];
-        nm[m++] = kn[q];
+        nm[m++] = (ids[q] == 5 && s->r23) ? "riemann23" : kn[q];
     }
+    const int NK = m;
     cudaEvent_t ev[11];
     for (int k = 0; k < 11; ++k) cudaEventCreate(&ev[k]);
     if (!s->dt_ready) {

@@ -23,7 +23,7 @@ def _bench():
 def test_kernel_bytes_headline():
     pkg = load_package()
     kb = _bench().kernel_bytes(pkg.configs.sedov128_pert(), NS)
-    assert set(kb) == {"front", "ghost", "trace", "trace2", "riemann1", "riemann2", "riemann3", "update"}
+    assert set(kb) == {"front", "ghost", "trace", "trace2", "riemann1", "riemann2", "riemann3", "riemann23", "update"}
     n = 128
     vd, g1d, g4d = n ** 3, (n + 2) ** 3, (n + 8) ** 3
     # ghost fills the domain halo of Q (grow 4) and Sborder (grow 1), read and written once
@@ -35,6 +35,8 @@ def test_kernel_bytes_headline():
     assert kb["riemann1"] == 8 * (tdd * 2 * NQS + g4d * 2 + tdd * NTF)
     assert kb["riemann2"] == 8 * (tdd * 2 * NQS + tdd * NTF + g4d * 2 + tab * NTF)
     assert kb["riemann3"] == 8 * (eb * 2 * NQS + tab * NTF + g1d * NV + g1d + g4d * 2 + eb * (NV + 1))
+    # the fused kernel reads what both read, less the cross-flux records the pair passes through HBM
+    assert kb["riemann23"] == kb["riemann2"] + kb["riemann3"] - 8 * (2 * tab * NTF + g4d * 2 + eb * 2 * NQS)
     # the two trace kernels write the 2 x NQS face-state components between them
     assert kb["trace"] + kb["trace2"] == 8 * (g4d * (9 + NS) + tdd * 2 * NQS + 2 * g1d)
     # front and update walk the 64 boxes of 32^3: the per-box terms add up to the domain's
