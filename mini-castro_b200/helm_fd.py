@@ -511,8 +511,15 @@ def write_table(path: str = DEFAULT_PATH, workers: int | None = None, rows=None,
 
 
 def ensure_table(path: str = DEFAULT_PATH) -> str:
+    """The table at ``path``, generated first when it is missing.  The generation
+    runs this file as a script in a process of its own: its worker pool is
+    started with ``spawn``, whose workers must import the row function by name,
+    and the package directory (``mini-castro_b200``) is not importable by name."""
     if not os.path.exists(path):
-        write_table(path)
+        import subprocess
+        import sys
+
+        subprocess.run([sys.executable, os.path.abspath(__file__), path], check=True, stdout=subprocess.DEVNULL)
     return path
 
 
