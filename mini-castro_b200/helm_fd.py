@@ -475,7 +475,17 @@ def fd_tables(rows=None, cols=None, workers=None):
     out = [[np.array(a) for a in block] for block in _ht.ideal_nd_tables()]
     args = [(t1[j], d1[cols]) for j in rows]
     if workers and workers > 1 and len(rows) > 1:
+        import importlib.machinery
         import multiprocessing as mp
+        import sys
+
+        # spawn workers import _row by its module name: run as a script (ensure_table
+        # does) when this module was loaded from a file path under a name a fresh
+        # interpreter cannot import
+        top = __name__.split(".")[0]
+        if __name__ != "__main__" and importlib.machinery.PathFinder.find_spec(top, sys.path) is None:
+            raise RuntimeError("helm_fd: a worker pool needs the module importable by name; "
+                               "use ensure_table() or run helm_fd.py as a script")
 
         with mp.get_context("spawn").Pool(workers) as pool:
             res = pool.map(_row, args)
