@@ -1148,15 +1148,12 @@ __device__ __forceinline__ void cross_flux_rec(const SimDev& S, const BoxDev& B,
     out[stride * T_::UG] = qg[GDU + A];
 }
 
-// the cross fluxes of the A-normal face (i,j,k) that the tile needs: F^{A|B1}
-// into o1 (null: not needed), F^{A|B2} into o2; the face's trace states,
-// gamma_1 and sound speeds are read once for both
-template <int NS, int A>
-__device__ __forceinline__ void cross_pair(const SimDev& S, const BoxDev& B, const InstDev& I, const QLoader<NS>& ld,
-                                           int i, int j, int k, double dt, double* o1, int s1, double* o2, int s2)
+// one cross flux F^{A|Bd} of the A-normal face (i,j,k) into out[c * stride]
+template <int NS, int A, int Bd>
+__device__ __forceinline__ void cross_one(const SimDev& S, const BoxDev& B, const InstDev& I, const QLoader<NS>& ld,
+                                          int i, int j, int k, double dt, double* out, int stride)
 {
     constexpr int NQS = Dims<NS>::NQS;
-    constexpr int B1 = A == 0 ? 1 : 0, B2 = A == 2 ? 1 : 2;
     constexpr int eax = A == 0, eay = A == 1, eaz = A == 2;
     const Reg RT = make_reg(B.lo, B.hi, R_TBX, 4 * A);
     const double* T = S.Tr + B.offTr[A];
@@ -1167,8 +1164,7 @@ __device__ __forceinline__ void cross_pair(const SimDev& S, const BoxDev& B, con
     const long long zl = ridx(ld.R, i - eax, j - eay, k - eaz), zr = ridx(ld.R, i, j, k);
     const double gl = ld.base[zl + ld.R.np * QF<NS>::GAMC], gr = ld.base[zr + ld.R.np * QF<NS>::GAMC];
     const double cl = ld.base[zl + ld.R.np * QF<NS>::C], cr = ld.base[zr + ld.R.np * QF<NS>::C];
-    if (o1) cross_flux_rec<NS, A, B1>(S, B, i, j, k, dt / I.dx[B1] / 3.0, lq, gl, gr, cl, cr, o1, s1);
-    if (o2) cross_flux_rec<NS, A, B2>(S, B, i, j, k, dt / I.dx[B2] / 3.0, lq, gl, gr, cl, cr, o2, s2);
+    cross_flux_rec<NS, A, Bd>(S, B, i, j, k, dt / I.dx[Bd] / 3.0, lq, gl, gr, cl, cr, out, stride);
 }
 
 template <int NS>
@@ -1193,62 +1189,75 @@ __global__ void __launch_bounds__(CASTRO_R23_NT, CASTRO_R23_MINB) k_riemann23(Si
     SmemTF YZ{r23_smem + L::O_YZ, L::S_YZ, xa - 1, ya, L::TX + 2, L::TY + 1, 0};
     SmemTF ZY{r23_smem + L::O_ZY, L::S_ZY, xa - 1, ya, L::TX + 2, L::TY, 1};
     SmemTF ZX{r23_smem + L::O_ZX, L::S_ZX, xa, ya - 1, L::TX, L::TY + 2, 1};
-    // phase A tasks: x-faces [xa, xb+1] x [ya-1, fyb], y-faces [xa-1, fxb] x
-    // [ya, yb+1], z-faces [xa-1, fxb] x [ya-1, fyb]
-    const int nxA = xb + 2 - xa, nyA = fyb - ya + 2;
-    const int nxB = fxb - xa + 2, nyB = yb + 2 - ya;
-    const int nxC = fxb - xa + 2, nyC = fyb - ya + 2;
-    const int cA = nxA * nyA, cB = nxB * nyB, cC = nxC * nyC;
+    // Phase A: six task lists, one cross flux per task, each list starting on a
+    // warp boundary, so that a warp runs one face direction and record pair.
+    const int wX = xb + 2 - xa, wT = xb - xa + 1, wH = fxb - xa + 2;      // x extents: [xa, xb+1], [xa, xb], [xa-1, fxb]
+    const int hT = yb - ya + 1, hT1 = yb - ya + 2, hH = fyb - ya + 2;     // y extents: [ya, yb], [ya, yb+1], [ya-1, fyb]
+    const int n[6] = {wX * hT, wX * hH, wT * hT1, wH * hT1, wH * hT, wT * hH};   // XY XZ YX YZ ZY ZX
     // phase B: x-faces [xa, fxb] x [ya, yb], y-faces [xa, xb] x [ya, fyb], z-faces [xa, xb] x [ya, yb]
-    const int fx_n = (fxb - xa + 1) * (yb - ya + 1), fy_n = (xb - xa + 1) * (fyb - ya + 1);
-    const int fz_n = (xb - xa + 1) * (yb - ya + 1);
+    const int wF = fxb - xa + 1;
+    const int nb[3] = {wF * hT, wT * (fyb - ya + 1), wT * hT};
     for (int m = za - 1; m <= fzb; ++m) {
         const bool pXZ = m >= za && m <= zb;               // XZ, YZ of plane m
-        const bool pZ = m <= zb;                           // z-face m+1 in [za, zb+1]
-        const int ntask = cA + cB + (pZ ? cC : 0);
-        for (int t = threadIdx.x; t < ntask; t += CASTRO_R23_NT) {
-            if (t < cA) {                                  // x-face (i, j, m): XY and XZ
-                const int i = xa + t % nxA, j = ya - 1 + t / nxA;
-                const bool xy = j >= ya && j <= yb;
-                if (!xy && !pXZ) continue;
-                cross_pair<NS, 0>(S, B, I, ld, i, j, m, dt, xy ? XY.base + XY.slot(i, j, m) : nullptr, XY.slots,
-                                  pXZ ? XZ.base + XZ.slot(i, j, m) : nullptr, XZ.slots);
-            } else if (t < cA + cB) {                      // y-face (i, j, m): YX and YZ
-                const int u = t - cA;
-                const int i = xa - 1 + u % nxB, j = ya + u / nxB;
-                const bool yx = i >= xa && i <= xb;
-                if (!yx && !pXZ) continue;
-                cross_pair<NS, 1>(S, B, I, ld, i, j, m, dt, yx ? YX.base + YX.slot(i, j, m) : nullptr, YX.slots,
-                                  pXZ ? YZ.base + YZ.slot(i, j, m) : nullptr, YZ.slots);
-            } else {                                       // z-face (i, j, m+1): ZX and ZY
-                const int u = t - cA - cB;
-                const int i = xa - 1 + u % nxC, j = ya - 1 + u / nxC;
-                const bool zy = j >= ya && j <= yb;
-                const bool zx = i >= xa && i <= xb;
-                if (!zy && !zx) continue;
-                cross_pair<NS, 2>(S, B, I, ld, i, j, m + 1, dt, zx ? ZX.base + ZX.slot(i, j, m + 1) : nullptr,
-                                  ZX.slots, zy ? ZY.base + ZY.slot(i, j, m + 1) : nullptr, ZY.slots);
+        const bool pZ = m <= zb;                           // ZY, ZX of the z-face m+1 (in [za, zb+1])
+        const bool act[6] = {true, pXZ, true, pXZ, pZ, pZ};
+        int o[7];
+        o[0] = 0;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) o[q + 1] = o[q] + (act[q] ? (n[q] + 31) & ~31 : 0);
+        for (int t = threadIdx.x; t < o[6]; t += CASTRO_R23_NT) {
+            int q = 0;
+#pragma unroll
+            for (int r = 1; r < 6; ++r) q += t >= o[r];
+            const int u = t - o[q];
+            if (u >= n[q]) continue;
+            switch (q) {
+            case 0: {
+                const int i = xa + u % wX, j = ya + u / wX;
+                cross_one<NS, 0, 1>(S, B, I, ld, i, j, m, dt, XY.base + XY.slot(i, j, m), XY.slots);
+            } break;
+            case 1: {
+                const int i = xa + u % wX, j = ya - 1 + u / wX;
+                cross_one<NS, 0, 2>(S, B, I, ld, i, j, m, dt, XZ.base + XZ.slot(i, j, m), XZ.slots);
+            } break;
+            case 2: {
+                const int i = xa + u % wT, j = ya + u / wT;
+                cross_one<NS, 1, 0>(S, B, I, ld, i, j, m, dt, YX.base + YX.slot(i, j, m), YX.slots);
+            } break;
+            case 3: {
+                const int i = xa - 1 + u % wH, j = ya + u / wH;
+                cross_one<NS, 1, 2>(S, B, I, ld, i, j, m, dt, YZ.base + YZ.slot(i, j, m), YZ.slots);
+            } break;
+            case 4: {
+                const int i = xa - 1 + u % wH, j = ya + u / wH;
+                cross_one<NS, 2, 1>(S, B, I, ld, i, j, m + 1, dt, ZY.base + ZY.slot(i, j, m + 1), ZY.slots);
+            } break;
+            default: {
+                const int i = xa + u % wT, j = ya - 1 + u / wT;
+                cross_one<NS, 2, 0>(S, B, I, ld, i, j, m + 1, dt, ZX.base + ZX.slot(i, j, m + 1), ZX.slots);
+            } break;
             }
         }
         __syncthreads();
         const bool fxy = m >= za && m <= zb;               // F^x(m), F^y(m)
         const bool fz = m >= za;                           // F^z of the face m-1/2 (m <= fzb)
-        const int nB = (fxy ? fx_n + fy_n : 0) + (fz ? fz_n : 0);
-        for (int t = threadIdx.x; t < nB; t += CASTRO_R23_NT) {
-            int u = fxy ? t : t + fx_n + fy_n;
-            if (u < fx_n) {
-                const int w = fxb - xa + 1;
-                const int i = xa + u % w, j = ya + u / w;
+        const bool bact[3] = {fxy, fxy, fz};
+        int ob[4];
+        ob[0] = 0;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) ob[q + 1] = ob[q] + (bact[q] ? (nb[q] + 31) & ~31 : 0);
+        for (int t = threadIdx.x; t < ob[3]; t += CASTRO_R23_NT) {
+            const int q = (t >= ob[1]) + (t >= ob[2]);
+            const int u = t - ob[q];
+            if (u >= nb[q]) continue;
+            if (q == 0) {
+                const int i = xa + u % wF, j = ya + u / wF;
                 final_flux<NS, 0, false>(S, B, I, ld, i, j, m, dt, SmemTFLoader<NS>{YZ}, SmemTFLoader<NS>{ZY}, nullptr);
-            } else if (u < fx_n + fy_n) {
-                u -= fx_n;
-                const int w = xb - xa + 1;
-                const int i = xa + u % w, j = ya + u / w;
+            } else if (q == 1) {
+                const int i = xa + u % wT, j = ya + u / wT;
                 final_flux<NS, 1, false>(S, B, I, ld, i, j, m, dt, SmemTFLoader<NS>{XZ}, SmemTFLoader<NS>{ZX}, nullptr);
             } else {
-                u -= fx_n + fy_n;
-                const int w = xb - xa + 1;
-                const int i = xa + u % w, j = ya + u / w;
+                const int i = xa + u % wT, j = ya + u / wT;
                 final_flux<NS, 2, false>(S, B, I, ld, i, j, m, dt, SmemTFLoader<NS>{XY}, SmemTFLoader<NS>{YX}, nullptr);
             }
         }
